@@ -1,0 +1,102 @@
+"""ctypes binding of libbspmv.so (the C ABI declared in include/bsp.h).
+
+Loading fails loudly: there is no CPU or PyTorch fallback behind these
+entry points.  Build the library with ``python -m benchsp_b200.build``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "lib" / "libbspmv.so"
+
+BSP_OK = 0
+BSP_ERR_INVALID = 1
+BSP_ERR_CUDA = 2
+BSP_ERR_ALLOC = 3
+BSP_ERR_NOT_CONVERGED = 4
+BSP_ERR_UNSUPPORTED = 5
+BSP_ERR_TIMEOUT = 6
+STATUS_NAMES = {0: "BSP_OK", 1: "BSP_ERR_INVALID", 2: "BSP_ERR_CUDA", 3: "BSP_ERR_ALLOC",
+                4: "BSP_ERR_NOT_CONVERGED", 5: "BSP_ERR_UNSUPPORTED", 6: "BSP_ERR_TIMEOUT"}
+
+F64, F32, F16, BF16 = 0, 1, 2, 3
+
+CSR_AUTO, CSR_VECTOR, CSR_MERGE, CSR_SCALAR = 0, 1, 2, 3
+BSR_AUTO, BSR_FFMA, BSR_DMMA, BSR_ADAPTIVE = 0, 1, 2, 3
+
+
+class BspError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+class BspBsr(C.Structure):
+    """Mirror of bsp_bsr (include/bsp.h), itself a mirror of the reference's
+    bsrMAT (include/matrixFormat.hpp:59-83)."""
+    _fields_ = [
+        ("row", C.c_int32), ("col", C.c_int32), ("nnz", C.c_int32),
+        ("blc_row", C.c_int32), ("blc_col", C.c_int32), ("blc_num", C.c_int32),
+        ("stand", C.c_double), ("avg_nnz", C.c_double),
+        ("blcPtr", C.c_void_p), ("blcIdx", C.c_void_p), ("blcVal", C.c_void_p), ("blcMap", C.c_void_p),
+        ("warpnum", C.c_int32), ("rowPtrbyWarp", C.c_void_p), ("rowIdxbyWarp", C.c_void_p),
+        ("bs", C.c_int32), ("true_nnz", C.c_int32), ("dense_blocks", C.c_int32),
+    ]
+
+
+_P = C.c_void_p
+_I32 = C.c_int32
+_I64 = C.c_int64
+_U64 = C.c_uint64
+_D = C.c_double
+_PI32 = C.POINTER(C.c_int32)
+_PI64 = C.POINTER(C.c_int64)
+
+# name -> (restype, argtypes)
+_PROTOS = {
+    "bsp_last_error": (C.c_char_p, []),
+    "bsp_version": (C.c_char_p, []),
+    "bsp_memcpy_d2h": (C.c_int, [_P, _P, C.c_size_t]),
+    "bsp_memcpy_h2d": (C.c_int, [_P, _P, C.c_size_t]),
+    "bsp_device_sync": (C.c_int, []),
+    "bsp_csr_spmv": (C.c_int, [_I32, _I32, _I32, _P, _P, _P, C.c_int, _P, _P, _D, _D, _I32, _I32, _P]),
+    "bsp_csr_merge_workspace": (C.c_size_t, [_I32, _I32]),
+    "bsp_csr_spmv_merge_f64": (C.c_int, [_I32, _I32, _I32, _P, _P, _P, _P, _P, _D, _D, _P, C.c_size_t, _P]),
+    "bsp_csr2bsr": (C.c_int, [_I32, _I32, _I32, _P, _P, _P, _I32, C.POINTER(BspBsr), _P]),
+    "bsp_bsr_free": (C.c_int, [C.POINTER(BspBsr)]),
+    "bsp_bsr_spmv": (C.c_int, [C.POINTER(BspBsr), _P, _P, _D, _D, _I32, _P]),
+    "bsp_bsr_spmv_host": (C.c_int, [C.POINTER(BspBsr), _P, _P, _D, _D, _I32, _P]),
+    "bsp_gen_laplace2d": (C.c_int, [_I32, _I32, _PI32, _PI32, _P, _P, _P]),
+    "bsp_gen_poisson3d": (C.c_int, [_I32, _PI32, _PI64, _P, _P, _P]),
+    "bsp_gen_stencil27": (C.c_int, [_I32, _I32, _U64, _PI32, _PI64, _P, _P, _P]),
+    "bsp_gen_random_bsr": (C.c_int, [_I32, _I32, _I32, _D, _D, _U64, _PI32, _PI64, _P, _P, _P]),
+    "bsp_gen_powerlaw": (C.c_int, [_I32, _D, _I32, _U64, _PI32, _PI64, _P, _P, _P]),
+    "bsp_gen_uniform": (C.c_int, [_I64, _U64, _P]),
+}
+
+_lib: C.CDLL | None = None
+
+
+def lib() -> C.CDLL:
+    """The loaded library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python -m benchsp_b200.build`")
+        L = C.CDLL(str(LIB_PATH))
+        for name, (res, args) in _PROTOS.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def declared_symbols() -> list[str]:
+    return list(_PROTOS)
+
+
+def check(status: int) -> None:
+    if status != BSP_OK:
+        raise BspError(status, lib().bsp_last_error().decode(errors="replace"))

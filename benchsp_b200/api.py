@@ -1,0 +1,244 @@
+"""Python host API over the C ABI (include/bsp.h).
+
+Device memory and streams come from PyTorch (plumbing only); every
+operation runs in libbspmv's CUDA kernels.  Names and argument meaning
+follow the reference's operator surface (jiajun-c/benchsp include/*.h):
+CSR SpMV (csrspmv.h / spmv.h), AmgT BSR (amgT.h, bsrMAT), and the
+synthetic inputs stand in for its .mtx matrices.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from ._lib import BspBsr, check, lib
+
+_ALGO_CSR = {"auto": _lib.CSR_AUTO, "vector": _lib.CSR_VECTOR, "merge": _lib.CSR_MERGE,
+             "scalar": _lib.CSR_SCALAR}
+_ALGO_BSR = {"auto": _lib.BSR_AUTO, "ffma": _lib.BSR_FFMA, "dmma": _lib.BSR_DMMA,
+             "adaptive": _lib.BSR_ADAPTIVE}
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _stream(stream=None) -> C.c_void_p:
+    torch = _torch()
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(s.cuda_stream)
+
+
+def _dptr(t, name: str) -> C.c_void_p:
+    if t is None:
+        return C.c_void_p(0)
+    if not t.is_cuda:
+        raise ValueError(f"{name} must be a CUDA tensor")
+    if not t.is_contiguous():
+        raise ValueError(f"{name} must be contiguous")
+    return C.c_void_p(t.data_ptr())
+
+
+def _dtype_code(t) -> int:
+    torch = _torch()
+    m = {torch.float64: _lib.F64, torch.float32: _lib.F32, torch.float16: _lib.F16,
+         torch.bfloat16: _lib.BF16}
+    if t.dtype not in m:
+        raise ValueError(f"unsupported dtype {t.dtype}")
+    return m[t.dtype]
+
+
+# ---------------------------------------------------------------------------
+# CSR SpMV (replaces spmv_fp64_warpper / spmv_fp64_balance_warpper,
+# reference src/csrspmv.cu:104,136, and MySpmvWithPrefp64/fp16, src/spmv.cu)
+
+def csr_spmv(rowptr, colidx, values, x, y=None, *, rows: int | None = None, cols: int | None = None,
+             alpha: float = 1.0, beta: float = 0.0, algo: str = "auto", lanes: int = 0, stream=None):
+    """y = alpha*A*x + beta*y for int32 CSR on the device; returns y."""
+    torch = _torch()
+    rows = rowptr.numel() - 1 if rows is None else rows
+    cols = x.numel() if cols is None else cols
+    nnz = colidx.numel()
+    if y is None:
+        y = torch.empty(rows, dtype=values.dtype, device=values.device)
+        beta = 0.0
+    dt = _dtype_code(values)
+    if x.dtype != values.dtype or y.dtype != values.dtype:
+        raise ValueError("values, x and y must share a dtype")
+    check(lib().bsp_csr_spmv(rows, cols, nnz, _dptr(rowptr, "rowptr"), _dptr(colidx, "colidx"),
+                             _dptr(values, "values"), dt, _dptr(x, "x"), _dptr(y, "y"), float(alpha),
+                             float(beta), _ALGO_CSR[algo], int(lanes), _stream(stream)))
+    return y
+
+
+def csr_merge_workspace_bytes(rows: int, nnz: int) -> int:
+    return int(lib().bsp_csr_merge_workspace(rows, nnz))
+
+
+def csr_spmv_merge(rowptr, colidx, values, x, y=None, *, workspace=None, alpha: float = 1.0,
+                   beta: float = 0.0, stream=None):
+    """FP64 merge-path SpMV with an explicit (caller-owned) workspace."""
+    torch = _torch()
+    rows = rowptr.numel() - 1
+    nnz = colidx.numel()
+    if y is None:
+        y = torch.empty(rows, dtype=torch.float64, device=values.device)
+        beta = 0.0
+    need = csr_merge_workspace_bytes(rows, nnz)
+    if workspace is None:
+        workspace = torch.empty(need, dtype=torch.uint8, device=values.device)
+    check(lib().bsp_csr_spmv_merge_f64(rows, x.numel(), nnz, _dptr(rowptr, "rowptr"), _dptr(colidx, "colidx"),
+                                       _dptr(values, "values"), _dptr(x, "x"), _dptr(y, "y"), float(alpha),
+                                       float(beta), _dptr(workspace, "workspace"), workspace.numel(),
+                                       _stream(stream)))
+    return y
+
+
+# ---------------------------------------------------------------------------
+# AmgT BSR (bsrMAT, reference include/matrixFormat.hpp:59-83; CSR2BSR_GPU,
+# src/amgT.cu:1114; amgT_spmv_fp64, src/amgT.cu:1355)
+
+def _d2h(ptr: int, count: int, dtype) -> np.ndarray:
+    out = np.empty(count, dtype=dtype)
+    if count:
+        check(lib().bsp_memcpy_d2h(out.ctypes.data_as(C.c_void_p), C.c_void_p(ptr), out.nbytes))
+    return out
+
+
+class BsrMatrix:
+    """Device BSR matrix built by the library (bs = 4 reproduces bsrMAT)."""
+
+    def __init__(self, desc: BspBsr):
+        self._d = desc
+        self._live = True
+
+    def __getattr__(self, name):
+        d = self.__dict__.get("_d")
+        if d is not None and name in dict(BspBsr._fields_):
+            return getattr(d, name)
+        raise AttributeError(name)
+
+    @property
+    def desc(self) -> BspBsr:
+        return self._d
+
+    def arrays(self) -> dict[str, np.ndarray]:
+        """Copies every array to host numpy arrays."""
+        d = self._d
+        maptype = np.uint16 if d.bs == 4 else np.uint64
+        return {
+            "blcPtr": _d2h(d.blcPtr, d.blc_row + 1, np.int32),
+            "blcIdx": _d2h(d.blcIdx, d.blc_num, np.int32),
+            "blcVal": _d2h(d.blcVal, d.blc_num * d.bs * d.bs, np.float64),
+            "blcMap": _d2h(d.blcMap, d.blc_num, maptype),
+            "rowPtrbyWarp": _d2h(d.rowPtrbyWarp, d.blc_row + 1, np.int32),
+            "rowIdxbyWarp": _d2h(d.rowIdxbyWarp, d.warpnum, np.int32),
+        }
+
+    def spmv(self, x, y=None, *, alpha: float = 1.0, beta: float = 0.0, algo: str = "auto", stream=None):
+        torch = _torch()
+        if y is None:
+            y = torch.empty(self._d.row, dtype=torch.float64, device=x.device)
+            beta = 0.0
+        check(lib().bsp_bsr_spmv(C.byref(self._d), _dptr(x, "x"), _dptr(y, "y"), float(alpha), float(beta),
+                                 _ALGO_BSR[algo], _stream(stream)))
+        return y
+
+    def spmv_host(self, x_host: np.ndarray, y_host: np.ndarray, *, alpha: float = 1.0, beta: float = 0.0,
+                  algo: str = "auto", stream=None) -> np.ndarray:
+        """Host-buffer SpMV (H2D x, SpMV, D2H y, wait); x_host/y_host are
+        float64 numpy arrays, ideally in pinned memory."""
+        check(lib().bsp_bsr_spmv_host(C.byref(self._d), C.c_void_p(x_host.ctypes.data),
+                                      C.c_void_p(y_host.ctypes.data), float(alpha), float(beta), _ALGO_BSR[algo],
+                                      _stream(stream)))
+        return y_host
+
+    def free(self) -> None:
+        if self._live:
+            self._live = False
+            check(lib().bsp_bsr_free(C.byref(self._d)))
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def csr2bsr(rowptr, colidx, values, *, rows: int, cols: int, bs: int = 4, stream=None) -> BsrMatrix:
+    d = BspBsr()
+    check(lib().bsp_csr2bsr(rows, cols, colidx.numel(), _dptr(rowptr, "rowptr"), _dptr(colidx, "colidx"),
+                            _dptr(values, "values"), bs, C.byref(d), _stream(stream)))
+    return BsrMatrix(d)
+
+
+# ---------------------------------------------------------------------------
+# Seeded synthetic inputs (host numpy arrays)
+
+@dataclass
+class HostCSR:
+    rows: int
+    cols: int
+    rowptr: np.ndarray
+    colidx: np.ndarray
+    values: np.ndarray
+
+    @property
+    def nnz(self) -> int:
+        return int(self.colidx.size)
+
+    def to_device(self, device="cuda"):
+        torch = _torch()
+        return (torch.from_numpy(self.rowptr).to(device), torch.from_numpy(self.colidx).to(device),
+                torch.from_numpy(self.values).to(device))
+
+
+def _two_phase(fn, *head) -> HostCSR:
+    rows = C.c_int32()
+    nnz = C.c_int64()
+    check(fn(*head, C.byref(rows), C.byref(nnz), None, None, None))
+    rp = np.empty(rows.value + 1, np.int32)
+    ci = np.empty(nnz.value, np.int32)
+    va = np.empty(nnz.value, np.float64)
+    check(fn(*head, C.byref(rows), C.byref(nnz), rp.ctypes.data_as(C.c_void_p), ci.ctypes.data_as(C.c_void_p),
+             va.ctypes.data_as(C.c_void_p)))
+    return HostCSR(rows.value, rows.value, rp, ci, va)
+
+
+def gen_laplace2d(nx: int, ny: int) -> HostCSR:
+    rows = C.c_int32()
+    nnz = C.c_int32()
+    L = lib()
+    check(L.bsp_gen_laplace2d(nx, ny, C.byref(rows), C.byref(nnz), None, None, None))
+    rp = np.empty(rows.value + 1, np.int32)
+    ci = np.empty(nnz.value, np.int32)
+    va = np.empty(nnz.value, np.float64)
+    check(L.bsp_gen_laplace2d(nx, ny, C.byref(rows), C.byref(nnz), rp.ctypes.data_as(C.c_void_p),
+                              ci.ctypes.data_as(C.c_void_p), va.ctypes.data_as(C.c_void_p)))
+    return HostCSR(rows.value, rows.value, rp, ci, va)
+
+
+def gen_poisson3d(n: int) -> HostCSR:
+    return _two_phase(lib().bsp_gen_poisson3d, n)
+
+
+def gen_stencil27(n: int, dof: int, seed: int) -> HostCSR:
+    return _two_phase(lib().bsp_gen_stencil27, n, dof, seed)
+
+
+def gen_random_bsr(nbr: int, bs: int, per_row: int, fill_lo: float, fill_hi: float, seed: int) -> HostCSR:
+    return _two_phase(lib().bsp_gen_random_bsr, nbr, bs, per_row, fill_lo, fill_hi, seed)
+
+
+def gen_powerlaw(n: int, alpha: float, max_len: int, seed: int) -> HostCSR:
+    return _two_phase(lib().bsp_gen_powerlaw, n, alpha, max_len, seed)
+
+
+def gen_uniform(n: int, seed: int) -> np.ndarray:
+    x = np.empty(n, np.float64)
+    check(lib().bsp_gen_uniform(n, seed, x.ctypes.data_as(C.c_void_p)))
+    return x

@@ -1,0 +1,173 @@
+// Error state, small C-ABI utilities and a device exclusive scan used by the
+// format conversions (the reference uses thrust::exclusive_scan for the same
+// steps: src/amgT.cu:1008,1043,1190 and src/csrspmv.cu:157).
+#include "bsp_internal.cuh"
+#include "util.cuh"
+
+namespace bsp {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string &msg) { g_last_error = msg; }
+void clear_error() { g_last_error.clear(); }
+
+// ---------------------------------------------------------------------------
+// Exclusive scan of int32 values, three phases (tile sums, scan of the tile
+// sums, rescan with offsets).  Each tile is 256 threads x 8 items.
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+// Block-wide exclusive sum of one int64 per thread: warp shuffle scans, then
+// warp 0 scans the per-warp totals.  Returns the block total in `total`.
+__device__ __forceinline__ void block_exclusive_sum(int64_t v, int64_t &excl, int64_t &total,
+                                                    int64_t *warp_tot /* [kScanThreads/32 + 1] smem */) {
+  constexpr int kWarps = kScanThreads / 32;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int64_t inc = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int64_t t = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += t;
+  }
+  if (lane == 31) warp_tot[w] = inc;
+  __syncthreads();
+  if (w == 0) {
+    const int64_t t = lane < kWarps ? warp_tot[lane] : 0;
+    int64_t ti = t;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int64_t u = __shfl_up_sync(0xffffffffu, ti, o);
+      if (lane >= o) ti += u;
+    }
+    if (lane < kWarps) warp_tot[lane] = ti - t;
+    if (lane == kWarps - 1) warp_tot[kWarps] = ti;
+  }
+  __syncthreads();
+  excl = inc - v + warp_tot[w];
+  total = warp_tot[kWarps];
+  __syncthreads();  // warp_tot may be reused by the caller's next call
+}
+
+__global__ void __launch_bounds__(kScanThreads) scan_tile_sums(const int32_t *__restrict__ in, int64_t n,
+                                                               int64_t *__restrict__ tile_sums) {
+  __shared__ int64_t wt[kScanThreads / 32 + 1];
+  const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+  int64_t s = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k)
+    if (base + k < n) s += in[base + k];
+  int64_t excl, total;
+  block_exclusive_sum(s, excl, total, wt);
+  if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
+}
+
+// Exclusive scan of n int64 values in place, one CTA walking the tiles.
+__global__ void __launch_bounds__(kScanThreads) scan_i64_single(int64_t *__restrict__ v, int64_t n) {
+  __shared__ int64_t wt[kScanThreads / 32 + 1];
+  int64_t carry = 0;
+  for (int64_t tile = 0; tile < n; tile += kScanTile) {
+    const int64_t base = tile + (int64_t)threadIdx.x * kScanItems;
+    int64_t items[kScanItems];
+    int64_t s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+      items[k] = base + k < n ? v[base + k] : 0;
+      s += items[k];
+    }
+    int64_t excl, total;
+    block_exclusive_sum(s, excl, total, wt);
+    excl += carry;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+      if (base + k < n) v[base + k] = excl;
+      excl += items[k];
+    }
+    carry += total;
+  }
+}
+
+// Rescans each tile with its offset.  in == out is allowed: every thread
+// reads its items before writing them.  The grand total goes to *total_out.
+__global__ void __launch_bounds__(kScanThreads) scan_rescan(const int32_t *in, int32_t *out, int64_t n,
+                                                            const int64_t *__restrict__ tile_off,
+                                                            int64_t *__restrict__ total_out, int64_t ntiles) {
+  __shared__ int64_t wt[kScanThreads / 32 + 1];
+  const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+  int32_t items[kScanItems];
+  int64_t s = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    items[k] = base + k < n ? in[base + k] : 0;
+    s += items[k];
+  }
+  int64_t excl, total;
+  block_exclusive_sum(s, excl, total, wt);
+  excl += tile_off[blockIdx.x];
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    if (base + k < n) out[base + k] = (int32_t)excl;
+    excl += items[k];
+  }
+  if (blockIdx.x == ntiles - 1 && threadIdx.x == kScanThreads - 1 && total_out) *total_out = excl;
+}
+
+bsp_status exclusive_scan_i32(const int32_t *in, int32_t *out, int64_t n, int64_t *d_total,
+                              cudaStream_t s) {
+  if (n <= 0) {
+    if (d_total) BSP_CUDA(cudaMemsetAsync(d_total, 0, sizeof(int64_t), s));
+    return BSP_OK;
+  }
+  const int64_t ntiles = ceil_div(n, kScanTile);
+  int64_t *tile = nullptr;
+  BSP_TRY(dalloc(&tile, ntiles, s));
+  scan_tile_sums<<<(unsigned)ntiles, kScanThreads, 0, s>>>(in, n, tile);
+  BSP_LAUNCH_CHECK();
+  scan_i64_single<<<1, kScanThreads, 0, s>>>(tile, ntiles);
+  BSP_LAUNCH_CHECK();
+  scan_rescan<<<(unsigned)ntiles, kScanThreads, 0, s>>>(in, out, n, tile, d_total, ntiles);
+  BSP_LAUNCH_CHECK();
+  dfree(tile, s);
+  return BSP_OK;
+}
+
+bsp_status read_i64(const int64_t *d, int64_t *h, cudaStream_t s) {
+  BSP_CUDA(cudaMemcpyAsync(h, d, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+  BSP_CUDA(cudaStreamSynchronize(s));
+  return BSP_OK;
+}
+
+bsp_status read_i32(const int32_t *d, int32_t *h, cudaStream_t s) {
+  BSP_CUDA(cudaMemcpyAsync(h, d, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  BSP_CUDA(cudaStreamSynchronize(s));
+  return BSP_OK;
+}
+
+}  // namespace bsp
+
+using namespace bsp;
+
+extern "C" const char *bsp_last_error(void) { return g_last_error.c_str(); }
+extern "C" const char *bsp_version(void) { return "libbspmv 0.1 (sm_100a)"; }
+
+extern "C" bsp_status bsp_memcpy_d2h(void *dst_host, const void *src_dev, size_t bytes) {
+  clear_error();
+  if (bytes == 0) return BSP_OK;
+  BSP_CHECK_ARG(dst_host && src_dev, "null pointer");
+  BSP_CUDA(cudaMemcpy(dst_host, src_dev, bytes, cudaMemcpyDeviceToHost));
+  return BSP_OK;
+}
+
+extern "C" bsp_status bsp_memcpy_h2d(void *dst_dev, const void *src_host, size_t bytes) {
+  clear_error();
+  if (bytes == 0) return BSP_OK;
+  BSP_CHECK_ARG(dst_dev && src_host, "null pointer");
+  BSP_CUDA(cudaMemcpy(dst_dev, src_host, bytes, cudaMemcpyHostToDevice));
+  return BSP_OK;
+}
+
+extern "C" bsp_status bsp_device_sync(void) {
+  clear_error();
+  BSP_CUDA(cudaDeviceSynchronize());
+  return BSP_OK;
+}

@@ -1,0 +1,191 @@
+/*
+ * bsp.h — C ABI of libbspmv, a B200-native (sm_100a) SpMV/SpMM library that
+ * drops in for the operator surface of jiajun-c/benchsp (include/spmv.h,
+ * include/csrspmv.h, include/amgT.h, include/dasp.h, include/smat.h,
+ * include/matrixFormat.hpp).
+ *
+ * Conventions
+ *  - Every entry point returns bsp_status; bsp_last_error() gives a message
+ *    for the last failure on the calling thread.  Nothing calls exit().
+ *  - Matrix/vector arguments are DEVICE pointers unless the name says _host.
+ *  - Every call takes an explicit stream (bsp_stream_t is a cudaStream_t;
+ *    NULL means the legacy default stream).  The library never calls
+ *    cudaSetDevice: it works on the device current on the calling thread.
+ *  - Format descriptors mirror the reference's classes field for field; their
+ *    arrays live in device memory allocated by the library and are released by
+ *    the matching *_free call.
+ *  - Indices are int32 (the reference's CSRFormat<double,int32_t>).  Column
+ *    indices of every input CSR must be ascending within a row, without
+ *    duplicates (the reference's bench drivers sort COO by (row, col) before
+ *    building CSR, bench/spmvfp64.cpp:64-78; its converters assume it).
+ */
+#ifndef BSP_H
+#define BSP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef void *bsp_stream_t;
+
+typedef enum {
+  BSP_OK = 0,
+  BSP_ERR_INVALID = 1,      /* bad argument or malformed matrix */
+  BSP_ERR_CUDA = 2,         /* a CUDA runtime call failed */
+  BSP_ERR_ALLOC = 3,        /* device or host allocation failed */
+  BSP_ERR_NOT_CONVERGED = 4,/* iterative solver stopped at its limit */
+  BSP_ERR_UNSUPPORTED = 5,  /* combination not implemented */
+  BSP_ERR_TIMEOUT = 6       /* a bounded device wait gave up */
+} bsp_status;
+
+typedef enum {
+  BSP_F64 = 0,
+  BSP_F32 = 1,
+  BSP_F16 = 2,
+  BSP_BF16 = 3
+} bsp_dtype;
+
+/* Message for the last non-OK status on this thread ("" if none). */
+const char *bsp_last_error(void);
+/* Library version string. */
+const char *bsp_version(void);
+
+/* ---------------------------------------------------------------------- */
+/* Utilities (thin, so tests and hosts without a CUDA binding can move data) */
+bsp_status bsp_memcpy_d2h(void *dst_host, const void *src_dev, size_t bytes);
+bsp_status bsp_memcpy_h2d(void *dst_dev, const void *src_host, size_t bytes);
+bsp_status bsp_device_sync(void);
+
+/* ---------------------------------------------------------------------- */
+/* CSR SpMV  y = alpha*A*x + beta*y
+ *
+ * Replaces spmv_fp64_warpper / spmv_fp64_balance_warpper
+ * (reference src/csrspmv.cu:104 and :136, declared include/csrspmv.h:2-3)
+ * and MySpmvWithPrefp64 / MySpmvWithPrefp16 (src/spmv.cu:323 and :197,
+ * include/spmv.h:2-3).  Those wrappers upload host arrays, run a timed
+ * loop and download y; here the arrays are already on the device and the
+ * call launches one kernel on `stream`.
+ *
+ * algo: BSP_CSR_AUTO picks from the row-length statistics; VECTOR uses a
+ * power-of-two group of lanes per row; MERGE is the merge-path (nnz+rows
+ * split) kernel, which needs a workspace (see bsp_csr_merge_workspace).
+ */
+typedef enum {
+  BSP_CSR_AUTO = 0,
+  BSP_CSR_VECTOR = 1,
+  BSP_CSR_MERGE = 2,
+  BSP_CSR_SCALAR = 3 /* one thread per row, summing left to right */
+} bsp_csr_algo;
+
+/* Values, x and y all have `dtype` storage; F64 accumulates in FP64, the
+ * others in FP32.  For F16/BF16 the result is rounded once to the storage
+ * type, like ref_spmv_fp16 (src/ref.cpp:3-13).  lanes_per_row: 0 = auto,
+ * else 1..32 (power of two) for VECTOR. */
+bsp_status bsp_csr_spmv(int32_t rows, int32_t cols, int32_t nnz,
+                        const int32_t *rowPtr, const int32_t *colIdx,
+                        const void *values, bsp_dtype dtype, const void *x,
+                        void *y, double alpha, double beta, int32_t algo,
+                        int32_t lanes_per_row, bsp_stream_t stream);
+
+/* Workspace bytes the merge-path kernel needs for (rows, nnz). */
+size_t bsp_csr_merge_workspace(int32_t rows, int32_t nnz);
+/* FP64 merge-path SpMV with a caller-provided workspace of at least
+ * bsp_csr_merge_workspace(rows, nnz) bytes (16-byte aligned). */
+bsp_status bsp_csr_spmv_merge_f64(int32_t rows, int32_t cols, int32_t nnz,
+                                  const int32_t *rowPtr, const int32_t *colIdx,
+                                  const double *values, const double *x,
+                                  double *y, double alpha, double beta,
+                                  void *workspace, size_t workspace_bytes,
+                                  bsp_stream_t stream);
+
+/* ---------------------------------------------------------------------- */
+/* AmgT-style BSR (bsrMAT, reference include/matrixFormat.hpp:59-83).
+ * bs = 4 reproduces the reference format exactly; bs = 8 is the same layout
+ * with 8x8 blocks (blcMap then holds uint64 bitmaps, bit r*8+c). */
+typedef struct {
+  int32_t row, col, nnz; /* nnz = blc_num*bs*bs, as CSR2BSR_GPU sets it */
+  int32_t blc_row, blc_col, blc_num;
+  double stand;   /* std-dev of blocks per block-row (amgT.cu:1146-1155) */
+  double avg_nnz; /* true nnz / blc_num (amgT.cu:1136) */
+  int32_t *blcPtr;  /* [blc_row+1] */
+  int32_t *blcIdx;  /* [blc_num], ascending within a block-row */
+  double *blcVal;   /* [blc_num*bs*bs], row-major blocks */
+  void *blcMap;     /* [blc_num+1] uint16 (bs=4) or uint64 (bs=8) */
+  int32_t warpnum;       /* chunks of <= 64 blocks (common.h:7) */
+  int32_t *rowPtrbyWarp; /* [blc_row+1] */
+  int32_t *rowIdxbyWarp; /* [warpnum] */
+  int32_t bs;
+  int32_t true_nnz;
+  int32_t dense_blocks; /* blocks whose bitmap is full */
+} bsp_bsr;
+
+/* CSR -> BSR on the device; replaces CSR2BSR_GPU + BSR_BALANCED_PREPROCESS_GPU
+ * (reference src/amgT.cu:1114 and :1174).  Output arrays are bit-identical to
+ * the reference's for bs = 4. */
+bsp_status bsp_csr2bsr(int32_t rows, int32_t cols, int32_t nnz,
+                       const int32_t *rowPtr, const int32_t *colIdx,
+                       const double *values, int32_t bs, bsp_bsr *out,
+                       bsp_stream_t stream);
+bsp_status bsp_bsr_free(bsp_bsr *m);
+
+typedef enum {
+  BSP_BSR_AUTO = 0,
+  BSP_BSR_FFMA = 1, /* CUDA-core FP64 FMA, 16-byte coalesced block loads */
+  BSP_BSR_DMMA = 2, /* FP64 mma.sync m8n8k4 on the blocks */
+  BSP_BSR_ADAPTIVE = 3 /* per-block switch: DMMA for full blocks, FFMA else */
+} bsp_bsr_algo;
+
+/* y = alpha*A*x + beta*y for a BSR matrix; replaces the kernels dispatched by
+ * amgT_spmv_fp64 (reference src/amgT.cu:1355-1488).  Deterministic: no
+ * atomics, every y element written exactly once. */
+bsp_status bsp_bsr_spmv(const bsp_bsr *m, const double *x, double *y,
+                        double alpha, double beta, int32_t algo,
+                        bsp_stream_t stream);
+
+/* Host-buffer form, the shape of the reference's wrappers (amgT_spmv_fp64,
+ * src/amgT.cu:1355, takes host x/y): copies x_host (col doubles) to the
+ * device, runs bsp_bsr_spmv, copies y back to y_host (row doubles) and waits
+ * for `stream`.  Pinned host buffers give full-bandwidth copies.  beta != 0
+ * also uploads y_host first. */
+bsp_status bsp_bsr_spmv_host(const bsp_bsr *m, const double *x_host, double *y_host,
+                             double alpha, double beta, int32_t algo,
+                             bsp_stream_t stream);
+
+/* ---------------------------------------------------------------------- */
+/* Synthetic matrix generators (host, seeded, deterministic).  Two-phase:
+ * call with NULL arrays to get the sizes, then with allocated arrays. */
+
+/* 2-D 5-point Laplacian on an nx*ny grid, natural ordering, diag 4, off -1. */
+bsp_status bsp_gen_laplace2d(int32_t nx, int32_t ny, int32_t *rows,
+                             int32_t *nnz, int32_t *rowPtr, int32_t *colIdx,
+                             double *values);
+/* 3-D 7-point Poisson on n^3 (diag 6, off -1). */
+bsp_status bsp_gen_poisson3d(int32_t n, int32_t *rows, int64_t *nnz,
+                             int32_t *rowPtr, int32_t *colIdx, double *values);
+/* 3-D 27-point stencil on n^3 nodes with `dof` unknowns per node: every
+ * coupled node pair is a dense dof x dof block of N(0,1) values. */
+bsp_status bsp_gen_stencil27(int32_t n, int32_t dof, uint64_t seed,
+                             int32_t *rows, int64_t *nnz, int32_t *rowPtr,
+                             int32_t *colIdx, double *values);
+/* Random block-sparse matrix: nbr block-rows of bs x bs blocks, `per_row`
+ * distinct random block columns per block-row, each block filled with
+ * probability U[fill_lo, fill_hi] per entry (at least one entry). */
+bsp_status bsp_gen_random_bsr(int32_t nbr, int32_t bs, int32_t per_row,
+                              double fill_lo, double fill_hi, uint64_t seed,
+                              int32_t *rows, int64_t *nnz, int32_t *rowPtr,
+                              int32_t *colIdx, double *values);
+/* Power-law rows: row lengths ~ Zipf(alpha) on [1, max_len], distinct
+ * uniform columns on [0, n), N(0,1) values. */
+bsp_status bsp_gen_powerlaw(int32_t n, double alpha, int32_t max_len,
+                            uint64_t seed, int32_t *rows, int64_t *nnz,
+                            int32_t *rowPtr, int32_t *colIdx, double *values);
+/* Uniform random x in [-1, 1]. */
+bsp_status bsp_gen_uniform(int64_t n, uint64_t seed, double *x);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BSP_H */

@@ -1,0 +1,65 @@
+/*
+ * oracle.h — CPU restatement of the reference's (jiajun-c/benchsp) hot-path
+ * algorithms.  TEST INFRASTRUCTURE ONLY: the parity tests, the smoke check
+ * and the CPU-baseline leg of bench.py use it as the checker.  The library
+ * (benchsp_b200, libbspmv.so) never links, loads or calls anything here.
+ *
+ * Each function cites the reference file:line it restates.  Parity pins:
+ * the restatement is checked against the reference's own code compiled
+ * from its sources into oracle/_ref (ref.cpp, include/dbsr.h,
+ * utils/utils.hpp through g++; src/dasp.cu's packing through a CPU stub
+ * of the CUDA runtime) on the committed golden fixtures.
+ */
+#ifndef BSP_ORACLE_H
+#define BSP_ORACLE_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* y_i = sum_j A_ij x_j, left to right, separately rounded mul and add
+ * (src/ref.cpp:26-37). */
+void orc_spmv_f64(int64_t rows, const int64_t *rowPtr, const int64_t *colIdx, const double *val,
+                  const double *x, double *y);
+/* Same on int32 CSR. */
+void orc_spmv_f64_i32(int32_t rows, const int32_t *rowPtr, const int32_t *colIdx, const double *val,
+                      const double *x, double *y);
+/* FP32 sum (src/ref.cpp:14-24). */
+void orc_spmv_f32(int32_t rows, const int32_t *rowPtr, const int32_t *colIdx, const float *val,
+                  const float *x, float *y);
+/* FP16 variant (src/ref.cpp:3-13): val/x given as IEEE half bit patterns,
+ * float sum of products, result rounded to half (bits returned). */
+void orc_spmv_f16(int32_t rows, const int32_t *rowPtr, const int32_t *colIdx, const uint16_t *val,
+                  const uint16_t *x, uint16_t *y);
+uint16_t orc_f32_to_f16(float f);  /* round to nearest even */
+float orc_f16_to_f32(uint16_t h);
+uint16_t orc_f32_to_bf16(float f); /* round to nearest even */
+float orc_bf16_to_f32(uint16_t h);
+
+/* |sum_j |A_ij x_j|| per row, the scale of the rounding-error bound used by
+ * the parity tests. */
+void orc_abs_rowsum(int32_t rows, const int32_t *rowPtr, const int32_t *colIdx, const double *val,
+                    const double *x, double *out);
+
+/* AmgT CSR -> BSR (CSR2BSR_GPU, src/amgT.cu:1114-1172): block columns
+ * ascending inside a block-row (rank by counting smaller keys, :823-835),
+ * row-major bs x bs values (:840-847), bitmap bit r*bs+c (:776,:836).
+ * Pass 1 (arrays NULL) returns blc_num; pass 2 fills caller arrays:
+ * blcPtr[blc_row+1], blcIdx[blc_num], blcVal[blc_num*bs*bs], blcMap[blc_num]
+ * (uint64 per block, low bs*bs bits). */
+int64_t orc_csr2bsr(int32_t rows, int32_t cols, const int32_t *rowPtr, const int32_t *colIdx,
+                    const double *val, int32_t bs, int32_t *blcPtr, int32_t *blcIdx, double *blcVal,
+                    uint64_t *blcMap);
+/* Balanced chunks (get_rowPtrbyWarp / get_rowIdxbyWarp + exclusive scan,
+ * src/amgT.cu:523-545, :1174-1200): rowPtrbyWarp[blc_row+1] = exclusive
+ * scan of ceil(len/64); rowIdxbyWarp (may be NULL) gets warpnum entries.
+ * Returns warpnum. */
+int32_t orc_bsr_chunks(int32_t blc_row, const int32_t *blcPtr, int32_t *rowPtrbyWarp, int32_t *rowIdxbyWarp);
+/* sqrtf(sum (len - avg)^2 / blc_row) (getStand, src/amgT.cu:546-575, :1146-1155). */
+double orc_bsr_stand(int32_t blc_row, const int32_t *blcPtr);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,165 @@
+"""ctypes loader for the CPU oracle (liboracle.so) and, when built, the
+reference's own code (oracle/_ref).  TEST INFRASTRUCTURE ONLY: imported by
+tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg as the
+checker; the library never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import struct
+import subprocess
+import tempfile
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ORACLE_SO = HERE / "liboracle.so"
+REF_DIR = HERE / "_ref"
+
+_P = C.c_void_p
+_I32 = C.c_int32
+_I64 = C.c_int64
+
+
+def _p(a: np.ndarray) -> C.c_void_p:
+    return a.ctypes.data_as(C.c_void_p)
+
+
+_orc = None
+
+
+def build() -> None:
+    """Builds liboracle.so (and oracle/_ref when the reference is present)."""
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+
+
+def orc() -> C.CDLL:
+    global _orc
+    if _orc is None:
+        if not ORACLE_SO.exists():
+            build()
+        L = C.CDLL(str(ORACLE_SO))
+        L.orc_spmv_f64.argtypes = [_I64, _P, _P, _P, _P, _P]
+        L.orc_spmv_f64_i32.argtypes = [_I32, _P, _P, _P, _P, _P]
+        L.orc_spmv_f32.argtypes = [_I32, _P, _P, _P, _P, _P]
+        L.orc_spmv_f16.argtypes = [_I32, _P, _P, _P, _P, _P]
+        L.orc_abs_rowsum.argtypes = [_I32, _P, _P, _P, _P, _P]
+        L.orc_csr2bsr.restype = _I64
+        L.orc_csr2bsr.argtypes = [_I32, _I32, _P, _P, _P, _I32, _P, _P, _P, _P]
+        L.orc_bsr_chunks.restype = _I32
+        L.orc_bsr_chunks.argtypes = [_I32, _P, _P, _P]
+        L.orc_bsr_stand.restype = C.c_double
+        L.orc_bsr_stand.argtypes = [_I32, _P]
+        L.orc_f32_to_f16.restype = C.c_uint16
+        L.orc_f32_to_f16.argtypes = [C.c_float]
+        _orc = L
+    return _orc
+
+
+# ---------------------------------------------------------------------------
+# SpMV (src/ref.cpp)
+
+def spmv_f64(rowptr, colidx, val, x) -> np.ndarray:
+    rows = rowptr.size - 1
+    y = np.empty(rows, np.float64)
+    orc().orc_spmv_f64_i32(rows, _p(rowptr), _p(colidx), _p(val), _p(x), _p(y))
+    return y
+
+
+def spmv_f32(rowptr, colidx, val, x) -> np.ndarray:
+    rows = rowptr.size - 1
+    y = np.empty(rows, np.float32)
+    orc().orc_spmv_f32(rows, _p(rowptr), _p(colidx), _p(np.ascontiguousarray(val, np.float32)),
+                       _p(np.ascontiguousarray(x, np.float32)), _p(y))
+    return y
+
+
+def spmv_f16(rowptr, colidx, val16: np.ndarray, x16: np.ndarray) -> np.ndarray:
+    """val16/x16 are float16 arrays; returns float16."""
+    rows = rowptr.size - 1
+    y = np.empty(rows, np.uint16)
+    orc().orc_spmv_f16(rows, _p(rowptr), _p(colidx), _p(val16.view(np.uint16)), _p(x16.view(np.uint16)), _p(y))
+    return y.view(np.float16)
+
+
+def abs_rowsum(rowptr, colidx, val, x) -> np.ndarray:
+    rows = rowptr.size - 1
+    y = np.empty(rows, np.float64)
+    orc().orc_abs_rowsum(rows, _p(rowptr), _p(colidx), _p(val), _p(x), _p(y))
+    return y
+
+
+def spmv_tolerance(rowptr, colidx, val, x, unit: float = 2.0 ** -53) -> np.ndarray:
+    """Per-row bound on |y_gpu - y_oracle| for any summation order:
+    2 * gamma_L * sum_j |a_ij x_j| with gamma_L = L*u/(1-L*u), L = row length
+    + 1 (both results carry at most gamma_L relative error)."""
+    L = np.diff(rowptr).astype(np.float64) + 1.0
+    g = L * unit / (1.0 - L * unit)
+    return 2.0 * g * abs_rowsum(rowptr, colidx, val, x) + np.finfo(np.float64).tiny
+
+
+# ---------------------------------------------------------------------------
+# AmgT BSR (src/amgT.cu:1114-1200)
+
+def csr2bsr(rows, cols, rowptr, colidx, val, bs=4) -> dict:
+    L = orc()
+    nb = int(L.orc_csr2bsr(rows, cols, _p(rowptr), _p(colidx), _p(val), bs, None, None, None, None))
+    brow = (rows + bs - 1) // bs
+    blcPtr = np.empty(brow + 1, np.int32)
+    blcIdx = np.empty(nb, np.int32)
+    blcVal = np.empty(nb * bs * bs, np.float64)
+    blcMap = np.empty(nb, np.uint64)
+    L.orc_csr2bsr(rows, cols, _p(rowptr), _p(colidx), _p(val), bs, _p(blcPtr), _p(blcIdx), _p(blcVal), _p(blcMap))
+    warpnum = int(L.orc_bsr_chunks(brow, _p(blcPtr), None, None))
+    rpw = np.empty(brow + 1, np.int32)
+    riw = np.empty(warpnum, np.int32)
+    L.orc_bsr_chunks(brow, _p(blcPtr), _p(rpw), _p(riw))
+    return {"blc_row": brow, "blc_num": nb, "blcPtr": blcPtr, "blcIdx": blcIdx, "blcVal": blcVal,
+            "blcMap": blcMap.astype(np.uint16) if bs == 4 else blcMap, "rowPtrbyWarp": rpw,
+            "rowIdxbyWarp": riw, "warpnum": warpnum, "stand": float(L.orc_bsr_stand(brow, _p(blcPtr))),
+            "avg_nnz": (colidx.size / nb) if nb else 0.0}
+
+
+# ---------------------------------------------------------------------------
+# The reference's own code (oracle/_ref), when built
+
+def ref_available() -> bool:
+    return (REF_DIR / "libref_host.so").exists()
+
+
+def write_csr_bin(path, rows, cols, rowptr, colidx, val, x, threshold=0.75, block_longest=256) -> None:
+    with open(path, "wb") as f:
+        f.write(struct.pack("<iiidi", rows, cols, int(colidx.size), float(threshold), int(block_longest)))
+        f.write(np.ascontiguousarray(rowptr, np.int32).tobytes())
+        f.write(np.ascontiguousarray(colidx, np.int32).tobytes())
+        f.write(np.ascontiguousarray(val, np.float64).tobytes())
+        f.write(np.ascontiguousarray(x, np.float64).tobytes())
+
+
+def read_records(path) -> dict:
+    d = Path(path).read_bytes()
+    o = 0
+    out = {}
+    while o < len(d):
+        (nl,) = struct.unpack_from("<i", d, o)
+        o += 4
+        name = d[o:o + nl].decode()
+        o += nl
+        (nb,) = struct.unpack_from("<q", d, o)
+        o += 8
+        out[name] = d[o:o + nb]
+        o += nb
+    return out
+
+
+def run_capture(exe: str, rows, cols, rowptr, colidx, val, x, threshold=0.75, block_longest=256) -> dict:
+    """Runs oracle/_ref/<exe> (dasp_capture or amgt_capture) on a CSR matrix."""
+    with tempfile.TemporaryDirectory() as td:
+        fin = Path(td) / "in.bin"
+        fout = Path(td) / "out.bin"
+        write_csr_bin(fin, rows, cols, rowptr, colidx, val, x, threshold, block_longest)
+        r = subprocess.run([str(REF_DIR / exe), str(fin), str(fout)], capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"{exe} failed ({r.returncode}): {r.stdout[-2000:]} {r.stderr[-2000:]}")
+        return read_records(fout)

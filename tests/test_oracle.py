@@ -1,0 +1,91 @@
+"""The CPU oracle (oracle/liboracle.so) against the golden fixtures made by
+the reference's own code (tests/golden/make_golden.py) and against scipy."""
+import glob
+from pathlib import Path
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from oracle import pyoracle
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+SPMV = sorted(Path(p).name for p in glob.glob(str(GOLDEN / "spmv_*.npz")))
+
+
+@pytest.mark.parametrize("name", SPMV)
+def test_spmv_fp64_bit_exact_with_reference(golden, name):
+    g = golden(name)
+    y = pyoracle.spmv_f64(g["rowptr"], g["colidx"], g["values"], g["x"])
+    assert np.array_equal(y.view(np.uint64), g["y_fp64"].view(np.uint64))
+
+
+@pytest.mark.parametrize("name", SPMV)
+def test_spmv_fp32_bit_exact_with_reference(golden, name):
+    g = golden(name)
+    y = pyoracle.spmv_f32(g["rowptr"], g["colidx"], g["values"].astype(np.float32), g["x"].astype(np.float32))
+    assert np.array_equal(y.view(np.uint32), g["y_fp32"].view(np.uint32))
+
+
+@pytest.mark.parametrize("name", SPMV)
+def test_spmv_fp16_bit_exact_with_reference(golden, name):
+    g = golden(name)
+    v16 = g["values"].astype(np.float32).astype(np.float16)
+    x16 = g["x"].astype(np.float32).astype(np.float16)
+    y = pyoracle.spmv_f16(g["rowptr"], g["colidx"], v16, x16).astype(np.float32)
+    ref = g["y_fp16"]
+    same = (y.view(np.uint32) == ref.view(np.uint32)) | (np.isnan(y) & np.isnan(ref))
+    assert same.all()
+
+
+def test_half_conversion_matches_numpy():
+    rng = np.random.default_rng(3)
+    v = (rng.standard_normal(50000) * 10.0 ** rng.integers(-8, 5, 50000)).astype(np.float32)
+    L = pyoracle.orc()
+    got = np.array([L.orc_f32_to_f16(float(a)) for a in v[:5000]], np.uint16)
+    assert np.array_equal(got, v[:5000].astype(np.float16).view(np.uint16))
+
+
+def _padded_scipy(rows, cols, rp, ci, va, bs):
+    R = -(-rows // bs) * bs
+    Cc = -(-cols // bs) * bs
+    return sp.csr_matrix((va, ci, rp), shape=(rows, cols)).tocoo().tocsr(), R, Cc
+
+
+@pytest.mark.parametrize("name", SPMV)
+@pytest.mark.parametrize("bs", [4, 8])
+def test_csr2bsr_oracle_against_scipy(golden, name, bs):
+    g = golden(name)
+    rows, cols = int(g["rows"]), int(g["cols"])
+    o = pyoracle.csr2bsr(rows, cols, g["rowptr"], g["colidx"], g["values"], bs)
+    R = -(-rows // bs) * bs
+    Cc = -(-cols // bs) * bs
+    M = sp.csr_matrix((g["values"], g["colidx"], g["rowptr"]), shape=(rows, cols))
+    M = sp.vstack([sp.hstack([M, sp.csr_matrix((rows, Cc - cols))]), sp.csr_matrix((R - rows, Cc))]).tocsr()
+    B = M.tobsr(blocksize=(bs, bs))
+    B.sort_indices()
+    assert np.array_equal(o["blcPtr"], B.indptr)
+    assert np.array_equal(o["blcIdx"], B.indices)
+    assert np.array_equal(o["blcVal"], B.data.reshape(-1))
+    # bitmap = structural pattern of the CSR entries
+    pat = sp.csr_matrix((np.ones_like(g["values"]), g["colidx"], g["rowptr"]), shape=(rows, cols))
+    pat = sp.vstack([sp.hstack([pat, sp.csr_matrix((rows, Cc - cols))]), sp.csr_matrix((R - rows, Cc))]).tocsr()
+    PB = pat.tobsr(blocksize=(bs, bs))
+    PB.sort_indices()
+    bits = (PB.data.reshape(-1, bs * bs) != 0) * (1 << np.arange(bs * bs, dtype=np.uint64))
+    assert np.array_equal(o["blcMap"].astype(np.uint64), bits.sum(axis=1).astype(np.uint64))
+    assert o["rowPtrbyWarp"][-1] == o["warpnum"]
+
+
+AMGT = sorted(Path(p).name for p in glob.glob(str(GOLDEN / "amgt_*.npz")))
+
+
+@pytest.mark.parametrize("name", AMGT)
+def test_csr2bsr_oracle_against_reference_gpu_capture(golden, name):
+    g = golden(name)
+    rows, cols = int(g["rows"]), int(g["cols"])
+    o = pyoracle.csr2bsr(rows, cols, g["rowptr"], g["colidx"], g["values"], 4)
+    for k in ("blcPtr", "blcIdx", "blcVal", "blcMap", "rowPtrbyWarp", "rowIdxbyWarp"):
+        assert np.array_equal(o[k], g[k]), k
+    assert o["warpnum"] == int(g["warpnum"]) and o["blc_num"] == int(g["blc_num"])
+    assert abs(o["stand"] - float(g["stand"])) <= 1e-6 * max(1.0, float(g["stand"]))
