@@ -182,9 +182,9 @@ def cpu_reference(A, x, max_seconds: float = 12.0, min_reps: int = 2) -> dict:
             "seconds_per_spmv": t, "y": y}
 
 
-def make_matrix():
+def make_matrix(grid: int = GRID):
     import benchsp_b200 as bsp
-    A = bsp.gen_stencil27(GRID, DOF, SEED)
+    A = bsp.gen_stencil27(grid, DOF, SEED)
     x = bsp.gen_uniform(A.cols, SEED + 1)
     return A, x
 
@@ -192,7 +192,7 @@ def make_matrix():
 def run_reference(args, ws, rank):
     if rank != 0:
         return
-    A, x = make_matrix()
+    A, x = make_matrix(args.grid)
     ref = cpu_reference(A, x, max_seconds=max(2.0, min(60.0, 0.6 * args.steps)), min_reps=max(1, args.warmup))
     v = ref["gflops"]
     line = {
@@ -216,7 +216,7 @@ def run_ours(args, ws, rank, local):
     import benchsp_b200 as bsp
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    A, x_h = make_matrix()
+    A, x_h = make_matrix(args.grid)
     rp, ci, va = (torch.from_numpy(a).to(dev) for a in (A.rowptr, A.colidx, A.values))
     x = torch.from_numpy(x_h).to(dev)
     torch.cuda.synchronize()
@@ -301,9 +301,10 @@ def run_ours(args, ws, rank, local):
         "metric": METRIC, "value": round(value, 3), "unit": "GFLOP/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_step, 6), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-        "config": {"workload": WORKLOAD, "n": A.rows, "nnz": A.nnz, "blocks": M.blc_num, "block": "4x4",
+        "config": {"workload": WORKLOAD if args.grid == GRID else f"bsr4_fp64_spmv_stencil27_{args.grid}cubed_4dof",
+                   "n": A.rows, "nnz": A.nnz, "blocks": M.blc_num, "block": "4x4",
                    "parallelism": f"replicas{ws}", "l2": "inputs larger than L2 (923 MB working set)",
-                   "kernel": "bsr_ffma_kernel<4,16,2>"},
+                   "kernel": "bsr_ffma_kernel<4,16,1>"},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": pk["hbm_gbs"], "unit": "GB/s",
                      "frac": round(achieved / pk["hbm_gbs"], 4), "traffic": traffic,
                      "peak_src": pk["src"], "algorithmic_bytes_per_launch": algo_bytes},
@@ -325,6 +326,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--grid", type=int, default=GRID, help="stencil grid edge (64 = the benchmark config; "
+                    "smaller values only for profiling captures)")
     args = ap.parse_args()
     ws, rank, local = dist_init()
     try:

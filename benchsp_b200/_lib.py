@@ -66,6 +66,7 @@ _PROTOS = {
     "bsp_csr2bsr": (C.c_int, [_I32, _I32, _I32, _P, _P, _P, _I32, C.POINTER(BspBsr), _P]),
     "bsp_bsr_free": (C.c_int, [C.POINTER(BspBsr)]),
     "bsp_bsr_spmv": (C.c_int, [C.POINTER(BspBsr), _P, _P, _D, _D, _I32, _P]),
+    "bsp_bsr_spmv_variant": (C.c_int, [C.POINTER(BspBsr), _P, _P, _D, _D, _I32, _I32, _I32, _P]),
     "bsp_bsr_spmv_host": (C.c_int, [C.POINTER(BspBsr), _P, _P, _D, _D, _I32, _P]),
     "bsp_gen_laplace2d": (C.c_int, [_I32, _I32, _PI32, _PI32, _P, _P, _P]),
     "bsp_gen_poisson3d": (C.c_int, [_I32, _PI32, _PI64, _P, _P, _P]),

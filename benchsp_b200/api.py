@@ -148,6 +148,13 @@ class BsrMatrix:
                                  _ALGO_BSR[algo], _stream(stream)))
         return y
 
+    def spmv_variant(self, x, y, *, lanes: int, unroll: int, l2_prefetch: int = 0, alpha: float = 1.0,
+                     beta: float = 0.0, stream=None):
+        """FFMA SpMV with an explicit kernel shape (autotuner candidates)."""
+        check(lib().bsp_bsr_spmv_variant(C.byref(self._d), _dptr(x, "x"), _dptr(y, "y"), float(alpha),
+                                         float(beta), lanes, unroll, l2_prefetch, _stream(stream)))
+        return y
+
     def spmv_host(self, x_host: np.ndarray, y_host: np.ndarray, *, alpha: float = 1.0, beta: float = 0.0,
                   algo: str = "auto", stream=None) -> np.ndarray:
         """Host-buffer SpMV (H2D x, SpMV, D2H y, wait); x_host/y_host are

@@ -98,6 +98,14 @@ __device__ __forceinline__ f64x4 ld_stream_f64x4(const double *p) {
                : "l"(p));
   return r;
 }
+// Same with a 256-byte L2 fetch granularity hint for long sequential streams.
+__device__ __forceinline__ f64x4 ld_stream_f64x4_pf(const double *p) {
+  f64x4 r;
+  asm("ld.global.nc.L1::no_allocate.L2::evict_first.L2::256B.v4.f64 {%0,%1,%2,%3}, [%4];"
+      : "=d"(r.x), "=d"(r.y), "=d"(r.z), "=d"(r.w)
+      : "l"(p));
+  return r;
+}
 // 256-bit read-only load with default caching (x gathers: keep in L2/L1).
 __device__ __forceinline__ f64x4 ld_x4(const double *p) {
   f64x4 r;

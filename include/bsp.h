@@ -145,6 +145,16 @@ bsp_status bsp_bsr_spmv(const bsp_bsr *m, const double *x, double *y,
                         double alpha, double beta, int32_t algo,
                         bsp_stream_t stream);
 
+/* FFMA BSR SpMV with an explicit kernel shape (used by the autotuner):
+ * lanes_per_blockrow in {4,8,16,32} (bs=4) or {16,32} (bs=8), unroll in
+ * {1,2,4} block steps whose loads are issued together, l2_prefetch = 1 adds
+ * the 256-byte L2 fetch hint to the value stream.  Shapes without a
+ * compiled kernel return BSP_ERR_UNSUPPORTED. */
+bsp_status bsp_bsr_spmv_variant(const bsp_bsr *m, const double *x, double *y,
+                                double alpha, double beta, int32_t lanes_per_blockrow,
+                                int32_t unroll, int32_t l2_prefetch,
+                                bsp_stream_t stream);
+
 /* Host-buffer form, the shape of the reference's wrappers (amgT_spmv_fp64,
  * src/amgT.cu:1355, takes host x/y): copies x_host (col doubles) to the
  * device, runs bsp_bsr_spmv, copies y back to y_host (row doubles) and waits
