@@ -45,6 +45,20 @@ class BspBsr(C.Structure):
     ]
 
 
+class BspDbsr(C.Structure):
+    """Mirror of bsp_dbsr (include/bsp.h), itself a mirror of the reference's
+    dbsrMat (include/matrixFormat.hpp:86-106)."""
+    _fields_ = [
+        ("row", C.c_int32), ("col", C.c_int32), ("nnz", C.c_int32),
+        ("blc_row", C.c_int32), ("blc_col", C.c_int32), ("blc_num", C.c_int32),
+        ("stand", C.c_double), ("avg_nnz", C.c_double),
+        ("blcPtr", C.c_void_p), ("colIdx", C.c_void_p), ("blcVal", C.c_void_p), ("blcMap", C.c_void_p),
+        ("blocknnz", C.c_int32), ("warpnum", C.c_int32), ("rowPtrbyWarp", C.c_void_p),
+        ("rowIdxbyWarp", C.c_void_p), ("recorderMap", C.c_void_p), ("prefix", C.c_void_p),
+        ("balance_overflow", C.c_int32),
+    ]
+
+
 _P = C.c_void_p
 _I32 = C.c_int32
 _I64 = C.c_int64
@@ -68,6 +82,9 @@ _PROTOS = {
     "bsp_bsr_spmv": (C.c_int, [C.POINTER(BspBsr), _P, _P, _D, _D, _I32, _P]),
     "bsp_bsr_spmv_variant": (C.c_int, [C.POINTER(BspBsr), _P, _P, _D, _D, _I32, _I32, _I32, _P]),
     "bsp_bsr_spmv_host": (C.c_int, [C.POINTER(BspBsr), _P, _P, _D, _D, _I32, _P]),
+    "bsp_csr2dbsr": (C.c_int, [_I32, _I32, _I32, _P, _P, _P, _I32, C.POINTER(BspDbsr), _P]),
+    "bsp_dbsr_free": (C.c_int, [C.POINTER(BspDbsr)]),
+    "bsp_dbsr_spmv": (C.c_int, [C.POINTER(BspDbsr), _P, _P, _D, _D, _I32, _P]),
     "bsp_gen_laplace2d": (C.c_int, [_I32, _I32, _PI32, _PI32, _P, _P, _P]),
     "bsp_gen_poisson3d": (C.c_int, [_I32, _PI32, _PI64, _P, _P, _P]),
     "bsp_gen_stencil27": (C.c_int, [_I32, _I32, _U64, _PI32, _PI64, _P, _P, _P]),

@@ -184,6 +184,65 @@ def csr2bsr(rowptr, colidx, values, *, rows: int, cols: int, bs: int = 4, stream
 
 
 # ---------------------------------------------------------------------------
+# DBSR (dbsrMat, reference include/matrixFormat.hpp:86-106; csrTodbsr /
+# csrTodbsrWithRecorder / balanceDbsr, include/dbsr.h; amgT_spmv_fp64_dbsr*,
+# src/amgT.cu:1202-1353)
+
+class DbsrMatrix:
+    """Device DBSR matrix (4x4 blocks of consecutive nonzeros per row quad)."""
+
+    def __init__(self, desc: _lib.BspDbsr):
+        self._d = desc
+        self._live = True
+
+    def __getattr__(self, name):
+        d = self.__dict__.get("_d")
+        if d is not None and name in dict(_lib.BspDbsr._fields_):
+            return getattr(d, name)
+        raise AttributeError(name)
+
+    def arrays(self) -> dict[str, np.ndarray]:
+        d = self._d
+        out = {
+            "blcPtr": _d2h(d.blcPtr, d.blc_row + 1, np.int32),
+            "colIdx": _d2h(d.colIdx, d.blocknnz, np.int32),
+            "blcVal": _d2h(d.blcVal, d.blocknnz, np.float64),
+            "blcMap": _d2h(d.blcMap, d.blc_num, np.uint16),
+            "prefix": _d2h(d.prefix, d.warpnum + 1, np.int32),
+        }
+        if d.recorderMap:
+            out["recorderMap"] = _d2h(d.recorderMap, d.row, np.int32)
+        return out
+
+    def spmv(self, x, y=None, *, alpha: float = 1.0, beta: float = 0.0, permuted: bool = False, stream=None):
+        torch = _torch()
+        if y is None:
+            y = torch.empty(self._d.row, dtype=torch.float64, device=x.device)
+            beta = 0.0
+        check(lib().bsp_dbsr_spmv(C.byref(self._d), _dptr(x, "x"), _dptr(y, "y"), float(alpha), float(beta),
+                                  int(permuted), _stream(stream)))
+        return y
+
+    def free(self) -> None:
+        if self._live:
+            self._live = False
+            check(lib().bsp_dbsr_free(C.byref(self._d)))
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def csr2dbsr(rowptr, colidx, values, *, rows: int, cols: int, recorder: bool = True, stream=None) -> DbsrMatrix:
+    d = _lib.BspDbsr()
+    check(lib().bsp_csr2dbsr(rows, cols, colidx.numel(), _dptr(rowptr, "rowptr"), _dptr(colidx, "colidx"),
+                             _dptr(values, "values"), int(recorder), C.byref(d), _stream(stream)))
+    return DbsrMatrix(d)
+
+
+# ---------------------------------------------------------------------------
 # Seeded synthetic inputs (host numpy arrays)
 
 @dataclass

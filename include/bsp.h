@@ -165,6 +165,50 @@ bsp_status bsp_bsr_spmv_host(const bsp_bsr *m, const double *x_host, double *y_h
                              bsp_stream_t stream);
 
 /* ---------------------------------------------------------------------- */
+/* DBSR, "denser" 4x4 blocks (dbsrMat, reference include/matrixFormat.hpp:86-106).
+ * The z-th nonzero of row i sits in block blcPtr[i/4] + z/4 at position
+ * (i%4)*4 + z%4, with its own column index (padding: column 0, value 0). */
+typedef struct {
+  int32_t row, col, nnz;
+  int32_t blc_row, blc_col, blc_num; /* blc_num = blocks (blocknnz / 16) */
+  double stand, avg_nnz;
+  int32_t *blcPtr;      /* [blc_row+1] */
+  int32_t *colIdx;      /* [blocknnz] per-element column indices */
+  double *blcVal;       /* [blocknnz] */
+  uint16_t *blcMap;     /* [blc_num] (+ padding to whole 32-bit words) */
+  int32_t blocknnz;     /* blc_num * 16 */
+  int32_t warpnum;      /* warps of <= 64 blocks from balanceDbsr */
+  int32_t *rowPtrbyWarp;/* unused (NULL), kept for the field layout */
+  int32_t *rowIdxbyWarp;/* unused (NULL) */
+  int32_t *recorderMap; /* [row] new -> old row (recorder variant), else NULL */
+  int32_t *prefix;      /* [warpnum+1] balanceDbsr warp -> block-row prefix */
+  int32_t balance_overflow; /* 1 where the reference's balanceDbsr would index
+                               past its warp vector (see bsp_csr2dbsr) */
+} bsp_dbsr;
+
+/* CSR -> DBSR on the device, bit-identical to the reference's host
+ * converters: recorder = 0 replaces csrTodbsr + balanceDbsr
+ * (include/dbsr.h:10 and :94); recorder = 1 replaces csrTodbsrWithRecorder
+ * (include/dbsr.h:208: rows sorted ascending by length, ties by index).
+ * balanceDbsr's second walk can run past the warp count of its first walk
+ * (the reference then writes out of bounds); the walk is replayed exactly,
+ * the warp list grows to hold it and balance_overflow is set. */
+bsp_status bsp_csr2dbsr(int32_t rows, int32_t cols, int32_t nnz,
+                        const int32_t *rowPtr, const int32_t *colIdx,
+                        const double *values, int32_t recorder, bsp_dbsr *out,
+                        bsp_stream_t stream);
+bsp_status bsp_dbsr_free(bsp_dbsr *m);
+/* y = alpha*A*x + beta*y; replaces amgT_spmv_fp64_dbsr(_balance)
+ * (reference src/amgT.cu:1202, :1280; include/amgT.h:4-5), whose kernels
+ * compute row sums (they overwrite the gathered x with 1.0, amgT.cu:356,
+ * :425) -- this one computes A*x.  permuted_output = 1 writes y in the
+ * recorder order (the reference's layout, un-permuted by its caller,
+ * bench/spmvfp64.cpp:162-166); 0 writes y in the original row order. */
+bsp_status bsp_dbsr_spmv(const bsp_dbsr *m, const double *x, double *y,
+                         double alpha, double beta, int32_t permuted_output,
+                         bsp_stream_t stream);
+
+/* ---------------------------------------------------------------------- */
 /* Synthetic matrix generators (host, seeded, deterministic).  Two-phase:
  * call with NULL arrays to get the sizes, then with allocated arrays. */
 

@@ -59,6 +59,25 @@ int32_t orc_bsr_chunks(int32_t blc_row, const int32_t *blcPtr, int32_t *rowPtrby
 /* sqrtf(sum (len - avg)^2 / blc_row) (getStand, src/amgT.cu:546-575, :1146-1155). */
 double orc_bsr_stand(int32_t blc_row, const int32_t *blcPtr);
 
+/* DBSR (include/dbsr.h).  orc_recorder: rows stably sorted ascending by
+ * length (csrRecorderSelf, :170-206), order[new] = old.  orc_dbsr_blocks:
+ * block pointer of csrTodbsr (:18-26), returns the block count.
+ * orc_dbsr_fill: its scatter (:65-79) into zero-filled arrays.
+ * orc_dbsr_balance: balanceDbsr's two walks (:94-168), prefix[warps+1]. */
+void orc_recorder(int32_t rows, const int32_t *rowPtr, const int32_t *colIdx, const double *val, int32_t *order,
+                  int32_t *newPtr, int32_t *newCol, double *newVal);
+int32_t orc_dbsr_blocks(int32_t rows, const int32_t *rowPtr, int32_t *blcPtr);
+void orc_dbsr_fill(int32_t rows, const int32_t *rowPtr, const int32_t *colIdx, const double *val,
+                   const int32_t *blcPtr, int32_t *outCol, double *outVal, uint16_t *map);
+int32_t orc_dbsr_balance(int32_t brow, const int32_t *blcPtr, int32_t *prefix, int32_t cap_prefix,
+                         int32_t *overflow);
+
+/* BCSR csrToBcsr (utils/utils.hpp:10-123): pass 1 (bRowPtr NULL) returns
+ * nonzeroBlocks; pass 2 fills bRowPtr[rowRegions+1], bColIdx, bVal
+ * (tm x tk row-major) and, if non-NULL, the dense mapping. */
+int64_t orc_csr2bcsr(int32_t rows, int32_t cols, const int32_t *rowPtr, const int32_t *colIdx, const double *val,
+                     int32_t tm, int32_t tk, int32_t *bRowPtr, int32_t *bColIdx, double *bVal, int32_t *mapping);
+
 #ifdef __cplusplus
 }
 #endif

@@ -51,6 +51,14 @@ def orc() -> C.CDLL:
         L.orc_bsr_chunks.argtypes = [_I32, _P, _P, _P]
         L.orc_bsr_stand.restype = C.c_double
         L.orc_bsr_stand.argtypes = [_I32, _P]
+        L.orc_recorder.argtypes = [_I32, _P, _P, _P, _P, _P, _P, _P]
+        L.orc_dbsr_blocks.restype = _I32
+        L.orc_dbsr_blocks.argtypes = [_I32, _P, _P]
+        L.orc_dbsr_fill.argtypes = [_I32, _P, _P, _P, _P, _P, _P, _P]
+        L.orc_dbsr_balance.restype = _I32
+        L.orc_dbsr_balance.argtypes = [_I32, _P, _P, _I32, _P]
+        L.orc_csr2bcsr.restype = _I64
+        L.orc_csr2bcsr.argtypes = [_I32, _I32, _P, _P, _P, _I32, _I32, _P, _P, _P, _P]
         L.orc_f32_to_f16.restype = C.c_uint16
         L.orc_f32_to_f16.argtypes = [C.c_float]
         _orc = L
@@ -119,6 +127,59 @@ def csr2bsr(rows, cols, rowptr, colidx, val, bs=4) -> dict:
             "blcMap": blcMap.astype(np.uint16) if bs == 4 else blcMap, "rowPtrbyWarp": rpw,
             "rowIdxbyWarp": riw, "warpnum": warpnum, "stand": float(L.orc_bsr_stand(brow, _p(blcPtr))),
             "avg_nnz": (colidx.size / nb) if nb else 0.0}
+
+
+# ---------------------------------------------------------------------------
+# DBSR (include/dbsr.h) and BCSR (utils/utils.hpp)
+
+def recorder(rowptr, colidx, val) -> dict:
+    rows = rowptr.size - 1
+    order = np.empty(rows, np.int32)
+    rp = np.empty(rows + 1, np.int32)
+    ci = np.empty(colidx.size, np.int32)
+    va = np.empty(colidx.size, np.float64)
+    orc().orc_recorder(rows, _p(rowptr), _p(colidx), _p(val), _p(order), _p(rp), _p(ci), _p(va))
+    return {"order": order, "rowptr": rp, "colidx": ci, "values": va}
+
+
+def csr2dbsr(rowptr, colidx, val, recorder_sort: bool) -> dict:
+    L = orc()
+    rows = rowptr.size - 1
+    out = {}
+    if recorder_sort:
+        rec = recorder(rowptr, colidx, val)
+        rowptr, colidx, val = rec["rowptr"], rec["colidx"], rec["values"]
+        out["recorderMap"] = rec["order"]
+        out["rec_rowptr"], out["rec_colidx"], out["rec_values"] = rowptr, colidx, val
+    brow = (rows + 3) // 4
+    blcPtr = np.empty(brow + 1, np.int32)
+    nb = int(L.orc_dbsr_blocks(rows, _p(rowptr), _p(blcPtr)))
+    col = np.zeros(nb * 16, np.int32)
+    bv = np.zeros(nb * 16, np.float64)
+    mp = np.zeros(max(nb, 1), np.uint16)
+    L.orc_dbsr_fill(rows, _p(rowptr), _p(colidx), _p(val), _p(blcPtr), _p(col), _p(bv), _p(mp))
+    of = C.c_int32()
+    wn = int(L.orc_dbsr_balance(brow, _p(blcPtr), None, 0, C.byref(of)))
+    prefix = np.empty(wn + 1, np.int32)
+    L.orc_dbsr_balance(brow, _p(blcPtr), _p(prefix), wn, C.byref(of))
+    out.update(blc_row=brow, blc_num=nb, blocknnz=nb * 16, blcPtr=blcPtr, colIdx=col, blcVal=bv, blcMap=mp[:nb],
+               warpnum=wn, prefix=prefix, balance_overflow=int(of.value))
+    return out
+
+
+def csr2bcsr(rows, cols, rowptr, colidx, val, tm, tk, with_mapping=True) -> dict:
+    L = orc()
+    nb = int(L.orc_csr2bcsr(rows, cols, _p(rowptr), _p(colidx), _p(val), tm, tk, None, None, None, None))
+    nr = (rows + tm - 1) // tm
+    nc = (cols + tk - 1) // tk
+    rp = np.empty(nr + 1, np.int32)
+    ci = np.empty(nb, np.int32)
+    bv = np.empty(nb * tm * tk, np.float64)
+    mp = np.empty(nr * nc, np.int32) if with_mapping else None
+    L.orc_csr2bcsr(rows, cols, _p(rowptr), _p(colidx), _p(val), tm, tk, _p(rp), _p(ci), _p(bv),
+                   _p(mp) if mp is not None else None)
+    return {"rowRegions": nr, "colRegions": nc, "nonzeroBlocks": nb, "bcsrRowPtr": rp, "bcsrColIdx": ci,
+            "bcsrVal": bv, "mapping": mp}
 
 
 # ---------------------------------------------------------------------------

@@ -89,3 +89,42 @@ def test_csr2bsr_oracle_against_reference_gpu_capture(golden, name):
         assert np.array_equal(o[k], g[k]), k
     assert o["warpnum"] == int(g["warpnum"]) and o["blc_num"] == int(g["blc_num"])
     assert abs(o["stand"] - float(g["stand"])) <= 1e-6 * max(1.0, float(g["stand"]))
+
+
+DBSR = sorted(Path(p).name for p in glob.glob(str(GOLDEN / "dbsr_*.npz")))
+
+
+@pytest.mark.parametrize("name", DBSR)
+def test_dbsr_oracle_against_reference(golden, name):
+    g = golden(name)
+    rec = name.endswith("_rec.npz")
+    o = pyoracle.csr2dbsr(g["rowptr"], g["colidx"], g["values"], rec)
+    if rec:
+        for k in ("rec_rowptr", "rec_colidx", "rec_values"):
+            assert np.array_equal(o[k], g[k]), k
+    assert o["blc_row"] == int(g["blc_row"]) and o["blocknnz"] == int(g["blocknnz"])
+    assert np.array_equal(o["blcPtr"], g["blcPtr"])
+    assert np.array_equal(o["colIdx"], g["colIdx_d"])
+    assert np.array_equal(o["blcVal"], g["blcVal"])
+    assert np.array_equal(o["blcMap"], g["blcMap"])
+    in_bounds = bool(int(g["balance_in_bounds"]))
+    assert o["balance_overflow"] == (0 if in_bounds else 1)
+    if in_bounds:
+        assert o["warpnum"] == int(g["warpnum"])
+        assert np.array_equal(o["prefix"], g["prefix"])
+        if rec:
+            assert np.array_equal(o["recorderMap"], g["recorderMap"])
+
+
+BCSR = sorted(Path(p).name for p in glob.glob(str(GOLDEN / "bcsr_*.npz")))
+
+
+@pytest.mark.parametrize("name", BCSR)
+def test_bcsr_oracle_against_reference(golden, name):
+    g = golden(name)
+    o = pyoracle.csr2bcsr(int(g["rows"]), int(g["cols"]), g["rowptr"], g["colidx"], g["values"],
+                          int(g["tile_m"]), int(g["tile_k"]))
+    assert o["nonzeroBlocks"] == int(g["nonzeroBlocks"])
+    assert o["rowRegions"] == int(g["rowRegions"]) and o["colRegions"] == int(g["colRegions"])
+    for k in ("bcsrRowPtr", "bcsrColIdx", "bcsrVal", "mapping"):
+        assert np.array_equal(o[k], g[k]), k
