@@ -59,6 +59,18 @@ class BspDbsr(C.Structure):
     ]
 
 
+class BspBcsr(C.Structure):
+    """Mirror of bsp_bcsr (include/bsp.h) / the reference's BCSRFormat
+    (include/matrixFormat.hpp:16-30)."""
+    _fields_ = [
+        ("bcsrRowPtr", C.c_void_p), ("bcsrcolIdx", C.c_void_p), ("relativeBlockIndexMapping", C.c_void_p),
+        ("values", C.c_void_p), ("row", C.c_int32), ("col", C.c_int32), ("blockNum", C.c_int64),
+        ("TILE_M", C.c_int32), ("TILE_N", C.c_int32), ("TILE_K", C.c_int32), ("nnz", C.c_int32),
+        ("colRegions", C.c_int32), ("rowRegions", C.c_int32), ("nonzeroBlocks", C.c_int32),
+        ("elemCount", C.c_int32), ("block_row", C.c_int32), ("block_col", C.c_int32),
+    ]
+
+
 _P = C.c_void_p
 _I32 = C.c_int32
 _I64 = C.c_int64
@@ -82,6 +94,9 @@ _PROTOS = {
     "bsp_bsr_spmv": (C.c_int, [C.POINTER(BspBsr), _P, _P, _D, _D, _I32, _P]),
     "bsp_bsr_spmv_variant": (C.c_int, [C.POINTER(BspBsr), _P, _P, _D, _D, _I32, _I32, _I32, _P]),
     "bsp_bsr_spmv_host": (C.c_int, [C.POINTER(BspBsr), _P, _P, _D, _D, _I32, _P]),
+    "bsp_csr2bcsr": (C.c_int, [_I32, _I32, _I32, _P, _P, _P, _I32, _I32, _I32, C.POINTER(BspBcsr), _P]),
+    "bsp_bcsr_free": (C.c_int, [C.POINTER(BspBcsr)]),
+    "bsp_bcsr_spmv": (C.c_int, [C.POINTER(BspBcsr), _P, _P, _D, _D, _P]),
     "bsp_csr2dbsr": (C.c_int, [_I32, _I32, _I32, _P, _P, _P, _I32, C.POINTER(BspDbsr), _P]),
     "bsp_dbsr_free": (C.c_int, [C.POINTER(BspDbsr)]),
     "bsp_dbsr_spmv": (C.c_int, [C.POINTER(BspDbsr), _P, _P, _D, _D, _I32, _P]),

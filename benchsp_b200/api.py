@@ -184,6 +184,59 @@ def csr2bsr(rowptr, colidx, values, *, rows: int, cols: int, bs: int = 4, stream
 
 
 # ---------------------------------------------------------------------------
+# Fixed-tile BCSR (BCSRFormat, reference include/matrixFormat.hpp:16-30;
+# csrToBcsr, utils/utils.hpp:10; bcsr_spmv_fp64, src/bcsr.cu:224)
+
+class BcsrMatrix:
+    def __init__(self, desc: _lib.BspBcsr):
+        self._d = desc
+        self._live = True
+
+    def __getattr__(self, name):
+        d = self.__dict__.get("_d")
+        if d is not None and name in dict(_lib.BspBcsr._fields_):
+            return getattr(d, name)
+        raise AttributeError(name)
+
+    def arrays(self) -> dict[str, np.ndarray]:
+        d = self._d
+        out = {"bcsrRowPtr": _d2h(d.bcsrRowPtr, d.rowRegions + 1, np.int32),
+               "bcsrColIdx": _d2h(d.bcsrcolIdx, d.nonzeroBlocks, np.int32),
+               "bcsrVal": _d2h(d.values, d.elemCount, np.float64)}
+        if d.relativeBlockIndexMapping:
+            out["mapping"] = _d2h(d.relativeBlockIndexMapping, d.blockNum, np.int32)
+        return out
+
+    def spmv(self, x, y=None, *, alpha: float = 1.0, beta: float = 0.0, stream=None):
+        torch = _torch()
+        if y is None:
+            y = torch.empty(self._d.row, dtype=torch.float64, device=x.device)
+            beta = 0.0
+        check(lib().bsp_bcsr_spmv(C.byref(self._d), _dptr(x, "x"), _dptr(y, "y"), float(alpha), float(beta),
+                                  _stream(stream)))
+        return y
+
+    def free(self) -> None:
+        if self._live:
+            self._live = False
+            check(lib().bsp_bcsr_free(C.byref(self._d)))
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def csr2bcsr(rowptr, colidx, values, *, rows: int, cols: int, tile_m: int, tile_k: int, mapping: bool = False,
+             stream=None) -> BcsrMatrix:
+    d = _lib.BspBcsr()
+    check(lib().bsp_csr2bcsr(rows, cols, colidx.numel(), _dptr(rowptr, "rowptr"), _dptr(colidx, "colidx"),
+                             _dptr(values, "values"), tile_m, tile_k, int(mapping), C.byref(d), _stream(stream)))
+    return BcsrMatrix(d)
+
+
+# ---------------------------------------------------------------------------
 # DBSR (dbsrMat, reference include/matrixFormat.hpp:86-106; csrTodbsr /
 # csrTodbsrWithRecorder / balanceDbsr, include/dbsr.h; amgT_spmv_fp64_dbsr*,
 # src/amgT.cu:1202-1353)

@@ -51,36 +51,37 @@ __device__ __forceinline__ int32_t lower_bound_i32(const int32_t *__restrict__ a
   return lo;
 }
 
-// Step 1: canonical flags; one warp per row (grid-stride over rows).
-__global__ void bsr_canonical_kernel(int32_t rows, int32_t bs, const int32_t *__restrict__ rowPtr,
+// Step 1: canonical flags; one warp per row (grid-stride over rows).  Blocks
+// are tm x tk: block-row r/tm, block column c/tk.
+__global__ void bsr_canonical_kernel(int32_t rows, int32_t tm, int32_t tk, const int32_t *__restrict__ rowPtr,
                                      const int32_t *__restrict__ colIdx, int32_t *__restrict__ flag) {
   const int lane = threadIdx.x & 31;
   const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
   for (int64_t rr = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; rr < rows; rr += nwarps) {
     const int32_t r = (int32_t)rr;
     const int32_t s = rowPtr[r], e = rowPtr[r + 1];
-    const int32_t r0 = (r / bs) * bs;
+    const int32_t r0 = (r / tm) * tm;
     for (int32_t j = s + lane; j < e; j += 32) {
-      const int32_t b = colIdx[j] / bs;
-      int32_t canon = (j == s) || (colIdx[j - 1] / bs != b);
+      const int32_t b = colIdx[j] / tk;
+      int32_t canon = (j == s) || (colIdx[j - 1] / tk != b);
       for (int32_t q = r0; q < r && canon; ++q) {
         const int32_t qs = rowPtr[q], qe = rowPtr[q + 1];
-        const int32_t p = lower_bound_i32(colIdx, qs, qe, b * bs);
-        if (p < qe && colIdx[p] / bs == b) canon = 0;
+        const int32_t p = lower_bound_i32(colIdx, qs, qe, b * tk);
+        if (p < qe && colIdx[p] / tk == b) canon = 0;
       }
       flag[j] = canon;
     }
   }
 }
 
-// blcPtr[br] = pos[rowPtr[br*bs]]: the block-row's nonzeros are contiguous,
+// blcPtr[br] = pos[rowPtr[br*tm]]: the block-row's nonzeros are contiguous,
 // so the scan of the canonical flags at its first nonzero counts the blocks
 // of all earlier block-rows.  pos has nnz+1 entries (pos[nnz] = blc_num).
-__global__ void bsr_ptr_kernel(int32_t rows, int32_t blc_row, int32_t bs, const int32_t *__restrict__ rowPtr,
+__global__ void bsr_ptr_kernel(int32_t rows, int32_t blc_row, int32_t tm, const int32_t *__restrict__ rowPtr,
                                const int32_t *__restrict__ pos, int32_t *__restrict__ blcPtr) {
   for (int64_t br = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; br <= blc_row;
        br += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t r = br * bs;
+    const int64_t r = br * tm;
     blcPtr[br] = pos[rowPtr[r < rows ? r : rows]];
   }
 }
@@ -97,12 +98,14 @@ template <>
 __device__ __forceinline__ void map_or<uint64_t>(uint64_t *map, int64_t blk, int bit) {
   atomicOr(reinterpret_cast<unsigned long long *>(map) + blk, 1ull << bit);
 }
+template <>
+__device__ __forceinline__ void map_or<char>(char *, int64_t, int) {}  // no bitmap for tiles > 64 entries
 
 // Step 3: every nonzero locates its block and scatters value + bitmap bit.
 // rank = number of distinct block columns < b in the block-row = sum over the
-// block-row's rows q of the canonical elements in q before lower_bound(b*bs).
+// block-row's rows q of the canonical elements in q before lower_bound(b*tk).
 template <typename MapT>
-__global__ void bsr_fill_kernel(int32_t rows, int32_t bs, const int32_t *__restrict__ rowPtr,
+__global__ void bsr_fill_kernel(int32_t rows, int32_t tm, int32_t tk, const int32_t *__restrict__ rowPtr,
                                 const int32_t *__restrict__ colIdx, const double *__restrict__ val,
                                 const int32_t *__restrict__ pos, const int32_t *__restrict__ blcPtr,
                                 int32_t *__restrict__ blcIdx, double *__restrict__ blcVal, MapT *blcMap) {
@@ -110,24 +113,24 @@ __global__ void bsr_fill_kernel(int32_t rows, int32_t bs, const int32_t *__restr
   const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
   for (int64_t rr = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; rr < rows; rr += nwarps) {
     const int32_t r = (int32_t)rr;
-    const int32_t br = r / bs, r0 = br * bs;
-    const int32_t r1 = r0 + bs < rows ? r0 + bs : rows;
+    const int32_t br = r / tm, r0 = br * tm;
+    const int32_t r1 = r0 + tm < rows ? r0 + tm : rows;
     const int32_t s = rowPtr[r], e = rowPtr[r + 1];
     const int32_t base = blcPtr[br], end_blk = blcPtr[br + 1];
     for (int32_t j = s + lane; j < e; j += 32) {
       const int32_t c = colIdx[j];
-      const int32_t b = c / bs;
+      const int32_t b = c / tk;
       int32_t rank = 0;
       for (int32_t q = r0; q < r1; ++q) {
         const int32_t qs = rowPtr[q], qe = rowPtr[q + 1];
-        const int32_t p = lower_bound_i32(colIdx, qs, qe, b * bs);
+        const int32_t p = lower_bound_i32(colIdx, qs, qe, b * tk);
         rank += pos[p] - pos[qs];
       }
       const int64_t blk = (int64_t)base + rank;
       if (blk >= end_blk) continue;  // only reachable for unsorted input
-      const int in_r = r - r0, in_c = c - b * bs;
-      blcVal[blk * bs * bs + in_r * bs + in_c] = val[j];
-      map_or<MapT>(blcMap, blk, in_r * bs + in_c);
+      const int in_r = r - r0, in_c = c - b * tk;
+      blcVal[blk * tm * tk + in_r * tk + in_c] = val[j];
+      map_or<MapT>(blcMap, blk, in_r * tk + in_c);
       blcIdx[blk] = b;
     }
   }
@@ -185,12 +188,68 @@ __global__ void count_full_blocks_kernel(int64_t nb, int bs, const void *map, in
   if (threadIdx.x == 0) atomicAdd(out, part[0]);
 }
 
-static unsigned grid_for(int64_t n, int threads = 256) {
+static unsigned grid_for(int64_t n, int threads) {
   int64_t b = ceil_div(n, threads);
   const int64_t cap = (int64_t)sm_count() * 32;
   if (b > cap) b = cap;
   if (b < 1) b = 1;
   return (unsigned)b;
+}
+
+static unsigned grid_for(int64_t n, int threads);
+
+// Canonical tm x tk blocking of a CSR matrix (block columns ascending per
+// block-row, row-major values).  map16 (tm*tk <= 16) or map64 (<= 64) get the
+// occupancy bitmaps when non-null.  Outputs are allocated here.
+bsp_status csr2blocks(int32_t rows, int32_t nnz, const int32_t *rowPtr, const int32_t *colIdx, const double *values,
+                      int32_t tm, int32_t tk, int32_t *blc_num_out, int32_t **blcPtr, int32_t **blcIdx,
+                      double **blcVal, uint16_t **map16, uint64_t **map64, cudaStream_t s) {
+  const int32_t blc_row = (int32_t)ceil_div(rows, tm);
+  int32_t *pos = nullptr;
+  int64_t *d_total = nullptr;
+  BSP_TRY(dalloc(&pos, (size_t)nnz + 1, s));
+  BSP_TRY(dalloc(&d_total, 2, s));
+  BSP_CUDA(cudaMemsetAsync(pos + nnz, 0, sizeof(int32_t), s));
+  if (nnz > 0) {
+    bsr_canonical_kernel<<<grid_for((int64_t)rows * 32, 256), 256, 0, s>>>(rows, tm, tk, rowPtr, colIdx, pos);
+    BSP_LAUNCH_CHECK();
+  }
+  BSP_TRY(exclusive_scan_i32(pos, pos, (int64_t)nnz + 1, d_total, s));
+  int64_t total = 0;
+  BSP_TRY(read_i64(d_total, &total, s));
+  dfree(d_total, s);
+  if (total > INT32_MAX / ((int64_t)tm * tk)) BSP_FAIL(BSP_ERR_UNSUPPORTED, "too many blocks for int32 indexing");
+  const int32_t nb = (int32_t)total;
+  *blc_num_out = nb;
+  BSP_TRY(dalloc(blcPtr, (size_t)blc_row + 1, s));
+  bsr_ptr_kernel<<<grid_for((int64_t)blc_row + 1, 256), 256, 0, s>>>(rows, blc_row, tm, rowPtr, pos, *blcPtr);
+  BSP_LAUNCH_CHECK();
+  BSP_TRY(dalloc(blcIdx, (size_t)nb, s));
+  BSP_TRY(dalloc(blcVal, (size_t)nb * tm * tk, s));
+  BSP_CUDA(cudaMemsetAsync(*blcVal, 0, sizeof(double) * (size_t)nb * tm * tk, s));
+  const unsigned g = grid_for((int64_t)rows * 32, 256);
+  if (map16) {
+    // blc_num + 1 entries as the reference allocates (amgT.cu:1162), rounded
+    // up to whole 32-bit words for the word-wide OR.
+    const size_t n16 = ((size_t)nb + 2) & ~size_t(1);
+    BSP_TRY(dalloc(map16, n16, s));
+    BSP_CUDA(cudaMemsetAsync(*map16, 0, sizeof(uint16_t) * n16, s));
+    if (nnz > 0)
+      bsr_fill_kernel<uint16_t><<<g, 256, 0, s>>>(rows, tm, tk, rowPtr, colIdx, values, pos, *blcPtr, *blcIdx,
+                                                  *blcVal, *map16);
+  } else if (map64) {
+    BSP_TRY(dalloc(map64, (size_t)nb + 1, s));
+    BSP_CUDA(cudaMemsetAsync(*map64, 0, sizeof(uint64_t) * ((size_t)nb + 1), s));
+    if (nnz > 0)
+      bsr_fill_kernel<uint64_t><<<g, 256, 0, s>>>(rows, tm, tk, rowPtr, colIdx, values, pos, *blcPtr, *blcIdx,
+                                                  *blcVal, *map64);
+  } else if (nnz > 0) {
+    bsr_fill_kernel<char><<<g, 256, 0, s>>>(rows, tm, tk, rowPtr, colIdx, values, pos, *blcPtr, *blcIdx, *blcVal,
+                                            nullptr);
+  }
+  BSP_LAUNCH_CHECK();
+  dfree(pos, s);
+  return BSP_OK;
 }
 
 bsp_status csr2bsr_impl(int32_t rows, int32_t cols, int32_t nnz, const int32_t *rowPtr, const int32_t *colIdx,
@@ -202,55 +261,15 @@ bsp_status csr2bsr_impl(int32_t rows, int32_t cols, int32_t nnz, const int32_t *
   m.blc_row = (int32_t)ceil_div(rows, bs);
   m.blc_col = (int32_t)ceil_div(cols, bs);
   m.true_nnz = nnz;
-
-  int32_t *pos = nullptr;
-  int64_t *d_total = nullptr;
-  BSP_TRY(dalloc(&pos, (size_t)nnz + 1, s));
-  BSP_TRY(dalloc(&d_total, 2, s));
-  BSP_CUDA(cudaMemsetAsync(pos + nnz, 0, sizeof(int32_t), s));
-  if (nnz > 0) {
-    bsr_canonical_kernel<<<grid_for((int64_t)rows * 32), 256, 0, s>>>(rows, bs, rowPtr, colIdx, pos);
-    BSP_LAUNCH_CHECK();
-  }
-  BSP_TRY(exclusive_scan_i32(pos, pos, (int64_t)nnz + 1, d_total, s));
-  int64_t total = 0;
-  BSP_TRY(read_i64(d_total, &total, s));
-  if (total > INT32_MAX / (bs * bs)) BSP_FAIL(BSP_ERR_UNSUPPORTED, "too many blocks for int32 indexing");
-  m.blc_num = (int32_t)total;
+  uint16_t *m16 = nullptr;
+  uint64_t *m64 = nullptr;
+  BSP_TRY(csr2blocks(rows, nnz, rowPtr, colIdx, values, bs, bs, &m.blc_num, &m.blcPtr, &m.blcIdx, &m.blcVal,
+                     bs == 4 ? &m16 : nullptr, bs == 4 ? nullptr : &m64, s));
+  m.blcMap = bs == 4 ? (void *)m16 : (void *)m64;
   m.nnz = m.blc_num * bs * bs;
   m.avg_nnz = m.blc_num > 0 ? (double)nnz / (double)m.blc_num : 0.0;
-
-  BSP_TRY(dalloc(&m.blcPtr, (size_t)m.blc_row + 1, s));
-  bsr_ptr_kernel<<<grid_for((int64_t)m.blc_row + 1), 256, 0, s>>>(rows, m.blc_row, bs, rowPtr, pos, m.blcPtr);
-  BSP_LAUNCH_CHECK();
-
-  BSP_TRY(dalloc(&m.blcIdx, (size_t)m.blc_num, s));
-  BSP_TRY(dalloc(&m.blcVal, (size_t)m.nnz, s));
-  BSP_CUDA(cudaMemsetAsync(m.blcVal, 0, sizeof(double) * (size_t)m.nnz, s));
-  if (bs == 4) {
-    uint16_t *map = nullptr;
-    // blc_num + 1 entries as the reference allocates (amgT.cu:1162), rounded
-    // up to whole 32-bit words for the word-wide OR.
-    BSP_TRY(dalloc(&map, ((size_t)m.blc_num + 2) & ~size_t(1), s));
-    BSP_CUDA(cudaMemsetAsync(map, 0, sizeof(uint16_t) * (((size_t)m.blc_num + 2) & ~size_t(1)), s));
-    m.blcMap = map;
-    if (nnz > 0) {
-      bsr_fill_kernel<uint16_t><<<grid_for((int64_t)rows * 32), 256, 0, s>>>(rows, bs, rowPtr, colIdx, values, pos,
-                                                              m.blcPtr, m.blcIdx, m.blcVal, map);
-      BSP_LAUNCH_CHECK();
-    }
-  } else {
-    uint64_t *map = nullptr;
-    BSP_TRY(dalloc(&map, (size_t)m.blc_num + 1, s));
-    BSP_CUDA(cudaMemsetAsync(map, 0, sizeof(uint64_t) * ((size_t)m.blc_num + 1), s));
-    m.blcMap = map;
-    if (nnz > 0) {
-      bsr_fill_kernel<uint64_t><<<grid_for((int64_t)rows * 32), 256, 0, s>>>(rows, bs, rowPtr, colIdx, values, pos,
-                                                              m.blcPtr, m.blcIdx, m.blcVal, map);
-      BSP_LAUNCH_CHECK();
-    }
-  }
-  dfree(pos, s);
+  int64_t *d_total = nullptr;
+  BSP_TRY(dalloc(&d_total, 1, s));
 
   // Balanced chunks and block-length statistics.
   double *sq = nullptr, *d_sum = nullptr;
@@ -260,7 +279,7 @@ bsp_status csr2bsr_impl(int32_t rows, int32_t cols, int32_t nnz, const int32_t *
   const double avg_len = m.blc_row > 0 ? (double)m.blc_num / (double)m.blc_row : 0.0;
   BSP_CUDA(cudaMemsetAsync(m.rowPtrbyWarp, 0, sizeof(int32_t) * ((size_t)m.blc_row + 1), s));
   if (m.blc_row > 0) {
-    bsr_chunks_kernel<<<grid_for(m.blc_row), 256, 0, s>>>(m.blc_row, m.blcPtr, m.rowPtrbyWarp, avg_len, sq);
+    bsr_chunks_kernel<<<grid_for(m.blc_row, 256), 256, 0, s>>>(m.blc_row, m.blcPtr, m.rowPtrbyWarp, avg_len, sq);
     BSP_LAUNCH_CHECK();
   }
   BSP_TRY(exclusive_scan_i32(m.rowPtrbyWarp, m.rowPtrbyWarp, (int64_t)m.blc_row + 1, d_total, s));
@@ -269,7 +288,7 @@ bsp_status csr2bsr_impl(int32_t rows, int32_t cols, int32_t nnz, const int32_t *
   m.warpnum = (int32_t)warpnum;
   BSP_TRY(dalloc(&m.rowIdxbyWarp, (size_t)m.warpnum, s));
   if (m.blc_row > 0) {
-    bsr_rowidx_kernel<<<grid_for(m.blc_row), 256, 0, s>>>(m.blc_row, m.rowPtrbyWarp, m.rowIdxbyWarp);
+    bsr_rowidx_kernel<<<grid_for(m.blc_row, 256), 256, 0, s>>>(m.blc_row, m.rowPtrbyWarp, m.rowIdxbyWarp);
     BSP_LAUNCH_CHECK();
     sum_f64_kernel<<<1, 256, 0, s>>>(sq, m.blc_row, d_sum);
     BSP_LAUNCH_CHECK();
@@ -283,7 +302,7 @@ bsp_status csr2bsr_impl(int32_t rows, int32_t cols, int32_t nnz, const int32_t *
   BSP_TRY(dalloc(&d_full, 1, s));
   BSP_CUDA(cudaMemsetAsync(d_full, 0, sizeof(int32_t), s));
   if (m.blc_num > 0) {
-    count_full_blocks_kernel<<<grid_for(m.blc_num), 256, 0, s>>>(m.blc_num, bs, m.blcMap, d_full);
+    count_full_blocks_kernel<<<grid_for(m.blc_num, 256), 256, 0, s>>>(m.blc_num, bs, m.blcMap, d_full);
     BSP_LAUNCH_CHECK();
   }
   BSP_TRY(read_i32(d_full, &m.dense_blocks, s));

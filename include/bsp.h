@@ -165,6 +165,38 @@ bsp_status bsp_bsr_spmv_host(const bsp_bsr *m, const double *x_host, double *y_h
                              bsp_stream_t stream);
 
 /* ---------------------------------------------------------------------- */
+/* Fixed-tile BCSR (BCSRFormat<double,int32_t>, reference
+ * include/matrixFormat.hpp:16-30).  blockNum is 64-bit (rowRegions *
+ * colRegions overflows int32 for n above ~46k with 1x1 tiles). */
+typedef struct {
+  int32_t *bcsrRowPtr;                /* [rowRegions+1] */
+  int32_t *bcsrcolIdx;                /* [nonzeroBlocks] block columns, ascending */
+  int32_t *relativeBlockIndexMapping; /* [rowRegions*colRegions], -1 = empty; NULL unless requested */
+  double *values;                     /* [nonzeroBlocks*TILE_M*TILE_K] row-major tiles */
+  int32_t row, col;
+  int64_t blockNum;                   /* rowRegions * colRegions */
+  int32_t TILE_M, TILE_N, TILE_K;     /* TILE_N = TILE_K */
+  int32_t nnz;                        /* nonzeros of the source CSR */
+  int32_t colRegions, rowRegions, nonzeroBlocks, elemCount;
+  int32_t block_row, block_col;       /* = rowRegions, colRegions */
+} bsp_bcsr;
+
+/* CSR -> BCSR with tile_m x tile_k tiles (1..64 each) on the device;
+ * replaces csrToBcsr (reference utils/utils.hpp:10), whose dense
+ * rowRegions x colRegions table limits it to small matrices.  Arrays are
+ * bit-identical to the reference's; with_mapping = 1 also builds the dense
+ * relativeBlockIndexMapping. */
+bsp_status bsp_csr2bcsr(int32_t rows, int32_t cols, int32_t nnz,
+                        const int32_t *rowPtr, const int32_t *colIdx,
+                        const double *values, int32_t tile_m, int32_t tile_k,
+                        int32_t with_mapping, bsp_bcsr *out, bsp_stream_t stream);
+bsp_status bsp_bcsr_free(bsp_bcsr *b);
+/* y = alpha*A*x + beta*y for any tile shape; replaces bcsr_spmv_fp64
+ * (reference src/bcsr.cu:224, include/bcsr.h:3). */
+bsp_status bsp_bcsr_spmv(const bsp_bcsr *b, const double *x, double *y,
+                         double alpha, double beta, bsp_stream_t stream);
+
+/* ---------------------------------------------------------------------- */
 /* DBSR, "denser" 4x4 blocks (dbsrMat, reference include/matrixFormat.hpp:86-106).
  * The z-th nonzero of row i sits in block blcPtr[i/4] + z/4 at position
  * (i%4)*4 + z%4, with its own column index (padding: column 0, value 0). */
