@@ -71,6 +71,30 @@ class BspBcsr(C.Structure):
     ]
 
 
+class BspDasp(C.Structure):
+    """Mirror of bsp_dasp (include/bsp.h): the DASP packing of spmv_all
+    (reference src/dasp.cu:814-1600)."""
+    _fields_ = [
+        ("rows", C.c_int32), ("cols", C.c_int32), ("nnz", C.c_int32), ("threshold", C.c_double),
+        ("block_longest", C.c_int32), ("row_long", C.c_int32), ("row_block", C.c_int32), ("row_zero", C.c_int32),
+        ("short_row_1", C.c_int32), ("short_row_2", C.c_int32), ("short_row_3", C.c_int32),
+        ("short_row_4", C.c_int32), ("common_13", C.c_int32), ("short_row_34", C.c_int32),
+        ("short_block13", C.c_int32), ("short_block34", C.c_int32), ("short_block22", C.c_int32),
+        ("blocknum", C.c_int32), ("long_warps", C.c_int32), ("warp_number", C.c_int32),
+        ("fill0_nnz_long", C.c_int32), ("fill0_nnz_short13", C.c_int32), ("fill0_nnz_short34", C.c_int32),
+        ("fill0_nnz_short22", C.c_int32), ("fill0_nnz_short", C.c_int32), ("fill0_nnz_reg", C.c_int32),
+        ("nnz_irreg", C.c_int32), ("offset_reg", C.c_int32), ("offset_short1", C.c_int32),
+        ("offset_short13", C.c_int32), ("offset_short34", C.c_int32), ("offset_short22", C.c_int32),
+        ("block_num_all", C.c_int32),
+        ("long_val", C.c_void_p), ("long_cid", C.c_void_p), ("long_ptr_warp", C.c_void_p),
+        ("long_row_of_warp", C.c_void_p), ("warp_val", C.c_void_p), ("long_done", C.c_void_p),
+        ("reg_val", C.c_void_p), ("reg_cid", C.c_void_p), ("block_ptr", C.c_void_p),
+        ("irreg_val", C.c_void_p), ("irreg_cid", C.c_void_p), ("irreg_rpt", C.c_void_p),
+        ("short_val", C.c_void_p), ("short_cid", C.c_void_p), ("order_rid", C.c_void_p),
+        ("sorted_rid", C.c_void_p), ("row_len_sorted", C.c_void_p),
+    ]
+
+
 _P = C.c_void_p
 _I32 = C.c_int32
 _I64 = C.c_int64
@@ -100,6 +124,9 @@ _PROTOS = {
     "bsp_csr2dbsr": (C.c_int, [_I32, _I32, _I32, _P, _P, _P, _I32, C.POINTER(BspDbsr), _P]),
     "bsp_dbsr_free": (C.c_int, [C.POINTER(BspDbsr)]),
     "bsp_dbsr_spmv": (C.c_int, [C.POINTER(BspDbsr), _P, _P, _D, _D, _I32, _P]),
+    "bsp_csr2dasp": (C.c_int, [_I32, _I32, _I32, _P, _P, _P, _D, _I32, C.POINTER(BspDasp), _P]),
+    "bsp_dasp_free": (C.c_int, [C.POINTER(BspDasp)]),
+    "bsp_dasp_spmv": (C.c_int, [C.POINTER(BspDasp), _P, _P, _D, _D, _I32, _P]),
     "bsp_gen_laplace2d": (C.c_int, [_I32, _I32, _PI32, _PI32, _P, _P, _P]),
     "bsp_gen_poisson3d": (C.c_int, [_I32, _PI32, _PI64, _P, _P, _P]),
     "bsp_gen_stencil27": (C.c_int, [_I32, _I32, _U64, _PI32, _PI64, _P, _P, _P]),

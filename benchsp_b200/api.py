@@ -296,6 +296,75 @@ def csr2dbsr(rowptr, colidx, values, *, rows: int, cols: int, recorder: bool = T
 
 
 # ---------------------------------------------------------------------------
+# DASP (spmv_all, reference src/dasp.cu:814; include/dasp.h)
+
+class DaspMatrix:
+    """Device DASP packing (long / row-block / short row classes)."""
+
+    INT_FIELDS = ("row_long", "row_block", "row_zero", "short_row_1", "short_row_2", "short_row_3", "short_row_4",
+                  "common_13", "short_row_34", "blocknum", "warp_number", "fill0_nnz_long", "fill0_nnz_short13",
+                  "fill0_nnz_short34", "fill0_nnz_short22", "fill0_nnz_short", "fill0_nnz_reg", "nnz_irreg",
+                  "offset_reg", "offset_short1", "offset_short13", "offset_short34", "offset_short22",
+                  "block_num_all")
+
+    def __init__(self, desc: _lib.BspDasp):
+        self._d = desc
+        self._live = True
+
+    def __getattr__(self, name):
+        d = self.__dict__.get("_d")
+        if d is not None and name in dict(_lib.BspDasp._fields_):
+            return getattr(d, name)
+        raise AttributeError(name)
+
+    def arrays(self) -> dict[str, np.ndarray]:
+        d = self._d
+        return {
+            "long_val": _d2h(d.long_val, d.fill0_nnz_long, np.float64),
+            "long_cid": _d2h(d.long_cid, d.fill0_nnz_long, np.int32),
+            "long_ptr_warp": _d2h(d.long_ptr_warp, d.row_long + 1, np.int32),
+            "reg_val": _d2h(d.reg_val, d.fill0_nnz_reg, np.float64),
+            "reg_cid": _d2h(d.reg_cid, d.fill0_nnz_reg, np.int32),
+            "block_ptr": _d2h(d.block_ptr, d.blocknum + 1, np.int32),
+            "irreg_val": _d2h(d.irreg_val, d.nnz_irreg, np.float64),
+            "irreg_cid": _d2h(d.irreg_cid, d.nnz_irreg, np.int32),
+            "irreg_rpt": _d2h(d.irreg_rpt, d.row_block + 1, np.int32),
+            "short_val": _d2h(d.short_val, d.fill0_nnz_short, np.float64),
+            "short_cid": _d2h(d.short_cid, d.fill0_nnz_short, np.int32),
+            "order_rid": _d2h(d.order_rid, d.rows, np.int32),
+        }
+
+    def spmv(self, x, y=None, *, alpha: float = 1.0, beta: float = 0.0, permuted: bool = False, stream=None):
+        torch = _torch()
+        if y is None:
+            y = torch.empty(self._d.rows, dtype=torch.float64, device=x.device)
+            beta = 0.0
+        check(lib().bsp_dasp_spmv(C.byref(self._d), _dptr(x, "x"), _dptr(y, "y"), float(alpha), float(beta),
+                                  int(permuted), _stream(stream)))
+        return y
+
+    def free(self) -> None:
+        if self._live:
+            self._live = False
+            check(lib().bsp_dasp_free(C.byref(self._d)))
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def csr2dasp(rowptr, colidx, values, *, rows: int, cols: int, threshold: float = 0.75, block_longest: int = 256,
+             stream=None) -> DaspMatrix:
+    d = _lib.BspDasp()
+    check(lib().bsp_csr2dasp(rows, cols, colidx.numel(), _dptr(rowptr, "rowptr"), _dptr(colidx, "colidx"),
+                             _dptr(values, "values"), float(threshold), int(block_longest), C.byref(d),
+                             _stream(stream)))
+    return DaspMatrix(d)
+
+
+# ---------------------------------------------------------------------------
 # Seeded synthetic inputs (host numpy arrays)
 
 @dataclass

@@ -241,6 +241,61 @@ bsp_status bsp_dbsr_spmv(const bsp_dbsr *m, const double *x, double *y,
                          bsp_stream_t stream);
 
 /* ---------------------------------------------------------------------- */
+/* DASP packing (the arrays spmv_all builds and uploads, reference
+ * src/dasp.cu:814-1600).  Row classes: len 1, 2, 3, 4, 0, long
+ * (>= block_longest) and row-block rows.  y slots run in order_rid order:
+ * long rows, row-block rows (sorted descending by length), len-1 rows,
+ * 1&3 tile pairs (8 len-1 then 8 len-3 rows per tile), remaining len-3,
+ * len-4, len-2 rows, empty rows. */
+typedef struct {
+  int32_t rows, cols, nnz;
+  double threshold;
+  int32_t block_longest;
+  int32_t row_long, row_block, row_zero;
+  int32_t short_row_1, short_row_2, short_row_3, short_row_4; /* _1/_3 after pairing */
+  int32_t common_13, short_row_34;
+  int32_t short_block13, short_block34, short_block22;
+  int32_t blocknum;       /* 8-row blocks, padded to a multiple of 4 */
+  int32_t long_warps;     /* 64-value chunks of the long rows */
+  int32_t warp_number;    /* long_warps padded to a multiple of 4 */
+  int32_t fill0_nnz_long, fill0_nnz_short13, fill0_nnz_short34, fill0_nnz_short22;
+  int32_t fill0_nnz_short, fill0_nnz_reg, nnz_irreg;
+  /* the reference kernel's block ranges (dasp.cu:1531-1539) */
+  int32_t offset_reg, offset_short1, offset_short13, offset_short34, offset_short22, block_num_all;
+  double *long_val;  int32_t *long_cid;        /* [fill0_nnz_long] */
+  int32_t *long_ptr_warp;                      /* [row_long+1] chunk prefix */
+  int32_t *long_row_of_warp;                   /* [warp_number], -1 = padding */
+  double *warp_val;  int32_t *long_done;       /* SpMV scratch: chunk partials, arrival counters */
+  double *reg_val;   int32_t *reg_cid;         /* [fill0_nnz_reg] 8x4 tiles */
+  int32_t *block_ptr;                          /* [blocknum+1] */
+  double *irreg_val; int32_t *irreg_cid;       /* [nnz_irreg] */
+  int32_t *irreg_rpt;                          /* [row_block+1] */
+  double *short_val; int32_t *short_cid;       /* [fill0_nnz_short] */
+  int32_t *order_rid;                          /* [rows] y slot -> row */
+  int32_t *sorted_rid;                         /* [row_block] row-block rows, sorted */
+  int32_t *row_len_sorted;                     /* [row_block+1] prefix of their lengths */
+} bsp_dasp;
+
+/* CSR -> DASP on the device, arrays bit-identical to spmv_all's host
+ * packing (reference src/dasp.cu:827-1482) for the same threshold and
+ * block_longest (the reference bench passes 0.75 and 256,
+ * bench/spmvfp64.cpp:177).  threshold must be > 0 (the reference loops
+ * forever on an empty block otherwise). */
+bsp_status bsp_csr2dasp(int32_t rows, int32_t cols, int32_t nnz,
+                        const int32_t *rowPtr, const int32_t *colIdx,
+                        const double *values, double threshold,
+                        int32_t block_longest, bsp_dasp *out, bsp_stream_t stream);
+bsp_status bsp_dasp_free(bsp_dasp *d);
+/* y = alpha*A*x + beta*y in one launch (the reference needs dasp_spmv2 +
+ * longPart_sum, dasp.cu:406, :381).  permuted_output = 1 writes y in
+ * order_rid order, as spmv_all returns it; 0 writes the original row order.
+ * Calls on one bsp_dasp must not overlap on the GPU (they share the
+ * long-row scratch). */
+bsp_status bsp_dasp_spmv(const bsp_dasp *d, const double *x, double *y,
+                         double alpha, double beta, int32_t permuted_output,
+                         bsp_stream_t stream);
+
+/* ---------------------------------------------------------------------- */
 /* Synthetic matrix generators (host, seeded, deterministic).  Two-phase:
  * call with NULL arrays to get the sizes, then with allocated arrays. */
 

@@ -78,6 +78,20 @@ int32_t orc_dbsr_balance(int32_t brow, const int32_t *blcPtr, int32_t *prefix, i
 int64_t orc_csr2bcsr(int32_t rows, int32_t cols, const int32_t *rowPtr, const int32_t *colIdx, const double *val,
                      int32_t tm, int32_t tk, int32_t *bRowPtr, int32_t *bColIdx, double *bVal, int32_t *mapping);
 
+/* DASP packing (spmv_all, src/dasp.cu:827-1482, rowloop = 1).  Arrays are
+ * malloc'd; release with orc_dasp_free. */
+typedef struct {
+  int32_t row_long, row_block, row_zero, short_row_1, short_row_2, short_row_3, short_row_4;
+  int32_t common_13, short_row_34, fill0_nnz_short13, fill0_nnz_short34, fill0_nnz_short;
+  int32_t fill0_nnz_long, blocknum, fill0_nnz_reg, nnz_irreg;
+  int32_t offset_reg, offset_short1, offset_short13, offset_short34, offset_short22, block_num_all;
+  double *short_val, *long_val, *reg_val, *irreg_val;
+  int32_t *short_cid, *long_cid, *long_ptr_warp, *reg_cid, *block_ptr, *irreg_cid, *irreg_rpt, *order_rid;
+} orc_dasp;
+void orc_dasp_pack(int32_t rows, const int32_t *rowPtr, const int32_t *colIdx, const double *val, double threshold,
+                   int32_t block_longest, orc_dasp *out);
+void orc_dasp_free(orc_dasp *o);
+
 #ifdef __cplusplus
 }
 #endif

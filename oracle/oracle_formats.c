@@ -175,3 +175,220 @@ int64_t orc_csr2bcsr(int32_t rows, int32_t cols, const int32_t *rowPtr, const in
   free(info);
   return nb;
 }
+
+/* ---- DASP packing (src/dasp.cu:827-1482) ------------------------------- */
+
+static int32_t *i32z(int64_t n) { return (int32_t *)calloc((size_t)(n > 0 ? n : 1), sizeof(int32_t)); }
+static double *f64z(int64_t n) { return (double *)calloc((size_t)(n > 0 ? n : 1), sizeof(double)); }
+
+/* Stable sort of row ids by length, descending (radix_sort with the
+ * descending count_sort, dasp.cu:214-246, :282-289). */
+static void sort_desc_stable(int32_t *len, int32_t *rid, int32_t n) {
+  int32_t mx = 0;
+  for (int32_t i = 0; i < n; i++)
+    if (len[i] > mx) mx = len[i];
+  int32_t *cnt = i32z((int64_t)mx + 2);
+  int32_t *l2 = i32z(n), *r2 = i32z(n);
+  for (int32_t i = 0; i < n; i++) cnt[mx - len[i]]++;
+  int32_t acc = 0;
+  for (int32_t k = 0; k <= mx; k++) {
+    const int32_t c = cnt[k];
+    cnt[k] = acc;
+    acc += c;
+  }
+  for (int32_t i = 0; i < n; i++) {
+    const int32_t p = cnt[mx - len[i]]++;
+    l2[p] = len[i];
+    r2[p] = rid[i];
+  }
+  memcpy(len, l2, sizeof(int32_t) * (size_t)n);
+  memcpy(rid, r2, sizeof(int32_t) * (size_t)n);
+  free(cnt);
+  free(l2);
+  free(r2);
+}
+
+void orc_dasp_pack(int32_t rows, const int32_t *rp, const int32_t *ci, const double *va, double threshold,
+                   int32_t block_longest, orc_dasp *o) {
+  memset(o, 0, sizeof(*o));
+  int32_t n1 = 0, n2 = 0, n3 = 0, n4 = 0, nl = 0, nb = 0, nz = 0;
+  for (int32_t i = 0; i < rows; i++) {  /* dasp.cu:827-859 */
+    const int32_t len = rp[i + 1] - rp[i];
+    if (len == 1) n1++;
+    else if (len == 3) n3++;
+    else if (len == 2) n2++;
+    else if (len == 0) nz++;
+    else if (len == 4) n4++;
+    else if (len >= block_longest) nl++;
+    else nb++;
+  }
+  int32_t *r1 = i32z(n1), *r2 = i32z(n2), *r3 = i32z(n3), *r4 = i32z(n4), *rl = i32z(nl), *rz = i32z(nz);
+  int32_t *rb = i32z(nb), *lb = i32z((int64_t)nb + 1), *ll = i32z((int64_t)nl + 1);
+  int32_t k1 = 0, k2 = 0, k3 = 0, k4 = 0, kl = 0, kb = 0, kz = 0;
+  for (int32_t i = 0; i < rows; i++) {  /* dasp.cu:876-918 */
+    const int32_t len = rp[i + 1] - rp[i];
+    if (len == 1) r1[k1++] = i;
+    else if (len == 3) r3[k3++] = i;
+    else if (len == 2) r2[k2++] = i;
+    else if (len == 0) rz[kz++] = i;
+    else if (len == 4) r4[k4++] = i;
+    else if (len >= block_longest) { ll[kl] = len; rl[kl++] = i; }
+    else { lb[kb] = len; rb[kb++] = i; }
+  }
+  int32_t c13 = n1 < n3 ? n1 : n3;  /* dasp.cu:922-933 */
+  if (c13 / 8 >= 16) c13 = 8 * (c13 / 8);
+  else c13 = 0;
+  const int32_t s1 = n1 - c13, s3 = n3 - c13, s34 = s3 + n4;
+  const int32_t sb13 = (c13 + 7) / 8, sb22 = ((n2 + 1) / 2 + 7) / 8, sb34 = (s34 + 7) / 8;
+  const int32_t tb13 = (sb13 + 7) / 8, tb22 = (sb22 + 7) / 8, tb34 = (sb34 + 15) / 16;
+  const int32_t f13 = tb13 * 8 * 32, f34 = tb34 * 16 * 32, f22 = tb22 * 8 * 32;
+  const int32_t fs = s1 + f13 + f34 + f22;
+  o->row_long = nl; o->row_block = nb; o->row_zero = nz; o->short_row_1 = s1; o->short_row_2 = n2;
+  o->short_row_3 = s3; o->short_row_4 = n4; o->common_13 = c13; o->short_row_34 = s34;
+  o->fill0_nnz_short13 = f13; o->fill0_nnz_short34 = f34; o->fill0_nnz_short = fs;
+  o->short_val = f64z(fs);
+  o->short_cid = i32z(fs);
+  for (int32_t i = 0; i < s1; i++) {  /* dasp.cu:961-966 */
+    o->short_val[i] = va[rp[r1[i]]];
+    o->short_cid[i] = ci[rp[r1[i]]];
+  }
+  for (int32_t i = 0; i < sb13; i++)  /* dasp.cu:968-988 */
+    for (int32_t j = 0; j < 8 && i * 8 + j < c13; j++) {
+      const int64_t b = s1 + (int64_t)i * 32 + j * 4;
+      const int32_t a = rp[r1[s1 + i * 8 + j]], c = rp[r3[i * 8 + j]];
+      o->short_val[b] = va[a];
+      o->short_cid[b] = ci[a];
+      for (int t = 0; t < 3; t++) {
+        o->short_val[b + 1 + t] = va[c + t];
+        o->short_cid[b + 1 + t] = ci[c + t];
+      }
+    }
+  for (int32_t i = 0; i < s3; i++) {  /* dasp.cu:990-1005 */
+    const int64_t b = s1 + f13 + (int64_t)i * 4;
+    const int32_t c = rp[r3[c13 + i]];
+    for (int t = 0; t < 3; t++) {
+      o->short_val[b + t] = va[c + t];
+      o->short_cid[b + t] = ci[c + t];
+    }
+  }
+  for (int32_t i = 0; i < n4; i++) {  /* dasp.cu:1007-1021 */
+    const int64_t b = s1 + f13 + ((int64_t)s3 + i) * 4;
+    const int32_t c = rp[r4[i]];
+    for (int t = 0; t < 4; t++) {
+      o->short_val[b + t] = va[c + t];
+      o->short_cid[b + t] = ci[c + t];
+    }
+  }
+  for (int32_t i = 0; i < sb22; i++)  /* dasp.cu:1023-1038 */
+    for (int32_t j = 0; j < 16 && i * 16 + j < n2; j++) {
+      const int64_t b = s1 + f13 + f34 + (int64_t)i * 32 + (j % 8) * 4 + (j / 8) * 2;
+      const int32_t c = rp[r2[i * 16 + j]];
+      o->short_val[b] = va[c];
+      o->short_val[b + 1] = va[c + 1];
+      o->short_cid[b] = ci[c];
+      o->short_cid[b + 1] = ci[c + 1];
+    }
+  sort_desc_stable(lb, rb, nb);  /* dasp.cu:1244 */
+  /* long rows (dasp.cu:1326-1369) */
+  o->long_ptr_warp = i32z((int64_t)nl + 1);
+  for (int32_t i = 0; i < nl; i++) o->long_ptr_warp[i + 1] = o->long_ptr_warp[i] + (ll[i] + 63) / 64;
+  const int32_t lw = o->long_ptr_warp[nl];
+  const int32_t bnl = (lw + 3) / 4;
+  o->fill0_nnz_long = bnl * 4 * 64;
+  o->long_val = f64z(o->fill0_nnz_long);
+  o->long_cid = i32z(o->fill0_nnz_long);
+  for (int32_t i = 0; i < nl; i++)
+    for (int32_t j = 0; j < ll[i]; j++) {
+      o->long_val[(int64_t)o->long_ptr_warp[i] * 64 + j] = va[rp[rl[i]] + j];
+      o->long_cid[(int64_t)o->long_ptr_warp[i] * 64 + j] = ci[rp[rl[i]] + j];
+    }
+  /* row-block part (dasp.cu:1374-1482), rowloop = 1 */
+  int32_t blocknum = (nb + 7) / 8;
+  blocknum = ((blocknum + 3) / 4) * 4;
+  o->blocknum = blocknum;
+  o->block_ptr = i32z((int64_t)blocknum + 1);
+  o->irreg_rpt = i32z((int64_t)nb + 1);
+  for (int32_t i = 0; i < blocknum; i++) {
+    const int32_t rs = i * 8, re = (i + 1) * 8 >= nb ? nb : (i + 1) * 8;
+    for (int32_t k = 1;; k++) {
+      int32_t block_nnz = 0;
+      for (int32_t r = rs; r < re; r++) {
+        if (lb[r] / 4 >= k) block_nnz += 4;
+        else if (lb[r] / 4 == k - 1) block_nnz += lb[r] % 4;
+      }
+      if (block_nnz >= threshold * 4 * 8) {
+        o->block_ptr[i] += 32;
+      } else {
+        for (int32_t r = rs; r < re; r++) o->irreg_rpt[r] = lb[r] - (k - 1) * 4 > 0 ? lb[r] - (k - 1) * 4 : 0;
+        break;
+      }
+    }
+  }
+  for (int32_t i = 0, acc = 0; i <= blocknum; i++) {
+    const int32_t c = o->block_ptr[i];
+    o->block_ptr[i] = acc;
+    acc += c;
+  }
+  for (int32_t i = 0, acc = 0; i <= nb; i++) {
+    const int32_t c = o->irreg_rpt[i];
+    o->irreg_rpt[i] = acc;
+    acc += c;
+  }
+  o->fill0_nnz_reg = o->block_ptr[blocknum];
+  o->nnz_irreg = o->irreg_rpt[nb];
+  o->irreg_val = f64z(o->nnz_irreg);
+  o->irreg_cid = i32z(o->nnz_irreg);
+  for (int32_t i = 0; i < nb; i++) {
+    const int32_t off = o->irreg_rpt[i], n = o->irreg_rpt[i + 1] - off, end = rp[rb[i] + 1];
+    for (int32_t j = 0; j < n; j++) {
+      o->irreg_val[off + j] = va[end - n + j];
+      o->irreg_cid[off + j] = ci[end - n + j];
+    }
+  }
+  o->reg_val = f64z(o->fill0_nnz_reg);
+  o->reg_cid = i32z(o->fill0_nnz_reg);
+  for (int32_t b = 0; b < blocknum; b++) {
+    const int32_t blocklen = (o->block_ptr[b + 1] - o->block_ptr[b]) / 8;
+    for (int32_t r = 0; r < 8; r++) {
+      const int32_t row = b * 8 + r;
+      for (int32_t i = 0; i < blocklen; i++) {
+        /* pre-layout index r*blocklen+i re-laid to tile-major (:1477-1482) */
+        const int64_t dst = o->block_ptr[b] + (i / 4) * 32 + r * 4 + i % 4;
+        if (row < nb && i < lb[row]) {
+          o->reg_val[dst] = va[rp[rb[row]] + i];
+          o->reg_cid[dst] = ci[rp[rb[row]] + i];
+        }
+      }
+    }
+  }
+  /* order_rid (dasp.cu:1289-1306) */
+  o->order_rid = i32z(rows);
+  int64_t p = 0;
+  for (int32_t i = 0; i < nl; i++) o->order_rid[p++] = rl[i];
+  for (int32_t i = 0; i < nb; i++) o->order_rid[p++] = rb[i];
+  for (int32_t i = 0; i < s1; i++) o->order_rid[p++] = r1[i];
+  for (int32_t i = 0; i < sb13; i++) {
+    for (int32_t j = 0; j < 8; j++) o->order_rid[p + j] = r1[s1 + i * 8 + j];
+    for (int32_t j = 0; j < 8; j++) o->order_rid[p + 8 + j] = r3[i * 8 + j];
+    p += 16;
+  }
+  for (int32_t i = 0; i < s3; i++) o->order_rid[p++] = r3[c13 + i];
+  for (int32_t i = 0; i < n4; i++) o->order_rid[p++] = r4[i];
+  for (int32_t i = 0; i < n2; i++) o->order_rid[p++] = r2[i];
+  for (int32_t i = 0; i < nz; i++) o->order_rid[p++] = rz[i];
+  /* the kernel's block ranges (dasp.cu:1513-1539) */
+  o->offset_reg = bnl;
+  o->offset_short1 = bnl + blocknum / 4;
+  o->offset_short13 = o->offset_short1 + (s1 + 127) / 128;
+  o->offset_short34 = o->offset_short13 + tb13;
+  o->offset_short22 = o->offset_short34 + tb34;
+  o->block_num_all = o->offset_short22 + tb22;
+  free(r1); free(r2); free(r3); free(r4); free(rl); free(rz); free(rb); free(lb); free(ll);
+}
+
+void orc_dasp_free(orc_dasp *o) {
+  free(o->short_val); free(o->short_cid); free(o->long_val); free(o->long_cid); free(o->long_ptr_warp);
+  free(o->reg_val); free(o->reg_cid); free(o->block_ptr); free(o->irreg_val); free(o->irreg_cid);
+  free(o->irreg_rpt); free(o->order_rid);
+  memset(o, 0, sizeof(*o));
+}

@@ -224,3 +224,48 @@ def run_capture(exe: str, rows, cols, rowptr, colidx, val, x, threshold=0.75, bl
         if r.returncode != 0:
             raise RuntimeError(f"{exe} failed ({r.returncode}): {r.stdout[-2000:]} {r.stderr[-2000:]}")
         return read_records(fout)
+
+
+# ---------------------------------------------------------------------------
+# DASP packing (src/dasp.cu:827-1482)
+
+_DASP_INTS = ["row_long", "row_block", "row_zero", "short_row_1", "short_row_2", "short_row_3", "short_row_4",
+              "common_13", "short_row_34", "fill0_nnz_short13", "fill0_nnz_short34", "fill0_nnz_short",
+              "fill0_nnz_long", "blocknum", "fill0_nnz_reg", "nnz_irreg", "offset_reg", "offset_short1",
+              "offset_short13", "offset_short34", "offset_short22", "block_num_all"]
+
+
+class _OrcDasp(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in _DASP_INTS] + [
+        ("short_val", C.POINTER(C.c_double)), ("long_val", C.POINTER(C.c_double)),
+        ("reg_val", C.POINTER(C.c_double)), ("irreg_val", C.POINTER(C.c_double)),
+        ("short_cid", C.POINTER(C.c_int32)), ("long_cid", C.POINTER(C.c_int32)),
+        ("long_ptr_warp", C.POINTER(C.c_int32)), ("reg_cid", C.POINTER(C.c_int32)),
+        ("block_ptr", C.POINTER(C.c_int32)), ("irreg_cid", C.POINTER(C.c_int32)),
+        ("irreg_rpt", C.POINTER(C.c_int32)), ("order_rid", C.POINTER(C.c_int32))]
+
+
+def dasp_pack(rowptr, colidx, val, threshold=0.75, block_longest=256) -> dict:
+    L = orc()
+    L.orc_dasp_pack.argtypes = [_I32, _P, _P, _P, C.c_double, _I32, C.POINTER(_OrcDasp)]
+    L.orc_dasp_free.argtypes = [C.POINTER(_OrcDasp)]
+    o = _OrcDasp()
+    rows = rowptr.size - 1
+    L.orc_dasp_pack(rows, _p(rowptr), _p(colidx), _p(val), float(threshold), int(block_longest), C.byref(o))
+
+    def arr(ptr, n, dt):
+        return np.ctypeslib.as_array(ptr, shape=(n,)).astype(dt).copy() if n > 0 else np.zeros(0, dt)
+
+    out = {n: int(getattr(o, n)) for n in _DASP_INTS}
+    lw = o.long_ptr_warp[o.row_long]
+    out.update(
+        short_val=arr(o.short_val, o.fill0_nnz_short, np.float64), short_cid=arr(o.short_cid, o.fill0_nnz_short, np.int32),
+        long_val=arr(o.long_val, o.fill0_nnz_long, np.float64), long_cid=arr(o.long_cid, o.fill0_nnz_long, np.int32),
+        long_ptr_warp=arr(o.long_ptr_warp, o.row_long + 1, np.int32),
+        reg_val=arr(o.reg_val, o.fill0_nnz_reg, np.float64), reg_cid=arr(o.reg_cid, o.fill0_nnz_reg, np.int32),
+        block_ptr=arr(o.block_ptr, o.blocknum + 1, np.int32),
+        irreg_val=arr(o.irreg_val, o.nnz_irreg, np.float64), irreg_cid=arr(o.irreg_cid, o.nnz_irreg, np.int32),
+        irreg_rpt=arr(o.irreg_rpt, o.row_block + 1, np.int32), order_rid=arr(o.order_rid, rows, np.int32),
+        long_warps=int(lw))
+    L.orc_dasp_free(C.byref(o))
+    return out

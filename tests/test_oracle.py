@@ -128,3 +128,43 @@ def test_bcsr_oracle_against_reference(golden, name):
     assert o["rowRegions"] == int(g["rowRegions"]) and o["colRegions"] == int(g["colRegions"])
     for k in ("bcsrRowPtr", "bcsrColIdx", "bcsrVal", "mapping"):
         assert np.array_equal(o[k], g[k]), k
+
+
+DASP = sorted(Path(p).name for p in glob.glob(str(GOLDEN / "dasp_*.npz")))
+DASP_ARRS = ("long_val", "long_cid", "long_ptr_warp", "reg_val", "reg_cid", "block_ptr", "irreg_val", "irreg_cid",
+             "irreg_rpt", "short_val", "short_cid", "order_rid")
+DASP_INTS = ("row_long", "row_block", "blocknum", "short_row_1", "common_13", "short_row_34", "short_row_2",
+             "offset_reg", "offset_short1", "offset_short13", "offset_short34", "offset_short22",
+             "fill0_nnz_short13", "fill0_nnz_short34")
+
+
+@pytest.mark.parametrize("name", DASP)
+def test_dasp_oracle_against_reference_capture(golden, name):
+    g = golden(name)
+    o = pyoracle.dasp_pack(g["rowptr"], g["colidx"], g["values"], float(g["threshold"]), int(g["block_longest"]))
+    for k in DASP_ARRS:
+        ref = g.get("arr_" + k, np.zeros(0))
+        assert np.array_equal(o[k], ref), k
+    for k in DASP_INTS:
+        assert o[k] == int(g["int_" + k]), k
+    assert o["block_num_all"] == int(g["int_grid_all"])
+
+
+@pytest.mark.parametrize("n,alpha,cap,th,bl", [(60000, 2.0, 10000, 0.75, 256), (20000, 1.6, 3000, 0.5, 64)])
+def test_dasp_oracle_against_live_reference(n, alpha, cap, th, bl):
+    """Runs the reference's spmv_all packing (oracle/_ref/dasp_capture) on a
+    larger seeded power-law matrix when it has been built."""
+    if not (pyoracle.REF_DIR / "dasp_capture").exists():
+        pytest.skip("oracle/_ref/dasp_capture not built")
+    rng = np.random.default_rng(n)
+    lens = np.minimum(rng.zipf(alpha, n), cap)
+    rp = np.zeros(n + 1, np.int32)
+    rp[1:] = np.cumsum(lens)
+    ci = np.concatenate([np.sort(rng.choice(n, int(L), replace=False)) for L in lens]).astype(np.int32)
+    va = rng.standard_normal(ci.size)
+    rec = pyoracle.run_capture("dasp_capture", n, n, rp, ci, va, np.zeros(n), th, bl)
+    o = pyoracle.dasp_pack(rp, ci, va, th, bl)
+    ints = {"long_ptr_warp", "reg_cid", "block_ptr", "irreg_cid", "irreg_rpt", "short_cid", "long_cid", "order_rid"}
+    for k in DASP_ARRS:
+        dt = np.int32 if k in ints else np.float64
+        assert np.array_equal(o[k], np.frombuffer(rec.get("arr:" + k, b""), dt)), k
