@@ -113,6 +113,7 @@ _PROTOS = {
     "bsp_csr_spmv": (C.c_int, [_I32, _I32, _I32, _P, _P, _P, C.c_int, _P, _P, _D, _D, _I32, _I32, _P]),
     "bsp_csr_merge_workspace": (C.c_size_t, [_I32, _I32]),
     "bsp_csr_spmv_merge_f64": (C.c_int, [_I32, _I32, _I32, _P, _P, _P, _P, _P, _D, _D, _P, C.c_size_t, _P]),
+    "bsp_csr_spmv_merge_f64_noalloc": (C.c_int, [_I32, _I32, _I32, _P, _P, _P, _P, _P, _D, _D, _P]),
     "bsp_csr2bsr": (C.c_int, [_I32, _I32, _I32, _P, _P, _P, _I32, C.POINTER(BspBsr), _P]),
     "bsp_bsr_free": (C.c_int, [C.POINTER(BspBsr)]),
     "bsp_bsr_spmv": (C.c_int, [C.POINTER(BspBsr), _P, _P, _D, _D, _I32, _P]),

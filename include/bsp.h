@@ -101,6 +101,24 @@ bsp_status bsp_csr_spmv_merge_f64(int32_t rows, int32_t cols, int32_t nnz,
                                   void *workspace, size_t workspace_bytes,
                                   bsp_stream_t stream);
 
+/* Allocation-free form of bsp_csr_spmv_merge_f64, for callers that may not
+ * allocate device memory once they are running (a host that gives all GPU
+ * memory to its own pool at start-up, or a latency-critical loop that must
+ * not call cudaMalloc/cudaFree, which can synchronize the device).  It has no
+ * counterpart in the reference.  The merge-path workspace is a fixed 3 MiB
+ * array inside the library, present on every GPU that loads it until the
+ * process exits, so rows + nnz must be at most 67,108,864; larger inputs are
+ * rejected with BSP_ERR_INVALID.  The array's device address is looked up on
+ * the first call on each device (make that first call before any stream
+ * capture).  All calls share the one array: calls that overlap on the GPU
+ * (concurrent streams, threads) race and must be serialized by the caller.
+ * Results match bsp_csr_spmv_merge_f64. */
+bsp_status bsp_csr_spmv_merge_f64_noalloc(int32_t rows, int32_t cols, int32_t nnz,
+                                          const int32_t *rowPtr, const int32_t *colIdx,
+                                          const double *values, const double *x,
+                                          double *y, double alpha, double beta,
+                                          bsp_stream_t stream);
+
 /* ---------------------------------------------------------------------- */
 /* AmgT-style BSR (bsrMAT, reference include/matrixFormat.hpp:59-83).
  * bs = 4 reproduces the reference format exactly; bs = 8 is the same layout
