@@ -128,6 +128,7 @@ _PROTOS = {
     "bsp_csr2dasp": (C.c_int, [_I32, _I32, _I32, _P, _P, _P, _D, _I32, C.POINTER(BspDasp), _P]),
     "bsp_dasp_free": (C.c_int, [C.POINTER(BspDasp)]),
     "bsp_dasp_spmv": (C.c_int, [C.POINTER(BspDasp), _P, _P, _D, _D, _I32, _P]),
+    "bsp_blockinfo": (C.c_int, [_I32, _I32, _I32, _P, _P, _PI64, _PI64, _P]),
     "bsp_gen_laplace2d": (C.c_int, [_I32, _I32, _PI32, _PI32, _P, _P, _P]),
     "bsp_gen_poisson3d": (C.c_int, [_I32, _PI32, _PI64, _P, _P, _P]),
     "bsp_gen_stencil27": (C.c_int, [_I32, _I32, _U64, _PI32, _PI64, _P, _P, _P]),

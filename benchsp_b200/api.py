@@ -365,6 +365,21 @@ def csr2dasp(rowptr, colidx, values, *, rows: int, cols: int, threshold: float =
 
 
 # ---------------------------------------------------------------------------
+# Block statistics (reference bench/blockinfo.cpp:96-119)
+
+def blockinfo(rowptr, colidx, *, rows: int, cols: int, stream=None) -> dict:
+    """Distinct 4x4 blocks without / with the row-packed (recorder) layout."""
+    b = C.c_int64()
+    br = C.c_int64()
+    nnz = colidx.numel()
+    check(lib().bsp_blockinfo(rows, cols, nnz, _dptr(rowptr, "rowptr"), _dptr(colidx, "colidx"), C.byref(b),
+                              C.byref(br), _stream(stream)))
+    return {"blocks": b.value, "blocks_recorder": br.value,
+            "avg_nnz": nnz / b.value if b.value else 0.0,
+            "avg_nnz_recorder": nnz / br.value if br.value else 0.0}
+
+
+# ---------------------------------------------------------------------------
 # Seeded synthetic inputs (host numpy arrays)
 
 @dataclass

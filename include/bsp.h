@@ -314,6 +314,17 @@ bsp_status bsp_dasp_spmv(const bsp_dasp *d, const double *x, double *y,
                          bsp_stream_t stream);
 
 /* ---------------------------------------------------------------------- */
+/* 4x4 block statistics of bench/blockinfo.cpp:96-119 (reference): the number
+ * of distinct 4x4 blocks of the matrix (keys row/4*1000005 + col/4) and of
+ * its DBSR-style packing (keys row/4*1000005 + z/4, z = position in the row),
+ * counted on wrapped 32-bit keys exactly as the reference's int arithmetic
+ * does.  Average nonzeros per block = nnz / count. */
+bsp_status bsp_blockinfo(int32_t rows, int32_t cols, int32_t nnz,
+                         const int32_t *rowPtr, const int32_t *colIdx,
+                         int64_t *blocks, int64_t *blocks_recorder,
+                         bsp_stream_t stream);
+
+/* ---------------------------------------------------------------------- */
 /* Synthetic matrix generators (host, seeded, deterministic).  Two-phase:
  * call with NULL arrays to get the sizes, then with allocated arrays. */
 

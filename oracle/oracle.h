@@ -92,6 +92,10 @@ void orc_dasp_pack(int32_t rows, const int32_t *rowPtr, const int32_t *colIdx, c
                    int32_t block_longest, orc_dasp *out);
 void orc_dasp_free(orc_dasp *o);
 
+/* Block statistics of bench/blockinfo.cpp:96-119 (wrapping 32-bit keys). */
+void orc_blockinfo(int32_t rows, const int32_t *rowPtr, const int32_t *colIdx, int64_t *blocks,
+                   int64_t *blocks_recorder);
+
 #ifdef __cplusplus
 }
 #endif

@@ -392,3 +392,36 @@ void orc_dasp_free(orc_dasp *o) {
   free(o->irreg_rpt); free(o->order_rid);
   memset(o, 0, sizeof(*o));
 }
+
+/* ---- Block statistics (bench/blockinfo.cpp:96-119) --------------------- */
+
+static int cmp_u32(const void *a, const void *b) {
+  const uint32_t x = *(const uint32_t *)a, y = *(const uint32_t *)b;
+  return (x > y) - (x < y);
+}
+
+static int64_t distinct_u32(uint32_t *k, int64_t n) {
+  qsort(k, (size_t)n, sizeof(uint32_t), cmp_u32);
+  int64_t c = 0;
+  for (int64_t i = 0; i < n; i++) c += (i == 0 || k[i] != k[i - 1]);
+  return c;
+}
+
+void orc_blockinfo(int32_t rows, const int32_t *rowPtr, const int32_t *colIdx, int64_t *blocks,
+                   int64_t *blocks_recorder) {
+  /* keys row/4*1000005 + col/4 and row/4*1000005 + z/4 in wrapping 32-bit
+   * arithmetic, as the reference's int expressions evaluate */
+  const int64_t nnz = rowPtr[rows];
+  uint32_t *kp = (uint32_t *)malloc(sizeof(uint32_t) * (size_t)(nnz > 0 ? nnz : 1));
+  uint32_t *kr = (uint32_t *)malloc(sizeof(uint32_t) * (size_t)(nnz > 0 ? nnz : 1));
+  for (int32_t r = 0; r < rows; r++)
+    for (int32_t j = rowPtr[r]; j < rowPtr[r + 1]; j++) {
+      const uint32_t base = (uint32_t)(r / 4) * 1000005u;
+      kp[j] = base + (uint32_t)(colIdx[j] / 4);
+      kr[j] = base + (uint32_t)((j - rowPtr[r]) / 4);
+    }
+  *blocks = distinct_u32(kp, nnz);
+  *blocks_recorder = distinct_u32(kr, nnz);
+  free(kp);
+  free(kr);
+}

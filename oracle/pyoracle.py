@@ -269,3 +269,34 @@ def dasp_pack(rowptr, colidx, val, threshold=0.75, block_longest=256) -> dict:
         long_warps=int(lw))
     L.orc_dasp_free(C.byref(o))
     return out
+
+
+# ---------------------------------------------------------------------------
+# Block statistics (bench/blockinfo.cpp:96-119)
+
+def blockinfo(rowptr, colidx) -> dict:
+    L = orc()
+    L.orc_blockinfo.argtypes = [_I32, _P, _P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+    b, br = C.c_int64(), C.c_int64()
+    L.orc_blockinfo(rowptr.size - 1, _p(rowptr), _p(colidx), C.byref(b), C.byref(br))
+    return {"blocks": b.value, "blocks_recorder": br.value}
+
+
+def write_mtx(path, rows, cols, rowptr, colidx, values) -> None:
+    """Matrix Market coordinate file (1-based, general, real)."""
+    r = np.repeat(np.arange(rows, dtype=np.int64), np.diff(rowptr)) + 1
+    with open(path, "w") as f:
+        f.write("%%MatrixMarket matrix coordinate real general\n")
+        f.write(f"{rows} {cols} {colidx.size}\n")
+        np.savetxt(f, np.column_stack([r, colidx.astype(np.int64) + 1, values]), fmt="%d %d %.17g")
+
+
+def run_ref_blockinfo(rows, cols, rowptr, colidx, values) -> dict:
+    """The reference's bench/blockinfo.cpp (oracle/_ref/blockinfo) on a matrix."""
+    import re
+    with tempfile.TemporaryDirectory() as td:
+        p = Path(td) / "m.mtx"
+        write_mtx(p, rows, cols, rowptr, colidx, values)
+        out = subprocess.run([str(REF_DIR / "blockinfo"), str(p)], capture_output=True, text=True, check=True).stdout
+    nums = re.findall(r"block num:(\d+)", out)
+    return {"blocks": int(nums[0]), "blocks_recorder": int(nums[1])}

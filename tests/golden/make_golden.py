@@ -270,6 +270,22 @@ def run_amgt(name, m) -> None:
                         rowIdxbyWarp=np.frombuffer(rec["arr:rowIdxbyWarp"], np.int32))
 
 
+def run_blockinfo() -> None:
+    """bench/blockinfo.cpp (oracle/_ref/blockinfo) on matrices regenerated
+    from the library's seeded generators (names match tests/test_oracle.py)."""
+    import benchsp_b200 as bsp
+    mats = {"powerlaw": bsp.gen_powerlaw(30000, 2.0, 10000, 17), "laplace": bsp.gen_laplace2d(64, 80),
+            "random": bsp.gen_random_bsr(1000, 4, 8, 0.3, 1.0, 5)}
+    names, b, br = [], [], []
+    for name, A in mats.items():
+        r = pyoracle.run_ref_blockinfo(A.rows, A.cols, A.rowptr, A.colidx, A.values)
+        names.append(name)
+        b.append(r["blocks"])
+        br.append(r["blocks_recorder"])
+    np.savez_compressed(OUT / "blockinfo_ref.npz", names=np.array(names), blocks=np.array(b),
+                        blocks_recorder=np.array(br))
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--amgt", action="store_true", help="only the AmgT fixtures (needs a GPU)")
@@ -290,6 +306,7 @@ def main() -> None:
         run_bcsr(name, mats[name], 4, 4)
     run_bcsr("randbsr64", mats["randbsr64"], 16, 16)
     run_bcsr("lap16", mats["lap16"], 3, 3)
+    run_blockinfo()
 
 
 if __name__ == "__main__":

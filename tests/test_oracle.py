@@ -168,3 +168,41 @@ def test_dasp_oracle_against_live_reference(n, alpha, cap, th, bl):
     for k in DASP_ARRS:
         dt = np.int32 if k in ints else np.float64
         assert np.array_equal(o[k], np.frombuffer(rec.get("arr:" + k, b""), dt)), k
+
+
+def _bi_matrices():
+    import benchsp_b200 as bsp
+    yield "powerlaw", bsp.gen_powerlaw(30000, 2.0, 10000, 17)
+    yield "laplace", bsp.gen_laplace2d(64, 80)
+    yield "random", bsp.gen_random_bsr(1000, 4, 8, 0.3, 1.0, 5)
+
+
+@pytest.mark.parametrize("name", ["powerlaw", "laplace", "random"])
+def test_blockinfo_oracle_against_live_reference(name):
+    """bench/blockinfo.cpp compiled from the reference (oracle/_ref/blockinfo)."""
+    if not (pyoracle.REF_DIR / "blockinfo").exists():
+        pytest.skip("oracle/_ref/blockinfo not built")
+    A = dict(_bi_matrices())[name]
+    ref = pyoracle.run_ref_blockinfo(A.rows, A.cols, A.rowptr, A.colidx, A.values)
+    assert pyoracle.blockinfo(A.rowptr, A.colidx) == ref
+
+
+def test_blockinfo_oracle_against_fixture(golden):
+    import benchsp_b200 as bsp
+    g = golden("blockinfo_ref.npz")
+    for i, name in enumerate(g["names"]):
+        A = dict(_bi_matrices())[str(name)]
+        o = pyoracle.blockinfo(A.rowptr, A.colidx)
+        assert o["blocks"] == int(g["blocks"][i]) and o["blocks_recorder"] == int(g["blocks_recorder"][i])
+
+
+def test_blockinfo_wrapped_keys_collide_like_the_reference():
+    """row/4*1000005 wraps in 32 bits: rows 4*4295 apart with block columns
+    54179 apart share a key, so the reference counts one block for two."""
+    rows = 4 * 4295 + 1
+    rp = np.zeros(rows + 1, np.int32)
+    rp[1:] = 1  # row 0 has one entry, rows 1.. none except the last
+    rp[-1] = 2
+    ci = np.array([4 * 54179, 0], np.int32)
+    o = pyoracle.blockinfo(rp, ci)
+    assert o["blocks"] == 1
