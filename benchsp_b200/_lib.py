@@ -162,3 +162,26 @@ def declared_symbols() -> list[str]:
 def check(status: int) -> None:
     if status != BSP_OK:
         raise BspError(status, lib().bsp_last_error().decode(errors="replace"))
+
+
+class BspCgOptions(C.Structure):
+    """Mirror of bsp_cg_options (include/bsp.h)."""
+    _fields_ = [("mode", C.c_int32), ("tol", C.c_double), ("max_iters", C.c_int32), ("check_every", C.c_int32),
+                ("inner_tol", C.c_double), ("max_outer", C.c_int32), ("use_graphs", C.c_int32)]
+
+
+class BspCgResult(C.Structure):
+    """Mirror of bsp_cg_result (include/bsp.h)."""
+    _fields_ = [("iterations", C.c_int32), ("outer_iterations", C.c_int32), ("rel_residual", C.c_double),
+                ("seconds", C.c_double), ("converged", C.c_int32), ("bytes_moved", C.c_int64),
+                ("delta16", C.c_int32)]
+
+
+CG_FP64, CG_MIXED_F32, CG_MIXED_F16, CG_MIXED_BF16 = 0, 1, 2, 3
+
+_PROTOS.update({
+    "bsp_cg_default_options": (C.c_int, [C.POINTER(BspCgOptions)]),
+    "bsp_cg_create": (C.c_int, [_I32, _I32, _P, _P, _P, C.POINTER(BspCgOptions), C.POINTER(C.c_void_p), _P]),
+    "bsp_cg_solve": (C.c_int, [C.c_void_p, _P, _P, C.POINTER(BspCgResult), _P]),
+    "bsp_cg_destroy": (C.c_int, [C.c_void_p]),
+})

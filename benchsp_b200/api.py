@@ -445,3 +445,47 @@ def gen_uniform(n: int, seed: int) -> np.ndarray:
     x = np.empty(n, np.float64)
     check(lib().bsp_gen_uniform(n, seed, x.ctypes.data_as(C.c_void_p)))
     return x
+
+
+# ---------------------------------------------------------------------------
+# Conjugate gradients: FP64, or mixed precision with FP64 refinement
+
+_CG_MODES = {"fp64": _lib.CG_FP64, "f32": _lib.CG_MIXED_F32, "f16": _lib.CG_MIXED_F16, "bf16": _lib.CG_MIXED_BF16}
+
+
+class CgSolver:
+    """Solver plan for an SPD CSR matrix on the device (arrays must stay alive)."""
+
+    def __init__(self, rowptr, colidx, values, *, mode: str = "f16", tol: float = 1e-10, max_iters: int = 20000,
+                 check_every: int = 16, inner_tol: float = 1e-4, max_outer: int = 30, use_graphs: bool = True,
+                 stream=None):
+        o = _lib.BspCgOptions()
+        check(lib().bsp_cg_default_options(C.byref(o)))
+        o.mode, o.tol, o.max_iters, o.check_every = _CG_MODES[mode], tol, max_iters, check_every
+        o.inner_tol, o.max_outer, o.use_graphs = inner_tol, max_outer, int(use_graphs)
+        self._keep = (rowptr, colidx, values)
+        self.n = rowptr.numel() - 1
+        self._plan = C.c_void_p()
+        check(lib().bsp_cg_create(self.n, colidx.numel(), _dptr(rowptr, "rowptr"), _dptr(colidx, "colidx"),
+                                  _dptr(values, "values"), C.byref(o), C.byref(self._plan), _stream(stream)))
+
+    def solve(self, b, x=None, *, stream=None, raise_on_stall: bool = True) -> tuple:
+        torch = _torch()
+        if x is None:
+            x = torch.zeros(self.n, dtype=torch.float64, device=b.device)
+        r = _lib.BspCgResult()
+        st = lib().bsp_cg_solve(self._plan, _dptr(b, "b"), _dptr(x, "x"), C.byref(r), _stream(stream))
+        if st != _lib.BSP_ERR_NOT_CONVERGED or raise_on_stall:
+            check(st)
+        return x, {k: getattr(r, k) for k, _ in _lib.BspCgResult._fields_}
+
+    def close(self) -> None:
+        if self._plan:
+            check(lib().bsp_cg_destroy(self._plan))
+            self._plan = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -314,6 +314,56 @@ bsp_status bsp_dasp_spmv(const bsp_dasp *d, const double *x, double *y,
                          bsp_stream_t stream);
 
 /* ---------------------------------------------------------------------- */
+/* Conjugate gradients (absent in the reference): plain FP64 CG, or
+ * mixed-precision CG with FP64 iterative refinement -- the inner solve keeps
+ * the matrix in FP32, or FP16/BF16 with one power-of-two exponent per 32
+ * nonzeros, with int16 column offsets when every |col - row| < 32768, and
+ * FP32 vectors; the outer loop keeps r = b - A x, ||r|| and x in FP64.
+ * Convergence: ||b - A x|| / ||b|| <= tol, computed in FP64. */
+typedef enum {
+  BSP_CG_FP64 = 0,
+  BSP_CG_MIXED_F32 = 1,
+  BSP_CG_MIXED_F16 = 2,
+  BSP_CG_MIXED_BF16 = 3
+} bsp_cg_mode;
+
+typedef struct {
+  int32_t mode;        /* bsp_cg_mode */
+  double tol;          /* relative residual target (1e-10) */
+  int32_t max_iters;   /* CG iterations over all refinement steps */
+  int32_t check_every; /* iterations per CUDA graph between host checks (rounded up to even) */
+  double inner_tol;    /* relative tolerance of each inner solve (mixed modes) */
+  int32_t max_outer;   /* refinement steps */
+  int32_t use_graphs;  /* 1: replay captured iteration chunks */
+} bsp_cg_options;
+
+typedef struct {
+  int32_t iterations;       /* CG iterations (inner ones in the mixed modes) */
+  int32_t outer_iterations; /* refinement steps */
+  double rel_residual;      /* final ||b - A x|| / ||b|| in FP64 */
+  double seconds;           /* device time of the solve (CUDA events) */
+  int32_t converged;
+  int64_t bytes_moved;      /* algorithmic bytes of all SpMVs and vector updates */
+  int32_t delta16;          /* int16 column offsets were used */
+} bsp_cg_result;
+
+typedef struct bsp_cg_plan_s *bsp_cg_plan;
+
+bsp_status bsp_cg_default_options(bsp_cg_options *opt);
+/* Prepares a solver for the SPD CSR matrix (device arrays, kept by
+ * reference: they must outlive the plan): the low-precision copy, vectors,
+ * and (on first solve) the captured iteration graphs. */
+bsp_status bsp_cg_create(int32_t n, int32_t nnz, const int32_t *rowPtr,
+                         const int32_t *colIdx, const double *values,
+                         const bsp_cg_options *opt, bsp_cg_plan *plan,
+                         bsp_stream_t stream);
+/* Solves A x = b; x holds the initial guess on entry.  Returns
+ * BSP_ERR_NOT_CONVERGED (with res filled) when tol is not reached. */
+bsp_status bsp_cg_solve(bsp_cg_plan plan, const double *b, double *x,
+                        bsp_cg_result *res, bsp_stream_t stream);
+bsp_status bsp_cg_destroy(bsp_cg_plan plan);
+
+/* ---------------------------------------------------------------------- */
 /* 4x4 block statistics of bench/blockinfo.cpp:96-119 (reference): the number
  * of distinct 4x4 blocks of the matrix (keys row/4*1000005 + col/4) and of
  * its DBSR-style packing (keys row/4*1000005 + z/4, z = position in the row),

@@ -217,3 +217,41 @@ double orc_bsr_stand(int32_t blc_row, const int32_t *blcPtr) {
   }
   return (double)sqrtf((float)(s / blc_row));
 }
+
+/* FP64 CG on the CPU with orc_spmv_f64_i32 as the operator (the reference has
+ * no solver; this is the FP64 oracle the GPU solves are compared against).
+ * Returns iterations; x holds the solution. */
+int32_t orc_cg(int32_t n, const int32_t *rowPtr, const int32_t *colIdx, const double *val, const double *b,
+               double *x, double tol, int32_t max_iters) {
+  double *r = (double *)malloc(sizeof(double) * n), *p = (double *)malloc(sizeof(double) * n);
+  double *q = (double *)malloc(sizeof(double) * n);
+  orc_spmv_f64_i32(n, rowPtr, colIdx, val, x, q);
+  double rr = 0, bb = 0;
+  for (int32_t i = 0; i < n; i++) {
+    r[i] = b[i] - q[i];
+    p[i] = r[i];
+    rr += r[i] * r[i];
+    bb += b[i] * b[i];
+  }
+  int32_t it = 0;
+  while (it < max_iters && rr > tol * tol * bb) {
+    orc_spmv_f64_i32(n, rowPtr, colIdx, val, p, q);
+    double pq = 0;
+    for (int32_t i = 0; i < n; i++) pq += p[i] * q[i];
+    const double a = rr / pq;
+    double rn = 0;
+    for (int32_t i = 0; i < n; i++) {
+      x[i] += a * p[i];
+      r[i] -= a * q[i];
+      rn += r[i] * r[i];
+    }
+    const double bt = rn / rr;
+    for (int32_t i = 0; i < n; i++) p[i] = r[i] + bt * p[i];
+    rr = rn;
+    it++;
+  }
+  free(r);
+  free(p);
+  free(q);
+  return it;
+}

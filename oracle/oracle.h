@@ -42,6 +42,11 @@ float orc_bf16_to_f32(uint16_t h);
 void orc_abs_rowsum(int32_t rows, const int32_t *rowPtr, const int32_t *colIdx, const double *val,
                     const double *x, double *out);
 
+/* FP64 CG with orc_spmv_f64_i32 (the CPU oracle of the GPU solves).  x holds
+ * the initial guess on entry and the solution on exit; returns iterations. */
+int32_t orc_cg(int32_t n, const int32_t *rowPtr, const int32_t *colIdx, const double *val, const double *b,
+               double *x, double tol, int32_t max_iters);
+
 /* AmgT CSR -> BSR (CSR2BSR_GPU, src/amgT.cu:1114-1172): block columns
  * ascending inside a block-row (rank by counting smaller keys, :823-835),
  * row-major bs x bs values (:840-847), bitmap bit r*bs+c (:776,:836).

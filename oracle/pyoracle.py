@@ -300,3 +300,20 @@ def run_ref_blockinfo(rows, cols, rowptr, colidx, values) -> dict:
         out = subprocess.run([str(REF_DIR / "blockinfo"), str(p)], capture_output=True, text=True, check=True).stdout
     nums = re.findall(r"block num:(\d+)", out)
     return {"blocks": int(nums[0]), "blocks_recorder": int(nums[1])}
+
+
+def cg(rowptr, colidx, val, b, tol=1e-10, max_iters=100000) -> tuple:
+    """FP64 CG on the CPU (x0 = 0); returns (x, iterations)."""
+    L = orc()
+    L.orc_cg.restype = _I32
+    L.orc_cg.argtypes = [_I32, _P, _P, _P, _P, _P, C.c_double, _I32]
+    n = rowptr.size - 1
+    x = np.zeros(n)
+    it = L.orc_cg(n, _p(rowptr), _p(colidx), _p(val), _p(np.ascontiguousarray(b, np.float64)), _p(x), tol, max_iters)
+    return x, int(it)
+
+
+def rel_residual(rowptr, colidx, val, b, x) -> float:
+    """||b - A x|| / ||b|| with the oracle SpMV."""
+    r = b - spmv_f64(rowptr, colidx, val, np.ascontiguousarray(x, np.float64))
+    return float(np.linalg.norm(r) / np.linalg.norm(b))

@@ -206,3 +206,12 @@ def test_blockinfo_wrapped_keys_collide_like_the_reference():
     ci = np.array([4 * 54179, 0], np.int32)
     o = pyoracle.blockinfo(rp, ci)
     assert o["blocks"] == 1
+
+
+def test_cpu_cg_oracle_converges():
+    import benchsp_b200 as bsp
+    A = bsp.gen_poisson3d(10)
+    b = bsp.gen_uniform(A.rows, 3)
+    x, it = pyoracle.cg(A.rowptr, A.colidx, A.values, b, 1e-10)
+    assert 0 < it < 500
+    assert pyoracle.rel_residual(A.rowptr, A.colidx, A.values, b, x) <= 1e-10
