@@ -167,12 +167,12 @@ def check(status: int) -> None:
 class BspCgOptions(C.Structure):
     """Mirror of bsp_cg_options (include/bsp.h)."""
     _fields_ = [("mode", C.c_int32), ("tol", C.c_double), ("max_iters", C.c_int32), ("check_every", C.c_int32),
-                ("inner_tol", C.c_double), ("max_outer", C.c_int32), ("use_graphs", C.c_int32)]
+                ("reliable_delta", C.c_double), ("use_graphs", C.c_int32)]
 
 
 class BspCgResult(C.Structure):
     """Mirror of bsp_cg_result (include/bsp.h)."""
-    _fields_ = [("iterations", C.c_int32), ("outer_iterations", C.c_int32), ("rel_residual", C.c_double),
+    _fields_ = [("iterations", C.c_int32), ("reliable_updates", C.c_int32), ("rel_residual", C.c_double),
                 ("seconds", C.c_double), ("converged", C.c_int32), ("bytes_moved", C.c_int64),
                 ("delta16", C.c_int32)]
 
@@ -184,4 +184,59 @@ _PROTOS.update({
     "bsp_cg_create": (C.c_int, [_I32, _I32, _P, _P, _P, C.POINTER(BspCgOptions), C.POINTER(C.c_void_p), _P]),
     "bsp_cg_solve": (C.c_int, [C.c_void_p, _P, _P, C.POINTER(BspCgResult), _P]),
     "bsp_cg_destroy": (C.c_int, [C.c_void_p]),
+})
+
+
+class BspSmat(C.Structure):
+    """Mirror of bsp_smat (include/bsp.h)."""
+    _fields_ = [("rows", C.c_int32), ("cols", C.c_int32), ("nnz", C.c_int32), ("dtype", C.c_int32),
+                ("tiles", BspBcsr), ("tile_val", C.c_void_p), ("err", C.c_void_p), ("fill", C.c_double)]
+
+
+class BspBatchMat(C.Structure):
+    """Mirror of bsp_batch_mat (include/bsp.h)."""
+    _fields_ = [("rows", C.c_int32), ("cols", C.c_int32), ("nnz", C.c_int32), ("rowPtr", C.c_void_p),
+                ("colIdx", C.c_void_p), ("values", C.c_void_p), ("x", C.c_void_p), ("y", C.c_void_p)]
+
+
+class BspBatchOptions(C.Structure):
+    """Mirror of bsp_batch_options (include/bsp.h)."""
+    _fields_ = [("tune", C.c_int32), ("seg_nnz", C.c_int32), ("long_row_nnz", C.c_int32), ("item_nnz", C.c_int32),
+                ("use_graph", C.c_int32)]
+
+
+_PROTOS.update({
+    "bsp_batch_default_options": (C.c_int, [C.POINTER(BspBatchOptions)]),
+    "bsp_batch_create": (C.c_int, [_I32, C.POINTER(BspBatchMat), C.c_int, _I32, C.POINTER(BspBatchOptions),
+                                   C.POINTER(C.c_void_p), _P]),
+    "bsp_batch_run": (C.c_int, [C.c_void_p, _P]),
+    "bsp_batch_run_separate": (C.c_int, [C.c_void_p, _P]),
+    "bsp_batch_set_vectors": (C.c_int, [C.c_void_p, _I32, _P, _P, _P]),
+    "bsp_batch_lanes": (C.c_int, [C.c_void_p, _P]),
+    "bsp_batch_stats": (C.c_int, [C.c_void_p, _PI64, _PI64, _PI64]),
+    "bsp_batch_destroy": (C.c_int, [C.c_void_p]),
+    "bsp_gen_banded": (C.c_int, [_I32, _I32, _U64, _PI32, _PI64, _P, _P, _P]),
+})
+
+
+class BspSpmmPlan(C.Structure):
+    """Mirror of bsp_spmm_plan (include/bsp.h)."""
+    _fields_ = [("rows", C.c_int32), ("chunk", C.c_int32), ("nchunks", C.c_int64), ("nparts", C.c_int64),
+                ("nsplit", C.c_int32), ("chunk_ptr", C.c_void_p), ("part_ptr", C.c_void_p),
+                ("chunk_row", C.c_void_p), ("split_rows", C.c_void_p)]
+
+
+_PROTOS.update({
+    "bsp_spmm_plan_create": (C.c_int, [_I32, _I32, _P, _I32, C.POINTER(BspSpmmPlan), _P]),
+    "bsp_spmm_plan_free": (C.c_int, [C.POINTER(BspSpmmPlan)]),
+    "bsp_spmm_plan_workspace": (C.c_size_t, [C.POINTER(BspSpmmPlan), _I32]),
+    "bsp_spmm_csr_planned": (C.c_int, [C.POINTER(BspSpmmPlan), _I32, _I32, _P, _P, _P, C.c_int, _P, _I32, _I64, _P,
+                                       _I64, C.c_float, C.c_float, _P, C.c_size_t, _P]),
+    "bsp_spmm_csr": (C.c_int, [_I32, _I32, _I32, _P, _P, _P, C.c_int, _P, _I32, _I64, _P, _I64, C.c_float,
+                               C.c_float, _P]),
+    "bsp_smat_create": (C.c_int, [_I32, _I32, _I32, _P, _P, _P, C.c_int, C.POINTER(BspSmat), _P]),
+    "bsp_smat_free": (C.c_int, [C.POINTER(BspSmat)]),
+    "bsp_smat_spmm": (C.c_int, [C.POINTER(BspSmat), _P, _I32, _I64, _P, _I64, C.c_float, C.c_float, _P]),
+    "bsp_smat_check": (C.c_int, [C.POINTER(BspSmat), _P]),
+    "bsp_gen_graph": (C.c_int, [_I32, _D, _D, _U64, _PI32, _PI64, _P, _P, _P]),
 })

@@ -457,12 +457,11 @@ class CgSolver:
     """Solver plan for an SPD CSR matrix on the device (arrays must stay alive)."""
 
     def __init__(self, rowptr, colidx, values, *, mode: str = "f16", tol: float = 1e-10, max_iters: int = 20000,
-                 check_every: int = 16, inner_tol: float = 1e-4, max_outer: int = 30, use_graphs: bool = True,
-                 stream=None):
+                 check_every: int = 16, reliable_delta: float = 0.1, use_graphs: bool = True, stream=None):
         o = _lib.BspCgOptions()
         check(lib().bsp_cg_default_options(C.byref(o)))
         o.mode, o.tol, o.max_iters, o.check_every = _CG_MODES[mode], tol, max_iters, check_every
-        o.inner_tol, o.max_outer, o.use_graphs = inner_tol, max_outer, int(use_graphs)
+        o.reliable_delta, o.use_graphs = reliable_delta, int(use_graphs)
         self._keep = (rowptr, colidx, values)
         self.n = rowptr.numel() - 1
         self._plan = C.c_void_p()
@@ -489,3 +488,214 @@ class CgSolver:
             self.close()
         except Exception:
             pass
+
+
+# ---------------------------------------------------------------------------
+# SpMM (replaces smatSpmmfp16, reference src/smat.cu:103; include/smat.h)
+
+def spmm_csr(rowptr, colidx, values, B, C=None, *, alpha: float = 1.0, beta: float = 0.0, stream=None):
+    """C = alpha*A*B + beta*C; values/B F16, BF16 or F32; C FP32 (rows x N)."""
+    torch = _torch()
+    rows = rowptr.numel() - 1
+    N = B.shape[1]
+    if C is None:
+        C = torch.empty(rows, N, dtype=torch.float32, device=B.device)
+        beta = 0.0
+    if values.dtype != B.dtype:
+        raise ValueError("values and B must share a dtype")
+    check(lib().bsp_spmm_csr(rows, B.shape[0], colidx.numel(), _dptr(rowptr, "rowptr"), _dptr(colidx, "colidx"),
+                             _dptr(values, "values"), _dtype_code(values), _dptr(B, "B"), N, B.stride(0),
+                             _dptr(C, "C"), C.stride(0), float(alpha), float(beta), _stream(stream)))
+    return C
+
+
+class SpmmPlan:
+    """Row-split plan for CSR SpMM on power-law matrices: rows longer than
+    `chunk` nonzeros are cut into chunks handled by separate warps and summed
+    in chunk order (deterministic)."""
+
+    def __init__(self, rowptr, colidx, values, *, cols: int, chunk: int = 256, stream=None):
+        self._d = _lib.BspSpmmPlan()
+        self.rowptr, self.colidx, self.values, self.cols = rowptr, colidx, values, cols
+        check(lib().bsp_spmm_plan_create(rowptr.numel() - 1, colidx.numel(), _dptr(rowptr, "rowptr"), chunk,
+                                         C.byref(self._d), _stream(stream)))
+        self._live = True
+        self._ws = None
+
+    @property
+    def nchunks(self) -> int:
+        return self._d.nchunks
+
+    @property
+    def nsplit(self) -> int:
+        return self._d.nsplit
+
+    def workspace_bytes(self, N: int) -> int:
+        return lib().bsp_spmm_plan_workspace(C.byref(self._d), N)
+
+    def spmm(self, B, C_out=None, *, alpha: float = 1.0, beta: float = 0.0, stream=None):
+        torch = _torch()
+        N = B.shape[1]
+        if self.values.dtype != B.dtype:
+            raise ValueError("values and B must share a dtype")
+        if C_out is None:
+            C_out = torch.empty(self._d.rows, N, dtype=torch.float32, device=B.device)
+            beta = 0.0
+        need = self.workspace_bytes(N)
+        if need and (self._ws is None or self._ws.numel() < need):
+            self._ws = torch.empty(need, dtype=torch.uint8, device=B.device)
+        ws = self._ws if need else None
+        check(lib().bsp_spmm_csr_planned(C.byref(self._d), self.cols, self.colidx.numel(),
+                                         _dptr(self.rowptr, "rowptr"), _dptr(self.colidx, "colidx"),
+                                         _dptr(self.values, "values"), _dtype_code(self.values), _dptr(B, "B"), N,
+                                         B.stride(0), _dptr(C_out, "C"), C_out.stride(0), float(alpha), float(beta),
+                                         ws.data_ptr() if ws is not None else None, need, _stream(stream)))
+        return C_out
+
+    def free(self) -> None:
+        if self._live:
+            self._live = False
+            check(lib().bsp_spmm_plan_free(C.byref(self._d)))
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class SmatMatrix:
+    """16x16-tile F16/BF16 matrix for the tensor-core (SMaT) SpMM."""
+
+    def __init__(self, rowptr, colidx, values, *, rows: int, cols: int, dtype: str = "f16", stream=None):
+        self._d = _lib.BspSmat()
+        dt = {"f16": _lib.F16, "bf16": _lib.BF16}[dtype]
+        check(lib().bsp_smat_create(rows, cols, colidx.numel(), _dptr(rowptr, "rowptr"), _dptr(colidx, "colidx"),
+                                    _dptr(values, "values"), dt, C.byref(self._d), _stream(stream)))
+        self._live = True
+
+    @property
+    def fill(self) -> float:
+        return self._d.fill
+
+    @property
+    def tiles(self) -> int:
+        return self._d.tiles.nonzeroBlocks
+
+    def spmm(self, B, C=None, *, alpha: float = 1.0, beta: float = 0.0, stream=None):
+        torch = _torch()
+        N = B.shape[1]
+        if C is None:
+            C = torch.empty(self._d.rows, N, dtype=torch.float32, device=B.device)
+            beta = 0.0
+        check(lib().bsp_smat_spmm(C_byref(self._d), _dptr(B, "B"), N, B.stride(0),
+                                  _dptr(C, "C"), C.stride(0), float(alpha), float(beta), _stream(stream)))
+        return C
+
+    def check(self, stream=None) -> None:
+        check(lib().bsp_smat_check(C_byref(self._d), _stream(stream)))
+
+    def free(self) -> None:
+        if self._live:
+            self._live = False
+            check(lib().bsp_smat_free(C_byref(self._d)))
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def C_byref(obj):
+    return C.byref(obj)
+
+
+def gen_graph(n: int, alpha: float, mean_deg: float, seed: int) -> HostCSR:
+    return _two_phase(lib().bsp_gen_graph, n, alpha, mean_deg, seed)
+
+
+def gen_banded(n: int, width: int, seed: int) -> HostCSR:
+    return _two_phase(lib().bsp_gen_banded, n, width, seed)
+
+
+# ---------------------------------------------------------------------------
+# Batched SpMV / 8-RHS SpMM (no reference counterpart; the reference runs one
+# matrix per call, src/csrspmv.cu:104-170)
+
+class BatchPlan:
+    """y_m = A_m x_m for many CSR matrices in one persistent, graph-captured
+    launch.  `mats` is a list of (rowptr, colidx, values, x, y) device tensors;
+    values/x/y F64 or F32; nrhs 1 or 8 (x: cols x 8, y: rows x 8 row-major).
+    tune=0 picks lanes per row from row statistics, tune=1 times the
+    candidates per matrix."""
+
+    def __init__(self, mats, *, nrhs: int = 1, tune: int = 0, seg_nnz: int = 1024, long_row_nnz: int = 2048,
+                 item_nnz: int = 0, use_graph: bool = True, stream=None):
+        torch = _torch()
+        if not mats:
+            raise ValueError("empty batch")
+        dt = mats[0][2].dtype
+        if dt not in (torch.float64, torch.float32):
+            raise ValueError("batched SpMV takes float64 or float32 values")
+        arr = (_lib.BspBatchMat * len(mats))()
+        for i, (rp, ci, va, x, y) in enumerate(mats):
+            if va.dtype != dt or x.dtype != dt or y.dtype != dt:
+                raise ValueError("all values, x and y must share one dtype")
+            rows = rp.numel() - 1
+            cols = x.shape[0] if nrhs > 1 else x.numel()
+            arr[i] = _lib.BspBatchMat(rows, cols, ci.numel(), _dptr(rp, "rowptr"), _dptr(ci, "colidx"),
+                                      _dptr(va, "values"), _dptr(x, "x"), _dptr(y, "y"))
+        opt = _lib.BspBatchOptions(tune, seg_nnz, long_row_nnz, item_nnz, 1 if use_graph else 0)
+        self._h = C.c_void_p()
+        self.count = len(mats)
+        self._keep = list(mats)
+        check(lib().bsp_batch_create(len(mats), arr, _lib.F64 if dt == torch.float64 else _lib.F32, nrhs,
+                                     C.byref(opt), C.byref(self._h), _stream(stream)))
+
+    def run(self, stream=None) -> None:
+        check(lib().bsp_batch_run(self._h, _stream(stream)))
+
+    def run_separate(self, stream=None) -> None:
+        check(lib().bsp_batch_run_separate(self._h, _stream(stream)))
+
+    def set_vectors(self, m: int, x, y, stream=None) -> None:
+        check(lib().bsp_batch_set_vectors(self._h, m, _dptr(x, "x"), _dptr(y, "y"), _stream(stream)))
+        rp, ci, va, _, _ = self._keep[m]
+        self._keep[m] = (rp, ci, va, x, y)
+
+    def lanes(self) -> np.ndarray:
+        out = np.empty(self.count, np.int32)
+        check(lib().bsp_batch_lanes(self._h, out.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def stats(self) -> dict:
+        a, b, c = C.c_int64(), C.c_int64(), C.c_int64()
+        check(lib().bsp_batch_stats(self._h, C.byref(a), C.byref(b), C.byref(c)))
+        return {"items": a.value, "long_segments": b.value, "nnz": c.value}
+
+    def close(self) -> None:
+        if self._h:
+            check(lib().bsp_batch_destroy(self._h))
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def gen_batch(count: int, seed: int, n_lo: int = 1000, n_hi: int = 65536) -> list:
+    """Seeded batch of matrices: n log-uniform in [n_lo, n_hi]; even entries
+    banded (width 3..27), odd entries Zipf(2.2) row lengths capped at n."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        n = int(round(np.exp(rng.uniform(np.log(n_lo), np.log(n_hi)))))
+        if i % 2 == 0:
+            out.append(gen_banded(n, int(rng.integers(3, 28)), seed * 1000 + i))
+        else:
+            out.append(gen_powerlaw(n, 2.2, n, seed * 1000 + i))
+    return out
+

@@ -1,0 +1,632 @@
+// Batched SpMV / 8-RHS SpMM over many independent CSR matrices in one
+// persistent launch.  The reference has no batched form: every operator
+// wrapper handles one matrix per call (src/csrspmv.cu:104-170,
+// src/spmv.cu:190-273).
+//
+// Plan (host, once): the row-length profile of every matrix gives
+//   * its lanes per row L (the tuner: a row-statistics model, or timing of
+//     the candidate L values with one launch per matrix);
+//   * row items: runs of consecutive rows holding about item_nnz nonzeros,
+//     processed by one warp, 32/L rows at a time; rows above 16*L nonzeros
+//     inside the run are taken by the whole warp after the pass;
+//   * long-row segments: rows above long_row_nnz are cut into seg_nnz pieces,
+//     one warp each; a piece's partial sum goes to a slot, and the warp that
+//     arrives last at the row's counter sums the slots in order and writes y
+//     (the counter is reset by that warp for the next launch).
+// Every output element is a fixed sum order of fixed products, whatever warp
+// runs an item, so results are deterministic and identical between the
+// batched launch and the per-matrix launches.
+//
+// Run: warps take items from a global counter; the long segments come first in
+// the list so the critical path starts at time zero.  Counter reset + kernel
+// are captured once in a CUDA graph.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "bsp_internal.cuh"
+#include "util.cuh"
+
+namespace bsp {
+
+struct BatchMatDev {
+  const int32_t *rp;
+  const int32_t *ci;
+  const void *val;
+  const void *x;
+  void *y;
+  int32_t rows, cols;
+};
+
+// info >= 0: row item, rows [a, b), info = lanes per row.
+// info < 0 : long-row segment, row a, segment b, long id = -(info + 1).
+struct BatchItem {
+  int32_t mat, a, b, info;
+};
+
+struct LongRow {
+  int32_t part_base, nseg;
+};
+
+constexpr int kBatchThreads = 256;
+constexpr int kMedFactor = 16;  // rows above 16*L nonzeros go to the whole warp
+
+template <typename V, int NRHS>
+struct Vec {
+  V v[NRHS];
+};
+
+// x row c (NRHS consecutive values) through the read-only path.
+template <typename V, int NRHS>
+__device__ __forceinline__ void load_xrow(const V *__restrict__ x, int32_t c, V (&out)[NRHS]) {
+  if constexpr (NRHS == 1) {
+    out[0] = __ldg(x + c);
+  } else if constexpr (sizeof(V) == 8) {
+    const double2 *p = reinterpret_cast<const double2 *>(x + (int64_t)c * NRHS);
+#pragma unroll
+    for (int k = 0; k < NRHS / 2; ++k) {
+      const double2 t = __ldg(p + k);
+      out[2 * k] = t.x;
+      out[2 * k + 1] = t.y;
+    }
+  } else {
+    const float4 *p = reinterpret_cast<const float4 *>(x + (int64_t)c * NRHS);
+#pragma unroll
+    for (int k = 0; k < NRHS / 4; ++k) {
+      const float4 t = __ldg(p + k);
+      out[4 * k] = t.x;
+      out[4 * k + 1] = t.y;
+      out[4 * k + 2] = t.z;
+      out[4 * k + 3] = t.w;
+    }
+  }
+}
+
+template <typename V, int NRHS>
+__device__ __forceinline__ void fma_row(V (&acc)[NRHS], V a, const V (&xr)[NRHS]) {
+#pragma unroll
+  for (int k = 0; k < NRHS; ++k) acc[k] = fma(a, xr[k], acc[k]);
+}
+
+// sum over nonzeros j = s + off, s + off + stride, ... < e (4 in flight)
+template <typename V, int NRHS>
+__device__ __forceinline__ void strided_dot(const int32_t *__restrict__ ci, const V *__restrict__ val,
+                                            const V *__restrict__ x, int32_t j, int32_t e, int32_t stride,
+                                            V (&acc)[NRHS]) {
+  for (; j + 3 * stride < e; j += 4 * stride) {
+    int32_t c[4];
+    V a[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      c[u] = __ldg(ci + j + u * stride);
+      a[u] = __ldg(val + j + u * stride);
+    }
+    V xr[4][NRHS];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) load_xrow<V, NRHS>(x, c[u], xr[u]);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) fma_row<V, NRHS>(acc, a[u], xr[u]);
+  }
+  for (; j < e; j += stride) {
+    V xr[NRHS];
+    load_xrow<V, NRHS>(x, __ldg(ci + j), xr);
+    fma_row<V, NRHS>(acc, __ldg(val + j), xr);
+  }
+}
+
+// The whole warp on one row (nonzeros [s, e)); every lane returns the sums.
+template <typename V, int NRHS>
+__device__ __forceinline__ void warp_row(const int32_t *ci, const V *val, const V *x, int32_t s, int32_t e,
+                                         int lane, V (&acc)[NRHS]) {
+#pragma unroll
+  for (int k = 0; k < NRHS; ++k) acc[k] = V(0);
+  strided_dot<V, NRHS>(ci, val, x, s + lane, e, 32, acc);
+#pragma unroll
+  for (int k = 0; k < NRHS; ++k) acc[k] = warp_sum(acc[k]);
+}
+
+template <typename V, int NRHS, int L>
+__device__ __forceinline__ void rows_item(const BatchMatDev &M, int32_t r0, int32_t r1, int32_t long_thr,
+                                          int lane) {
+  constexpr int RPP = 32 / L;
+  const int sub = lane % L, rl = lane / L;
+  const V *val = static_cast<const V *>(M.val);
+  const V *x = static_cast<const V *>(M.x);
+  V *y = static_cast<V *>(M.y);
+  for (int32_t base = r0; base < r1; base += RPP) {
+    const int32_t row = base + rl;
+    const bool active = row < r1;
+    int32_t s = 0, e = 0;
+    if (active) {
+      s = __ldg(M.rp + row);
+      e = __ldg(M.rp + row + 1);
+    }
+    const int32_t len = e - s;
+    const bool mine = len <= kMedFactor * L && len <= long_thr;
+    const bool medium = active && len > kMedFactor * L && len <= long_thr;
+    if (!mine) e = s;  // medium rows below, long rows in their segments
+    V acc[NRHS];
+#pragma unroll
+    for (int k = 0; k < NRHS; ++k) acc[k] = V(0);
+    strided_dot<V, NRHS>(M.ci, val, x, s + sub, e, L, acc);
+#pragma unroll
+    for (int o = L / 2; o > 0; o >>= 1)
+#pragma unroll
+      for (int k = 0; k < NRHS; ++k) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
+    if (active && sub == 0 && mine) {
+#pragma unroll
+      for (int k = 0; k < NRHS; ++k) y[(int64_t)row * NRHS + k] = acc[k];
+    }
+    unsigned med = __ballot_sync(0xffffffffu, medium && sub == 0);
+    while (med) {
+      const int b = __ffs(med) - 1;
+      med &= med - 1;
+      const int32_t mrow = base + b / L;
+      const int32_t ms = __ldg(M.rp + mrow), me = __ldg(M.rp + mrow + 1);
+      V w[NRHS];
+      warp_row<V, NRHS>(M.ci, val, x, ms, me, lane, w);
+      if (lane < NRHS) {
+        V o = w[0];
+#pragma unroll
+        for (int k = 1; k < NRHS; ++k)
+          if (lane == k) o = w[k];
+        y[(int64_t)mrow * NRHS + lane] = o;
+      }
+    }
+  }
+}
+
+template <typename V, int NRHS>
+__device__ __forceinline__ void segment_item(const BatchMatDev &M, int32_t row, int32_t seg, int32_t lid,
+                                             int32_t seg_nnz, const LongRow *__restrict__ longs,
+                                             V *__restrict__ part, int32_t *__restrict__ arrive, int lane) {
+  const V *val = static_cast<const V *>(M.val);
+  const V *x = static_cast<const V *>(M.x);
+  const LongRow lr = longs[lid];
+  const int32_t s0 = __ldg(M.rp + row), e0 = __ldg(M.rp + row + 1);
+  const int32_t s = s0 + seg * seg_nnz;
+  const int32_t e = min(s + seg_nnz, e0);
+  V w[NRHS];
+  warp_row<V, NRHS>(M.ci, val, x, s, e, lane, w);
+  if (lane < NRHS) {
+    V o = w[0];
+#pragma unroll
+    for (int k = 1; k < NRHS; ++k)
+      if (lane == k) o = w[k];
+    part[(int64_t)(lr.part_base + seg) * NRHS + lane] = o;
+    __threadfence();
+  }
+  __syncwarp();
+  int last = 0;
+  if (lane == 0) last = atomicAdd(arrive + lid, 1) == lr.nseg - 1;
+  last = __shfl_sync(0xffffffffu, last, 0);
+  if (!last) return;
+  __threadfence();
+  if (lane < NRHS) {
+    V acc = V(0);
+    for (int32_t t = 0; t < lr.nseg; ++t) acc += __ldcg(part + (int64_t)(lr.part_base + t) * NRHS + lane);
+    static_cast<V *>(M.y)[(int64_t)row * NRHS + lane] = acc;
+  }
+  if (lane == 0) atomicExch(arrive + lid, 0);  // ready for the next launch
+}
+
+template <typename V, int NRHS>
+__global__ void __launch_bounds__(kBatchThreads) batch_kernel(const BatchMatDev *__restrict__ mats,
+                                                              const BatchItem *__restrict__ items, int32_t nitems,
+                                                              int32_t *__restrict__ next,
+                                                              const LongRow *__restrict__ longs,
+                                                              V *__restrict__ part, int32_t *__restrict__ arrive,
+                                                              int32_t seg_nnz, int32_t long_thr) {
+  const int lane = threadIdx.x & 31;
+  for (;;) {
+    int32_t it = 0;
+    if (lane == 0) it = atomicAdd(next, 1);
+    it = __shfl_sync(0xffffffffu, it, 0);
+    if (it >= nitems) return;
+    const BatchItem I = items[it];
+    const BatchMatDev M = mats[I.mat];
+    if (I.info < 0) {
+      segment_item<V, NRHS>(M, I.a, I.b, -(I.info + 1), seg_nnz, longs, part, arrive, lane);
+      continue;
+    }
+    switch (I.info) {
+      case 1: rows_item<V, NRHS, 1>(M, I.a, I.b, long_thr, lane); break;
+      case 2: rows_item<V, NRHS, 2>(M, I.a, I.b, long_thr, lane); break;
+      case 4: rows_item<V, NRHS, 4>(M, I.a, I.b, long_thr, lane); break;
+      case 8: rows_item<V, NRHS, 8>(M, I.a, I.b, long_thr, lane); break;
+      case 16: rows_item<V, NRHS, 16>(M, I.a, I.b, long_thr, lane); break;
+      default: rows_item<V, NRHS, 32>(M, I.a, I.b, long_thr, lane); break;
+    }
+  }
+}
+
+}  // namespace bsp
+
+using namespace bsp;
+
+struct bsp_batch_plan_s {
+  int32_t count = 0, nrhs = 1;
+  bsp_dtype dtype = BSP_F64;
+  bsp_batch_options opt{};
+  std::vector<bsp_batch_mat> host_mats;
+  std::vector<std::vector<int32_t>> lens;  // row lengths per matrix
+  std::vector<int32_t> lanes;
+  BatchMatDev *d_mats = nullptr;
+  // batched list (long segments first) and per-matrix lists
+  BatchItem *d_items = nullptr, *d_items_sep = nullptr;
+  int64_t nitems = 0;
+  std::vector<int64_t> sep_off;  // [count+1] offsets into d_items_sep
+  LongRow *d_longs = nullptr;
+  int64_t nlong = 0, nseg = 0, total_nnz = 0;
+  void *d_part = nullptr;
+  int32_t *d_arrive = nullptr;
+  int32_t *d_next = nullptr;  // [count + 1]: batched counter, then one per matrix
+  int grid = 0;
+  cudaStream_t graph_stream = nullptr;
+  cudaGraphExec_t graph = nullptr;
+};
+
+namespace {
+
+int model_lanes(const std::vector<int32_t> &len, int32_t long_thr, int nrhs) {
+  double s = 0;
+  int64_t n = 0;
+  for (int32_t l : len)
+    if (l <= long_thr) {
+      s += l;
+      ++n;
+    }
+  const double mean = n ? s / (double)n : 0.0;
+  const double per_lane = nrhs > 1 ? 2.0 : 4.0;  // nonzeros a lane should own
+  int L = 1;
+  while (L < 32 && (double)L * per_lane < mean) L <<= 1;
+  return mean <= 2.0 * per_lane ? 1 : L;
+}
+
+// Items of matrix m for lanes L: long segments (appended to `lng`, with
+// their long-row entries), then row items (to `rows`).
+void build_items(int32_t m, const std::vector<int32_t> &len, int L, const bsp_batch_options &o,
+                 std::vector<BatchItem> &lng, std::vector<BatchItem> &rows, std::vector<LongRow> &longs,
+                 int64_t &parts, int64_t item_nnz) {
+  const int32_t n = (int32_t)len.size();
+  for (int32_t r = 0; r < n; ++r)
+    if (len[r] > o.long_row_nnz) {
+      const int32_t ns = (len[r] + o.seg_nnz - 1) / o.seg_nnz;
+      const int32_t lid = (int32_t)longs.size();
+      longs.push_back({(int32_t)parts, ns});
+      parts += ns;
+      for (int32_t s = 0; s < ns; ++s) lng.push_back({m, r, s, -(lid + 1)});
+    }
+  const int64_t max_rows = (int64_t)(32 / L) * 256;
+  int32_t r0 = 0;
+  int64_t acc = 0;
+  for (int32_t r = 0; r < n; ++r) {
+    acc += (len[r] <= o.long_row_nnz ? len[r] : 0) + 2;  // a row costs ~2 nonzeros of overhead
+    if (acc >= item_nnz || r + 1 - r0 >= max_rows) {
+      rows.push_back({m, r0, r + 1, L});
+      r0 = r + 1;
+      acc = 0;
+    }
+  }
+  if (r0 < n) rows.push_back({m, r0, n, L});
+}
+
+}  // namespace
+
+static bsp_status batch_build(bsp_batch_plan P, cudaStream_t s);
+static bsp_status batch_launch_one(bsp_batch_plan P, int32_t m, cudaStream_t s);
+
+extern "C" bsp_status bsp_batch_default_options(bsp_batch_options *o) {
+  clear_error();
+  BSP_CHECK_ARG(o, "null pointer");
+  o->tune = 0;
+  o->seg_nnz = 1024;
+  o->long_row_nnz = 2048;
+  o->item_nnz = 0;
+  o->use_graph = 1;
+  return BSP_OK;
+}
+
+template <typename V, int NRHS>
+static bsp_status launch_batch(bsp_batch_plan P, const BatchItem *items, int64_t nitems, int32_t *next,
+                               int grid, cudaStream_t s) {
+  batch_kernel<V, NRHS><<<grid, kBatchThreads, 0, s>>>(P->d_mats, items, (int32_t)nitems, next, P->d_longs,
+                                                       static_cast<V *>(P->d_part), P->d_arrive, P->opt.seg_nnz,
+                                                       P->opt.long_row_nnz);
+  BSP_LAUNCH_CHECK();
+  return BSP_OK;
+}
+
+static bsp_status dispatch(bsp_batch_plan P, const BatchItem *items, int64_t nitems, int32_t *next, int grid,
+                           cudaStream_t s) {
+  if (nitems == 0) return BSP_OK;
+  if (P->dtype == BSP_F64)
+    return P->nrhs == 8 ? launch_batch<double, 8>(P, items, nitems, next, grid, s)
+                        : launch_batch<double, 1>(P, items, nitems, next, grid, s);
+  return P->nrhs == 8 ? launch_batch<float, 8>(P, items, nitems, next, grid, s)
+                      : launch_batch<float, 1>(P, items, nitems, next, grid, s);
+}
+
+template <typename V, int NRHS>
+static int occupancy() {
+  int b = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, batch_kernel<V, NRHS>, kBatchThreads, 0) != cudaSuccess ||
+      b < 1)
+    b = 1;
+  return b;
+}
+
+static bsp_status batch_build(bsp_batch_plan P, cudaStream_t s) {
+  const bsp_batch_options &o = P->opt;
+  std::vector<BatchItem> lng, rows, sep;
+  std::vector<LongRow> longs;
+  int64_t parts = 0;
+  int64_t item_nnz = o.item_nnz;
+  const int warps_per_cta = kBatchThreads / 32;
+  int occ = 1;
+  if (P->dtype == BSP_F64)
+    occ = P->nrhs == 8 ? occupancy<double, 8>() : occupancy<double, 1>();
+  else
+    occ = P->nrhs == 8 ? occupancy<float, 8>() : occupancy<float, 1>();
+  P->grid = sm_count() * occ;
+  if (item_nnz <= 0) {
+    const int64_t warps = (int64_t)P->grid * warps_per_cta;
+    item_nnz = P->total_nnz / (warps * 6);
+    item_nnz = std::max<int64_t>(256, std::min<int64_t>(item_nnz, 8192));
+    if (P->nrhs == 8) item_nnz = std::max<int64_t>(128, item_nnz / 4);
+  }
+  P->sep_off.assign(P->count + 1, 0);
+  for (int32_t m = 0; m < P->count; ++m) {
+    std::vector<BatchItem> l1, r1;
+    build_items(m, P->lens[m], P->lanes[m], o, l1, r1, longs, parts, item_nnz);
+    lng.insert(lng.end(), l1.begin(), l1.end());
+    rows.insert(rows.end(), r1.begin(), r1.end());
+    sep.insert(sep.end(), l1.begin(), l1.end());
+    sep.insert(sep.end(), r1.begin(), r1.end());
+    P->sep_off[m + 1] = (int64_t)sep.size();
+  }
+  std::vector<BatchItem> all(lng);
+  all.insert(all.end(), rows.begin(), rows.end());
+  BSP_CHECK_ARG(all.size() < (size_t)INT32_MAX, "too many work items");
+  P->nitems = (int64_t)all.size();
+  P->nlong = (int64_t)longs.size();
+  P->nseg = (int64_t)lng.size();
+  dfree(P->d_items, s);
+  dfree(P->d_items_sep, s);
+  dfree(P->d_longs, s);
+  dfree(P->d_arrive, s);
+  if (P->d_part) cudaFreeAsync(P->d_part, s);
+  P->d_part = nullptr;
+  BSP_TRY(dalloc(&P->d_items, all.size(), s));
+  BSP_TRY(dalloc(&P->d_items_sep, sep.size(), s));
+  BSP_TRY(dalloc(&P->d_longs, longs.size(), s));
+  BSP_TRY(dalloc(&P->d_arrive, longs.size(), s));
+  const size_t es = P->dtype == BSP_F64 ? 8 : 4;
+  BSP_CUDA(cudaMallocAsync(&P->d_part, (size_t)std::max<int64_t>(1, parts) * P->nrhs * es, s));
+  if (!all.empty())
+    BSP_CUDA(cudaMemcpyAsync(P->d_items, all.data(), all.size() * sizeof(BatchItem), cudaMemcpyHostToDevice, s));
+  if (!sep.empty())
+    BSP_CUDA(
+        cudaMemcpyAsync(P->d_items_sep, sep.data(), sep.size() * sizeof(BatchItem), cudaMemcpyHostToDevice, s));
+  if (!longs.empty()) {
+    BSP_CUDA(cudaMemcpyAsync(P->d_longs, longs.data(), longs.size() * sizeof(LongRow), cudaMemcpyHostToDevice, s));
+    BSP_CUDA(cudaMemsetAsync(P->d_arrive, 0, longs.size() * sizeof(int32_t), s));
+  }
+  BSP_CUDA(cudaStreamSynchronize(s));  // host vectors go out of scope
+  return BSP_OK;
+}
+
+static bsp_status batch_launch_one(bsp_batch_plan P, int32_t m, cudaStream_t s) {
+  const int64_t a = P->sep_off[m], b = P->sep_off[m + 1];
+  if (b == a) return BSP_OK;
+  const int warps_per_cta = kBatchThreads / 32;
+  int grid = (int)std::min<int64_t>(ceil_div(b - a, warps_per_cta), (int64_t)P->grid);
+  BSP_CUDA(cudaMemsetAsync(P->d_next + 1 + m, 0, sizeof(int32_t), s));
+  return dispatch(P, P->d_items_sep + a, b - a, P->d_next + 1 + m, grid, s);
+}
+
+static bsp_status capture(bsp_batch_plan P) {
+  if (P->graph) {
+    cudaGraphExecDestroy(P->graph);
+    P->graph = nullptr;
+  }
+  if (!P->opt.use_graph) return BSP_OK;
+  if (!P->graph_stream) BSP_CUDA(cudaStreamCreateWithFlags(&P->graph_stream, cudaStreamNonBlocking));
+  cudaGraph_t g = nullptr;
+  BSP_CUDA(cudaStreamBeginCapture(P->graph_stream, cudaStreamCaptureModeThreadLocal));
+  cudaMemsetAsync(P->d_next, 0, sizeof(int32_t), P->graph_stream);
+  const bsp_status st = dispatch(P, P->d_items, P->nitems, P->d_next, P->grid, P->graph_stream);
+  cudaError_t e = cudaStreamEndCapture(P->graph_stream, &g);
+  if (st != BSP_OK) {
+    if (g) cudaGraphDestroy(g);
+    return st;
+  }
+  BSP_CUDA(e);
+  e = cudaGraphInstantiate(&P->graph, g, 0);
+  cudaGraphDestroy(g);
+  BSP_CUDA(e);
+  return BSP_OK;
+}
+
+extern "C" bsp_status bsp_batch_destroy(bsp_batch_plan P) {
+  clear_error();
+  if (!P) return BSP_OK;
+  cudaStream_t s = 0;
+  if (P->graph) cudaGraphExecDestroy(P->graph);
+  if (P->graph_stream) cudaStreamDestroy(P->graph_stream);
+  dfree(P->d_mats, s);
+  dfree(P->d_items, s);
+  dfree(P->d_items_sep, s);
+  dfree(P->d_longs, s);
+  dfree(P->d_arrive, s);
+  dfree(P->d_next, s);
+  if (P->d_part) cudaFreeAsync(P->d_part, s);
+  cudaStreamSynchronize(s);
+  delete P;
+  return BSP_OK;
+}
+
+extern "C" bsp_status bsp_batch_create(int32_t count, const bsp_batch_mat *mats, bsp_dtype dtype, int32_t nrhs,
+                                       const bsp_batch_options *opt, bsp_batch_plan *out, bsp_stream_t stream) {
+  clear_error();
+  BSP_CHECK_ARG(out && (count == 0 || mats) && count >= 0, "bad argument");
+  BSP_CHECK_ARG(dtype == BSP_F64 || dtype == BSP_F32, "batched SpMV takes F64 or F32 values");
+  BSP_CHECK_ARG(nrhs == 1 || nrhs == 8, "nrhs must be 1 or 8");
+  *out = nullptr;
+  bsp_batch_options o;
+  bsp_batch_default_options(&o);
+  if (opt) o = *opt;
+  BSP_CHECK_ARG(o.seg_nnz >= 32 && o.long_row_nnz >= o.seg_nnz, "need 32 <= seg_nnz <= long_row_nnz");
+  const size_t es = dtype == BSP_F64 ? 8 : 4;
+  for (int32_t m = 0; m < count; ++m) {
+    const bsp_batch_mat &A = mats[m];
+    BSP_CHECK_ARG(A.rows >= 0 && A.cols >= 0 && A.nnz >= 0 && A.rowPtr, "bad matrix descriptor");
+    BSP_CHECK_ARG(A.nnz == 0 || (A.colIdx && A.values), "bad matrix descriptor");
+    BSP_CHECK_ARG(A.rows == 0 || A.y, "null y");
+    BSP_CHECK_ARG(A.cols == 0 || A.x, "null x");
+    if (nrhs == 8)
+      BSP_CHECK_ARG((uintptr_t)A.x % 16 == 0 && (uintptr_t)A.y % 16 == 0, "8-RHS x / y must be 16-byte aligned");
+    (void)es;
+  }
+  cudaStream_t s = as_stream(stream);
+  bsp_batch_plan P = new bsp_batch_plan_s();
+  P->count = count;
+  P->nrhs = nrhs;
+  P->dtype = dtype;
+  P->opt = o;
+  P->host_mats.assign(mats, mats + count);
+  P->lens.resize(count);
+  P->lanes.assign(count, 1);
+  auto fail = [&](bsp_status st) {
+    bsp_batch_destroy(P);
+    return st;
+  };
+  // row lengths from the device row pointers
+  std::vector<int32_t> rp;
+  for (int32_t m = 0; m < count; ++m) {
+    const bsp_batch_mat &A = mats[m];
+    rp.resize((size_t)A.rows + 1);
+    if (cudaMemcpyAsync(rp.data(), A.rowPtr, rp.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, s) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess) {
+      set_error("bsp_batch_create: reading a row pointer failed");
+      return fail(BSP_ERR_CUDA);
+    }
+    if (rp[0] != 0 || rp[A.rows] != A.nnz) {
+      set_error("bsp_batch_create: rowPtr[0] must be 0 and rowPtr[rows] == nnz");
+      return fail(BSP_ERR_INVALID);
+    }
+    auto &L = P->lens[m];
+    L.resize(A.rows);
+    for (int32_t r = 0; r < A.rows; ++r) L[r] = rp[r + 1] - rp[r];
+    P->total_nnz += A.nnz;
+    P->lanes[m] = model_lanes(L, o.long_row_nnz, nrhs);
+  }
+  std::vector<BatchMatDev> dm(count);
+  for (int32_t m = 0; m < count; ++m)
+    dm[m] = {mats[m].rowPtr, mats[m].colIdx, mats[m].values, mats[m].x, mats[m].y, mats[m].rows, mats[m].cols};
+  if (dalloc(&P->d_mats, (size_t)count, s) != BSP_OK || dalloc(&P->d_next, (size_t)count + 1, s) != BSP_OK)
+    return fail(BSP_ERR_ALLOC);
+  if (count > 0 &&
+      cudaMemcpyAsync(P->d_mats, dm.data(), dm.size() * sizeof(BatchMatDev), cudaMemcpyHostToDevice, s) !=
+          cudaSuccess) {
+    set_error("bsp_batch_create: copying descriptors failed");
+    return fail(BSP_ERR_CUDA);
+  }
+  bsp_status st = batch_build(P, s);
+  if (st != BSP_OK) return fail(st);
+  if (o.tune == 1) {
+    // time every candidate lanes value with one launch per matrix; keep the
+    // fastest (outputs are overwritten, inputs untouched)
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const int cand[6] = {1, 2, 4, 8, 16, 32};
+    std::vector<float> best(count, 1e30f);
+    std::vector<int> best_l(P->lanes);
+    for (int ci = 0; ci < 6 && st == BSP_OK; ++ci) {
+      std::fill(P->lanes.begin(), P->lanes.end(), cand[ci]);
+      st = batch_build(P, s);
+      for (int32_t m = 0; m < count && st == BSP_OK; ++m) {
+        float tmin = 1e30f;
+        for (int rep = 0; rep < 3 && st == BSP_OK; ++rep) {
+          cudaEventRecord(e0, s);
+          st = batch_launch_one(P, m, s);
+          cudaEventRecord(e1, s);
+          cudaEventSynchronize(e1);
+          float ms = 0;
+          cudaEventElapsedTime(&ms, e0, e1);
+          if (rep > 0) tmin = std::min(tmin, ms);
+        }
+        if (tmin < best[m]) {
+          best[m] = tmin;
+          best_l[m] = cand[ci];
+        }
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st != BSP_OK) return fail(st);
+    P->lanes = best_l;
+    st = batch_build(P, s);
+    if (st != BSP_OK) return fail(st);
+  }
+  st = capture(P);
+  if (st != BSP_OK) return fail(st);
+  *out = P;
+  return BSP_OK;
+}
+
+extern "C" bsp_status bsp_batch_run(bsp_batch_plan P, bsp_stream_t stream) {
+  clear_error();
+  BSP_CHECK_ARG(P, "null plan");
+  cudaStream_t s = as_stream(stream);
+  if (P->graph) {
+    BSP_CUDA(cudaGraphLaunch(P->graph, s));
+    return BSP_OK;
+  }
+  BSP_CUDA(cudaMemsetAsync(P->d_next, 0, sizeof(int32_t), s));
+  return dispatch(P, P->d_items, P->nitems, P->d_next, P->grid, s);
+}
+
+extern "C" bsp_status bsp_batch_run_separate(bsp_batch_plan P, bsp_stream_t stream) {
+  clear_error();
+  BSP_CHECK_ARG(P, "null plan");
+  cudaStream_t s = as_stream(stream);
+  for (int32_t m = 0; m < P->count; ++m) BSP_TRY(batch_launch_one(P, m, s));
+  return BSP_OK;
+}
+
+extern "C" bsp_status bsp_batch_set_vectors(bsp_batch_plan P, int32_t m, const void *x, void *y,
+                                            bsp_stream_t stream) {
+  clear_error();
+  BSP_CHECK_ARG(P && m >= 0 && m < P->count, "bad plan or matrix index");
+  if (P->nrhs == 8) BSP_CHECK_ARG((uintptr_t)x % 16 == 0 && (uintptr_t)y % 16 == 0, "x / y must be 16-byte aligned");
+  const bsp_batch_mat &A = P->host_mats[m];
+  BSP_CHECK_ARG((A.cols == 0 || x) && (A.rows == 0 || y), "null vector");
+  cudaStream_t s = as_stream(stream);
+  P->host_mats[m].x = x;
+  P->host_mats[m].y = y;
+  const BatchMatDev d{A.rowPtr, A.colIdx, A.values, x, y, A.rows, A.cols};
+  // the descriptor is read by the kernel: update it in stream order
+  BSP_CUDA(cudaMemcpyAsync(P->d_mats + m, &d, sizeof(d), cudaMemcpyHostToDevice, s));
+  BSP_CUDA(cudaStreamSynchronize(s));
+  return BSP_OK;
+}
+
+extern "C" bsp_status bsp_batch_lanes(bsp_batch_plan P, int32_t *lanes) {
+  clear_error();
+  BSP_CHECK_ARG(P && lanes, "null pointer");
+  for (int32_t m = 0; m < P->count; ++m) lanes[m] = P->lanes[m];
+  return BSP_OK;
+}
+
+extern "C" bsp_status bsp_batch_stats(bsp_batch_plan P, int64_t *items, int64_t *long_segments,
+                                      int64_t *total_nnz) {
+  clear_error();
+  BSP_CHECK_ARG(P, "null plan");
+  if (items) *items = P->nitems;
+  if (long_segments) *long_segments = P->nseg;
+  if (total_nnz) *total_nnz = P->total_nnz;
+  return BSP_OK;
+}

@@ -38,9 +38,9 @@ inline cudaStream_t as_stream(bsp_stream_t s) { return reinterpret_cast<cudaStre
     }                                                                         \
   } while (0)
 
-// Checks the launch that was just issued (configuration errors only; the
-// kernel itself runs asynchronously).
-#define BSP_LAUNCH_CHECK() BSP_CUDA(cudaPeekAtLastError())
+// Checks (and clears) the launch error of the kernel just issued
+// (configuration errors only; the kernel itself runs asynchronously).
+#define BSP_LAUNCH_CHECK() BSP_CUDA(cudaGetLastError())
 
 #define BSP_TRY(expr)                                                         \
   do {                                                                        \

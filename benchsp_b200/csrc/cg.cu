@@ -1,7 +1,7 @@
 // Conjugate gradients on the device: plain FP64 CG and mixed-precision CG
-// with FP64 iterative refinement.  The reference has no solver (SURVEY: the
-// CG / mixed-precision rows are absent there); this is the precision form of
-// the benchmark's CG configuration: 3-D 7-point Poisson, tolerance 1e-10 on
+// with reliable updates.  The reference has no solver (the CG /
+// mixed-precision rows are absent there); this is the precision form of the
+// benchmark's CG configuration: 3-D 7-point Poisson, tolerance 1e-10 on
 // ||b - A x|| / ||b|| checked in FP64.
 //
 // Mixed precision: the matrix is stored a second time with values in FP32,
@@ -9,22 +9,26 @@
 // 32 consecutive nonzeros (v = stored * 2^e, the group maximum scaled into
 // [1, 2)), and column indices are stored as int16 offsets from the row when
 // every |col - row| < 32768 (banded matrices), else int32.  A nonzero then
-// moves 4 bytes (FP16/BF16 + int16) instead of 12 (FP64 + int32).  The outer
-// loop keeps r = b - A x, ||r|| and x += d in FP64 with the FP64 matrix; the
-// inner CG solves A d = r / ||r|| in FP32 vectors to a relative tolerance,
-// with FP64 dot products.
+// moves 4 bytes (FP16/BF16 + int16) instead of 12 (FP64 + int32).  CG
+// iterations run on that matrix with FP32 vectors (dot products in FP64).
+// The FP64 state is the solution x64 and the true residual: whenever the
+// iterated residual has dropped by `reliable_delta` since the last update,
+// x64 += x32, r = b - A x64 is recomputed in FP64 with the FP64 matrix and
+// replaces the iterated residual, and the search direction is kept (CG with
+// reliable updates), so the iteration count stays close to plain FP64 CG while
+// most bytes move at low precision.
 //
-// Kernels per CG iteration (one CUDA graph captures `check_every`
-// iterations; the host reads the residual between graphs):
-//   1. q = A p fused with per-CTA partials of p.q;
-//   2. alpha = rr / p.q (every CTA reduces the partials in the same order:
-//      deterministic, no atomics), x += alpha p, r -= alpha q, partials of r.r;
-//   3. beta = rr_new / rr, p = r + beta p (CTA 0 records rr_new).
-// Zero denominators freeze the iteration (alpha = beta = 0), so iterations
-// run after convergence inside a graph are harmless.
+// One CG iteration is two kernels:
+//   A. beta = rr_k / rr_{k-1}; p_k = r_k + beta p_{k-1} formed on the fly for
+//      every gathered column (r and p_{k-1} are read, p_k written for the own
+//      row into the other p buffer); q = A p_k; partials of p_k.q;
+//   B. alpha = rr_k / p.q; x += alpha p_k; r -= alpha q; partials of r.r.
+// Every CTA reduces the previous kernel's per-CTA partials in the same order
+// (deterministic, no atomics).  Scalars ping-pong between two slots by
+// iteration parity so no CTA reads a value written in its own launch.  Zero
+// denominators freeze the iteration (alpha = beta = 0), so iterations run
+// after convergence inside a captured graph are harmless.
 #include <math.h>
-
-#include <vector>
 
 #include "bsp_internal.cuh"
 #include "util.cuh"
@@ -33,6 +37,7 @@ namespace bsp {
 
 constexpr int kCgThreads = 256;
 constexpr int kScaleGroup = 32;
+constexpr int kRowFirst = 8;  // row entries loaded together per lane
 
 template <typename V> __device__ __forceinline__ float lp_to_float(V v);
 template <> __device__ __forceinline__ float lp_to_float<float>(float v) { return v; }
@@ -43,7 +48,7 @@ template <> __device__ __forceinline__ float lp_to_float<__nv_bfloat16>(__nv_bfl
 __device__ __forceinline__ float pow2f(int e) { return __int_as_float((127 + e) << 23); }
 
 // Deterministic block sum of one double per thread (fixed shuffle tree, then
-// warp totals in order).  Result valid in thread 0.
+// the warp totals in order).  Valid in thread 0.
 __device__ __forceinline__ double block_sum(double v, double *smem /* [kCgThreads/32] */) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -56,7 +61,7 @@ __device__ __forceinline__ double block_sum(double v, double *smem /* [kCgThread
   return t;
 }
 
-// Sum of the n partials in index order; every CTA gets the same value.
+// Sum of n partials in index order; every CTA gets the same value.
 __device__ __forceinline__ double reduce_partials(const double *__restrict__ part, int n, double *smem) {
   double s = 0.0;
   for (int i = threadIdx.x; i < n; i += kCgThreads) s += __ldcg(part + i);
@@ -67,89 +72,79 @@ __device__ __forceinline__ double reduce_partials(const double *__restrict__ par
   return bcast;
 }
 
-// q = A p and partial p.q.  Matrix values V (double, float, half, bf16),
-// optional group exponents, int32 columns or int16 offsets from the row.
-// Vectors VT (double for FP64 CG, float for the inner solve).  LPR lanes per row.
-template <typename V, typename VT, bool SCALED, bool DELTA16, int LPR>
-__global__ void __launch_bounds__(kCgThreads) cg_spmv_dot_kernel(int32_t n, const int32_t *__restrict__ rowPtr,
-                                                                 const void *__restrict__ cols,
-                                                                 const V *__restrict__ val,
-                                                                 const int8_t *__restrict__ exps,
-                                                                 const VT *__restrict__ p, VT *__restrict__ q,
-                                                                 double *__restrict__ part) {
+// Matrix access: values V with optional group exponents, columns int32 or
+// int16 offsets from the row.
+template <typename V, typename VT, bool SCALED, bool DELTA16>
+struct CgMat {
+  const int32_t *rowPtr;
+  const void *cols;
+  const V *val;
+  const int8_t *exps;
+  __device__ __forceinline__ int64_t col(int64_t r, int32_t j) const {
+    if (DELTA16) return r + (int64_t) reinterpret_cast<const int16_t *>(cols)[j];
+    return reinterpret_cast<const int32_t *>(cols)[j];
+  }
+  __device__ __forceinline__ VT value(int32_t j) const {
+    if constexpr (sizeof(V) == 8) {
+      return (VT)val[j];
+    } else {
+      float af = lp_to_float<V>(val[j]);
+      if (SCALED) af *= pow2f(exps[j / kScaleGroup]);
+      return (VT)af;
+    }
+  }
+};
+
+// Kernel A: p_k = r + beta p_prev (own row stored, gathered columns formed on
+// the fly), q = A p_k, partials of p_k.q.  rr_part = partials of rr_k;
+// rr_prev_slot = rr_{k-1}; rr_slot receives rr_k (written by CTA 0).
+template <typename V, typename VT, bool SCALED, bool DELTA16>
+__global__ void __launch_bounds__(kCgThreads) cg_dir_spmv_kernel(int32_t n, CgMat<V, VT, SCALED, DELTA16> A,
+                                                                 const VT *__restrict__ r,
+                                                                 const VT *__restrict__ p_prev,
+                                                                 VT *__restrict__ p, VT *__restrict__ q,
+                                                                 const double *__restrict__ rr_part, int npart,
+                                                                 const double *__restrict__ rr_prev_slot,
+                                                                 double *__restrict__ rr_slot,
+                                                                 double *__restrict__ pq_part) {
   __shared__ double smem[kCgThreads / 32];
-  const int sub = threadIdx.x & (LPR - 1);
-  const int64_t groups = (int64_t)gridDim.x * (kCgThreads / LPR);
+  const double rr = reduce_partials(rr_part, npart, smem);
+  const double rr_prev = *rr_prev_slot;
+  const double beta = (rr_prev != 0.0 && isfinite(rr)) ? rr / rr_prev : 0.0;
+  const VT bt = (VT)beta;
   double dot = 0.0;
-  const int64_t warp_first = ((int64_t)blockIdx.x * kCgThreads + (threadIdx.x & ~31)) / LPR;
-  for (int64_t base = warp_first; base < n; base += groups) {
-    const int64_t r = base + (threadIdx.x & 31) / LPR;
-    const bool active = r < n;
-    const int32_t s = active ? rowPtr[r] : 0, e = active ? rowPtr[r + 1] : 0;
-    VT acc = VT(0);
-    for (int32_t j = s + sub; j < e; j += LPR) {
-      int64_t c;
-      if (DELTA16)
-        c = r + (int64_t) reinterpret_cast<const int16_t *>(cols)[j];
-      else
-        c = reinterpret_cast<const int32_t *>(cols)[j];
-      VT a;
-      if constexpr (sizeof(V) == 8) {
-        a = (VT)val[j];
-      } else {
-        float af = lp_to_float<V>(val[j]);
-        if (SCALED) af *= pow2f(exps[j / kScaleGroup]);
-        a = (VT)af;
-      }
-      acc = fma(a, __ldg(p + c), acc);
-    }
+  const int64_t stride = (int64_t)gridDim.x * kCgThreads;
+  for (int64_t i = (int64_t)blockIdx.x * kCgThreads + threadIdx.x; i < n; i += stride) {
+    const int32_t s = A.rowPtr[i], e = A.rowPtr[i + 1];
+    int64_t c[kRowFirst];
+    VT a[kRowFirst];
 #pragma unroll
-    for (int o = LPR / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o, LPR);
-    if (active && sub == 0) {
-      q[r] = acc;
-      dot += (double)acc * (double)p[r];
+    for (int k = 0; k < kRowFirst; ++k) {
+      const int32_t j = s + k;
+      c[k] = j < e ? A.col(i, j) : -1;
+      a[k] = j < e ? A.value(j) : VT(0);
     }
+    VT acc = VT(0);
+#pragma unroll
+    for (int k = 0; k < kRowFirst; ++k)
+      if (c[k] >= 0) acc = fma(a[k], fma(bt, __ldg(p_prev + c[k]), __ldg(r + c[k])), acc);
+    for (int32_t j = s + kRowFirst; j < e; ++j) {
+      const int64_t cj = A.col(i, j);
+      acc = fma(A.value(j), fma(bt, __ldg(p_prev + cj), __ldg(r + cj)), acc);
+    }
+    const VT pi = fma(bt, p_prev[i], r[i]);
+    p[i] = pi;
+    q[i] = acc;
+    dot += (double)acc * (double)pi;
   }
   const double t = block_sum(dot, smem);
-  if (threadIdx.x == 0) part[blockIdx.x] = t;
-}
-
-// r = b - A x and partial ||r||^2, all FP64 (outer refinement / FP64 CG start).
-__global__ void __launch_bounds__(kCgThreads) cg_residual_kernel(int32_t n, const int32_t *__restrict__ rowPtr,
-                                                                 const int32_t *__restrict__ colIdx,
-                                                                 const double *__restrict__ val,
-                                                                 const double *__restrict__ b,
-                                                                 const double *__restrict__ x,
-                                                                 double *__restrict__ r, double *__restrict__ part) {
-  __shared__ double smem[kCgThreads / 32];
-  constexpr int LPR = 8;
-  const int sub = threadIdx.x & (LPR - 1);
-  const int64_t groups = (int64_t)gridDim.x * (kCgThreads / LPR);
-  double nrm = 0.0;
-  const int64_t warp_first = ((int64_t)blockIdx.x * kCgThreads + (threadIdx.x & ~31)) / LPR;
-  for (int64_t base = warp_first; base < n; base += groups) {
-    const int64_t i = base + (threadIdx.x & 31) / LPR;
-    const bool active = i < n;
-    const int32_t s = active ? rowPtr[i] : 0, e = active ? rowPtr[i + 1] : 0;
-    double acc = 0.0;
-    for (int32_t j = s + sub; j < e; j += LPR) acc = fma(val[j], __ldg(x + colIdx[j]), acc);
-#pragma unroll
-    for (int o = LPR / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o, LPR);
-    if (active && sub == 0) {
-      const double ri = b[i] - acc;
-      r[i] = ri;
-      nrm += ri * ri;
-    }
+  if (threadIdx.x == 0) {
+    pq_part[blockIdx.x] = t;
+    if (blockIdx.x == 0) *rr_slot = rr;
   }
-  const double t = block_sum(nrm, smem);
-  if (threadIdx.x == 0) part[blockIdx.x] = t;
 }
 
-// Scalars kept on the device (sc[]): [0], [1] = r.r of even / odd iterations
-// (ping-pong: iteration k reads slot k%2 and writes slot (k+1)%2, so no CTA
-// can see a value written in its own launch), [2] = r.r at the start,
-// [3] = iterations, [4] = ||b||^2, [5] = ||b - A x||^2 of the last residual.
-// alpha = rr / pq; x += alpha p; r -= alpha q; partial r.r.
+// Kernel B: alpha = rr_k / p.q; x += alpha p; r -= alpha q; partials of r.r.
 template <typename VT>
 __global__ void __launch_bounds__(kCgThreads) cg_update_kernel(int32_t n, const double *__restrict__ pq_part,
                                                                int npart, const double *__restrict__ rr_slot,
@@ -162,80 +157,86 @@ __global__ void __launch_bounds__(kCgThreads) cg_update_kernel(int32_t n, const 
   const double alpha = (pq != 0.0 && rr != 0.0 && isfinite(pq)) ? rr / pq : 0.0;
   const VT a = (VT)alpha;
   double s = 0.0;
-  for (int64_t i = (int64_t)blockIdx.x * kCgThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kCgThreads) {
-    x[i] = fma(a, p[i], x[i]);
-    const VT ri = fma(-a, q[i], r[i]);
-    r[i] = ri;
-    s += (double)ri * (double)ri;
+  const int64_t stride = (int64_t)gridDim.x * kCgThreads;
+  for (int64_t i0 = (int64_t)blockIdx.x * kCgThreads + threadIdx.x; i0 < n; i0 += 4 * stride) {
+    VT pv[4], qv[4], xv[4], rv[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int64_t i = i0 + k * stride;
+      if (i < n) {
+        pv[k] = p[i];
+        qv[k] = q[i];
+        xv[k] = x[i];
+        rv[k] = r[i];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int64_t i = i0 + k * stride;
+      if (i < n) {
+        x[i] = fma(a, pv[k], xv[k]);
+        const VT ri = fma(-a, qv[k], rv[k]);
+        r[i] = ri;
+        s += (double)ri * (double)ri;
+      }
+    }
   }
   const double t = block_sum(s, smem);
   if (threadIdx.x == 0) rr_part[blockIdx.x] = t;
 }
 
-// beta = rr_new / rr; p = r + beta p; CTA 0 stores rr_new in the other slot.
+// FP64 true residual r = b - A x, partials of ||r||^2; optionally also the
+// inner-precision copy r_lp = (VT) r and its partials (reliable update).
 template <typename VT>
-__global__ void __launch_bounds__(kCgThreads) cg_direction_kernel(int32_t n, const double *__restrict__ rr_part,
-                                                                  int npart, const double *__restrict__ rr_slot,
-                                                                  double *__restrict__ rr_next,
-                                                                  double *__restrict__ sc,
-                                                                  const VT *__restrict__ r, VT *__restrict__ p) {
+__global__ void __launch_bounds__(kCgThreads) cg_residual_kernel(int32_t n, const int32_t *__restrict__ rowPtr,
+                                                                 const int32_t *__restrict__ colIdx,
+                                                                 const double *__restrict__ val,
+                                                                 const double *__restrict__ b,
+                                                                 const double *__restrict__ x,
+                                                                 double *__restrict__ r, VT *__restrict__ r_lp,
+                                                                 double *__restrict__ part,
+                                                                 double *__restrict__ part_lp) {
   __shared__ double smem[kCgThreads / 32];
-  const double rr_new = reduce_partials(rr_part, npart, smem);
-  const double rr = *rr_slot;
-  const double beta = (rr != 0.0 && isfinite(rr_new)) ? rr_new / rr : 0.0;
-  const VT bt = (VT)beta;
-  for (int64_t i = (int64_t)blockIdx.x * kCgThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kCgThreads)
-    p[i] = fma(bt, p[i], r[i]);
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    *rr_next = rr_new;
-    sc[3] += 1.0;
+  double nrm = 0.0, nrm_lp = 0.0;
+  const int64_t stride = (int64_t)gridDim.x * kCgThreads;
+  for (int64_t i = (int64_t)blockIdx.x * kCgThreads + threadIdx.x; i < n; i += stride) {
+    const int32_t s = rowPtr[i], e = rowPtr[i + 1];
+    int32_t c[kRowFirst];
+    double a[kRowFirst];
+#pragma unroll
+    for (int k = 0; k < kRowFirst; ++k) {
+      c[k] = s + k < e ? colIdx[s + k] : -1;
+      a[k] = s + k < e ? val[s + k] : 0.0;
+    }
+    double acc = 0.0;
+#pragma unroll
+    for (int k = 0; k < kRowFirst; ++k)
+      if (c[k] >= 0) acc = fma(a[k], __ldg(x + c[k]), acc);
+    for (int32_t j = s + kRowFirst; j < e; ++j) acc = fma(val[j], __ldg(x + colIdx[j]), acc);
+    const double ri = b[i] - acc;
+    if (r) r[i] = ri;
+    nrm += ri * ri;
+    if (r_lp) {
+      const VT v = (VT)ri;
+      r_lp[i] = v;
+      nrm_lp += (double)v * (double)v;
+    }
+  }
+  double t = block_sum(nrm, smem);
+  if (threadIdx.x == 0) part[blockIdx.x] = t;
+  if (r_lp) {
+    t = block_sum(nrm_lp, smem);
+    if (threadIdx.x == 0) part_lp[blockIdx.x] = t;
   }
 }
 
-// Start of a (inner or FP64) CG: r given, p = r, rr = r.r from partials, x = 0.
+// x64 += x_lp; x_lp = 0 (reliable update of the solution).
 template <typename VT>
-__global__ void __launch_bounds__(kCgThreads) cg_start_kernel(int32_t n, const double *__restrict__ rr_part,
-                                                              int npart, double *__restrict__ sc,
-                                                              const VT *__restrict__ r, VT *__restrict__ p,
-                                                              VT *__restrict__ x, int zero_x) {
-  __shared__ double smem[kCgThreads / 32];
-  const double rr = reduce_partials(rr_part, npart, smem);
-  for (int64_t i = (int64_t)blockIdx.x * kCgThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kCgThreads) {
-    p[i] = r[i];
-    if (zero_x) x[i] = VT(0);
+__global__ void cg_fold_kernel(int32_t n, VT *__restrict__ x_lp, double *__restrict__ x) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    x[i] += (double)x_lp[i];
+    x_lp[i] = VT(0);
   }
-  __syncthreads();
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    sc[0] = rr;
-    sc[2] = rr;
-    sc[3] = 0.0;
-  }
-}
-
-// Inner start from the FP64 residual: r32 = r64 / ||r64||, partial r32.r32.
-__global__ void __launch_bounds__(kCgThreads) cg_scale_rhs_kernel(int32_t n, const double *__restrict__ r64,
-                                                                  const double *__restrict__ nrm2_p,
-                                                                  float *__restrict__ r32,
-                                                                  double *__restrict__ rr_part) {
-  __shared__ double smem[kCgThreads / 32];
-  const double nrm2 = *nrm2_p;
-  const double inv = nrm2 > 0.0 ? 1.0 / sqrt(nrm2) : 0.0;
-  double s = 0.0;
-  for (int64_t i = (int64_t)blockIdx.x * kCgThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kCgThreads) {
-    const float v = (float)(r64[i] * inv);
-    r32[i] = v;
-    s += (double)v * (double)v;
-  }
-  const double t = block_sum(s, smem);
-  if (threadIdx.x == 0) rr_part[blockIdx.x] = t;
-}
-
-// x64 += ||r64|| * d32 (refinement update).
-__global__ void cg_refine_kernel(int32_t n, const double *__restrict__ nrm2_p, const float *__restrict__ d,
-                                 double *__restrict__ x) {
-  const double nrm = sqrt(*nrm2_p);
-  for (int64_t i = (int64_t)blockIdx.x * kCgThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kCgThreads)
-    x[i] = fma(nrm, (double)d[i], x[i]);
 }
 
 __global__ void sum_partials_kernel(const double *__restrict__ part, int npart, double *__restrict__ out) {
@@ -300,6 +301,7 @@ __global__ void f64_to_f32_kernel(int64_t n, const double *__restrict__ a, float
     b[i] = (float)a[i];
 }
 
+
 }  // namespace bsp
 
 // ---------------------------------------------------------------------------
@@ -308,96 +310,92 @@ struct bsp_cg_plan_s {
   bsp_cg_options opt{};
   const int32_t *rowPtr = nullptr, *colIdx = nullptr;
   const double *val = nullptr;
-  // low-precision copy
+  // low-precision copy of the matrix (mixed modes)
   void *lp_val = nullptr;
   int8_t *exps = nullptr;
-  void *lp_cols = nullptr;  // int16 offsets or nullptr (then colIdx)
+  int16_t *lp_cols = nullptr;  // int16 offsets, or nullptr (then colIdx)
   bool delta16 = false;
-  // vectors
-  double *r64 = nullptr, *p64 = nullptr, *q64 = nullptr, *x64 = nullptr;
-  float *x32 = nullptr, *r32 = nullptr, *p32 = nullptr, *q32 = nullptr;
-  double *part_a = nullptr, *part_b = nullptr, *sc = nullptr, *h_sc = nullptr;
+  // FP64 state
+  double *x64 = nullptr, *r64 = nullptr;
+  // iteration vectors: FP64 (mode FP64) or FP32 (mixed); p ping-pongs
+  void *x = nullptr, *r = nullptr, *p[2] = {nullptr, nullptr}, *q = nullptr;
+  double *part_pq = nullptr, *part_rr = nullptr, *part_res = nullptr;
+  double *sc = nullptr, *h_sc = nullptr;  // [0],[1] rr slots, [2] ||b-Ax||^2, [3] ||b||^2, [4] rr after a chunk
   int grid = 0;
-  cudaGraphExec_t graph64 = nullptr, graph32 = nullptr;
+  cudaGraphExec_t graph = nullptr;
   cudaStream_t graph_stream = nullptr;
-  int64_t bytes_inner_iter = 0, bytes_fp64_iter = 0, bytes_residual = 0;
+  int64_t bytes_iter = 0, bytes_residual = 0;
 };
 
 namespace bsp {
 
 static int cg_grid(int32_t n) {
   int64_t g = ceil_div(n, kCgThreads);
-  const int64_t cap = (int64_t)sm_count() * 8;
+  const int64_t cap = (int64_t)sm_count() * 4;  // one wave at <= 64 registers per thread
   if (g > cap) g = cap;
   if (g < 1) g = 1;
   return (int)g;
 }
 
-// Launches q = A p (+ partials) for the plan's matrix in precision `inner`.
-static bsp_status launch_spmv_dot(bsp_cg_plan_s *P, bool inner, cudaStream_t s) {
+static bool cg_mixed(const bsp_cg_plan_s *P) { return P->opt.mode != BSP_CG_FP64; }
+
+template <typename V, typename VT, bool SC, bool D16>
+static void launch_iter(bsp_cg_plan_s *P, int k, cudaStream_t s) {
+  CgMat<V, VT, SC, D16> A{P->rowPtr, D16 ? (const void *)P->lp_cols : (const void *)P->colIdx,
+                           (const V *)(sizeof(V) == 8 ? (const void *)P->val : P->lp_val), P->exps};
+  VT *r = (VT *)P->r, *x = (VT *)P->x, *q = (VT *)P->q;
+  VT *pp = (VT *)P->p[k & 1], *pn = (VT *)P->p[(k + 1) & 1];
   const int g = P->grid;
-  if (!inner) {
-    cg_spmv_dot_kernel<double, double, false, false, 8><<<g, kCgThreads, 0, s>>>(
-        P->n, P->rowPtr, P->colIdx, P->val, nullptr, P->p64, P->q64, P->part_a);
-    BSP_LAUNCH_CHECK();
-    return BSP_OK;
-  }
-  const void *cols = P->delta16 ? P->lp_cols : (const void *)P->colIdx;
-#define BSP_CG_LAUNCH(V, SC)                                                                             \
-  do {                                                                                                   \
-    if (P->delta16)                                                                                      \
-      cg_spmv_dot_kernel<V, float, SC, true, 8><<<g, kCgThreads, 0, s>>>(                                \
-          P->n, P->rowPtr, cols, (const V *)P->lp_val, P->exps, P->p32, P->q32, P->part_a);              \
-    else                                                                                                 \
-      cg_spmv_dot_kernel<V, float, SC, false, 8><<<g, kCgThreads, 0, s>>>(                               \
-          P->n, P->rowPtr, cols, (const V *)P->lp_val, P->exps, P->p32, P->q32, P->part_a);              \
-  } while (0)
-  switch (P->opt.mode) {
-    case BSP_CG_MIXED_F32: BSP_CG_LAUNCH(float, false); break;
-    case BSP_CG_MIXED_F16: BSP_CG_LAUNCH(__half, true); break;
-    case BSP_CG_MIXED_BF16: BSP_CG_LAUNCH(__nv_bfloat16, true); break;
-    default: BSP_FAIL(BSP_ERR_INVALID, "unknown CG mode");
-  }
-#undef BSP_CG_LAUNCH
-  BSP_LAUNCH_CHECK();
-  return BSP_OK;
+  cg_dir_spmv_kernel<V, VT, SC, D16><<<g, kCgThreads, 0, s>>>(P->n, A, r, pp, pn, q, P->part_rr, g,
+                                                               P->sc + ((k + 1) & 1), P->sc + (k & 1),
+                                                               P->part_pq);
+  cg_update_kernel<VT><<<g, kCgThreads, 0, s>>>(P->n, P->part_pq, g, P->sc + (k & 1), x, r, pn, q, P->part_rr);
 }
 
-// One CG iteration (3 launches) on the inner (FP32) or FP64 vectors; `k`
-// selects the r.r slot (iteration parity).
-static bsp_status cg_iteration(bsp_cg_plan_s *P, bool inner, int k, cudaStream_t s) {
-  BSP_TRY(launch_spmv_dot(P, inner, s));
-  const int g = P->grid;
-  const double *cur = P->sc + (k & 1);
-  double *next = P->sc + ((k + 1) & 1);
-  if (inner) {
-    cg_update_kernel<float><<<g, kCgThreads, 0, s>>>(P->n, P->part_a, g, cur, P->x32, P->r32, P->p32, P->q32,
-                                                      P->part_b);
-    cg_direction_kernel<float><<<g, kCgThreads, 0, s>>>(P->n, P->part_b, g, cur, next, P->sc, P->r32, P->p32);
+static bsp_status cg_iteration(bsp_cg_plan_s *P, int k, cudaStream_t s) {
+  if (!cg_mixed(P)) {
+    launch_iter<double, double, false, false>(P, k, s);
   } else {
-    cg_update_kernel<double><<<g, kCgThreads, 0, s>>>(P->n, P->part_a, g, cur, P->x64, P->r64, P->p64, P->q64,
-                                                       P->part_b);
-    cg_direction_kernel<double><<<g, kCgThreads, 0, s>>>(P->n, P->part_b, g, cur, next, P->sc, P->r64, P->p64);
+    const bool d = P->delta16;
+    switch (P->opt.mode) {
+      case BSP_CG_MIXED_F32:
+        d ? launch_iter<float, float, false, true>(P, k, s) : launch_iter<float, float, false, false>(P, k, s);
+        break;
+      case BSP_CG_MIXED_F16:
+        d ? launch_iter<__half, float, true, true>(P, k, s) : launch_iter<__half, float, true, false>(P, k, s);
+        break;
+      default:
+        d ? launch_iter<__nv_bfloat16, float, true, true>(P, k, s)
+          : launch_iter<__nv_bfloat16, float, true, false>(P, k, s);
+    }
   }
   BSP_LAUNCH_CHECK();
   return BSP_OK;
 }
 
-// Builds (once per precision) a graph of `check_every` iterations (an even
-// count, so r.r is back in slot 0 after every graph).
-static bsp_status cg_graph(bsp_cg_plan_s *P, bool inner, cudaGraphExec_t *exec) {
-  if (!P->graph_stream) BSP_CUDA(cudaStreamCreateWithFlags(&P->graph_stream, cudaStreamNonBlocking));
-  cudaStream_t cs = P->graph_stream;
-  cudaGraph_t graph = nullptr;
-  BSP_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-  bsp_status st = BSP_OK;
-  for (int k = 0; k < P->opt.check_every && st == BSP_OK; ++k) st = cg_iteration(P, inner, k, cs);
-  cudaError_t e = cudaStreamEndCapture(cs, &graph);
-  if (st != BSP_OK) return st;
-  if (e != cudaSuccess) BSP_FAIL(BSP_ERR_CUDA, cudaGetErrorString(e));
-  e = cudaGraphInstantiate(exec, graph, 0);
-  cudaGraphDestroy(graph);
-  if (e != cudaSuccess) BSP_FAIL(BSP_ERR_CUDA, cudaGetErrorString(e));
+// `check_every` iterations (even) followed by rr -> sc[4].
+static bsp_status cg_chunk(bsp_cg_plan_s *P, cudaStream_t s) {
+  for (int k = 0; k < P->opt.check_every; ++k) BSP_TRY(cg_iteration(P, k, s));
+  sum_partials_kernel<<<1, kCgThreads, 0, s>>>(P->part_rr, P->grid, P->sc + 4);
+  BSP_LAUNCH_CHECK();
+  return BSP_OK;
+}
+
+static bsp_status cg_run_chunk(bsp_cg_plan_s *P, cudaStream_t s) {
+  if (!P->opt.use_graphs) return cg_chunk(P, s);
+  if (!P->graph) {
+    if (!P->graph_stream) BSP_CUDA(cudaStreamCreateWithFlags(&P->graph_stream, cudaStreamNonBlocking));
+    cudaGraph_t graph = nullptr;
+    BSP_CUDA(cudaStreamBeginCapture(P->graph_stream, cudaStreamCaptureModeThreadLocal));
+    bsp_status st = cg_chunk(P, P->graph_stream);
+    cudaError_t e = cudaStreamEndCapture(P->graph_stream, &graph);
+    if (st != BSP_OK) return st;
+    if (e != cudaSuccess) BSP_FAIL(BSP_ERR_CUDA, cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&P->graph, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) BSP_FAIL(BSP_ERR_CUDA, cudaGetErrorString(e));
+  }
+  BSP_CUDA(cudaGraphLaunch(P->graph, s));
   return BSP_OK;
 }
 
@@ -407,26 +405,22 @@ static bsp_status read_scalars(bsp_cg_plan_s *P, cudaStream_t s) {
   return BSP_OK;
 }
 
-// Runs CG iterations (graph chunks) until r.r <= rel_tol^2 * r.r(start) or the
-// budget is spent.  Returns the iterations executed.
-static bsp_status cg_loop(bsp_cg_plan_s *P, bool inner, double rel_tol, int32_t max_iters, int32_t *iters,
-                          cudaStream_t s) {
-  *iters = 0;
-  BSP_TRY(read_scalars(P, s));
-  const double target = rel_tol * rel_tol * P->h_sc[2];
-  if (P->h_sc[0] <= target) return BSP_OK;
-  cudaGraphExec_t *exec = inner ? &P->graph32 : &P->graph64;
-  if (P->opt.use_graphs && !*exec) BSP_TRY(cg_graph(P, inner, exec));
-  while (*iters < max_iters) {
-    if (P->opt.use_graphs) {
-      BSP_CUDA(cudaGraphLaunch(*exec, s));
-    } else {
-      for (int k = 0; k < P->opt.check_every; ++k) BSP_TRY(cg_iteration(P, inner, k, s));
-    }
-    *iters += P->opt.check_every;
-    BSP_TRY(read_scalars(P, s));
-    if (!(P->h_sc[0] > target)) break;  // also stops on NaN
+// True FP64 residual of x64 -> sc[2]; the iterated residual (and its r.r
+// partials for the next iteration) is replaced by it.
+static bsp_status cg_true_residual(bsp_cg_plan_s *P, const double *b, cudaStream_t s) {
+  const int g = P->grid;
+  if (cg_mixed(P))
+    cg_residual_kernel<float><<<g, kCgThreads, 0, s>>>(P->n, P->rowPtr, P->colIdx, P->val, b, P->x64, nullptr,
+                                                        (float *)P->r, P->part_res, P->part_rr);
+  else
+    cg_residual_kernel<double><<<g, kCgThreads, 0, s>>>(P->n, P->rowPtr, P->colIdx, P->val, b, P->x64,
+                                                         (double *)P->r, nullptr, P->part_res, nullptr);
+  BSP_LAUNCH_CHECK();
+  if (!cg_mixed(P)) {  // the FP64 residual is the iterated one
+    BSP_CUDA(cudaMemcpyAsync(P->part_rr, P->part_res, sizeof(double) * g, cudaMemcpyDeviceToDevice, s));
   }
+  sum_partials_kernel<<<1, kCgThreads, 0, s>>>(P->part_res, g, P->sc + 2);
+  BSP_LAUNCH_CHECK();
   return BSP_OK;
 }
 
@@ -441,9 +435,31 @@ extern "C" bsp_status bsp_cg_default_options(bsp_cg_options *o) {
   o->tol = 1e-10;
   o->max_iters = 20000;
   o->check_every = 16;
-  o->inner_tol = 1e-4;
-  o->max_outer = 30;
+  o->reliable_delta = 0.1;
   o->use_graphs = 1;
+  return BSP_OK;
+}
+
+extern "C" bsp_status bsp_cg_destroy(bsp_cg_plan P) {
+  clear_error();
+  if (!P) return BSP_OK;
+  cudaStream_t s = 0;
+  if (P->graph) cudaGraphExecDestroy(P->graph);
+  if (P->graph_stream) cudaStreamDestroy(P->graph_stream);
+  if (P->x == P->x64) P->x = nullptr;  // FP64 mode iterates on x64 itself
+  dfree(P->x64, s);
+  dfree(P->r64, s);
+  for (void *v : {P->x, P->r, P->p[0], P->p[1], P->q, P->lp_val})
+    if (v) cudaFreeAsync(v, s);
+  dfree(P->lp_cols, s);
+  dfree(P->exps, s);
+  dfree(P->part_pq, s);
+  dfree(P->part_rr, s);
+  dfree(P->part_res, s);
+  dfree(P->sc, s);
+  if (P->h_sc) cudaFreeHost(P->h_sc);
+  cudaStreamSynchronize(s);
+  delete P;
   return BSP_OK;
 }
 
@@ -454,54 +470,61 @@ extern "C" bsp_status bsp_cg_create(int32_t n, int32_t nnz, const int32_t *rowPt
   BSP_CHECK_ARG(out && opt, "null argument");
   BSP_CHECK_ARG(n > 0 && nnz >= 0 && rowPtr && colIdx && values, "bad matrix");
   BSP_CHECK_ARG(opt->mode >= BSP_CG_FP64 && opt->mode <= BSP_CG_MIXED_BF16, "unknown mode");
-  BSP_CHECK_ARG(opt->tol > 0 && opt->check_every >= 1 && opt->max_iters >= 1 && opt->max_outer >= 1,
-                "bad options");
-  BSP_CHECK_ARG(opt->inner_tol > 0 && opt->inner_tol < 1, "inner_tol must be in (0, 1)");
+  BSP_CHECK_ARG(opt->tol > 0 && opt->check_every >= 1 && opt->max_iters >= 1, "bad options");
+  BSP_CHECK_ARG(opt->reliable_delta > 0 && opt->reliable_delta < 1, "reliable_delta must be in (0, 1)");
   cudaStream_t s = as_stream(stream);
   bsp_cg_plan_s *P = new bsp_cg_plan_s();
   P->n = n;
   P->nnz = nnz;
   P->opt = *opt;
-  P->opt.check_every += P->opt.check_every & 1;  // even: r.r ends in slot 0
+  P->opt.check_every += P->opt.check_every & 1;  // even: iteration parity restarts at every chunk
   P->rowPtr = rowPtr;
   P->colIdx = colIdx;
   P->val = values;
   P->grid = cg_grid(n);
-  auto fail = [&](bsp_status st) {
+  const bool mixed = cg_mixed(P);
+  const size_t vt = mixed ? 4 : 8;
+  bsp_status st = BSP_OK;
+  auto fail = [&](bsp_status e) {
     bsp_cg_destroy(P);
-    return st;
+    return e;
   };
-  bsp_status st;
-#define BSP_CG_TRY(x)                 \
-  do {                                \
+#define BSP_CG_TRY(x)                         \
+  do {                                        \
     if ((st = (x)) != BSP_OK) return fail(st); \
   } while (0)
-  BSP_CG_TRY(dalloc(&P->r64, (size_t)n, s));
-  BSP_CG_TRY(dalloc(&P->p64, (size_t)n, s));
-  BSP_CG_TRY(dalloc(&P->q64, (size_t)n, s));
+#define BSP_CG_CUDA(x)                                                              \
+  do {                                                                              \
+    cudaError_t e_ = (x);                                                           \
+    if (e_ != cudaSuccess) {                                                        \
+      set_error(std::string("bsp_cg_create: ") + #x + " -> " + cudaGetErrorString(e_)); \
+      return fail(BSP_ERR_ALLOC);                                                   \
+    }                                                                               \
+  } while (0)
   BSP_CG_TRY(dalloc(&P->x64, (size_t)n, s));
-  BSP_CG_TRY(dalloc(&P->part_a, (size_t)P->grid, s));
-  BSP_CG_TRY(dalloc(&P->part_b, (size_t)P->grid, s));
+  BSP_CG_TRY(dalloc(&P->part_pq, (size_t)P->grid, s));
+  BSP_CG_TRY(dalloc(&P->part_rr, (size_t)P->grid, s));
+  BSP_CG_TRY(dalloc(&P->part_res, (size_t)P->grid, s));
   BSP_CG_TRY(dalloc(&P->sc, 8, s));
-  if (cudaMallocHost(reinterpret_cast<void **>(&P->h_sc), 8 * sizeof(double)) != cudaSuccess)
-    return fail(BSP_ERR_ALLOC);
-  const int64_t vb = 8;  // FP64 vector bytes
-  P->bytes_residual = (int64_t)nnz * 12 + 4 * ((int64_t)n + 1) + 3 * vb * n;
-  P->bytes_fp64_iter = (int64_t)nnz * 12 + 4 * ((int64_t)n + 1) + 3 * vb * n /* spmv: p gathers, q, p */ +
-                       6 * vb * n /* update */ + 3 * vb * n /* direction */;
-  if (opt->mode != BSP_CG_FP64) {
-    BSP_CG_TRY(dalloc(&P->x32, (size_t)n, s));
-    BSP_CG_TRY(dalloc(&P->r32, (size_t)n, s));
-    BSP_CG_TRY(dalloc(&P->p32, (size_t)n, s));
-    BSP_CG_TRY(dalloc(&P->q32, (size_t)n, s));
+  BSP_CG_CUDA(cudaMallocHost(reinterpret_cast<void **>(&P->h_sc), 8 * sizeof(double)));
+  if (mixed) {
+    P->x = nullptr;  // x32 allocated below
+  }
+  for (void **v : {&P->x, &P->r, &P->p[0], &P->p[1], &P->q}) BSP_CG_CUDA(cudaMallocAsync(v, vt * (size_t)n, s));
+  if (!mixed) {  // FP64 mode iterates directly on x64
+    cudaFreeAsync(P->x, s);
+    P->x = P->x64;
+  }
+  int64_t mat_bytes = (int64_t)nnz * 12;
+  if (mixed) {
     const bool scaled = opt->mode != BSP_CG_MIXED_F32;
     const size_t vsz = opt->mode == BSP_CG_MIXED_F32 ? 4 : 2;
-    if (cudaMallocAsync(&P->lp_val, vsz * (size_t)(nnz > 0 ? nnz : 1), s) != cudaSuccess) return fail(BSP_ERR_ALLOC);
+    BSP_CG_CUDA(cudaMallocAsync(&P->lp_val, vsz * (size_t)(nnz > 0 ? nnz : 1), s));
     int64_t gq = ceil_div(nnz, 256);
     if (gq > (int64_t)sm_count() * 32) gq = (int64_t)sm_count() * 32;
     if (gq < 1) gq = 1;
+    const int64_t ng = ceil_div(nnz, kScaleGroup);
     if (scaled) {
-      const int64_t ng = ceil_div(nnz, kScaleGroup);
       BSP_CG_TRY(dalloc(&P->exps, (size_t)(ng > 0 ? ng : 1), s));
       cg_group_exp_kernel<<<(unsigned)ceil_div(ng > 0 ? ng : 1, 256), 256, 0, s>>>(nnz, values, P->exps);
     }
@@ -512,8 +535,10 @@ extern "C" bsp_status bsp_cg_create(int32_t n, int32_t nnz, const int32_t *rowPt
     else
       cg_quantize_kernel<__nv_bfloat16, true><<<(unsigned)gq, 256, 0, s>>>(nnz, values, P->exps,
                                                                            (__nv_bfloat16 *)P->lp_val);
-    if (cudaPeekAtLastError() != cudaSuccess) return fail(BSP_ERR_CUDA);
-    // int16 column offsets when every |col - row| fits
+    if (cudaGetLastError() != cudaSuccess) {
+      set_error("bsp_cg_create: quantization kernel launch failed");
+      return fail(BSP_ERR_CUDA);
+    }
     int32_t *bad = nullptr;
     BSP_CG_TRY(dalloc(&bad, 1, s));
     cudaMemsetAsync(bad, 0, sizeof(int32_t), s);
@@ -524,46 +549,24 @@ extern "C" bsp_status bsp_cg_create(int32_t n, int32_t nnz, const int32_t *rowPt
     BSP_CG_TRY(read_i32(bad, &h_bad, s));
     dfree(bad, s);
     if (!h_bad) {
-      int16_t *d16 = nullptr;
-      BSP_CG_TRY(dalloc(&d16, (size_t)(nnz > 0 ? nnz : 1), s));
-      cg_delta_fill_kernel<<<(unsigned)gr, 256, 0, s>>>(n, rowPtr, colIdx, d16);
-      P->lp_cols = d16;
+      BSP_CG_TRY(dalloc(&P->lp_cols, (size_t)(nnz > 0 ? nnz : 1), s));
+      cg_delta_fill_kernel<<<(unsigned)gr, 256, 0, s>>>(n, rowPtr, colIdx, P->lp_cols);
       P->delta16 = true;
     }
-    const int64_t ib = P->delta16 ? 2 : 4;
-    P->bytes_inner_iter = (int64_t)nnz * ((int64_t)vsz + ib) + (scaled ? ceil_div(nnz, kScaleGroup) : 0) +
-                          4 * ((int64_t)n + 1) + 3 * 4 * (int64_t)n + 6 * 4 * (int64_t)n + 3 * 4 * (int64_t)n;
+    mat_bytes = (int64_t)nnz * ((int64_t)vsz + (P->delta16 ? 2 : 4)) + (scaled ? ng : 0);
   }
 #undef BSP_CG_TRY
-  if (cudaStreamSynchronize(s) != cudaSuccess) return fail(BSP_ERR_CUDA);
+#undef BSP_CG_CUDA
+  // algorithmic bytes: kernel A reads the matrix, r and p_prev (own rows;
+  // gathers counted once) and writes p and q; kernel B reads p, q, x, r and
+  // writes x, r.
+  P->bytes_iter = mat_bytes + 4 * ((int64_t)n + 1) + 10 * (int64_t)vt * n;
+  P->bytes_residual = (int64_t)nnz * 12 + 4 * ((int64_t)n + 1) + 3 * 8 * (int64_t)n;
+  if (cudaStreamSynchronize(s) != cudaSuccess) {
+    set_error("bsp_cg_create: preparing the matrix failed");
+    return fail(BSP_ERR_CUDA);
+  }
   *out = P;
-  return BSP_OK;
-}
-
-extern "C" bsp_status bsp_cg_destroy(bsp_cg_plan P) {
-  clear_error();
-  if (!P) return BSP_OK;
-  cudaStream_t s = 0;
-  if (P->graph64) cudaGraphExecDestroy(P->graph64);
-  if (P->graph32) cudaGraphExecDestroy(P->graph32);
-  if (P->graph_stream) cudaStreamDestroy(P->graph_stream);
-  dfree(P->r64, s);
-  dfree(P->p64, s);
-  dfree(P->q64, s);
-  dfree(P->x64, s);
-  dfree(P->x32, s);
-  dfree(P->r32, s);
-  dfree(P->p32, s);
-  dfree(P->q32, s);
-  dfree(P->part_a, s);
-  dfree(P->part_b, s);
-  dfree(P->sc, s);
-  if (P->lp_val) cudaFreeAsync(P->lp_val, s);
-  if (P->lp_cols) cudaFreeAsync(P->lp_cols, s);
-  dfree(P->exps, s);
-  if (P->h_sc) cudaFreeHost(P->h_sc);
-  cudaStreamSynchronize(s);
-  delete P;
   return BSP_OK;
 }
 
@@ -574,71 +577,70 @@ extern "C" bsp_status bsp_cg_solve(bsp_cg_plan P, const double *b, double *x, bs
   cudaStream_t s = as_stream(stream);
   *res = bsp_cg_result{};
   const int g = P->grid;
+  const bool mixed = cg_mixed(P);
+  const size_t vt = mixed ? 4 : 8;
   cudaEvent_t e0, e1;
   BSP_CUDA(cudaEventCreate(&e0));
   BSP_CUDA(cudaEventCreate(&e1));
   BSP_CUDA(cudaEventRecord(e0, s));
-  // x64 = initial guess; ||b||^2 from the residual of x = 0 (q64 as zero vector)
-  BSP_CUDA(cudaMemcpyAsync(P->x64, x, sizeof(double) * P->n, cudaMemcpyDeviceToDevice, s));
-  BSP_CUDA(cudaMemsetAsync(P->q64, 0, sizeof(double) * P->n, s));
-  cg_residual_kernel<<<g, kCgThreads, 0, s>>>(P->n, P->rowPtr, P->colIdx, P->val, b, P->q64, P->r64, P->part_a);
-  sum_partials_kernel<<<1, kCgThreads, 0, s>>>(P->part_a, g, P->sc + 4);
+  // ||b||^2 via the residual of x = 0 (x64 zeroed), then x64 = x0
+  BSP_CUDA(cudaMemsetAsync(P->x64, 0, sizeof(double) * P->n, s));
+  cg_residual_kernel<double><<<g, kCgThreads, 0, s>>>(P->n, P->rowPtr, P->colIdx, P->val, b, P->x64, nullptr,
+                                                       nullptr, P->part_res, nullptr);
+  sum_partials_kernel<<<1, kCgThreads, 0, s>>>(P->part_res, g, P->sc + 3);
   BSP_LAUNCH_CHECK();
+  BSP_CUDA(cudaMemcpyAsync(P->x64, x, sizeof(double) * P->n, cudaMemcpyDeviceToDevice, s));
+  // start: iterated residual, p_prev = 0, rr_prev = 0 (beta_0 = 0)
+  if (mixed) BSP_CUDA(cudaMemsetAsync(P->x, 0, vt * P->n, s));
+  BSP_CUDA(cudaMemsetAsync(P->p[0], 0, vt * P->n, s));
+  BSP_CUDA(cudaMemsetAsync(P->sc, 0, 2 * sizeof(double), s));
+  BSP_TRY(cg_true_residual(P, b, s));
   BSP_TRY(read_scalars(P, s));
-  const double bb = P->h_sc[4];
-  int64_t spmv_fp64 = 1, spmv_inner = 0, fp64_iters = 0;
-  int32_t total = 0;
-  const bool inner = P->opt.mode != BSP_CG_FP64;
-  for (int outer = 0; bb > 0.0 && outer < P->opt.max_outer; ++outer) {
-    // FP64 true residual r = b - A x and ||r||^2 -> sc[5]
-    cg_residual_kernel<<<g, kCgThreads, 0, s>>>(P->n, P->rowPtr, P->colIdx, P->val, b, P->x64, P->r64,
-                                                 P->part_a);
-    sum_partials_kernel<<<1, kCgThreads, 0, s>>>(P->part_a, g, P->sc + 5);
-    BSP_LAUNCH_CHECK();
-    spmv_fp64++;
+  const double bb = P->h_sc[3];
+  const double target = P->opt.tol * P->opt.tol * bb;
+  const double delta2 = P->opt.reliable_delta * P->opt.reliable_delta;
+  double rmax2 = P->h_sc[2];
+  int64_t residuals = 2, iters = 0;
+  int32_t updates = 0;
+  bool done = bb == 0.0 || P->h_sc[2] <= target;
+  while (!done && iters < P->opt.max_iters) {
+    BSP_TRY(cg_run_chunk(P, s));
+    iters += P->opt.check_every;
     BSP_TRY(read_scalars(P, s));
-    res->outer_iterations = outer;
-    if (P->h_sc[5] <= P->opt.tol * P->opt.tol * bb) break;
-    if (total >= P->opt.max_iters) break;
-    int32_t it = 0;
-    if (inner) {
-      // solve A d = r / ||r|| in the inner precision, then x += ||r|| d
-      cg_scale_rhs_kernel<<<g, kCgThreads, 0, s>>>(P->n, P->r64, P->sc + 5, P->r32, P->part_b);
-      cg_start_kernel<float><<<g, kCgThreads, 0, s>>>(P->n, P->part_b, g, P->sc, P->r32, P->p32, P->x32, 1);
-      BSP_LAUNCH_CHECK();
-      BSP_TRY(cg_loop(P, true, P->opt.inner_tol, P->opt.max_iters - total, &it, s));
-      cg_refine_kernel<<<g, kCgThreads, 0, s>>>(P->n, P->sc + 5, P->x32, P->x64);
-      BSP_LAUNCH_CHECK();
-      spmv_inner += it;
-    } else {
-      // FP64 CG from the current x (restarted with the true residual when the
-      // recursive one has converged but the true one has not)
-      cg_start_kernel<double><<<g, kCgThreads, 0, s>>>(P->n, P->part_a, g, P->sc, P->r64, P->p64, P->x64, 0);
-      BSP_LAUNCH_CHECK();
-      const double rel = P->opt.tol * sqrt(bb / P->h_sc[5]);
-      BSP_TRY(cg_loop(P, false, rel < 1.0 ? rel : 1.0, P->opt.max_iters - total, &it, s));
-      fp64_iters += it;
+    const double rr = P->h_sc[4];
+    const bool stalled = !(rr == rr);  // NaN
+    if (rr <= target || (mixed && rr <= delta2 * rmax2) || stalled) {
+      // reliable update: fold the inner solution, replace the residual
+      if (mixed) {
+        cg_fold_kernel<float><<<g, kCgThreads, 0, s>>>(P->n, (float *)P->x, P->x64);
+        BSP_LAUNCH_CHECK();
+      }
+      BSP_TRY(cg_true_residual(P, b, s));
+      BSP_TRY(read_scalars(P, s));
+      ++residuals;
+      ++updates;
+      rmax2 = P->h_sc[2];
+      done = P->h_sc[2] <= target || stalled;
     }
-    total += it;
-    res->outer_iterations = outer + 1;
+  }
+  if (!done && mixed) {  // iteration budget spent: fold what the inner solve has
+    cg_fold_kernel<float><<<g, kCgThreads, 0, s>>>(P->n, (float *)P->x, P->x64);
+    BSP_TRY(cg_true_residual(P, b, s));
+    ++residuals;
   }
   BSP_CUDA(cudaMemcpyAsync(x, P->x64, sizeof(double) * P->n, cudaMemcpyDeviceToDevice, s));
-  // the last residual in sc[5] is the true FP64 residual of the returned x
-  // unless the loop ran out; recompute it to report it exactly
-  cg_residual_kernel<<<g, kCgThreads, 0, s>>>(P->n, P->rowPtr, P->colIdx, P->val, b, P->x64, P->r64, P->part_a);
-  sum_partials_kernel<<<1, kCgThreads, 0, s>>>(P->part_a, g, P->sc + 5);
-  BSP_LAUNCH_CHECK();
   BSP_CUDA(cudaEventRecord(e1, s));
   BSP_TRY(read_scalars(P, s));
   float ms = 0;
   cudaEventElapsedTime(&ms, e0, e1);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  res->iterations = total;
+  res->iterations = (int32_t)iters;
+  res->reliable_updates = updates;
   res->seconds = ms * 1e-3;
-  res->rel_residual = bb > 0 ? sqrt(P->h_sc[5] / bb) : 0.0;
+  res->rel_residual = bb > 0 ? sqrt(P->h_sc[2] / bb) : 0.0;
   res->converged = res->rel_residual <= P->opt.tol;
-  res->bytes_moved = spmv_fp64 * P->bytes_residual + fp64_iters * P->bytes_fp64_iter + spmv_inner * P->bytes_inner_iter;
+  res->bytes_moved = residuals * P->bytes_residual + iters * P->bytes_iter;
   res->delta16 = P->delta16 ? 1 : 0;
   if (!res->converged) {
     set_error("CG stopped at relative residual " + std::to_string(res->rel_residual));

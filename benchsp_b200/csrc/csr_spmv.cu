@@ -83,9 +83,24 @@ __global__ void __launch_bounds__(256) csr_vector_kernel(int32_t rows, const int
     const int64_t r = base + (threadIdx.x & 31) / LPR;
     const bool active = r < rows;
     const int32_t s = active ? rowPtr[r] : 0, e = active ? rowPtr[r + 1] : 0;
+    // The first kFirst entries of each lane are loaded together, then their x
+    // gathers together: the rowPtr -> column -> x chain is paid once per
+    // kFirst entries instead of once per entry.
+    constexpr int kFirst = LPR == 1 ? 8 : 4;
+    int32_t c[kFirst];
+    V a[kFirst];
+#pragma unroll
+    for (int k = 0; k < kFirst; ++k) {
+      const int32_t j = s + sub + k * LPR;
+      c[k] = j < e ? colIdx[j] : -1;
+      a[k] = j < e ? val[j] : V(0);
+    }
     A sum = A(0);
+#pragma unroll
+    for (int k = 0; k < kFirst; ++k)
+      if (c[k] >= 0) sum = fma(to_acc<V>(a[k]), to_acc<V>(__ldg(&x[c[k]])), sum);
 #pragma unroll 4
-    for (int32_t j = s + sub; j < e; j += LPR)
+    for (int32_t j = s + sub + kFirst * LPR; j < e; j += LPR)
       sum = fma(to_acc<V>(val[j]), to_acc<V>(__ldg(&x[colIdx[j]])), sum);
 #pragma unroll
     for (int o = LPR / 2; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o, LPR);
@@ -266,12 +281,14 @@ static bsp_status launch_scalar(int32_t rows, const int32_t *rp, const int32_t *
   return BSP_OK;
 }
 
-// Lanes per row from the mean row length: the smallest power of two >= mean,
-// clamped to [2, 32].
+// Lanes per row from the mean row length: one lane per row up to 8 entries
+// (those are loaded together), then the smallest power of two >= mean/4,
+// up to 32.
 int auto_lanes(int32_t rows, int32_t nnz) {
   const double mean = rows > 0 ? (double)nnz / rows : 0.0;
+  if (mean <= 8.0) return 1;
   int l = 2;
-  while (l < 32 && l < mean) l <<= 1;
+  while (l < 32 && 4.0 * l < mean) l <<= 1;
   return l;
 }
 

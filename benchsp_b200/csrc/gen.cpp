@@ -183,22 +183,32 @@ void distinct_draws(uint64_t seed, uint64_t stream, uint64_t row, int64_t count,
   }
 }
 
-uint64_t block_mask(uint64_t seed, int64_t br, int k, int bs, double lo, double hi) {
+struct BlockMask {
+  uint64_t w[4] = {0, 0, 0, 0};
+  bool get(int e) const { return (w[e >> 6] >> (e & 63)) & 1; }
+  void set(int e) { w[e >> 6] |= 1ull << (e & 63); }
+  bool empty() const { return !(w[0] | w[1] | w[2] | w[3]); }
+};
+
+BlockMask block_mask(uint64_t seed, int64_t br, int k, int bs, double lo, double hi) {
   const int ne = bs * bs;
   const double p = lo + (hi - lo) * u01(h3(seed, kStreamFill, ((uint64_t)br << 8) | (uint64_t)k));
-  uint64_t mask = 0;
-  for (int e = 0; e < ne; ++e)
-    if (u01(h3(seed, kStreamMask, ((uint64_t)br << 14) | ((uint64_t)k << 7) | (uint64_t)e)) < p)
-      mask |= 1ull << e;
-  if (mask == 0) mask = 1ull << (h3(seed, kStreamMask, ~(uint64_t)br ^ (uint64_t)k) % ne);
-  return mask;
+  BlockMask m;
+  for (int e = 0; e < ne; ++e) {
+    const uint64_t idx = bs <= 8 ? (((uint64_t)br << 14) | ((uint64_t)k << 7) | (uint64_t)e)
+                                 : (((uint64_t)br << 16) | ((uint64_t)k << 8) | (uint64_t)e);
+    if (u01(h3(seed, kStreamMask, idx)) < p) m.set(e);
+  }
+  if (m.empty()) m.set((int)(h3(seed, kStreamMask, ~(uint64_t)br ^ (uint64_t)k) % ne));
+  return m;
 }
 }  // namespace
 
 extern "C" bsp_status bsp_gen_random_bsr(int32_t nbr, int32_t bs, int32_t per_row, double fill_lo,
                                          double fill_hi, uint64_t seed, int32_t *rows, int64_t *nnz,
                                          int32_t *rowPtr, int32_t *colIdx, double *values) {
-  if (nbr <= 0 || (bs != 4 && bs != 8) || per_row <= 0 || per_row > 255 || !rows || !nnz) return BSP_ERR_INVALID;
+  if (nbr <= 0 || (bs != 4 && bs != 8 && bs != 16) || per_row <= 0 || per_row > 255 || !rows || !nnz)
+    return BSP_ERR_INVALID;
   const int64_t n = (int64_t)nbr * bs;
   if (n > INT32_MAX) return BSP_ERR_INVALID;
   std::vector<int32_t> cnt(n, 0);
@@ -209,8 +219,9 @@ extern "C" bsp_status bsp_gen_random_bsr(int32_t nbr, int32_t bs, int32_t per_ro
     for (int64_t br = 0; br < nbr; ++br) {
       distinct_draws(seed, kStreamCol, (uint64_t)br, per_row, nbr, bc);
       for (int k = 0; k < (int)bc.size(); ++k) {
-        const uint64_t mask = block_mask(seed, br, k, bs, fill_lo, fill_hi);
-        for (int i = 0; i < bs; ++i) cnt[br * bs + i] += __builtin_popcountll((mask >> (i * bs)) & ((1ull << bs) - 1));
+        const BlockMask mask = block_mask(seed, br, k, bs, fill_lo, fill_hi);
+        for (int i = 0; i < bs; ++i)
+          for (int j = 0; j < bs; ++j) cnt[br * bs + i] += mask.get(i * bs + j);
       }
     }
   }
@@ -222,7 +233,7 @@ extern "C" bsp_status bsp_gen_random_bsr(int32_t nbr, int32_t bs, int32_t per_ro
 #pragma omp parallel
   {
     std::vector<int32_t> bc;
-    std::vector<uint64_t> masks;
+    std::vector<BlockMask> masks;
 #pragma omp for schedule(static)
     for (int64_t br = 0; br < nbr; ++br) {
       distinct_draws(seed, kStreamCol, (uint64_t)br, per_row, nbr, bc);
@@ -233,7 +244,7 @@ extern "C" bsp_status bsp_gen_random_bsr(int32_t nbr, int32_t bs, int32_t per_ro
         int64_t kk = rowPtr[row];
         for (int k = 0; k < (int)bc.size(); ++k)
           for (int j = 0; j < bs; ++j)
-            if ((masks[k] >> (i * bs + j)) & 1) {
+            if (masks[k].get(i * bs + j)) {
               colIdx[kk] = (int32_t)((int64_t)bc[k] * bs + j);
               values[kk] = normal(seed, kStreamVal, (uint64_t)kk);
               ++kk;
@@ -288,5 +299,88 @@ extern "C" bsp_status bsp_gen_uniform(int64_t n, uint64_t seed, double *x) {
   if (n < 0 || (n > 0 && !x)) return BSP_ERR_INVALID;
 #pragma omp parallel for schedule(static)
   for (int64_t i = 0; i < n; ++i) x[i] = 2.0 * u01(h3(seed, kStreamX, (uint64_t)i)) - 1.0;
+  return BSP_OK;
+}
+
+// Power-law graph for the SpMM benchmark: out-degrees ~ Zipf(alpha) on
+// [1, d_max] with d_max chosen so the mean degree is `mean_deg` (bisection),
+// distinct uniform targets, values 1/degree (row-stochastic).
+extern "C" bsp_status bsp_gen_graph(int32_t n, double alpha, double mean_deg, uint64_t seed, int32_t *rows,
+                                    int64_t *nnz, int32_t *rowPtr, int32_t *colIdx, double *values) {
+  if (n <= 0 || alpha <= 1.0 || mean_deg < 1.0 || !rows || !nnz) return BSP_ERR_INVALID;
+  // prefix sums of k^-alpha and k^(1-alpha): mean(dmax) = S1[dmax] / S0[dmax]
+  std::vector<double> S0(n + 1, 0.0), S1(n + 1, 0.0);
+  for (int64_t k = 1; k <= n; ++k) {
+    const double p = pow((double)k, -alpha);
+    S0[k] = S0[k - 1] + p;
+    S1[k] = S1[k - 1] + p * (double)k;
+  }
+  auto mean_for = [&](int64_t dmax) { return S1[dmax] / S0[dmax]; };
+  int64_t lo = 1, hi = n;
+  if (mean_for(hi) < mean_deg) return BSP_ERR_INVALID;
+  while (hi - lo > 1) {
+    const int64_t mid = (lo + hi) / 2;
+    (mean_for(mid) < mean_deg ? lo : hi) = mid;
+  }
+  const int64_t dmax = hi;
+  std::vector<double> cdf(dmax);
+  double acc = 0.0;
+  for (int64_t k = 1; k <= dmax; ++k) {
+    acc += pow((double)k, -alpha);
+    cdf[k - 1] = acc;
+  }
+  for (auto &c : cdf) c /= acc;
+  std::vector<int32_t> cnt(n);
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < n; ++i) {
+    const double u = u01(h3(seed, kStreamLen, (uint64_t)i));
+    cnt[i] = (int32_t)(std::lower_bound(cdf.begin(), cdf.end(), u) - cdf.begin()) + 1;
+  }
+  *rows = n;
+  const int64_t total = prefix(cnt, rowPtr);
+  *nnz = total;
+  if (total > INT32_MAX) return BSP_ERR_INVALID;
+  if (!rowPtr) return BSP_OK;
+#pragma omp parallel
+  {
+    std::vector<int32_t> cols;
+#pragma omp for schedule(dynamic, 1024)
+    for (int64_t i = 0; i < n; ++i) {
+      distinct_draws(seed, kStreamCol, (uint64_t)i, cnt[i], n, cols);
+      int64_t k = rowPtr[i];
+      for (int32_t c : cols) {
+        colIdx[k] = c;
+        values[k] = 1.0 / (double)cnt[i];
+        ++k;
+      }
+    }
+  }
+  return BSP_OK;
+}
+
+// Banded matrix: row i holds columns [i - (width-1)/2, i + width/2] clipped to
+// [0, n), values N(0, 1).
+extern "C" bsp_status bsp_gen_banded(int32_t n, int32_t width, uint64_t seed, int32_t *rows, int64_t *nnz,
+                                     int32_t *rowPtr, int32_t *colIdx, double *values) {
+  if (n <= 0 || width <= 0 || !rows || !nnz) return BSP_ERR_INVALID;
+  const int32_t lo = (width - 1) / 2, hi = width / 2;
+  std::vector<int32_t> cnt(n);
+  for (int64_t i = 0; i < n; ++i) {
+    const int64_t a = std::max<int64_t>(0, i - lo), b = std::min<int64_t>(n - 1, i + hi);
+    cnt[i] = (int32_t)(b - a + 1);
+  }
+  *rows = n;
+  const int64_t total = prefix(cnt, rowPtr);
+  *nnz = total;
+  if (total > INT32_MAX) return BSP_ERR_INVALID;
+  if (!rowPtr) return BSP_OK;
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < n; ++i) {
+    int64_t k = rowPtr[i];
+    for (int64_t c = std::max<int64_t>(0, i - lo); c <= std::min<int64_t>(n - 1, i + hi); ++c, ++k) {
+      colIdx[k] = (int32_t)c;
+      values[k] = normal(seed, kStreamVal, (uint64_t)k);
+    }
+  }
   return BSP_OK;
 }

@@ -1,0 +1,746 @@
+// SpMM C = alpha*A*B + beta*C with A sparse, B and C dense row-major.
+//
+// Replaces the reference's SMaT-style FP16 SpMM (mmaSmatKernelfp16 /
+// smatSpmmfp16, src/smat.cu:22-201): one warp per 16x8 C tile, a 16x16 A
+// block and a 16x8 B tile copied to shared memory, ldmatrix and
+// mma.sync m16n8k16 with FP16 accumulation.  (It also divides an already
+// block-level column index by 16 again, smat.cu:49, addresses B correctly
+// only for K = 16, smat.cu:62-64, and never writes its output.)  Two paths:
+//
+//  * CSR SpMM (any sparsity): one warp per row; the row's column indices and
+//    values are loaded 32 at a time and broadcast by shuffle; every lane owns
+//    CPL consecutive columns of B/C and streams its slice of each gathered B
+//    row with one vector load; FP32 accumulation, FP32 C.
+//  * Block SpMM (16x16 tiles, for matrices whose tiles are dense): one warp
+//    per (block-row, 8*NT columns).  Lane 0 stages every A tile (512 B) and
+//    the 16 matching B row segments with cp.async.bulk (the TMA copy engine)
+//    into a STAGES-deep shared-memory ring completed on mbarriers; the warp
+//    reads fragments with ldmatrix (.trans for B) and issues
+//    mma.sync.m16n8k16 with FP32 accumulators.  Every wait is bounded: on
+//    timeout the kernel records an error, waits (bounded) for its own copies
+//    and returns.
+#include "bsp_internal.cuh"
+#include "util.cuh"
+
+namespace bsp {
+
+template <typename T> __device__ __forceinline__ float sp_to_float(T v);
+template <> __device__ __forceinline__ float sp_to_float<float>(float v) { return v; }
+template <> __device__ __forceinline__ float sp_to_float<__half>(__half v) { return __half2float(v); }
+template <> __device__ __forceinline__ float sp_to_float<__nv_bfloat16>(__nv_bfloat16 v) { return __bfloat162float(v); }
+
+// CPL consecutive elements of type T as one vector load.
+template <typename T, int CPL>
+__device__ __forceinline__ void load_cols(const T *p, float (&out)[CPL]) {
+  constexpr int BYTES = CPL * (int)sizeof(T);
+  if constexpr (BYTES == 16) {
+    const uint4 u = __ldg(reinterpret_cast<const uint4 *>(p));
+    const T *t = reinterpret_cast<const T *>(&u);
+#pragma unroll
+    for (int k = 0; k < CPL; ++k) out[k] = sp_to_float<T>(t[k]);
+  } else if constexpr (BYTES == 8) {
+    const uint2 u = __ldg(reinterpret_cast<const uint2 *>(p));
+    const T *t = reinterpret_cast<const T *>(&u);
+#pragma unroll
+    for (int k = 0; k < CPL; ++k) out[k] = sp_to_float<T>(t[k]);
+  } else if constexpr (BYTES == 4) {
+    const unsigned u = __ldg(reinterpret_cast<const unsigned *>(p));
+    const T *t = reinterpret_cast<const T *>(&u);
+#pragma unroll
+    for (int k = 0; k < CPL; ++k) out[k] = sp_to_float<T>(t[k]);
+  } else {
+#pragma unroll
+    for (int k = 0; k < CPL; ++k) out[k] = sp_to_float<T>(p[k]);
+  }
+}
+
+// Warp per row; lane owns columns c0 + lane*CPL .. +CPL of each 32*CPL chunk.
+template <typename T, int CPL>
+__global__ void __launch_bounds__(256) spmm_csr_kernel(int32_t rows, int32_t N, const int32_t *__restrict__ rowPtr,
+                                                       const int32_t *__restrict__ colIdx,
+                                                       const T *__restrict__ val, const T *__restrict__ B,
+                                                       int64_t ldb, float *__restrict__ C, int64_t ldc,
+                                                       float alpha, float beta) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < rows; r += nwarps) {
+    const int32_t s = rowPtr[r], e = rowPtr[r + 1];
+    for (int32_t c0 = 0; c0 < N; c0 += 32 * CPL) {
+      const int32_t cl = c0 + lane * CPL;
+      const bool own = cl < N;  // N is a multiple of CPL
+      float acc[CPL];
+#pragma unroll
+      for (int k = 0; k < CPL; ++k) acc[k] = 0.f;
+      for (int32_t j0 = s; j0 < e; j0 += 32) {
+        const int32_t j = j0 + lane;
+        const int32_t cj = j < e ? colIdx[j] : 0;
+        const float vj = j < e ? sp_to_float<T>(val[j]) : 0.f;
+        const int cnt = e - j0 < 32 ? e - j0 : 32;
+        int t = 0;
+        for (; t + 4 <= cnt; t += 4) {  // four B rows in flight
+          float b[4][CPL];
+          float v[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const int32_t c = __shfl_sync(0xffffffffu, cj, t + u);
+            v[u] = __shfl_sync(0xffffffffu, vj, t + u);
+            if (own) load_cols<T, CPL>(B + (int64_t)c * ldb + cl, b[u]);
+          }
+#pragma unroll
+          for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int k = 0; k < CPL; ++k) acc[k] = fmaf(v[u], b[u][k], acc[k]);
+        }
+        for (; t < cnt; ++t) {
+          const int32_t c = __shfl_sync(0xffffffffu, cj, t);
+          const float v = __shfl_sync(0xffffffffu, vj, t);
+          float b[CPL];
+          if (own) {
+            load_cols<T, CPL>(B + (int64_t)c * ldb + cl, b);
+#pragma unroll
+            for (int k = 0; k < CPL; ++k) acc[k] = fmaf(v, b[k], acc[k]);
+          }
+        }
+      }
+      if (own) {
+        float *cp = C + r * ldc + cl;
+#pragma unroll
+        for (int k = 0; k < CPL; ++k) {
+          float o = alpha * acc[k];
+          if (beta != 0.f) o += beta * cp[k];
+          cp[k] = o;
+        }
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Block (16x16) tensor-core SpMM.
+constexpr int kTS = 16;            // tile side
+constexpr int kStages = 4;         // shared-memory ring depth per warp
+constexpr int kWarpsPerCta = 4;
+constexpr long long kSpinLimit = 1ll << 24;  // bounded mbarrier waits
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait; returns false on timeout.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity) {
+  for (long long i = 0; i < kSpinLimit; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void ldm_x4(uint32_t (&r)[4], const void *p) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(smem_u32(p)));
+}
+__device__ __forceinline__ void ldm_x4_trans(uint32_t (&r)[4], const void *p) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(smem_u32(p)));
+}
+template <typename T>
+__device__ __forceinline__ void mma16816(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1);
+template <>
+__device__ __forceinline__ void mma16816<__half>(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+template <>
+__device__ __forceinline__ void mma16816<__nv_bfloat16>(float (&c)[4], const uint32_t (&a)[4], uint32_t b0,
+                                                        uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// Per-warp ring slot: A tile (16x16) then B rows (16 x 8*NT) at a padded
+// row stride so the 8 rows an ldmatrix reads fall in different banks.
+template <int NT>
+struct SpmmStage {
+  static constexpr int kBStride = 8 * NT * 2 + 16;  // bytes per staged B row
+  alignas(128) unsigned char a[kTS * kTS * 2];
+  alignas(16) unsigned char b[kTS * kBStride];
+};
+
+template <typename T, int NT>
+__global__ void __launch_bounds__(kWarpsPerCta * 32) spmm_block_kernel(
+    int32_t M, int32_t K, int32_t N, int32_t nbr, const int32_t *__restrict__ bptr,
+    const int32_t *__restrict__ bcol, const T *__restrict__ bval, const T *__restrict__ B, int64_t ldb,
+    float *__restrict__ C, int64_t ldc, float alpha, float beta, int32_t *__restrict__ err) {
+  __shared__ SpmmStage<NT> ring[kWarpsPerCta][kStages];
+  __shared__ uint64_t bars[kWarpsPerCta][kStages];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  SpmmStage<NT> *st = ring[w];
+  uint64_t *bar = bars[w];
+  if (lane == 0) {
+    for (int i = 0; i < kStages; ++i) mbar_init(&bar[i], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncwarp();
+  const int nchunks = N / (8 * NT);
+  const int64_t items = (int64_t)nbr * nchunks;
+  const int64_t gw = (int64_t)blockIdx.x * kWarpsPerCta + w;
+  const int64_t nw = (int64_t)gridDim.x * kWarpsPerCta;
+  unsigned uses[kStages];
+#pragma unroll
+  for (int i = 0; i < kStages; ++i) uses[i] = 0;
+  const int g = lane >> 2, t4 = lane & 3;
+  for (int64_t item = gw; item < items; item += nw) {
+    const int32_t br = (int32_t)(item / nchunks);
+    const int32_t n0 = (int32_t)(item % nchunks) * 8 * NT;
+    const int32_t k0 = bptr[br], k1 = bptr[br + 1];
+    float acc[NT][4];
+#pragma unroll
+    for (int j = 0; j < NT; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
+    // producer (lane 0): stage tile k into slot k % kStages
+    auto issue = [&](int32_t k) {
+      const int slot = (k - k0) % kStages;
+      SpmmStage<NT> &S = st[slot];
+      const int32_t bc = bcol[k];
+      int rows_in = K - bc * kTS;
+      rows_in = rows_in > kTS ? kTS : rows_in;
+      const unsigned bytes = kTS * kTS * 2 + (unsigned)rows_in * (8 * NT * 2);
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      mbar_expect_tx(&bar[slot], bytes);
+      bulk_g2s(S.a, bval + (int64_t)k * kTS * kTS, kTS * kTS * 2, &bar[slot]);
+      for (int rr = 0; rr < rows_in; ++rr)
+        bulk_g2s(S.b + rr * SpmmStage<NT>::kBStride, B + ((int64_t)bc * kTS + rr) * ldb + n0, 8 * NT * 2,
+                 &bar[slot]);
+    };
+    // rows of B beyond K are never copied: zero them (generic proxy) and
+    // order those writes before the slot's next asynchronous copies
+    auto zero_tail = [&](SpmmStage<NT> &S, int32_t k) {
+      const int32_t bc = bcol[k];
+      const int64_t rows_in = (int64_t)K - (int64_t)bc * kTS;
+      if (rows_in < kTS) {
+        constexpr int kWords = SpmmStage<NT>::kBStride / 4;
+        uint32_t *tail = reinterpret_cast<uint32_t *>(S.b + rows_in * SpmmStage<NT>::kBStride);
+        for (int i = lane; i < (kTS - (int)rows_in) * kWords; i += 32) tail[i] = 0u;
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncwarp();
+      }
+    };
+    const int32_t nk = k1 - k0;
+    for (int32_t k = k0; k < k0 + (nk < kStages ? nk : kStages); ++k) {
+      zero_tail(st[(k - k0) % kStages], k);
+      if (lane == 0) issue(k);
+    }
+    bool ok = true;
+    for (int32_t k = k0; k < k1; ++k) {
+      const int slot = (k - k0) % kStages;
+      if (!mbar_wait(&bar[slot], uses[slot] & 1u)) {
+        ok = false;
+        break;
+      }
+      uses[slot]++;
+      SpmmStage<NT> &S = st[slot];
+      uint32_t a[4];
+      ldm_x4(a, S.a + ((lane & 15) * kTS + (lane >> 4) * 8) * 2);
+#pragma unroll
+      for (int j = 0; j < NT; j += 2) {
+        uint32_t b[4];
+        ldm_x4_trans(b, S.b + (lane & 15) * SpmmStage<NT>::kBStride + (8 * j + 8 * (lane >> 4)) * 2);
+        mma16816<T>(acc[j], a, b[0], b[1]);
+        mma16816<T>(acc[j + 1], a, b[2], b[3]);
+      }
+      __syncwarp();  // every lane has read the slot before it is refilled
+      const int32_t kn = k + kStages;
+      if (kn < k1) {
+        zero_tail(S, kn);
+        if (lane == 0) issue(kn);
+      }
+    }
+    if (!ok) {
+      if (lane == 0) atomicExch(err, 1);
+      // let this warp's own copies in flight land (bounded), then stop
+      for (int i = 0; i < kStages; ++i) (void)mbar_wait(&bar[i], uses[i] & 1u);
+      return;
+    }
+    // epilogue: C rows br*16 + g and + 8, columns n0 + 8j + 2*t4
+#pragma unroll
+    for (int j = 0; j < NT; ++j) {
+      const int32_t col = n0 + 8 * j + 2 * t4;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int64_t row = (int64_t)br * kTS + g + 8 * h;
+        if (row < M) {
+          float *cp = C + row * ldc + col;
+          float o0 = alpha * acc[j][2 * h], o1 = alpha * acc[j][2 * h + 1];
+          if (beta != 0.f) {
+            o0 += beta * cp[0];
+            o1 += beta * cp[1];
+          }
+          cp[0] = o0;
+          cp[1] = o1;
+        }
+      }
+    }
+  }
+}
+
+template <typename T>
+__global__ void tiles_to_lp_kernel(int64_t n, const double *__restrict__ v, T *__restrict__ out);
+template <>
+__global__ void tiles_to_lp_kernel<__half>(int64_t n, const double *__restrict__ v, __half *__restrict__ out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = __double2half(v[i]);
+}
+template <>
+__global__ void tiles_to_lp_kernel<__nv_bfloat16>(int64_t n, const double *__restrict__ v,
+                                                  __nv_bfloat16 *__restrict__ out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = __float2bfloat16_rn((float)v[i]);
+}
+
+template <typename T, int CPL>
+static bsp_status launch_spmm_csr(int32_t rows, int32_t N, const int32_t *rp, const int32_t *ci, const void *val,
+                                  const void *B, int64_t ldb, float *C, int64_t ldc, float a, float b,
+                                  cudaStream_t s) {
+  int64_t blocks = ceil_div(rows, 8);
+  const int64_t cap = (int64_t)sm_count() * 32;
+  if (blocks > cap) blocks = cap;
+  if (blocks < 1) blocks = 1;
+  spmm_csr_kernel<T, CPL><<<(unsigned)blocks, 256, 0, s>>>(rows, N, rp, ci, (const T *)val, (const T *)B, ldb, C,
+                                                           ldc, a, b);
+  BSP_LAUNCH_CHECK();
+  return BSP_OK;
+}
+
+template <typename T>
+static bsp_status spmm_csr_typed(int32_t rows, int32_t N, const int32_t *rp, const int32_t *ci, const void *val,
+                                 const void *B, int64_t ldb, float *C, int64_t ldc, float a, float b,
+                                 cudaStream_t s) {
+  // widest per-lane vector that divides N/32 and keeps B loads aligned
+  const size_t es = sizeof(T);
+  const bool al16 = ((uintptr_t)B % 16 == 0) && ((ldb * es) % 16 == 0);
+  const bool al8 = ((uintptr_t)B % 8 == 0) && ((ldb * es) % 8 == 0);
+  if (es == 2) {
+    if (N % 256 == 0 && al16) return launch_spmm_csr<T, 8>(rows, N, rp, ci, val, B, ldb, C, ldc, a, b, s);
+    if (N % 128 == 0 && al8) return launch_spmm_csr<T, 4>(rows, N, rp, ci, val, B, ldb, C, ldc, a, b, s);
+    if (N % 64 == 0 && ((uintptr_t)B % 4 == 0) && ((ldb * es) % 4 == 0))
+      return launch_spmm_csr<T, 2>(rows, N, rp, ci, val, B, ldb, C, ldc, a, b, s);
+    return launch_spmm_csr<T, 1>(rows, N, rp, ci, val, B, ldb, C, ldc, a, b, s);
+  }
+  if (N % 128 == 0 && al16) return launch_spmm_csr<T, 4>(rows, N, rp, ci, val, B, ldb, C, ldc, a, b, s);
+  if (N % 64 == 0 && al8) return launch_spmm_csr<T, 2>(rows, N, rp, ci, val, B, ldb, C, ldc, a, b, s);
+  return launch_spmm_csr<T, 1>(rows, N, rp, ci, val, B, ldb, C, ldc, a, b, s);
+}
+
+}  // namespace bsp
+
+using namespace bsp;
+
+extern "C" bsp_status bsp_spmm_csr(int32_t rows, int32_t cols, int32_t nnz, const int32_t *rowPtr,
+                                   const int32_t *colIdx, const void *values, bsp_dtype dtype, const void *B,
+                                   int32_t N, int64_t ldb, float *C, int64_t ldc, float alpha, float beta,
+                                   bsp_stream_t stream) {
+  clear_error();
+  BSP_CHECK_ARG(rows >= 0 && cols >= 0 && nnz >= 0 && N >= 0, "negative size");
+  if (rows == 0 || N == 0) return BSP_OK;
+  BSP_CHECK_ARG(rowPtr && C && (nnz == 0 || (colIdx && values && B)), "null pointer");
+  BSP_CHECK_ARG(ldb >= N && ldc >= N, "leading dimension smaller than N");
+  cudaStream_t s = as_stream(stream);
+  switch (dtype) {
+    case BSP_F16:
+      return spmm_csr_typed<__half>(rows, N, rowPtr, colIdx, values, B, ldb, C, ldc, alpha, beta, s);
+    case BSP_BF16:
+      return spmm_csr_typed<__nv_bfloat16>(rows, N, rowPtr, colIdx, values, B, ldb, C, ldc, alpha, beta, s);
+    case BSP_F32:
+      return spmm_csr_typed<float>(rows, N, rowPtr, colIdx, values, B, ldb, C, ldc, alpha, beta, s);
+    default:
+      BSP_FAIL(BSP_ERR_UNSUPPORTED, "SpMM takes F16, BF16 or F32 values");
+  }
+}
+
+extern "C" bsp_status bsp_smat_create(int32_t rows, int32_t cols, int32_t nnz, const int32_t *rowPtr,
+                                      const int32_t *colIdx, const double *values, bsp_dtype dtype, bsp_smat *out,
+                                      bsp_stream_t stream) {
+  clear_error();
+  BSP_CHECK_ARG(out, "null output");
+  BSP_CHECK_ARG(dtype == BSP_F16 || dtype == BSP_BF16, "block SpMM takes F16 or BF16");
+  cudaStream_t s = as_stream(stream);
+  bsp_smat m{};
+  m.rows = rows;
+  m.cols = cols;
+  m.nnz = nnz;
+  m.dtype = dtype;
+  BSP_TRY(bsp_csr2bcsr(rows, cols, nnz, rowPtr, colIdx, values, kTS, kTS, 0, &m.tiles, stream));
+  const int64_t ne = (int64_t)m.tiles.nonzeroBlocks * kTS * kTS;
+  BSP_TRY(dalloc(reinterpret_cast<uint16_t **>(&m.tile_val), (size_t)(ne > 0 ? ne : 1), s));
+  BSP_TRY(dalloc(&m.err, 1, s));
+  BSP_CUDA(cudaMemsetAsync(m.err, 0, sizeof(int32_t), s));
+  if (ne > 0) {
+    int64_t g = ceil_div(ne, 256);
+    if (g > (int64_t)sm_count() * 32) g = (int64_t)sm_count() * 32;
+    if (dtype == BSP_F16)
+      tiles_to_lp_kernel<__half><<<(unsigned)g, 256, 0, s>>>(ne, m.tiles.values, (__half *)m.tile_val);
+    else
+      tiles_to_lp_kernel<__nv_bfloat16><<<(unsigned)g, 256, 0, s>>>(ne, m.tiles.values,
+                                                                    (__nv_bfloat16 *)m.tile_val);
+    BSP_LAUNCH_CHECK();
+  }
+  // the FP64 tile values are not needed by the SpMM
+  dfree(m.tiles.values, s);
+  m.fill = m.tiles.nonzeroBlocks > 0 ? (double)nnz / ((double)m.tiles.nonzeroBlocks * kTS * kTS) : 0.0;
+  BSP_CUDA(cudaStreamSynchronize(s));
+  *out = m;
+  return BSP_OK;
+}
+
+extern "C" bsp_status bsp_smat_free(bsp_smat *m) {
+  clear_error();
+  if (!m) return BSP_OK;
+  cudaStream_t s = 0;
+  if (m->tile_val) cudaFreeAsync(m->tile_val, s);
+  m->tile_val = nullptr;
+  dfree(m->err, s);
+  BSP_TRY(bsp_bcsr_free(&m->tiles));
+  return BSP_OK;
+}
+
+extern "C" bsp_status bsp_smat_spmm(const bsp_smat *m, const void *B, int32_t N, int64_t ldb, float *C,
+                                    int64_t ldc, float alpha, float beta, bsp_stream_t stream) {
+  clear_error();
+  BSP_CHECK_ARG(m && B && C, "null pointer");
+  BSP_CHECK_ARG(N > 0 && N % 32 == 0, "N must be a positive multiple of 32");
+  BSP_CHECK_ARG(ldb >= N && ldc >= N, "leading dimension smaller than N");
+  // cp.async.bulk needs 16-byte aligned sources and sizes
+  BSP_CHECK_ARG((uintptr_t)B % 16 == 0 && (ldb * 2) % 16 == 0, "B must be 16-byte aligned with ldb % 8 == 0");
+  BSP_CHECK_ARG((uintptr_t)m->tile_val % 16 == 0, "tile values must be 16-byte aligned");
+  if (m->tiles.rowRegions == 0) return BSP_OK;
+  cudaStream_t s = as_stream(stream);
+  const int nt = (N % 64 == 0) ? 8 : 4;
+  const int64_t items = (int64_t)m->tiles.rowRegions * (N / (8 * nt));
+  int64_t blocks = ceil_div(items, kWarpsPerCta);
+  const int64_t cap = (int64_t)sm_count() * 16;
+  if (blocks > cap) blocks = cap;
+  const int32_t M = m->rows, K = m->cols, nbr = m->tiles.rowRegions;
+#define BSP_SMAT_LAUNCH(T, NT)                                                                                 \
+  spmm_block_kernel<T, NT><<<(unsigned)blocks, kWarpsPerCta * 32, 0, s>>>(                                   \
+      M, K, N, nbr, m->tiles.bcsrRowPtr, m->tiles.bcsrcolIdx, (const T *)m->tile_val, (const T *)B, ldb, C, ldc, \
+      alpha, beta, m->err)
+  if (m->dtype == BSP_F16) {
+    if (nt == 8)
+      BSP_SMAT_LAUNCH(__half, 8);
+    else
+      BSP_SMAT_LAUNCH(__half, 4);
+  } else {
+    if (nt == 8)
+      BSP_SMAT_LAUNCH(__nv_bfloat16, 8);
+    else
+      BSP_SMAT_LAUNCH(__nv_bfloat16, 4);
+  }
+#undef BSP_SMAT_LAUNCH
+  BSP_LAUNCH_CHECK();
+  return BSP_OK;
+}
+
+extern "C" bsp_status bsp_smat_check(const bsp_smat *m, bsp_stream_t stream) {
+  clear_error();
+  BSP_CHECK_ARG(m, "null pointer");
+  int32_t e = 0;
+  BSP_TRY(read_i32(m->err, &e, as_stream(stream)));
+  if (e) BSP_FAIL(BSP_ERR_TIMEOUT, "a bounded copy wait of the block SpMM timed out");
+  return BSP_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Row-split CSR SpMM for power-law rows: a plan cuts every row longer than
+// `chunk` nonzeros into chunks; one warp per chunk.  Chunks of a split row
+// write their partial rows to a scratch buffer and a second kernel sums them
+// in chunk order (deterministic, no atomics).
+namespace bsp {
+
+__global__ void spmm_plan_count_kernel(int32_t rows, const int32_t *__restrict__ rowPtr, int32_t chunk,
+                                       int32_t *__restrict__ nch, int32_t *__restrict__ npart) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t len = rowPtr[r + 1] - rowPtr[r];
+    const int32_t c = len > chunk ? (len + chunk - 1) / chunk : 1;
+    nch[r] = c;
+    npart[r] = c > 1 ? c : 0;
+  }
+}
+
+__global__ void spmm_plan_fill_kernel(int32_t rows, const int32_t *__restrict__ chunk_ptr,
+                                      int32_t *__restrict__ chunk_row) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += (int64_t)gridDim.x * blockDim.x)
+    for (int32_t c = chunk_ptr[r]; c < chunk_ptr[r + 1]; ++c) chunk_row[c] = (int32_t)r;
+}
+
+template <typename T, int CPL>
+__global__ void __launch_bounds__(256) spmm_chunk_kernel(int64_t nchunks, int32_t N, int32_t chunk,
+                                                         const int32_t *__restrict__ chunk_row,
+                                                         const int32_t *__restrict__ chunk_ptr,
+                                                         const int32_t *__restrict__ part_ptr,
+                                                         const int32_t *__restrict__ rowPtr,
+                                                         const int32_t *__restrict__ colIdx,
+                                                         const T *__restrict__ val, const T *__restrict__ B,
+                                                         int64_t ldb, float *__restrict__ C, int64_t ldc,
+                                                         float *__restrict__ part, float alpha, float beta) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < nchunks; w += nwarps) {
+    const int32_t r = chunk_row[w];
+    const int32_t ci = (int32_t)(w - chunk_ptr[r]);
+    const bool split = chunk_ptr[r + 1] - chunk_ptr[r] > 1;
+    const int32_t s0 = rowPtr[r], e0 = rowPtr[r + 1];
+    const int32_t s = split ? s0 + ci * chunk : s0;
+    const int32_t e = split ? min(s + chunk, e0) : e0;
+    for (int32_t c0 = 0; c0 < N; c0 += 32 * CPL) {
+      const int32_t cl = c0 + lane * CPL;
+      const bool own = cl < N;
+      float acc[CPL];
+#pragma unroll
+      for (int k = 0; k < CPL; ++k) acc[k] = 0.f;
+      for (int32_t j0 = s; j0 < e; j0 += 32) {
+        const int32_t j = j0 + lane;
+        const int32_t cj = j < e ? colIdx[j] : 0;
+        const float vj = j < e ? sp_to_float<T>(val[j]) : 0.f;
+        const int cnt = e - j0 < 32 ? e - j0 : 32;
+        int t = 0;
+        for (; t + 4 <= cnt; t += 4) {
+          float b[4][CPL];
+          float v[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const int32_t c = __shfl_sync(0xffffffffu, cj, t + u);
+            v[u] = __shfl_sync(0xffffffffu, vj, t + u);
+            if (own) load_cols<T, CPL>(B + (int64_t)c * ldb + cl, b[u]);
+          }
+#pragma unroll
+          for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int k = 0; k < CPL; ++k) acc[k] = fmaf(v[u], b[u][k], acc[k]);
+        }
+        for (; t < cnt; ++t) {
+          const int32_t c = __shfl_sync(0xffffffffu, cj, t);
+          const float v = __shfl_sync(0xffffffffu, vj, t);
+          float b[CPL];
+          if (own) {
+            load_cols<T, CPL>(B + (int64_t)c * ldb + cl, b);
+#pragma unroll
+            for (int k = 0; k < CPL; ++k) acc[k] = fmaf(v, b[k], acc[k]);
+          }
+        }
+      }
+      if (own) {
+        if (split) {
+          float *pp = part + ((int64_t)part_ptr[r] + ci) * N + cl;
+#pragma unroll
+          for (int k = 0; k < CPL; ++k) pp[k] = acc[k];
+        } else {
+          float *cp = C + (int64_t)r * ldc + cl;
+#pragma unroll
+          for (int k = 0; k < CPL; ++k) {
+            float o = alpha * acc[k];
+            if (beta != 0.f) o += beta * cp[k];
+            cp[k] = o;
+          }
+        }
+      }
+    }
+  }
+}
+
+// One warp per split row: C row = alpha * sum of its chunk partials (in order).
+__global__ void spmm_split_reduce_kernel(int32_t nsplit, const int32_t *__restrict__ split_rows,
+                                         const int32_t *__restrict__ chunk_ptr,
+                                         const int32_t *__restrict__ part_ptr, int32_t N,
+                                         const float *__restrict__ part, float *__restrict__ C, int64_t ldc,
+                                         float alpha, float beta) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < nsplit; i += nwarps) {
+    const int32_t r = split_rows[i];
+    const int32_t nc = chunk_ptr[r + 1] - chunk_ptr[r];
+    const float *pp = part + (int64_t)part_ptr[r] * N;
+    for (int32_t c = lane; c < N; c += 32) {
+      float acc = 0.f;
+      for (int32_t k = 0; k < nc; ++k) acc += pp[(int64_t)k * N + c];
+      float *cp = C + (int64_t)r * ldc + c;
+      float o = alpha * acc;
+      if (beta != 0.f) o += beta * *cp;
+      *cp = o;
+    }
+  }
+}
+
+__global__ void spmm_split_list_kernel(int32_t rows, const int32_t *__restrict__ chunk_ptr,
+                                       const int32_t *__restrict__ split_pos, int32_t *__restrict__ split_rows) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += (int64_t)gridDim.x * blockDim.x)
+    if (chunk_ptr[r + 1] - chunk_ptr[r] > 1) split_rows[split_pos[r]] = (int32_t)r;
+}
+
+__global__ void spmm_split_flag_kernel(int32_t rows, const int32_t *__restrict__ chunk_ptr,
+                                       int32_t *__restrict__ flag) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r <= rows; r += (int64_t)gridDim.x * blockDim.x)
+    flag[r] = r < rows && chunk_ptr[r + 1] - chunk_ptr[r] > 1;
+}
+
+}  // namespace bsp
+
+extern "C" bsp_status bsp_spmm_plan_create(int32_t rows, int32_t nnz, const int32_t *rowPtr, int32_t chunk,
+                                           bsp_spmm_plan *out, bsp_stream_t stream) {
+  clear_error();
+  BSP_CHECK_ARG(out && rowPtr && rows >= 0 && nnz >= 0, "bad argument");
+  BSP_CHECK_ARG(chunk >= 32, "chunk must be >= 32");
+  cudaStream_t s = as_stream(stream);
+  bsp_spmm_plan p{};
+  p.rows = rows;
+  p.chunk = chunk;
+  int32_t *flag = nullptr;
+  int64_t *tot = nullptr;
+  BSP_TRY(dalloc(&p.chunk_ptr, (size_t)rows + 1, s));
+  BSP_TRY(dalloc(&p.part_ptr, (size_t)rows + 1, s));
+  BSP_TRY(dalloc(&tot, 1, s));
+  BSP_CUDA(cudaMemsetAsync(p.chunk_ptr + rows, 0, sizeof(int32_t), s));
+  BSP_CUDA(cudaMemsetAsync(p.part_ptr + rows, 0, sizeof(int32_t), s));
+  const unsigned g = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div(rows + 1, 256), (int64_t)sm_count() * 32));
+  if (rows > 0) {
+    spmm_plan_count_kernel<<<g, 256, 0, s>>>(rows, rowPtr, chunk, p.chunk_ptr, p.part_ptr);
+    BSP_LAUNCH_CHECK();
+  }
+  BSP_TRY(exclusive_scan_i32(p.chunk_ptr, p.chunk_ptr, (int64_t)rows + 1, tot, s));
+  int64_t h = 0;
+  BSP_TRY(read_i64(tot, &h, s));
+  p.nchunks = h;
+  BSP_TRY(exclusive_scan_i32(p.part_ptr, p.part_ptr, (int64_t)rows + 1, tot, s));
+  BSP_TRY(read_i64(tot, &h, s));
+  p.nparts = h;
+  BSP_TRY(dalloc(&p.chunk_row, (size_t)(p.nchunks > 0 ? p.nchunks : 1), s));
+  if (rows > 0) {
+    spmm_plan_fill_kernel<<<g, 256, 0, s>>>(rows, p.chunk_ptr, p.chunk_row);
+    BSP_LAUNCH_CHECK();
+  }
+  BSP_TRY(dalloc(&flag, (size_t)rows + 1, s));
+  spmm_split_flag_kernel<<<g, 256, 0, s>>>(rows, p.chunk_ptr, flag);
+  BSP_LAUNCH_CHECK();
+  BSP_TRY(exclusive_scan_i32(flag, flag, (int64_t)rows + 1, tot, s));
+  BSP_TRY(read_i64(tot, &h, s));
+  p.nsplit = (int32_t)h;
+  BSP_TRY(dalloc(&p.split_rows, (size_t)(p.nsplit > 0 ? p.nsplit : 1), s));
+  if (rows > 0) {
+    spmm_split_list_kernel<<<g, 256, 0, s>>>(rows, p.chunk_ptr, flag, p.split_rows);
+    BSP_LAUNCH_CHECK();
+  }
+  dfree(flag, s);
+  dfree(tot, s);
+  BSP_CUDA(cudaStreamSynchronize(s));
+  *out = p;
+  return BSP_OK;
+}
+
+extern "C" bsp_status bsp_spmm_plan_free(bsp_spmm_plan *p) {
+  clear_error();
+  if (!p) return BSP_OK;
+  cudaStream_t s = 0;
+  dfree(p->chunk_ptr, s);
+  dfree(p->part_ptr, s);
+  dfree(p->chunk_row, s);
+  dfree(p->split_rows, s);
+  BSP_CUDA(cudaStreamSynchronize(s));
+  return BSP_OK;
+}
+
+namespace bsp {
+template <typename T, int CPL>
+static bsp_status launch_chunked(const bsp_spmm_plan *p, int32_t N, const int32_t *rp, const int32_t *ci,
+                                 const void *val, const void *B, int64_t ldb, float *C, int64_t ldc, float *part,
+                                 float a, float b, cudaStream_t s) {
+  int64_t blocks = ceil_div(p->nchunks, 8);
+  const int64_t cap = (int64_t)sm_count() * 32;
+  if (blocks > cap) blocks = cap;
+  if (blocks < 1) blocks = 1;
+  spmm_chunk_kernel<T, CPL><<<(unsigned)blocks, 256, 0, s>>>(p->nchunks, N, p->chunk, p->chunk_row, p->chunk_ptr,
+                                                             p->part_ptr, rp, ci, (const T *)val, (const T *)B, ldb,
+                                                             C, ldc, part, a, b);
+  BSP_LAUNCH_CHECK();
+  return BSP_OK;
+}
+
+template <typename T>
+static bsp_status chunked_typed(const bsp_spmm_plan *p, int32_t N, const int32_t *rp, const int32_t *ci,
+                                const void *val, const void *B, int64_t ldb, float *C, int64_t ldc, float *part,
+                                float a, float b, cudaStream_t s) {
+  const size_t es = sizeof(T);
+  const bool al16 = ((uintptr_t)B % 16 == 0) && ((ldb * es) % 16 == 0);
+  const bool al8 = ((uintptr_t)B % 8 == 0) && ((ldb * es) % 8 == 0);
+  if (es == 2) {
+    if (N % 256 == 0 && al16) return launch_chunked<T, 8>(p, N, rp, ci, val, B, ldb, C, ldc, part, a, b, s);
+    if (N % 128 == 0 && al8) return launch_chunked<T, 4>(p, N, rp, ci, val, B, ldb, C, ldc, part, a, b, s);
+    return launch_chunked<T, 1>(p, N, rp, ci, val, B, ldb, C, ldc, part, a, b, s);
+  }
+  if (N % 128 == 0 && al16) return launch_chunked<T, 4>(p, N, rp, ci, val, B, ldb, C, ldc, part, a, b, s);
+  return launch_chunked<T, 1>(p, N, rp, ci, val, B, ldb, C, ldc, part, a, b, s);
+}
+}  // namespace bsp
+
+extern "C" size_t bsp_spmm_plan_workspace(const bsp_spmm_plan *p, int32_t N) {
+  return p ? (size_t)p->nparts * (size_t)(N > 0 ? N : 0) * sizeof(float) : 0;
+}
+
+extern "C" bsp_status bsp_spmm_csr_planned(const bsp_spmm_plan *p, int32_t cols, int32_t nnz,
+                                           const int32_t *rowPtr, const int32_t *colIdx, const void *values,
+                                           bsp_dtype dtype, const void *B, int32_t N, int64_t ldb, float *C,
+                                           int64_t ldc, float alpha, float beta, void *workspace,
+                                           size_t workspace_bytes, bsp_stream_t stream) {
+  clear_error();
+  BSP_CHECK_ARG(p && rowPtr && C, "null pointer");
+  BSP_CHECK_ARG(N >= 0 && ldb >= N && ldc >= N, "bad N / leading dimensions");
+  if (p->rows == 0 || N == 0) return BSP_OK;
+  BSP_CHECK_ARG(nnz == 0 || (colIdx && values && B), "null pointer");
+  const size_t need = bsp_spmm_plan_workspace(p, N);
+  BSP_CHECK_ARG(workspace_bytes >= need && (need == 0 || workspace), "workspace too small");
+  cudaStream_t s = as_stream(stream);
+  float *part = reinterpret_cast<float *>(workspace);
+  bsp_status st;
+  switch (dtype) {
+    case BSP_F16:
+      st = chunked_typed<__half>(p, N, rowPtr, colIdx, values, B, ldb, C, ldc, part, alpha, beta, s);
+      break;
+    case BSP_BF16:
+      st = chunked_typed<__nv_bfloat16>(p, N, rowPtr, colIdx, values, B, ldb, C, ldc, part, alpha, beta, s);
+      break;
+    case BSP_F32:
+      st = chunked_typed<float>(p, N, rowPtr, colIdx, values, B, ldb, C, ldc, part, alpha, beta, s);
+      break;
+    default:
+      BSP_FAIL(BSP_ERR_UNSUPPORTED, "SpMM takes F16, BF16 or F32 values");
+  }
+  if (st != BSP_OK) return st;
+  if (p->nsplit > 0) {
+    int64_t blocks = ceil_div(p->nsplit, 8);
+    if (blocks > (int64_t)sm_count() * 32) blocks = (int64_t)sm_count() * 32;
+    spmm_split_reduce_kernel<<<(unsigned)blocks, 256, 0, s>>>(p->nsplit, p->split_rows, p->chunk_ptr, p->part_ptr,
+                                                              N, part, C, ldc, alpha, beta);
+    BSP_LAUNCH_CHECK();
+  }
+  return BSP_OK;
+}

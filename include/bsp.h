@@ -151,9 +151,10 @@ bsp_status bsp_bsr_free(bsp_bsr *m);
 
 typedef enum {
   BSP_BSR_AUTO = 0,
-  BSP_BSR_FFMA = 1, /* CUDA-core FP64 FMA, 16-byte coalesced block loads */
-  BSP_BSR_DMMA = 2, /* FP64 mma.sync m8n8k4 on the blocks */
-  BSP_BSR_ADAPTIVE = 3 /* per-block switch: DMMA for full blocks, FFMA else */
+  BSP_BSR_FFMA = 1, /* CUDA-core FP64 FMA, one 256-bit load per block row */
+  BSP_BSR_DMMA = 2, /* FP64 mma.sync m8n8k4 on block pairs (4x4 only) */
+  BSP_BSR_ADAPTIVE = 3 /* the reference's rule (amgT.cu:1394): DMMA when the
+                          average block holds >= 10 nonzeros, FFMA otherwise */
 } bsp_bsr_algo;
 
 /* y = alpha*A*x + beta*y for a BSR matrix; replaces the kernels dispatched by
@@ -314,12 +315,80 @@ bsp_status bsp_dasp_spmv(const bsp_dasp *d, const double *x, double *y,
                          bsp_stream_t stream);
 
 /* ---------------------------------------------------------------------- */
+/* SpMM C = alpha*A*B + beta*C (B: cols x N, C: rows x N, both row-major;
+ * C is FP32).  Replaces smatSpmmfp16 (reference src/smat.cu:103,
+ * include/smat.h:1), whose kernel accumulates in FP16 and never writes its
+ * output; here the accumulation is FP32.
+ *
+ * CSR form: values and B share `dtype` (F16, BF16 or F32), any sparsity. */
+bsp_status bsp_spmm_csr(int32_t rows, int32_t cols, int32_t nnz,
+                        const int32_t *rowPtr, const int32_t *colIdx,
+                        const void *values, bsp_dtype dtype, const void *B,
+                        int32_t N, int64_t ldb, float *C, int64_t ldc,
+                        float alpha, float beta, bsp_stream_t stream);
+
+/* Row-split CSR form for power-law rows: the plan cuts rows longer than
+ * `chunk` nonzeros into chunks processed by separate warps; their partial
+ * rows go to a workspace of bsp_spmm_plan_workspace(plan, N) bytes and are
+ * summed in chunk order (deterministic). */
+typedef struct {
+  int32_t rows, chunk;
+  int64_t nchunks, nparts;
+  int32_t nsplit;
+  int32_t *chunk_ptr;  /* [rows+1] */
+  int32_t *part_ptr;   /* [rows+1] partial-row slots of split rows */
+  int32_t *chunk_row;  /* [nchunks] */
+  int32_t *split_rows; /* [nsplit] */
+} bsp_spmm_plan;
+
+bsp_status bsp_spmm_plan_create(int32_t rows, int32_t nnz, const int32_t *rowPtr,
+                                int32_t chunk, bsp_spmm_plan *plan,
+                                bsp_stream_t stream);
+bsp_status bsp_spmm_plan_free(bsp_spmm_plan *plan);
+size_t bsp_spmm_plan_workspace(const bsp_spmm_plan *plan, int32_t N);
+bsp_status bsp_spmm_csr_planned(const bsp_spmm_plan *plan, int32_t cols, int32_t nnz,
+                                const int32_t *rowPtr, const int32_t *colIdx,
+                                const void *values, bsp_dtype dtype, const void *B,
+                                int32_t N, int64_t ldb, float *C, int64_t ldc,
+                                float alpha, float beta, void *workspace,
+                                size_t workspace_bytes, bsp_stream_t stream);
+
+/* Block (SMaT) form: 16x16 tiles of the matrix (the reference's csrToBcsr
+ * with TILE_M = TILE_K = 16, smat.cu:116-120) in F16 or BF16, staged with
+ * bulk asynchronous copies and multiplied with tensor-core MMA (FP32
+ * accumulation).  Pays when tiles are dense (`fill` = nnz / stored tile
+ * entries). */
+typedef struct {
+  int32_t rows, cols, nnz;
+  int32_t dtype;      /* BSP_F16 or BSP_BF16 */
+  bsp_bcsr tiles;     /* 16x16 structure (tiles.values released) */
+  void *tile_val;     /* [tiles.nonzeroBlocks*256] F16/BF16 row-major tiles */
+  int32_t *err;       /* device flag: a bounded wait timed out */
+  double fill;
+} bsp_smat;
+
+bsp_status bsp_smat_create(int32_t rows, int32_t cols, int32_t nnz,
+                           const int32_t *rowPtr, const int32_t *colIdx,
+                           const double *values, bsp_dtype dtype, bsp_smat *out,
+                           bsp_stream_t stream);
+bsp_status bsp_smat_free(bsp_smat *m);
+/* B: dtype of the matrix, 16-byte aligned, ldb % 8 == 0; N % 32 == 0. */
+bsp_status bsp_smat_spmm(const bsp_smat *m, const void *B, int32_t N,
+                         int64_t ldb, float *C, int64_t ldc, float alpha,
+                         float beta, bsp_stream_t stream);
+/* Reads the device error flag (waits for `stream`): BSP_ERR_TIMEOUT when a
+ * bounded copy wait gave up. */
+bsp_status bsp_smat_check(const bsp_smat *m, bsp_stream_t stream);
+
+/* ---------------------------------------------------------------------- */
 /* Conjugate gradients (absent in the reference): plain FP64 CG, or
- * mixed-precision CG with FP64 iterative refinement -- the inner solve keeps
- * the matrix in FP32, or FP16/BF16 with one power-of-two exponent per 32
+ * mixed-precision CG with reliable updates -- iterations run on the matrix
+ * stored in FP32, or FP16/BF16 with one power-of-two exponent per 32
  * nonzeros, with int16 column offsets when every |col - row| < 32768, and
- * FP32 vectors; the outer loop keeps r = b - A x, ||r|| and x in FP64.
- * Convergence: ||b - A x|| / ||b|| <= tol, computed in FP64. */
+ * FP32 vectors; whenever the iterated residual has dropped by reliable_delta
+ * the solution is folded into the FP64 x and the residual is replaced by the
+ * FP64 b - A x (search direction kept).  Convergence: ||b - A x|| / ||b|| <=
+ * tol, computed in FP64. */
 typedef enum {
   BSP_CG_FP64 = 0,
   BSP_CG_MIXED_F32 = 1,
@@ -328,22 +397,21 @@ typedef enum {
 } bsp_cg_mode;
 
 typedef struct {
-  int32_t mode;        /* bsp_cg_mode */
-  double tol;          /* relative residual target (1e-10) */
-  int32_t max_iters;   /* CG iterations over all refinement steps */
-  int32_t check_every; /* iterations per CUDA graph between host checks (rounded up to even) */
-  double inner_tol;    /* relative tolerance of each inner solve (mixed modes) */
-  int32_t max_outer;   /* refinement steps */
-  int32_t use_graphs;  /* 1: replay captured iteration chunks */
+  int32_t mode;          /* bsp_cg_mode */
+  double tol;            /* relative residual target (1e-10) */
+  int32_t max_iters;     /* CG iteration budget */
+  int32_t check_every;   /* iterations per CUDA graph between host checks (rounded up to even) */
+  double reliable_delta; /* mixed modes: residual drop that triggers an FP64 update (0.1) */
+  int32_t use_graphs;    /* 1: replay captured iteration chunks */
 } bsp_cg_options;
 
 typedef struct {
-  int32_t iterations;       /* CG iterations (inner ones in the mixed modes) */
-  int32_t outer_iterations; /* refinement steps */
+  int32_t iterations;       /* CG iterations */
+  int32_t reliable_updates; /* FP64 residual replacements */
   double rel_residual;      /* final ||b - A x|| / ||b|| in FP64 */
   double seconds;           /* device time of the solve (CUDA events) */
   int32_t converged;
-  int64_t bytes_moved;      /* algorithmic bytes of all SpMVs and vector updates */
+  int64_t bytes_moved;      /* algorithmic bytes of all kernels */
   int32_t delta16;          /* int16 column offsets were used */
 } bsp_cg_result;
 
@@ -375,6 +443,56 @@ bsp_status bsp_blockinfo(int32_t rows, int32_t cols, int32_t nnz,
                          bsp_stream_t stream);
 
 /* ---------------------------------------------------------------------- */
+/* Batched SpMV / SpMM over many independent CSR matrices (no reference
+ * counterpart: the reference launches one matrix at a time, e.g.
+ * src/csrspmv.cu:104-170).  One persistent kernel processes a work list
+ * built at plan time: row items (a run of consecutive rows, `lanes` lanes
+ * per row, chosen per matrix by the tuner) and long-row segments (rows
+ * longer than long_row_nnz, cut into seg_nnz-sized pieces whose partial
+ * sums the last-arriving warp adds in segment order).  Results are
+ * deterministic.  Warps take items from a counter, long segments first.
+ * The launch (counter reset + kernel) is captured once in a CUDA graph.
+ * y_m = A_m x_m for every matrix m; with nrhs = 8, x_m and y_m are
+ * row-major rows x 8 / cols x 8 blocks. */
+typedef struct {
+  int32_t rows, cols, nnz;
+  const int32_t *rowPtr; /* device */
+  const int32_t *colIdx; /* device */
+  const void *values;    /* device, F64 or F32 */
+  const void *x;         /* device, cols * nrhs */
+  void *y;               /* device, rows * nrhs */
+} bsp_batch_mat;
+
+typedef struct {
+  int32_t tune;         /* 0: row-statistics model, 1: time candidates */
+  int32_t seg_nnz;      /* nonzeros per long-row segment (default 1024) */
+  int32_t long_row_nnz; /* rows above this are split (default 2048) */
+  int32_t item_nnz;     /* target nonzeros per row item, 0 = automatic */
+  int32_t use_graph;    /* capture the launch in a CUDA graph (default 1) */
+} bsp_batch_options;
+
+typedef struct bsp_batch_plan_s *bsp_batch_plan;
+
+bsp_status bsp_batch_default_options(bsp_batch_options *opt);
+/* mats: host array of `count` descriptors (device pointers inside). */
+bsp_status bsp_batch_create(int32_t count, const bsp_batch_mat *mats,
+                            bsp_dtype dtype, int32_t nrhs,
+                            const bsp_batch_options *opt, bsp_batch_plan *plan,
+                            bsp_stream_t stream);
+/* One launch for the whole batch (graph replay when use_graph). */
+bsp_status bsp_batch_run(bsp_batch_plan plan, bsp_stream_t stream);
+/* The same products as one plain kernel launch per matrix (comparison). */
+bsp_status bsp_batch_run_separate(bsp_batch_plan plan, bsp_stream_t stream);
+/* Replaces the x / y pointers of matrix m (no re-capture needed). */
+bsp_status bsp_batch_set_vectors(bsp_batch_plan plan, int32_t m, const void *x,
+                                 void *y, bsp_stream_t stream);
+/* Per-matrix choice of the tuner: lanes per row (1..32). */
+bsp_status bsp_batch_lanes(bsp_batch_plan plan, int32_t *lanes /* count */);
+bsp_status bsp_batch_stats(bsp_batch_plan plan, int64_t *items,
+                           int64_t *long_segments, int64_t *total_nnz);
+bsp_status bsp_batch_destroy(bsp_batch_plan plan);
+
+/* ---------------------------------------------------------------------- */
 /* Synthetic matrix generators (host, seeded, deterministic).  Two-phase:
  * call with NULL arrays to get the sizes, then with allocated arrays. */
 
@@ -390,9 +508,10 @@ bsp_status bsp_gen_poisson3d(int32_t n, int32_t *rows, int64_t *nnz,
 bsp_status bsp_gen_stencil27(int32_t n, int32_t dof, uint64_t seed,
                              int32_t *rows, int64_t *nnz, int32_t *rowPtr,
                              int32_t *colIdx, double *values);
-/* Random block-sparse matrix: nbr block-rows of bs x bs blocks, `per_row`
- * distinct random block columns per block-row, each block filled with
- * probability U[fill_lo, fill_hi] per entry (at least one entry). */
+/* Random block-sparse matrix: nbr block-rows of bs x bs blocks (bs 4, 8 or
+ * 16), `per_row` distinct random block columns per block-row, each block
+ * filled with probability U[fill_lo, fill_hi] per entry (at least one
+ * entry). */
 bsp_status bsp_gen_random_bsr(int32_t nbr, int32_t bs, int32_t per_row,
                               double fill_lo, double fill_hi, uint64_t seed,
                               int32_t *rows, int64_t *nnz, int32_t *rowPtr,
@@ -402,6 +521,16 @@ bsp_status bsp_gen_random_bsr(int32_t nbr, int32_t bs, int32_t per_row,
 bsp_status bsp_gen_powerlaw(int32_t n, double alpha, int32_t max_len,
                             uint64_t seed, int32_t *rows, int64_t *nnz,
                             int32_t *rowPtr, int32_t *colIdx, double *values);
+/* Power-law graph: out-degrees ~ Zipf(alpha) on [1, d_max], d_max chosen so
+ * the mean degree is mean_deg; distinct uniform targets; values 1/degree. */
+bsp_status bsp_gen_graph(int32_t n, double alpha, double mean_deg, uint64_t seed,
+                         int32_t *rows, int64_t *nnz, int32_t *rowPtr,
+                         int32_t *colIdx, double *values);
+/* Banded matrix: row i holds columns i-(width-1)/2 .. i+width/2 inside
+ * [0, n), N(0,1) values. */
+bsp_status bsp_gen_banded(int32_t n, int32_t width, uint64_t seed,
+                          int32_t *rows, int64_t *nnz, int32_t *rowPtr,
+                          int32_t *colIdx, double *values);
 /* Uniform random x in [-1, 1]. */
 bsp_status bsp_gen_uniform(int64_t n, uint64_t seed, double *x);
 

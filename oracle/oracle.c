@@ -129,6 +129,26 @@ void orc_abs_rowsum(int32_t rows, const int32_t *rowPtr, const int32_t *colIdx, 
   }
 }
 
+/* Dense-output SpMM in FP64: C[i,:] = sum_j a_ij * B[j,:] and, for the error
+ * bound, absC[i,:] = sum_j |a_ij * B[j,:]|.  The reference's SpMM
+ * (src/smat.cu:22-101, FP16 accumulation) computes the same product; its
+ * kernel never stores the result, so this is the mathematical oracle. */
+void orc_spmm_f64(int32_t rows, const int32_t *rowPtr, const int32_t *colIdx, const double *val, int32_t N,
+                  const double *B, double *Cout, double *absC) {
+  for (int32_t i = 0; i < rows; i++) {
+    double *c = Cout + (int64_t)i * N, *a = absC + (int64_t)i * N;
+    for (int32_t k = 0; k < N; k++) c[k] = a[k] = 0;
+    for (int32_t j = rowPtr[i]; j < rowPtr[i + 1]; j++) {
+      const double v = val[j];
+      const double *b = B + (int64_t)colIdx[j] * N;
+      for (int32_t k = 0; k < N; k++) {
+        c[k] += v * b[k];
+        a[k] += fabs(v * b[k]);
+      }
+    }
+  }
+}
+
 /* ------------------------------------------------------------------------ */
 static int cmp_i32(const void *a, const void *b) {
   const int32_t x = *(const int32_t *)a, y = *(const int32_t *)b;

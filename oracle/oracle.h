@@ -39,6 +39,8 @@ float orc_bf16_to_f32(uint16_t h);
 
 /* |sum_j |A_ij x_j|| per row, the scale of the rounding-error bound used by
  * the parity tests. */
+void orc_spmm_f64(int32_t rows, const int32_t *rowPtr, const int32_t *colIdx, const double *val, int32_t N,
+                  const double *B, double *Cout, double *absC);
 void orc_abs_rowsum(int32_t rows, const int32_t *rowPtr, const int32_t *colIdx, const double *val,
                     const double *x, double *out);
 

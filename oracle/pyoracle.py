@@ -45,6 +45,7 @@ def orc() -> C.CDLL:
         L.orc_spmv_f32.argtypes = [_I32, _P, _P, _P, _P, _P]
         L.orc_spmv_f16.argtypes = [_I32, _P, _P, _P, _P, _P]
         L.orc_abs_rowsum.argtypes = [_I32, _P, _P, _P, _P, _P]
+        L.orc_spmm_f64.argtypes = [_I32, _P, _P, _P, _I32, _P, _P, _P]
         L.orc_csr2bsr.restype = _I64
         L.orc_csr2bsr.argtypes = [_I32, _I32, _P, _P, _P, _I32, _P, _P, _P, _P]
         L.orc_bsr_chunks.restype = _I32
@@ -96,6 +97,18 @@ def abs_rowsum(rowptr, colidx, val, x) -> np.ndarray:
     y = np.empty(rows, np.float64)
     orc().orc_abs_rowsum(rows, _p(rowptr), _p(colidx), _p(val), _p(x), _p(y))
     return y
+
+
+def spmm_f64(rowptr, colidx, val, B):
+    """FP64 C = A*B and |A|*|B| (for the error bound)."""
+    rows = rowptr.size - 1
+    B = np.ascontiguousarray(B, np.float64)
+    N = B.shape[1]
+    Cm = np.empty((rows, N), np.float64)
+    absC = np.empty((rows, N), np.float64)
+    orc().orc_spmm_f64(rows, _p(np.ascontiguousarray(rowptr, np.int32)), _p(np.ascontiguousarray(colidx, np.int32)),
+                       _p(np.ascontiguousarray(val, np.float64)), N, _p(B), _p(Cm), _p(absC))
+    return Cm, absC
 
 
 def spmv_tolerance(rowptr, colidx, val, x, unit: float = 2.0 ** -53) -> np.ndarray:

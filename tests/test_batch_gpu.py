@@ -1,0 +1,148 @@
+"""Batched SpMV / 8-RHS SpMM (one persistent launch over many matrices)
+against the CPU oracle's FP64 SpMV / SpMM, with the error bound
+2*gamma_L*sum|a_ij x_j| (u = 2^-53 for F64, 2^-24 for F32 on inputs already
+rounded to F32).  The batched launch, the per-matrix launches, the graph and
+the plain launch must agree bit for bit (fixed sum order per output)."""
+import numpy as np
+import pytest
+
+import benchsp_b200 as bsp
+from oracle import pyoracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _small_batch(seed, count=20):
+    rng = np.random.default_rng(seed)
+    mats = []
+    for i in range(count):
+        n = int(rng.integers(50, 3000))
+        if i % 3 == 0:
+            mats.append(bsp.gen_banded(n, int(rng.integers(3, 28)), seed + i))
+        elif i % 3 == 1:
+            mats.append(bsp.gen_powerlaw(n, 2.2, n, seed + i))
+        else:   # long rows and empty rows
+            lens = rng.integers(0, 12, n)
+            lens[rng.integers(0, n, 3)] = rng.integers(n // 2, n, 3)
+            lens[::7] = 0
+            rp = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+            ci = np.concatenate([np.sort(rng.choice(n, l, replace=False)) for l in lens]).astype(np.int32)
+            mats.append(bsp.HostCSR(n, n, rp, ci, rng.standard_normal(rp[-1])))
+    return mats
+
+
+def _upload(cuda, mats, dtype, nrhs, seed):
+    import torch
+    tdt = torch.float64 if dtype == "f64" else torch.float32
+    rng = np.random.default_rng(seed)
+    dev, host = [], []
+    for A in mats:
+        vals = A.values.astype(np.float32).astype(np.float64) if dtype == "f32" else A.values
+        x = rng.uniform(-1, 1, (A.cols, nrhs) if nrhs > 1 else A.cols)
+        if dtype == "f32":
+            x = x.astype(np.float32).astype(np.float64)
+        y = torch.full((A.rows, nrhs) if nrhs > 1 else (A.rows,), float("nan"), dtype=tdt, device=cuda)
+        dev.append((torch.from_numpy(A.rowptr).to(cuda), torch.from_numpy(A.colidx).to(cuda),
+                    torch.from_numpy(vals).to(tdt).to(cuda), torch.from_numpy(x).to(tdt).to(cuda), y))
+        host.append((vals, x))
+    return dev, host
+
+
+def _check(mats, dev, host, dtype, nrhs):
+    unit = 2.0 ** -53 if dtype == "f64" else 2.0 ** -24
+    for A, (_, _, _, _, y), (vals, x) in zip(mats, dev, host):
+        got = y.cpu().numpy().astype(np.float64)
+        if nrhs == 1:
+            want = pyoracle.spmv_f64(A.rowptr, A.colidx, vals, x)
+            tol = pyoracle.spmv_tolerance(A.rowptr, A.colidx, vals, x, unit)
+        else:
+            want, absC = pyoracle.spmm_f64(A.rowptr, A.colidx, vals, x)
+            L = (np.diff(A.rowptr).astype(np.float64) + 1.0)[:, None]
+            tol = 2.0 * (L * unit / (1 - L * unit)) * absC + np.finfo(np.float64).tiny
+        assert np.all(np.abs(got - want) <= tol)
+
+
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+@pytest.mark.parametrize("nrhs", [1, 8])
+def test_batch_matches_oracle_and_separate_launches(cuda, dtype, nrhs):
+    import torch
+    mats = _small_batch(11 + nrhs)
+    dev, host = _upload(cuda, mats, dtype, nrhs, 3)
+    P = bsp.BatchPlan(dev, nrhs=nrhs, long_row_nnz=256, seg_nnz=64)
+    st = P.stats()
+    assert st["long_segments"] > 0 and st["nnz"] == sum(int(A.rowptr[-1]) for A in mats)
+    P.run()
+    torch.cuda.synchronize()
+    _check(mats, dev, host, dtype, nrhs)
+    first = [d[4].clone() for d in dev]
+    for d in dev:
+        d[4].fill_(float("nan"))
+    P.run_separate()
+    for a, d in zip(first, dev):
+        assert torch.equal(a, d[4])
+    for _ in range(3):   # counters reset themselves between launches
+        P.run()
+    for a, d in zip(first, dev):
+        assert torch.equal(a, d[4])
+    P.close()
+
+
+def test_batch_graph_and_plain_launch_agree(cuda):
+    import torch
+    mats = _small_batch(5)
+    dev, host = _upload(cuda, mats, "f64", 1, 8)
+    P1 = bsp.BatchPlan(dev, long_row_nnz=128, seg_nnz=32, use_graph=True)
+    P1.run()
+    a = [d[4].clone() for d in dev]
+    P2 = bsp.BatchPlan(dev, long_row_nnz=128, seg_nnz=32, use_graph=False)
+    P2.run()
+    torch.cuda.synchronize()
+    for u, d in zip(a, dev):
+        assert torch.equal(u, d[4])
+    P1.close()
+    P2.close()
+
+
+def test_batch_tuner_choices_and_results(cuda):
+    mats = _small_batch(21, count=12)
+    dev, host = _upload(cuda, mats, "f64", 1, 9)
+    P = bsp.BatchPlan(dev, tune=1)
+    lanes = P.lanes()
+    assert set(lanes.tolist()) <= {1, 2, 4, 8, 16, 32}
+    P.run()
+    _check(mats, dev, host, "f64", 1)
+    P.close()
+
+
+def test_batch_set_vectors_and_empty_matrix(cuda):
+    import torch
+    mats = _small_batch(31, count=6)
+    mats.append(bsp.HostCSR(0, 0, np.zeros(1, np.int32), np.zeros(0, np.int32), np.zeros(0)))
+    dev, host = _upload(cuda, mats, "f64", 1, 10)
+    P = bsp.BatchPlan(dev)
+    A = mats[2]
+    x2 = torch.from_numpy(np.random.default_rng(2).uniform(-1, 1, A.cols)).to(cuda)
+    y2 = torch.empty(A.rows, dtype=torch.float64, device=cuda)
+    P.set_vectors(2, x2, y2)
+    P.run()
+    torch.cuda.synchronize()
+    host[2] = (host[2][0], x2.cpu().numpy())
+    dev[2] = (*dev[2][:3], x2, y2)
+    _check(mats, dev, host, "f64", 1)
+    P.close()
+
+
+def test_batch_rejects_bad_arguments(cuda):
+    import torch
+    mats = _small_batch(41, count=2)
+    dev, _ = _upload(cuda, mats, "f64", 1, 1)
+    with pytest.raises(bsp.BspError):
+        bsp.BatchPlan(dev, seg_nnz=16)
+    with pytest.raises(bsp.BspError):
+        bsp.BatchPlan(dev, nrhs=3)
+    bad = [(dev[0][0], dev[0][1], dev[0][2].float(), dev[0][3].float(), dev[0][4].float())]
+    P = bsp.BatchPlan(bad)   # F32 is fine
+    P.close()
+    with pytest.raises(ValueError):
+        bsp.BatchPlan([(dev[0][0], dev[0][1], dev[0][2].half(), dev[0][3].half(), dev[0][4].half())])
+    _ = torch

@@ -16,7 +16,8 @@ def _dev(cuda, *arrs):
 
 
 def _permuted_laplace(nx, seed):
-    """A symmetric permutation of a 2-D Laplacian: SPD, not banded."""
+    """A symmetric permutation of a 2-D Laplacian: SPD, and with nx*nx > 32768
+    rows some |col - row| exceed the int16 offset range."""
     import scipy.sparse as sp
     A = bsp.gen_laplace2d(nx, nx)
     M = sp.csr_matrix((A.values, A.colidx, A.rowptr), shape=(A.rows, A.rows))
@@ -29,7 +30,7 @@ def _permuted_laplace(nx, seed):
 @pytest.mark.parametrize("mode", ["fp64", "f32", "f16", "bf16"])
 @pytest.mark.parametrize("kind", ["poisson24", "permuted_laplace"])
 def test_cg_reaches_1e10(cuda, mode, kind):
-    A = bsp.gen_poisson3d(24) if kind == "poisson24" else _permuted_laplace(60, 4)
+    A = bsp.gen_poisson3d(24) if kind == "poisson24" else _permuted_laplace(200, 4)
     b = bsp.gen_uniform(A.rows, 11)
     rp, ci, va, bb = _dev(cuda, A.rowptr, A.colidx, A.values, b)
     S = bsp.CgSolver(rp, ci, va, mode=mode, tol=1e-10)
@@ -38,7 +39,7 @@ def test_cg_reaches_1e10(cuda, mode, kind):
     assert res["converged"] == 1 and res["rel_residual"] <= 1e-10
     assert pyoracle.rel_residual(A.rowptr, A.colidx, A.values, b, x) <= 2e-10
     if mode != "fp64":
-        assert res["outer_iterations"] >= 2
+        assert res["reliable_updates"] >= 2
         assert res["delta16"] == (1 if kind == "poisson24" else 0)
     xr, _ = pyoracle.cg(A.rowptr, A.colidx, A.values, b, 1e-12)
     assert np.linalg.norm(x - xr) / np.linalg.norm(xr) < 1e-7

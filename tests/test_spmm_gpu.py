@@ -1,0 +1,173 @@
+"""SpMM on the GPU (C = alpha*A*B + beta*C, FP32 accumulation): the CSR path,
+the row-split CSR path for power-law rows, and the 16x16-tile tensor-core
+(SMaT) path, each against the CPU oracle's FP64 SpMM of the same quantized
+inputs.  Products of two F16 (or two BF16) numbers are exact in FP32, so the
+only error is FP32 accumulation: |C - C_fp64| <= 2*gamma_L*(|A||B|) with
+gamma_L = L*u/(1-L*u), u = 2^-24, L = row length + 2 (the tolerance below)."""
+import numpy as np
+import pytest
+
+import benchsp_b200 as bsp
+from oracle import pyoracle
+
+pytestmark = pytest.mark.gpu
+
+_NP = {"f16": np.float16, "bf16": None, "f32": np.float32}
+
+
+def _torch_dtype(name):
+    import torch
+    return {"f16": torch.float16, "bf16": torch.bfloat16, "f32": torch.float32}[name]
+
+
+def _quantize(a: np.ndarray, name: str):
+    """Rounds FP64 data to `name` on the host; returns (torch CPU tensor of that
+    dtype, FP64 copy of the rounded values)."""
+    import torch
+    t = torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(_torch_dtype(name))
+    return t, t.to(torch.float64).numpy()
+
+
+def _tol(A, absC, alpha=1.0, Cin=None, beta=0.0):
+    L = (np.diff(A.rowptr).astype(np.float64) + 2.0)[:, None]
+    u = 2.0 ** -24
+    g = L * u / (1.0 - L * u)
+    t = 2.0 * g * abs(alpha) * absC + 1e-30
+    if Cin is not None:
+        t = t + 4.0 * u * (abs(alpha) * absC + abs(beta) * np.abs(Cin))
+    return t
+
+
+def _case(A, N, name, seed):
+    rng = np.random.default_rng(seed)
+    vals_t, vals64 = _quantize(A.values, name)
+    B_t, B64 = _quantize(rng.uniform(-1, 1, (A.cols, N)), name)
+    return vals_t, vals64, B_t, B64
+
+
+def _dev(cuda, *arrs):
+    import torch
+    return [torch.from_numpy(np.ascontiguousarray(a)).to(cuda) for a in arrs]
+
+
+@pytest.mark.parametrize("name", ["f16", "bf16", "f32"])
+@pytest.mark.parametrize("N", [32, 40, 128, 256])
+def test_spmm_csr_matches_fp64(cuda, name, N):
+    A = bsp.gen_powerlaw(3001, 1.6, 700, 9)
+    vals_t, vals64, B_t, B64 = _case(A, N, name, N)
+    rp, ci = _dev(cuda, A.rowptr, A.colidx)
+    C = bsp.spmm_csr(rp, ci, vals_t.to(cuda), B_t.to(cuda)).cpu().numpy().astype(np.float64)
+    Cref, absC = pyoracle.spmm_f64(A.rowptr, A.colidx, vals64, B64)
+    assert np.all(np.abs(C - Cref) <= _tol(A, absC))
+
+
+@pytest.mark.parametrize("name", ["f16", "bf16"])
+def test_spmm_csr_alpha_beta(cuda, name):
+    import torch
+    A = bsp.gen_powerlaw(1500, 1.8, 300, 3)
+    N = 64
+    vals_t, vals64, B_t, B64 = _case(A, N, name, 5)
+    Cin = np.random.default_rng(1).uniform(-1, 1, (A.rows, N)).astype(np.float32)
+    rp, ci = _dev(cuda, A.rowptr, A.colidx)
+    Cd = torch.from_numpy(Cin.copy()).to(cuda)
+    bsp.spmm_csr(rp, ci, vals_t.to(cuda), B_t.to(cuda), Cd, alpha=0.5, beta=-1.5)
+    Cref, absC = pyoracle.spmm_f64(A.rowptr, A.colidx, vals64, B64)
+    want = 0.5 * Cref - 1.5 * Cin.astype(np.float64)
+    got = Cd.cpu().numpy().astype(np.float64)
+    assert np.all(np.abs(got - want) <= _tol(A, absC, 0.5, Cin, -1.5))
+
+
+@pytest.mark.parametrize("chunk", [32, 64, 256])
+@pytest.mark.parametrize("N", [32, 128])
+def test_spmm_planned_matches_fp64_and_is_deterministic(cuda, chunk, N):
+    A = bsp.gen_powerlaw(4000, 1.4, 3000, 17)   # rows up to 3000 long
+    assert np.diff(A.rowptr).max() > 4 * chunk
+    vals_t, vals64, B_t, B64 = _case(A, N, "f16", chunk + N)
+    rp, ci = _dev(cuda, A.rowptr, A.colidx)
+    vd, Bd = vals_t.to(cuda), B_t.to(cuda)
+    P = bsp.SpmmPlan(rp, ci, vd, cols=A.cols, chunk=chunk)
+    lens = np.diff(A.rowptr)
+    assert P.nsplit == int(np.sum(lens > chunk))
+    assert P.nchunks == int(np.sum(np.maximum(1, (lens + chunk - 1) // chunk)))
+    C1 = P.spmm(Bd).cpu().numpy()
+    C2 = P.spmm(Bd).cpu().numpy()
+    assert np.array_equal(C1, C2)
+    Cref, absC = pyoracle.spmm_f64(A.rowptr, A.colidx, vals64, B64)
+    assert np.all(np.abs(C1.astype(np.float64) - Cref) <= _tol(A, absC))
+    P.free()
+
+
+def test_spmm_planned_empty_rows_and_beta(cuda):
+    import torch
+    # every third row empty
+    rng = np.random.default_rng(2)
+    rows, cols = 900, 700
+    lens = rng.integers(0, 600, rows)
+    lens[::3] = 0
+    rowptr = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    colidx = np.concatenate([np.sort(rng.choice(cols, l, replace=False)) for l in lens]).astype(np.int32)
+    A = bsp.HostCSR(rows, cols, rowptr, colidx, rng.uniform(-1, 1, rowptr[-1]))
+    N = 32
+    vals_t, vals64, B_t, B64 = _case(A, N, "bf16", 8)
+    Cin = rng.uniform(-1, 1, (rows, N)).astype(np.float32)
+    rp, ci = _dev(cuda, A.rowptr, A.colidx)
+    P = bsp.SpmmPlan(rp, ci, vals_t.to(cuda), cols=cols, chunk=128)
+    Cd = torch.from_numpy(Cin.copy()).to(cuda)
+    P.spmm(B_t.to(cuda), Cd, alpha=2.0, beta=0.25)
+    Cref, absC = pyoracle.spmm_f64(A.rowptr, A.colidx, vals64, B64)
+    want = 2.0 * Cref + 0.25 * Cin.astype(np.float64)
+    got = Cd.cpu().numpy().astype(np.float64)
+    assert np.all(np.abs(got - want) <= _tol(A, absC, 2.0, Cin, 0.25))
+    assert np.array_equal(got[::3], (0.25 * Cin[::3]).astype(np.float32).astype(np.float64))
+
+
+@pytest.mark.parametrize("name", ["f16", "bf16"])
+@pytest.mark.parametrize("N", [32, 64, 256])
+@pytest.mark.parametrize("kind", ["dense_tiles", "ragged"])
+def test_smat_block_spmm_matches_fp64(cuda, name, N, kind):
+    if kind == "dense_tiles":
+        A = bsp.gen_random_bsr(96, 16, 6, 1.0, 1.0, 4)
+    else:   # partially filled tiles, rows/cols not multiples of 16
+        A = bsp.gen_powerlaw(1003, 1.7, 400, 12)
+    vals_t, vals64, B_t, B64 = _case(A, N, name, N + 1)
+    rp, ci, v64 = _dev(cuda, A.rowptr, A.colidx, vals64)
+    M = bsp.SmatMatrix(rp, ci, v64, rows=A.rows, cols=A.cols, dtype=name)
+    if kind == "dense_tiles":
+        assert M.fill == 1.0
+    C1 = M.spmm(B_t.to(cuda))
+    M.check()
+    C1 = C1.cpu().numpy()
+    C2 = M.spmm(B_t.to(cuda)).cpu().numpy()
+    assert np.array_equal(C1, C2)
+    Cref, absC = pyoracle.spmm_f64(A.rowptr, A.colidx, vals64, B64)
+    # the tile MMA sums 16 products per step in an unspecified order: bound
+    # with the full tile row length instead of the CSR row length
+    tiles_per_row = (A.cols + 15) // 16
+    L = np.full((A.rows, 1), 16.0 * tiles_per_row + 2.0)
+    u = 2.0 ** -24
+    tol = 2.0 * (L * u / (1 - L * u)) * absC + 1e-30
+    assert np.all(np.abs(C1.astype(np.float64) - Cref) <= tol)
+    M.free()
+
+
+def test_smat_alpha_beta_and_argument_errors(cuda):
+    import torch
+    A = bsp.gen_random_bsr(40, 16, 4, 0.5, 1.0, 6)
+    N = 32
+    vals_t, vals64, B_t, B64 = _case(A, N, "f16", 3)
+    rp, ci, v64 = _dev(cuda, A.rowptr, A.colidx, vals64)
+    M = bsp.SmatMatrix(rp, ci, v64, rows=A.rows, cols=A.cols, dtype="f16")
+    Cin = np.random.default_rng(4).uniform(-1, 1, (A.rows, N)).astype(np.float32)
+    Cd = torch.from_numpy(Cin.copy()).to(cuda)
+    M.spmm(B_t.to(cuda), Cd, alpha=-1.0, beta=0.5)
+    Cref, absC = pyoracle.spmm_f64(A.rowptr, A.colidx, vals64, B64)
+    want = -Cref + 0.5 * Cin.astype(np.float64)
+    L = np.full((A.rows, 1), 16.0 * ((A.cols + 15) // 16) + 2.0)
+    u = 2.0 ** -24
+    tol = 2.0 * (L * u / (1 - L * u)) * absC + 4 * u * (absC + 0.5 * np.abs(Cin)) + 1e-30
+    assert np.all(np.abs(Cd.cpu().numpy().astype(np.float64) - want) <= tol)
+    with pytest.raises(bsp.BspError):
+        M.spmm(torch.zeros(A.cols, 40, dtype=torch.float16, device=cuda))   # N not a multiple of 32
+    with pytest.raises(ValueError):
+        bsp.spmm_csr(rp, ci, vals_t.to(cuda), B_t.to(cuda).to(torch.bfloat16))
+    M.free()
