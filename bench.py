@@ -319,6 +319,223 @@ def run_ours(args, ws, rank, local):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# --suite: one JSON line per further workload (CSR Laplacian, BSR 8x8 and
+# random-fill BSR, DASP on power-law rows, CG, SpMM on a power-law graph,
+# batched SpMV).  Not part of the headline line; single GPU.
+
+def _timed(fn, steps: int, flush=None) -> float:
+    """Seconds per call, CUDA events on the current stream.  With `flush`, L2
+    is overwritten between calls and only the calls themselves are timed."""
+    import torch
+    for _ in range(3):
+        fn()
+    torch.cuda.synchronize()
+    if flush is None:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps / 1e3
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for a, b in evs:
+        flush()
+        a.record()
+        fn()
+        b.record()
+    torch.cuda.synchronize()
+    return sum(a.elapsed_time(b) for a, b in evs) / steps / 1e3
+
+
+def _csr_bytes(rows: int, cols: int, nnz: int, vbytes: int = 8) -> int:
+    return nnz * (vbytes + 4) + (rows + 1) * 4 + cols * vbytes + rows * vbytes
+
+
+def _emit(name: str, **kw) -> None:
+    print(json.dumps({"suite": name, **kw}), flush=True)
+
+
+def _roof(nbytes: int, t: float, pk: float) -> dict:
+    a = nbytes / t / 1e9
+    return {"bound": "hbm", "achieved": round(a, 1), "peak": pk, "unit": "GB/s", "frac": round(a / pk, 4),
+            "algorithmic_bytes": int(nbytes)}
+
+
+def _cusparse_spmv(rp, ci, va, x, rows, cols):
+    """torch.sparse CSR matvec (cuSPARSE) for comparison only."""
+    import torch
+    T = torch.sparse_csr_tensor(rp.long(), ci.long(), va, size=(rows, cols))
+    return lambda: T @ x
+
+
+def run_suite(args) -> None:
+    import torch
+
+    import benchsp_b200 as bsp
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    pk = peaks()["hbm_gbs"]
+    scratch = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    flush = scratch.zero_
+    steps = max(10, min(args.steps, 200))
+
+    def up(*arrs):
+        return [torch.from_numpy(np.ascontiguousarray(a)).to(dev) for a in arrs]
+
+    # --- CSR FP64 SpMV, 2-D Laplacian 512x512 (L2 flushed between calls)
+    A = bsp.gen_laplace2d(512, 512)
+    xh = bsp.gen_uniform(A.cols, SEED + 10)
+    rp, ci, va, x = up(A.rowptr, A.colidx, A.values, xh)
+    y = torch.empty(A.rows, dtype=torch.float64, device=dev)
+    nb = _csr_bytes(A.rows, A.cols, A.nnz)
+    ref = cpu_reference(A, xh, max_seconds=3.0)
+    res = {}
+    for algo in ("auto", "vector", "merge", "scalar"):
+        t = _timed(lambda: bsp.csr_spmv(rp, ci, va, x, y, algo=algo), steps, flush)
+        yy = y.cpu().numpy()
+        res[algo] = {"us": round(t * 1e6, 2), "gflops": round(2 * A.nnz / t / 1e9, 2),
+                     "bit_exact_vs_reference": bool(np.array_equal(yy, ref["y"])),
+                     "max_rel_err": float(np.max(np.abs(yy - ref["y"]) / (np.abs(ref["y"]) + 1e-300)))}
+    tcs = _timed(_cusparse_spmv(rp, ci, va, x, A.rows, A.cols), steps, flush)
+    _emit("csr_fp64_laplace2d_512", n=A.rows, nnz=A.nnz, l2="flushed between calls", variants=res,
+          roofline=_roof(nb, res["auto"]["us"] / 1e6, pk), cusparse_us=round(tcs * 1e6, 2),
+          cpu_baseline={"value": round(ref["gflops"], 3), "unit": "GFLOP/s", "cores": ref["cores"],
+                        "kind": ref["kind"]})
+    del rp, ci, va, x, y
+
+    # --- BSR FP64: stencil 64^3 x 4 dof as 4x4 and 8x8 blocks; random-fill 4x4
+    A, xh = make_matrix(GRID)
+    rp, ci, va, x = up(A.rowptr, A.colidx, A.values, xh)
+    y = torch.empty(A.rows, dtype=torch.float64, device=dev)
+    tcs = _timed(_cusparse_spmv(rp, ci, va, x, A.rows, A.cols), steps)
+    for bs in (4, 8):
+        M = bsp.csr2bsr(rp, ci, va, rows=A.rows, cols=A.cols, bs=bs)
+        nb = algorithmic_bytes_bsr(M.blc_num, M.blc_row, A.rows, bs)
+        res = {}
+        for algo in (("auto", "ffma", "dmma") if bs == 4 else ("auto", "ffma")):   # DMMA: 4x4 blocks only
+            t = _timed(lambda: M.spmv(x, y, algo=algo), steps)
+            res[algo] = {"us": round(t * 1e6, 2), "gflops": round(2 * A.nnz / t / 1e9, 1),
+                         "gbs": round(nb / t / 1e9, 1)}
+        _emit(f"bsr{bs}_fp64_stencil27_64cubed_4dof", n=A.rows, nnz=A.nnz, blocks=M.blc_num,
+              fill=round(A.nnz / (M.blc_num * bs * bs), 4), variants=res,
+              roofline=_roof(nb, res["auto"]["us"] / 1e6, pk), cusparse_csr_us=round(tcs * 1e6, 2))
+        M.free()
+    del rp, ci, va, x, y
+    torch.cuda.empty_cache()
+    A = bsp.gen_random_bsr(262144, 4, 16, 0.3, 1.0, SEED + 11)
+    xh = bsp.gen_uniform(A.cols, SEED + 12)
+    rp, ci, va, x = up(A.rowptr, A.colidx, A.values, xh)
+    y = torch.empty(A.rows, dtype=torch.float64, device=dev)
+    M = bsp.csr2bsr(rp, ci, va, rows=A.rows, cols=A.cols, bs=4)
+    nb = algorithmic_bytes_bsr(M.blc_num, M.blc_row, A.rows, 4)
+    res = {}
+    for algo in ("auto", "ffma", "dmma", "adaptive"):
+        t = _timed(lambda: M.spmv(x, y, algo=algo), steps)
+        res[algo] = {"us": round(t * 1e6, 2), "gflops": round(2 * A.nnz / t / 1e9, 1), "gbs": round(nb / t / 1e9, 1)}
+    tcs = _timed(_cusparse_spmv(rp, ci, va, x, A.rows, A.cols), steps)
+    _emit("bsr4_fp64_random_16perrow_fill30to100", n=A.rows, nnz=A.nnz, blocks=M.blc_num,
+          fill=round(A.nnz / (M.blc_num * 16), 4), variants=res, roofline=_roof(nb, res["auto"]["us"] / 1e6, pk),
+          cusparse_csr_us=round(tcs * 1e6, 2))
+    M.free()
+    del rp, ci, va, x, y
+
+    # --- DASP vs CSR on power-law rows (Zipf 2.0, capped at 10k, n = 2M)
+    A = bsp.gen_powerlaw(1 << 21, 2.0, 10000, SEED + 13)
+    xh = bsp.gen_uniform(A.cols, SEED + 14)
+    rp, ci, va, x = up(A.rowptr, A.colidx, A.values, xh)
+    y = torch.empty(A.rows, dtype=torch.float64, device=dev)
+    D = bsp.csr2dasp(rp, ci, va, rows=A.rows, cols=A.cols)
+    nb = _csr_bytes(A.rows, A.cols, A.nnz)
+    res = {}
+    for name, fn in (("dasp", lambda: D.spmv(x, y)), ("csr_auto", lambda: bsp.csr_spmv(rp, ci, va, x, y)),
+                     ("csr_merge", lambda: bsp.csr_spmv(rp, ci, va, x, y, algo="merge"))):
+        t = _timed(fn, steps)
+        res[name] = {"us": round(t * 1e6, 2), "gflops": round(2 * A.nnz / t / 1e9, 1), "gbs": round(nb / t / 1e9, 1)}
+    tcs = _timed(_cusparse_spmv(rp, ci, va, x, A.rows, A.cols), steps)
+    _emit("dasp_fp64_powerlaw_2M_zipf2", n=A.rows, nnz=A.nnz, variants=res,
+          roofline=_roof(nb, res["dasp"]["us"] / 1e6, pk), cusparse_us=round(tcs * 1e6, 2))
+    D.free()
+    del rp, ci, va, x, y
+
+    # --- CG on the 7-point Poisson 128^3 to 1e-10: FP64 vs mixed precision
+    A = bsp.gen_poisson3d(128)
+    bh = bsp.gen_uniform(A.rows, SEED + 3)
+    rp, ci, va, b = up(A.rowptr, A.colidx, A.values, bh)
+    res = {}
+    for mode in ("fp64", "f32", "f16", "bf16"):
+        S = bsp.CgSolver(rp, ci, va, mode=mode, tol=1e-10)
+        S.solve(b)
+        best = None
+        for _ in range(3):
+            xs, r = S.solve(b)
+            best = r if best is None or r["seconds"] < best["seconds"] else best
+        res[mode] = {"ms": round(best["seconds"] * 1e3, 3), "iterations": best["iterations"],
+                     "reliable_updates": best["reliable_updates"], "rel_residual": best["rel_residual"],
+                     "gbs": round(best["bytes_moved"] / best["seconds"] / 1e9, 1)}
+        S.close()
+    _emit("cg_poisson3d_128_tol1e-10", n=A.rows, nnz=A.nnz, modes=res,
+          mixed_speedup_vs_fp64=round(res["fp64"]["ms"] / min(res[m]["ms"] for m in ("f32", "f16", "bf16")), 3))
+    del rp, ci, va, b
+
+    # --- SpMM on a power-law graph (n = 2^20, Zipf 1.8, mean degree 32)
+    A = bsp.gen_graph(1 << 20, 1.8, 32, SEED + 4)
+    rp, ci, v64 = up(A.rowptr, A.colidx, A.values)
+    A64 = torch.sparse_csr_tensor(rp.long(), ci.long(), v64, size=(A.rows, A.cols))
+    res = {}
+    for name, tdt in (("f16", torch.float16), ("bf16", torch.bfloat16)):
+        v = v64.to(tdt)
+        P = bsp.SpmmPlan(rp, ci, v, cols=A.cols, chunk=256)
+        for N in (32, 128, 256):
+            g = torch.Generator(device="cpu").manual_seed(N)
+            B = (torch.rand(A.cols, N, generator=g, dtype=torch.float64) * 2 - 1).to(tdt).to(dev)
+            Cm = P.spmm(B)
+            Cref = A64 @ B.double()
+            err = float(torch.linalg.norm(Cm.double() - Cref) / torch.linalg.norm(Cref))
+            t = _timed(lambda: P.spmm(B, Cm), 10)
+            Af = torch.sparse_csr_tensor(rp.long(), ci.long(), v.float(), size=(A.rows, A.cols))
+            Bf = B.float()
+            tcs = _timed(lambda: Af @ Bf, 5)
+            nb = A.nnz * 6 + (A.rows + 1) * 4 + A.cols * N * 2 + A.rows * N * 4
+            res[f"{name}_N{N}"] = {"ms": round(t * 1e3, 3), "gflops": round(2 * A.nnz * N / t / 1e9, 1),
+                                   "rel_err_vs_fp64": err, "cusparse_f32_ms": round(tcs * 1e3, 3),
+                                   "min_bytes_gbs": round(nb / t / 1e9, 1)}
+        P.free()
+    _emit("spmm_graph_1M_zipf1.8_deg32", n=A.rows, nnz=A.nnz, max_row=int(np.diff(A.rowptr).max()), variants=res)
+    del rp, ci, v64, A64
+
+    # --- 512 independent SpMVs (and 8-RHS SpMMs) in one persistent launch
+    mats = bsp.gen_batch(512, SEED + 6)
+    nnz = sum(int(m.rowptr[-1]) for m in mats)
+    rows = sum(m.rows for m in mats)
+    res = {}
+    for dname, tdt, es in (("f64", torch.float64, 8), ("f32", torch.float32, 4)):
+        base = [up(m.rowptr, m.colidx) + [torch.from_numpy(m.values).to(tdt).to(dev)] for m in mats]
+        for nrhs in (1, 8):
+            g = torch.Generator(device="cpu").manual_seed(nrhs)
+            d = []
+            for m, (rp, ci, va) in zip(mats, base):
+                shp = (m.cols, nrhs) if nrhs > 1 else (m.cols,)
+                xx = (torch.rand(shp, generator=g, dtype=torch.float64) * 2 - 1).to(tdt).to(dev)
+                yy = torch.empty((m.rows, nrhs) if nrhs > 1 else (m.rows,), dtype=tdt, device=dev)
+                d.append((rp, ci, va, xx, yy))
+            P = bsp.BatchPlan(d, nrhs=nrhs, tune=1)
+            tb = _timed(P.run, 50)
+            ts = _timed(P.run_separate, 5)
+            nb = nnz * (es + 4) + (rows + len(mats)) * 4 + 2 * rows * nrhs * es
+            res[f"{dname}_rhs{nrhs}"] = {"batched_us": round(tb * 1e6, 1), "separate_us": round(ts * 1e6, 1),
+                                         "speedup": round(ts / tb, 2), "gbs": round(nb / tb / 1e9, 1),
+                                         "frac": round(nb / tb / 1e9 / pk, 4),
+                                         "gflops": round(2 * nnz * nrhs / tb / 1e9, 1), "launches_batched": 1,
+                                         "launches_separate": len(mats)}
+            if nrhs == 1:
+                fns = [_cusparse_spmv(rp, ci, va, xx, m.rows, m.cols) for m, (rp, ci, va, xx, _) in zip(mats, d)]
+                res[f"{dname}_rhs1"]["cusparse_separate_us"] = round(_timed(lambda: [f() for f in fns], 5) * 1e6, 1)
+            P.close()
+    _emit("batch_512_banded_and_zipf2.2", matrices=len(mats), rows=rows, nnz=nnz, variants=res)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -326,9 +543,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--suite", action="store_true", help="one JSON line per further workload (1 GPU)")
     ap.add_argument("--grid", type=int, default=GRID, help="stencil grid edge (64 = the benchmark config; "
                     "smaller values only for profiling captures)")
     args = ap.parse_args()
+    if args.suite:
+        run_suite(args)
+        return
     ws, rank, local = dist_init()
     try:
         if args.impl == "reference":
