@@ -83,7 +83,31 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         if r.returncode != 0:
             raise RuntimeError(f"link failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
         os.replace(tmp, LIB)
+    _build_compat(force)
     return LIB
+
+
+COMPAT_SRC = PKG / "compat"
+COMPAT_LIB = PKG / "lib" / "libbspmv_compat.so"
+
+
+def _build_compat(force: bool = False) -> Path:
+    """Links libbspmv_compat.so: the reference's C++ operator names
+    (include/benchsp_compat.hpp) over libbspmv's C ABI, plus the cuSPARSE
+    comparison wrappers.  Host code only (g++)."""
+    srcs = sorted(COMPAT_SRC.glob("*.cpp"))
+    deps = [*srcs, INCLUDE / "benchsp_compat.hpp", INCLUDE / "bsp.h", LIB]
+    if not force and COMPAT_LIB.exists() and COMPAT_LIB.stat().st_mtime >= max(d.stat().st_mtime for d in deps):
+        return COMPAT_LIB
+    tmp = COMPAT_LIB.with_suffix(".so.tmp")
+    cmd = ["g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-Wall", f"-I{INCLUDE}", f"-I{CUDA_HOME}/include",
+           "-o", str(tmp), *map(str, srcs), f"-L{LIB.parent}", "-lbspmv", f"-L{CUDA_HOME}/lib64", "-lcusparse",
+           "-Wl,-rpath,$ORIGIN", f"-Wl,-rpath,{CUDA_HOME}/lib64"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"compat link failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+    os.replace(tmp, COMPAT_LIB)
+    return COMPAT_LIB
 
 
 def main() -> None:

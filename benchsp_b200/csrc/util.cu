@@ -171,3 +171,22 @@ extern "C" bsp_status bsp_device_sync(void) {
   BSP_CUDA(cudaDeviceSynchronize());
   return BSP_OK;
 }
+
+extern "C" bsp_status bsp_device_alloc(void **ptr, size_t bytes) {
+  clear_error();
+  BSP_CHECK_ARG(ptr, "null pointer");
+  *ptr = nullptr;
+  if (bytes == 0) return BSP_OK;
+  const cudaError_t e = cudaMalloc(ptr, bytes);
+  if (e != cudaSuccess) {
+    *ptr = nullptr;
+    BSP_FAIL(BSP_ERR_ALLOC, std::string("cudaMalloc(") + std::to_string(bytes) + " B) -> " + cudaGetErrorString(e));
+  }
+  return BSP_OK;
+}
+
+extern "C" bsp_status bsp_device_free(void *ptr) {
+  clear_error();
+  if (ptr) BSP_CUDA(cudaFree(ptr));
+  return BSP_OK;
+}

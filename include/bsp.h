@@ -58,6 +58,10 @@ const char *bsp_version(void);
 bsp_status bsp_memcpy_d2h(void *dst_host, const void *src_dev, size_t bytes);
 bsp_status bsp_memcpy_h2d(void *dst_dev, const void *src_host, size_t bytes);
 bsp_status bsp_device_sync(void);
+/* Device memory for hosts without their own CUDA binding (cudaMalloc /
+ * cudaFree on the current device). */
+bsp_status bsp_device_alloc(void **ptr, size_t bytes);
+bsp_status bsp_device_free(void *ptr);
 
 /* ---------------------------------------------------------------------- */
 /* CSR SpMV  y = alpha*A*x + beta*y

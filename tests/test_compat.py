@@ -1,0 +1,171 @@
+"""The reference's C++ operator surface (include/benchsp_compat.hpp, built into
+libbspmv_compat.so): every name is exported; a C++ program calling all of
+them links; on the GPU each result matches the CPU oracle; and the
+reference's own bench drivers, compiled unchanged against the compat
+library (oracle/_ref/*_on_bsp), run and pass their own checks."""
+import os
+import re
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import benchsp_b200 as bsp
+from oracle import pyoracle
+
+ROOT = Path(__file__).resolve().parents[1]
+LIBDIR = ROOT / "benchsp_b200" / "lib"
+COMPAT = LIBDIR / "libbspmv_compat.so"
+HEADER = ROOT / "include" / "benchsp_compat.hpp"
+CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+
+
+def _declared_names():
+    src = HEADER.read_text()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"^(?:extern \"C\" )?(?:int|void)\s+(\w+)\(", src, flags=re.M)))
+
+
+def test_compat_library_exports_every_reference_name():
+    out = subprocess.run(["nm", "-DC", "--defined-only", str(COMPAT)], capture_output=True, text=True,
+                         check=True).stdout
+    names = _declared_names()
+    assert len(names) == 17
+    for n in names:
+        assert re.search(rf"\b{n}\(|\b{n}$", out, flags=re.M), n
+
+
+def _build_check(tmp: Path) -> Path:
+    exe = tmp / "compat_check"
+    subprocess.run(["g++", "-O2", "-std=c++17", f"-I{ROOT / 'include'}", f"-I{CUDA}/include",
+                    str(ROOT / "tests" / "compat" / "compat_check.cpp"), f"-L{LIBDIR}", "-lbspmv_compat", "-lbspmv",
+                    f"-Wl,-rpath,{LIBDIR}", "-o", str(exe)], check=True)
+    return exe
+
+
+def test_compat_check_driver_links(tmp_path):
+    assert _build_check(tmp_path).exists()
+
+
+# ---------------------------------------------------------------------------
+# GPU: every compat function against the oracle
+
+def _matrix(kind):
+    if kind == "laplace":
+        return bsp.gen_laplace2d(40, 37)
+    if kind == "powerlaw":
+        return bsp.gen_powerlaw(3001, 1.5, 1500, 5)
+    return bsp.gen_random_bsr(64, 4, 5, 0.3, 1.0, 2)
+
+
+def _write_inputs(d: Path, A, x, yin, n):
+    dbsr = pyoracle.csr2dbsr(A.rowptr, A.colidx, A.values, True)
+    with open(d / "meta.txt", "w") as f:
+        f.write(f"{A.rows} {A.cols} {A.nnz} {dbsr['blc_row']} {dbsr['blocknnz']} {n}\n")
+    for name, arr, dt in (("rowptr.i32", A.rowptr, np.int32), ("colidx.i32", A.colidx, np.int32),
+                          ("values.f64", A.values, np.float64), ("x.f64", x, np.float64),
+                          ("yin.f64", yin, np.float64), ("dbsr_blcPtr.i32", dbsr["blcPtr"], np.int32),
+                          ("dbsr_colIdx.i32", dbsr["colIdx"], np.int32), ("dbsr_blcVal.f64", dbsr["blcVal"], np.float64),
+                          ("dbsr_blcMap.u16", dbsr["blcMap"], np.uint16)):
+        np.ascontiguousarray(arr, dt).tofile(d / name)
+    return dbsr
+
+
+def _out(d: Path, name, dt, count=None):
+    a = np.fromfile(d / f"out_{name}.bin", dtype=dt)
+    return a if count is None else a[:count]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["laplace", "powerlaw", "randbsr"])
+def test_compat_functions_match_oracle(cuda, tmp_path, kind):
+    A = _matrix(kind)
+    rng = np.random.default_rng(3)
+    x = rng.uniform(-1, 1, A.cols)
+    yin = rng.uniform(-1, 1, A.rows)
+    n = 32
+    dbsr = _write_inputs(tmp_path, A, x, yin, n)
+    exe = _build_check(tmp_path)
+    r = subprocess.run([str(exe), str(tmp_path)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+
+    want = pyoracle.spmv_f64(A.rowptr, A.colidx, A.values, x)
+    tol = pyoracle.spmv_tolerance(A.rowptr, A.colidx, A.values, x)
+    for name in ("spmv_fp64_warpper", "spmv_fp64_balance_warpper", "MySpmvWithPrefp64", "amgT_spmv_fp64",
+                 "bcsr_spmv_fp64", "cusparse_spmv_fp64"):
+        assert np.all(np.abs(_out(tmp_path, name, np.float64) - want) <= tol), name
+    for name in ("accumulate_spmv_fp64_warpper", "accumulate_amgT_spmv_fp64"):
+        assert np.all(np.abs(_out(tmp_path, name, np.float64) - (want + yin)) <= tol + 2.0 ** -52 * np.abs(want + yin)), name
+
+    # DBSR results come in the recorder's row order
+    perm = dbsr["recorderMap"]
+    for name in ("amgT_spmv_fp64_dbsr", "amgT_spmv_fp64_dbsr_balance"):
+        assert np.all(np.abs(_out(tmp_path, name, np.float64) - want[perm]) <= tol[perm]), name
+
+    # DASP: Y in order_rid order, order_rid as the reference packs it
+    order = _out(tmp_path, "spmv_all_order", np.int32)
+    assert np.array_equal(order, pyoracle.dasp_pack(A.rowptr, A.colidx, A.values)["order_rid"])
+    assert np.all(np.abs(_out(tmp_path, "spmv_all", np.float64) - want[order]) <= tol[order])
+
+    # FP32 and FP16 paths
+    v32, x32 = A.values.astype(np.float32), x.astype(np.float32)
+    w32 = pyoracle.spmv_f64(A.rowptr, A.colidx, v32.astype(np.float64), x32.astype(np.float64))
+    t32 = pyoracle.spmv_tolerance(A.rowptr, A.colidx, v32.astype(np.float64), x32.astype(np.float64), 2.0 ** -24)
+    for name in ("MySpmvWithPre", "cusparse_spmv"):
+        assert np.all(np.abs(_out(tmp_path, name, np.float32).astype(np.float64) - w32) <= t32 + 2.0 ** -23 * np.abs(w32)), name
+    # the compat API takes float values and x, rounded to half from float
+    v16, x16 = v32.astype(np.float16), x32.astype(np.float16)
+    w16 = pyoracle.spmv_f64(A.rowptr, A.colidx, v16.astype(np.float64), x16.astype(np.float64))
+    t16 = pyoracle.spmv_tolerance(A.rowptr, A.colidx, v16.astype(np.float64), x16.astype(np.float64), 2.0 ** -24)
+    got16 = _out(tmp_path, "MySpmvWithPrefp16", np.float32).astype(np.float64)
+    assert np.all(np.abs(got16 - w16) <= t16 + 2.0 ** -10 * np.abs(w16) + 2.0 ** -24)
+    assert np.all(np.abs(_out(tmp_path, "cusparse_spmv_fp16_warpper", np.float32) - w16) <= 1e-2 * (1 + np.abs(w16)))
+
+    # SpMM with B = ones: every column holds the row sums of the FP16 values
+    C = _out(tmp_path, "smatSpmmfp16", np.float32).reshape(A.rows, n).astype(np.float64)
+    rs = pyoracle.spmv_f64(A.rowptr, A.colidx, v16.astype(np.float64), np.ones(A.cols))
+    ts = pyoracle.spmv_tolerance(A.rowptr, A.colidx, v16.astype(np.float64), np.ones(A.cols), 2.0 ** -24)
+    assert np.all(np.abs(C - rs[:, None]) <= ts[:, None])
+
+
+# ---------------------------------------------------------------------------
+# GPU: the reference's own bench drivers on the compat library
+
+def _driver(name):
+    exe = pyoracle.REF_DIR / f"{name}_on_bsp"
+    if not exe.exists():
+        pytest.skip(f"{exe.name} not built (needs the reference sources at build time)")
+    return exe
+
+
+@pytest.mark.gpu
+def test_reference_spmvfp64_driver_runs_and_passes(cuda, tmp_path):
+    exe = _driver("spmvfp64")
+    A = bsp.gen_powerlaw(5000, 1.6, 2000, 8)
+    # the driver runs the reference's host csrTodbsrWithRecorder, whose
+    # balanceDbsr step indexes past its warp vector on some matrices
+    # (include/dbsr.h:94-168); this one stays in bounds
+    assert pyoracle.csr2dbsr(A.rowptr, A.colidx, A.values, True)["balance_overflow"] == 0
+    p = tmp_path / "m.mtx"
+    pyoracle.write_mtx(p, A.rows, A.cols, A.rowptr, A.colidx, A.values)
+    r = subprocess.run([str(exe), str(p), "5"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "===benchmark fp64 summary===" in r.stdout
+    assert "PASS" in r.stdout.splitlines()[-1], r.stdout[-2000:]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["spmvfp16", "spmmfp16"])
+def test_reference_fp16_drivers_run(cuda, tmp_path, name):
+    exe = _driver(name)
+    A = bsp.gen_laplace2d(48, 48) if name == "spmvfp16" else bsp.gen_random_bsr(32, 4, 4, 0.5, 1.0, 3)
+    p = tmp_path / "m.mtx"
+    pyoracle.write_mtx(p, A.rows, A.cols, A.rowptr, A.colidx, A.values)
+    env = dict(os.environ, FMM_STUB_FILE=str(p))
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=600, env=env)
+    assert r.returncode == 0, r.stdout + r.stderr
+    if name == "spmvfp16":
+        assert r.stdout.strip().splitlines()[-1] == "PASS"
+    else:
+        assert r.stdout.count("smat time:") == 40   # n = 256..2048, 10 calls each
