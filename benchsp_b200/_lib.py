@@ -92,6 +92,7 @@ class BspDasp(C.Structure):
         ("irreg_val", C.c_void_p), ("irreg_cid", C.c_void_p), ("irreg_rpt", C.c_void_p),
         ("short_val", C.c_void_p), ("short_cid", C.c_void_p), ("order_rid", C.c_void_p),
         ("sorted_rid", C.c_void_p), ("row_len_sorted", C.c_void_p),
+        ("long_groups", C.c_int32), ("long_group_ptr", C.c_void_p), ("long_group_info", C.c_void_p),
     ]
 
 

@@ -25,11 +25,13 @@
 // SpMV: the reference launches dasp_spmv2 then longPart_sum and extracts the
 // diagonal of FP64 mma.sync.m8n8k4 products (1/8 of the MMA output is used).
 // Here one launch covers every part with CUDA-core FP64 FMA (the path is
-// bandwidth-bound; the tiles are read as whole 32-byte rows where
-// alignment allows).  Long rows: every warp reduces its 64-value chunk,
-// stores the partial, and the last warp to finish a row (per-row arrival
-// counter, no waiting) sums the row's partials in chunk order and resets the
-// counter, so the result is deterministic.
+// bandwidth- and gather-bound; tiles are read as whole 32-byte rows where
+// alignment allows, and each thread issues all its loads before its x
+// gathers).  Long rows: a warp takes a group of up to 4 of the row's 64-value
+// chunks, publishes its partial with a release increment of the row's
+// counter, and the warp that completes the count sums the row's partials in
+// group order and resets the counter (no waiting), so the result is
+// deterministic.
 #include "bsp_internal.cuh"
 #include "util.cuh"
 
@@ -37,6 +39,7 @@ namespace bsp {
 
 constexpr int kTile = 32;          // MMA_M * MMA_K
 constexpr int kLongChunk = 64;     // MMA_M * MMA_K * loopNum_long
+constexpr int kLongGroup = 4;      // chunks of one long row per SpMV warp
 enum : int32_t { kC1 = 0, kC2 = 1, kC3 = 2, kC4 = 3, kCLong = 4, kCBlock = 5, kCZero = 6 };
 
 __global__ void dasp_classify_kernel(int32_t rows, const int32_t *__restrict__ rowPtr, int32_t block_longest,
@@ -163,6 +166,26 @@ __global__ void dasp_long_fill_kernel(int32_t row_long, const int32_t *__restric
       lcid[o + (j - s)] = colIdx[j];
     }
     for (int32_t w = wptr[i] + lane; w < wptr[i + 1]; w += 32) wrow[w] = (int32_t)i;
+  }
+}
+
+__global__ void dasp_long_groups_kernel(int32_t row_long, const int32_t *__restrict__ wptr,
+                                        int32_t *__restrict__ ngroups) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < row_long; i += (int64_t)gridDim.x * blockDim.x)
+    ngroups[i] = (wptr[i + 1] - wptr[i] + kLongGroup - 1) / kLongGroup;
+}
+
+__global__ void dasp_group_info_kernel(int32_t row_long, const int32_t *__restrict__ gptr,
+                                       const int32_t *__restrict__ wptr, int4 *__restrict__ info) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < row_long; i += nwarps) {
+    const int32_t g0 = gptr[i], ng = gptr[i + 1] - g0;
+    for (int32_t k = lane; k < ng; k += 32) {
+      const int32_t c0 = wptr[i] + k * kLongGroup;
+      const int32_t nc = min(kLongGroup, wptr[i + 1] - c0);
+      info[g0 + k] = make_int4((int32_t)i, c0, g0, nc | (ng << 4));
+    }
   }
 }
 
@@ -401,6 +424,23 @@ bsp_status csr2dasp_impl(int32_t rows, int32_t cols, int32_t nnz, const int32_t 
         d.row_long, lrid, rowPtr, colIdx, values, d.long_ptr_warp, d.long_val, d.long_cid, d.long_row_of_warp);
     BSP_LAUNCH_CHECK();
   }
+  // SpMV work split: groups of kLongGroup chunks of one row
+  BSP_TRY(dalloc(&d.long_group_ptr, (size_t)d.row_long + 1, s));
+  BSP_CUDA(cudaMemsetAsync(d.long_group_ptr + d.row_long, 0, sizeof(int32_t), s));
+  if (d.row_long > 0) {
+    dasp_long_groups_kernel<<<dgrid(d.row_long), 256, 0, s>>>(d.row_long, d.long_ptr_warp, d.long_group_ptr);
+    BSP_LAUNCH_CHECK();
+  }
+  BSP_TRY(exclusive_scan_i32(d.long_group_ptr, d.long_group_ptr, (int64_t)d.row_long + 1, d_total, s));
+  int64_t ng = 0;
+  BSP_TRY(read_i64(d_total, &ng, s));
+  d.long_groups = (int32_t)ng;
+  BSP_TRY(dalloc(&d.long_group_info, (size_t)(ng > 0 ? 4 * ng : 4), s));
+  if (d.row_long > 0) {
+    dasp_group_info_kernel<<<dgrid((int64_t)d.row_long * 32), 256, 0, s>>>(
+        d.row_long, d.long_group_ptr, d.long_ptr_warp, reinterpret_cast<int4 *>(d.long_group_info));
+    BSP_LAUNCH_CHECK();
+  }
   // --- row-block part (dasp.cu:1244, :1374-1482)
   int32_t *bkey = nullptr;
   BSP_TRY(dalloc(&bkey, (size_t)d.row_block + 1, s));
@@ -482,16 +522,32 @@ bsp_status csr2dasp_impl(int32_t rows, int32_t cols, int32_t nnz, const int32_t 
 
 // ---------------------------------------------------------------------------
 // Fused SpMV.  Grid sections (CTAs of 256 threads = 8 warps), in order:
-// long chunks (warp each), row blocks (warp each), len-1 rows (thread each),
-// 1&3 tile pairs (warp per 2 tiles), 3/4 tiles (warp per 4 tiles), 2&2 tile
-// pairs (warp per 2 tiles), empty rows (thread each).
+// long-row groups (warp each, up to 4 chunks of 64), row blocks (warp each),
+// len-1 rows (8 per thread), 1&3 tile slots (2 per thread), 3/4 tile rows
+// (2 per thread), 2&2 tile rows (2 per thread), empty rows (thread each).
+// Every thread issues all of its loads before the dependent x gathers, so
+// each warp keeps several independent memory requests in flight.
 struct DaspSections {
   int32_t long_cta, reg_cta, s1_cta, t13_cta, t34_cta, t22_cta, zero_cta;
 };
+constexpr int kS1PerThread = 8;
+constexpr int kShortPerThread = 2;
 
-__device__ __forceinline__ void dasp_store(double *y, const int32_t *outIdx, int64_t k, double v, double alpha,
-                                           double beta) {
-  const int64_t yi = outIdx ? outIdx[k] : k;
+// Device-scope atomic add with acquire-release ordering: the caller's earlier
+// stores are visible to whoever acquires through this counter later, and the
+// caller sees every store released into it before.
+__device__ __forceinline__ int32_t atomic_add_acq_rel(int32_t *p, int32_t v) {
+  int32_t old;
+  asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
+
+// y slot k -> element index (order_rid when the output is not permuted)
+__device__ __forceinline__ int64_t dasp_yidx(const int32_t *outIdx, int64_t k) {
+  return outIdx ? (int64_t)__ldg(outIdx + k) : k;
+}
+
+__device__ __forceinline__ void dasp_put(double *y, int64_t yi, double v, double alpha, double beta) {
   double r = alpha * v;
   if (beta != 0.0) r += beta * y[yi];
   y[yi] = r;
@@ -511,29 +567,44 @@ __global__ void __launch_bounds__(256) dasp_spmv_kernel(bsp_dasp D, DaspSections
   const int wib = threadIdx.x >> 5;
   int32_t b = blockIdx.x;
   if (b < S.long_cta) {
-    const int64_t w = (int64_t)b * 8 + wib;
-    if (w >= D.long_warps) return;
-    const double2 v = __ldg(reinterpret_cast<const double2 *>(D.long_val + w * kLongChunk) + lane);
-    const int2 c = __ldg(reinterpret_cast<const int2 *>(D.long_cid + w * kLongChunk) + lane);
-    double p = fma(v.x, ld_x(x + c.x), v.y * ld_x(x + c.y));
+    const int64_t g = (int64_t)b * 8 + wib;
+    if (g >= D.long_groups) return;
+    const int4 gi = __ldg(reinterpret_cast<const int4 *>(D.long_group_info) + g);
+    const int32_t row = gi.x, c0 = gi.y, g0 = gi.z, nc = gi.w & 15, ng = gi.w >> 4;
+    const uint64_t pol = evict_first_policy();
+    const int64_t yi = lane == 0 ? dasp_yidx(outIdx, row) : 0;
+    double2 v[kLongGroup];
+    int2 c[kLongGroup];
+#pragma unroll
+    for (int k = 0; k < kLongGroup; ++k)
+      if (k < nc) {
+        v[k] = ld_stream_f64x2(D.long_val + (int64_t)(c0 + k) * kLongChunk + 2 * lane, pol);
+        c[k] = __ldg(reinterpret_cast<const int2 *>(D.long_cid + (int64_t)(c0 + k) * kLongChunk) + lane);
+      }
+    double p = 0.0;
+#pragma unroll
+    for (int k = 0; k < kLongGroup; ++k)
+      if (k < nc) p = fma(v[k].y, ld_x(x + c[k].y), fma(v[k].x, ld_x(x + c[k].x), p));
     p = warp_sum(p);
-    const int32_t row = D.long_row_of_warp[w];
+    if (ng == 1) {  // the whole row in this warp
+      if (lane == 0) dasp_put(y, yi, p, alpha, beta);
+      return;
+    }
+    // publish the partial with a release increment; the warp that brings the
+    // counter to ng acquires every other group's partial and sums them
     int32_t last = 0;
     if (lane == 0) {
-      D.warp_val[w] = p;
-      __threadfence();
-      const int32_t nw = D.long_ptr_warp[row + 1] - D.long_ptr_warp[row];
-      last = atomicAdd(&D.long_done[row], 1) == nw - 1;
+      D.warp_val[g] = p;
+      last = atomic_add_acq_rel(&D.long_done[row], 1) == ng - 1;
     }
     last = __shfl_sync(0xffffffffu, last, 0);
-    if (last) {  // every chunk of this row is stored: sum them in order
-      __threadfence();
-      const int32_t w0 = D.long_ptr_warp[row], w1 = D.long_ptr_warp[row + 1];
+    if (last) {  // every group of this row is stored: sum them in order
+      __syncwarp();
       double sum = 0.0;
-      for (int32_t k = w0 + lane; k < w1; k += 32) sum += __ldcg(D.warp_val + k);
+      for (int32_t k = g0 + lane; k < g0 + ng; k += 32) sum += __ldcg(D.warp_val + k);
       sum = warp_sum(sum);
       if (lane == 0) {
-        dasp_store(y, outIdx, row, sum, alpha, beta);
+        dasp_put(y, yi, sum, alpha, beta);
         D.long_done[row] = 0;  // ready for the next call
       }
     }
@@ -543,96 +614,193 @@ __global__ void __launch_bounds__(256) dasp_spmv_kernel(bsp_dasp D, DaspSections
   if (b < S.reg_cta) {
     const int64_t bid = (int64_t)b * 8 + wib;
     if (bid * 8 >= D.row_block) return;
-    const int32_t p0 = D.block_ptr[bid], p1 = D.block_ptr[bid + 1];
-    // lane: tile slot t (4 tiles per step), row r of the 8-row block
+    // lane: tile slot t (4 tiles per step, two steps in flight), row r; the
+    // row's irregular tail is split over the same 4 slots
     const int t = lane >> 3, r = lane & 7;
+    const int64_t row = bid * 8 + r;
+    const bool live = row < D.row_block;
+    const int32_t p0 = D.block_ptr[bid], p1 = D.block_ptr[bid + 1];
+    const int32_t i0 = live ? __ldg(D.irreg_rpt + row) : 0, i1 = live ? __ldg(D.irreg_rpt + row + 1) : 0;
+    const int64_t yi = (live && t == 0) ? dasp_yidx(outIdx, D.row_long + row) : 0;
     double acc = 0.0;
-    for (int32_t o = p0 + t * kTile; o < p1; o += 4 * kTile) {
-      const f64x4 v = ld_stream_f64x4(D.reg_val + o + r * 4);
-      const int4 c = __ldg(reinterpret_cast<const int4 *>(D.reg_cid + o + r * 4));
-      acc = fma(v.x, ld_x(x + c.x), acc);
-      acc = fma(v.y, ld_x(x + c.y), acc);
-      acc = fma(v.z, ld_x(x + c.z), acc);
-      acc = fma(v.w, ld_x(x + c.w), acc);
+    int32_t o = p0 + t * kTile;
+    int32_t j = i0 + t;
+    for (; o + 4 * kTile < p1; o += 8 * kTile) {
+      const f64x4 v0 = ld_stream_f64x4(D.reg_val + o + r * 4);
+      const int4 c0 = __ldg(reinterpret_cast<const int4 *>(D.reg_cid + o + r * 4));
+      const f64x4 v1 = ld_stream_f64x4(D.reg_val + o + 4 * kTile + r * 4);
+      const int4 c1 = __ldg(reinterpret_cast<const int4 *>(D.reg_cid + o + 4 * kTile + r * 4));
+      acc = fma(v0.x, ld_x(x + c0.x), acc);
+      acc = fma(v0.y, ld_x(x + c0.y), acc);
+      acc = fma(v0.z, ld_x(x + c0.z), acc);
+      acc = fma(v0.w, ld_x(x + c0.w), acc);
+      acc = fma(v1.x, ld_x(x + c1.x), acc);
+      acc = fma(v1.y, ld_x(x + c1.y), acc);
+      acc = fma(v1.z, ld_x(x + c1.z), acc);
+      acc = fma(v1.w, ld_x(x + c1.w), acc);
     }
+    {  // last step of tiles together with the first irregular element
+      const bool has_t = o < p1, has_i = j < i1;
+      f64x4 v = {0.0, 0.0, 0.0, 0.0};
+      int4 c = {0, 0, 0, 0};
+      double iv = 0.0;
+      int32_t ic = 0;
+      if (has_t) {
+        v = ld_stream_f64x4(D.reg_val + o + r * 4);
+        c = __ldg(reinterpret_cast<const int4 *>(D.reg_cid + o + r * 4));
+      }
+      if (has_i) {
+        iv = __ldg(D.irreg_val + j);
+        ic = __ldg(D.irreg_cid + j);
+      }
+      if (has_t) {
+        acc = fma(v.x, ld_x(x + c.x), acc);
+        acc = fma(v.y, ld_x(x + c.y), acc);
+        acc = fma(v.z, ld_x(x + c.z), acc);
+        acc = fma(v.w, ld_x(x + c.w), acc);
+      }
+      if (has_i) acc = fma(iv, ld_x(x + ic), acc);
+    }
+    for (j += 4; j < i1; j += 4) acc = fma(__ldg(D.irreg_val + j), ld_x(x + __ldg(D.irreg_cid + j)), acc);
     acc += __shfl_xor_sync(0xffffffffu, acc, 8);
     acc += __shfl_xor_sync(0xffffffffu, acc, 16);
-    const int64_t row = bid * 8 + r;
-    if (t == 0 && row < D.row_block) {
-      for (int32_t j = D.irreg_rpt[row]; j < D.irreg_rpt[row + 1]; ++j)
-        acc = fma(D.irreg_val[j], ld_x(x + D.irreg_cid[j]), acc);
-      dasp_store(y, outIdx, D.row_long + row, acc, alpha, beta);
-    }
+    if (t == 0 && live) dasp_put(y, yi, acc, alpha, beta);
     return;
   }
   b -= S.reg_cta;
   const int64_t ybase = (int64_t)D.row_long + D.row_block;
   if (b < S.s1_cta) {
-    const int64_t i = (int64_t)b * 256 + threadIdx.x;
-    if (i < D.short_row_1) dasp_store(y, outIdx, ybase + i, D.short_val[i] * ld_x(x + D.short_cid[i]), alpha, beta);
+    const int64_t i0 = (int64_t)b * 256 * kS1PerThread + threadIdx.x;
+    double v[kS1PerThread];
+    int32_t c[kS1PerThread];
+    int64_t yi[kS1PerThread];
+    const uint64_t pol = evict_first_policy();
+#pragma unroll
+    for (int k = 0; k < kS1PerThread; ++k) {
+      const int64_t i = i0 + k * 256;
+      if (i < D.short_row_1) {
+        v[k] = ld_stream_f64(D.short_val + i, pol);
+        c[k] = ld_stream_s32(D.short_cid + i, pol);
+        yi[k] = dasp_yidx(outIdx, ybase + i);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < kS1PerThread; ++k) {
+      const int64_t i = i0 + k * 256;
+      if (i < D.short_row_1) dasp_put(y, yi[k], v[k] * ld_x(x + c[k]), alpha, beta);
+    }
     return;
   }
   b -= S.s1_cta;
   const double *sv = D.short_val + D.short_row_1;
   const int32_t *sc = D.short_cid + D.short_row_1;
   if (b < S.t13_cta) {
-    // warp w: tiles 2w, 2w+1; lane o -> tile T = o/16, q = o%16: q < 8 the len-1
-    // row of tile row q, else the len-3 row of tile row q-8
-    const int64_t w = (int64_t)b * 8 + wib;
-    const int T = lane >> 4, q = lane & 15, j = q & 7;
-    const int64_t tile = 2 * w + T;
-    const int64_t slot = w * 32 + lane;
-    if (tile >= D.short_block13 || slot >= 2 * (int64_t)D.common_13) return;
-    const double *pv = sv + tile * kTile + j * 4;
-    const int32_t *pc = sc + tile * kTile + j * 4;
-    double v;
-    if (q < 8) {
-      v = __ldg(pv) * ld_x(x + __ldg(pc));
-    } else {
-      v = fma(__ldg(pv + 3), ld_x(x + __ldg(pc + 3)),
-              fma(__ldg(pv + 2), ld_x(x + __ldg(pc + 2)), __ldg(pv + 1) * ld_x(x + __ldg(pc + 1))));
+    // slot s: tile s/16, q = s%16: q < 8 the len-1 row of tile row q, else
+    // the len-3 row of tile row q-8
+    const int64_t s0 = (int64_t)b * 256 * kShortPerThread + threadIdx.x;
+    const int64_t ns = 2 * (int64_t)D.common_13;
+    double v[kShortPerThread][3];
+    int32_t c[kShortPerThread][3];
+    int64_t yi[kShortPerThread];
+#pragma unroll
+    for (int k = 0; k < kShortPerThread; ++k) {
+      const int64_t s = s0 + k * 256;
+      if (s < ns) {
+        yi[k] = dasp_yidx(outIdx, ybase + D.short_row_1 + s);
+        const int q = (int)(s & 15), j = q & 7;
+        const int64_t o = (s >> 4) * kTile + j * 4;
+        if (q < 8) {
+          v[k][0] = __ldg(sv + o);
+          c[k][0] = __ldg(sc + o);
+        } else {
+#pragma unroll
+          for (int m = 0; m < 3; ++m) {
+            v[k][m] = __ldg(sv + o + 1 + m);
+            c[k][m] = __ldg(sc + o + 1 + m);
+          }
+        }
+      }
     }
-    dasp_store(y, outIdx, ybase + D.short_row_1 + slot, v, alpha, beta);
+#pragma unroll
+    for (int k = 0; k < kShortPerThread; ++k) {
+      const int64_t s = s0 + k * 256;
+      if (s < ns) {
+        double a;
+        if ((s & 15) < 8)
+          a = v[k][0] * ld_x(x + c[k][0]);
+        else
+          a = fma(v[k][2], ld_x(x + c[k][2]), fma(v[k][1], ld_x(x + c[k][1]), v[k][0] * ld_x(x + c[k][0])));
+        dasp_put(y, yi[k], a, alpha, beta);
+      }
+    }
     return;
   }
   b -= S.t13_cta;
   const double *sv34 = sv + D.fill0_nnz_short13;
   const int32_t *sc34 = sc + D.fill0_nnz_short13;
   if (b < S.t34_cta) {
-    // warp w: tiles 4w..4w+3; lane o = row o%8 of tile 4w + o/8 (4 values)
-    const int64_t w = (int64_t)b * 8 + wib;
-    const int64_t slot = w * 32 + lane;
-    if (slot >= D.short_row_34) return;
-    const f64x4 v = dasp_ld4<SHORT_ALIGNED>(sv34 + slot * 4);
-    const int4 c = make_int4(__ldg(sc34 + slot * 4), __ldg(sc34 + slot * 4 + 1), __ldg(sc34 + slot * 4 + 2),
-                             __ldg(sc34 + slot * 4 + 3));
-    double a = v.x * ld_x(x + c.x);
-    a = fma(v.y, ld_x(x + c.y), a);
-    a = fma(v.z, ld_x(x + c.z), a);
-    a = fma(v.w, ld_x(x + c.w), a);
-    dasp_store(y, outIdx, ybase + D.short_row_1 + 2 * (int64_t)D.common_13 + slot, a, alpha, beta);
+    // slot s = row s%8 of tile s/8: 4 values at sv34 + 4s
+    const int64_t s0 = (int64_t)b * 256 * kShortPerThread + threadIdx.x;
+    f64x4 v[kShortPerThread];
+    int4 c[kShortPerThread];
+    int64_t yi[kShortPerThread];
+#pragma unroll
+    for (int k = 0; k < kShortPerThread; ++k) {
+      const int64_t s = s0 + k * 256;
+      if (s < D.short_row_34) {
+        yi[k] = dasp_yidx(outIdx, ybase + D.short_row_1 + 2 * (int64_t)D.common_13 + s);
+        v[k] = dasp_ld4<SHORT_ALIGNED>(sv34 + s * 4);
+        c[k] = make_int4(__ldg(sc34 + s * 4), __ldg(sc34 + s * 4 + 1), __ldg(sc34 + s * 4 + 2),
+                         __ldg(sc34 + s * 4 + 3));
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < kShortPerThread; ++k) {
+      const int64_t s = s0 + k * 256;
+      if (s < D.short_row_34) {
+        double a = v[k].x * ld_x(x + c[k].x);
+        a = fma(v[k].y, ld_x(x + c[k].y), a);
+        a = fma(v[k].z, ld_x(x + c[k].z), a);
+        a = fma(v[k].w, ld_x(x + c[k].w), a);
+        dasp_put(y, yi[k], a, alpha, beta);
+      }
+    }
     return;
   }
   b -= S.t34_cta;
   const double *sv22 = sv34 + D.fill0_nnz_short34;
   const int32_t *sc22 = sc34 + D.fill0_nnz_short34;
   if (b < S.t22_cta) {
-    // warp w: tiles 2w, 2w+1; lane o -> tile T = o/16, q = o%16 = row j of
-    // 16: positions (j%8)*4 + (j/8)*2 + {0,1}
-    const int64_t w = (int64_t)b * 8 + wib;
-    const int T = lane >> 4, q = lane & 15;
-    const int64_t slot = w * 32 + lane;
-    if (slot >= D.short_row_2) return;
-    const int64_t o = (2 * w + T) * kTile + (q & 7) * 4 + (q >> 3) * 2;
-    const double a = fma(__ldg(sv22 + o + 1), ld_x(x + __ldg(sc22 + o + 1)), __ldg(sv22 + o) * ld_x(x + __ldg(sc22 + o)));
-    dasp_store(y, outIdx, ybase + D.short_row_1 + 2 * (int64_t)D.common_13 + D.short_row_34 + slot, a, alpha,
-               beta);
+    // slot s: tile s/16, q = s%16 -> positions (q%8)*4 + (q/8)*2 + {0,1}
+    const int64_t s0 = (int64_t)b * 256 * kShortPerThread + threadIdx.x;
+    double2 v[kShortPerThread];
+    int2 c[kShortPerThread];
+    int64_t yi[kShortPerThread];
+#pragma unroll
+    for (int k = 0; k < kShortPerThread; ++k) {
+      const int64_t s = s0 + k * 256;
+      if (s < D.short_row_2) {
+        yi[k] = dasp_yidx(outIdx, ybase + D.short_row_1 + 2 * (int64_t)D.common_13 + D.short_row_34 + s);
+        const int q = (int)(s & 15);
+        const int64_t o = (s >> 4) * kTile + (q & 7) * 4 + (q >> 3) * 2;
+        v[k] = make_double2(__ldg(sv22 + o), __ldg(sv22 + o + 1));
+        c[k] = make_int2(__ldg(sc22 + o), __ldg(sc22 + o + 1));
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < kShortPerThread; ++k) {
+      const int64_t s = s0 + k * 256;
+      if (s < D.short_row_2) {
+        const double a = fma(v[k].y, ld_x(x + c[k].y), v[k].x * ld_x(x + c[k].x));
+        dasp_put(y, yi[k], a, alpha, beta);
+      }
+    }
     return;
   }
   b -= S.t22_cta;
   {
     const int64_t i = (int64_t)b * 256 + threadIdx.x;
-    if (i < D.row_zero) dasp_store(y, outIdx, (int64_t)D.rows - D.row_zero + i, 0.0, alpha, beta);
+    if (i < D.row_zero) dasp_put(y, dasp_yidx(outIdx, (int64_t)D.rows - D.row_zero + i), 0.0, alpha, beta);
   }
 }
 
@@ -640,12 +808,12 @@ bsp_status dasp_spmv_impl(const bsp_dasp *d, const double *x, double *y, double 
                           int32_t permuted_output, cudaStream_t s) {
   if (d->rows == 0) return BSP_OK;
   DaspSections S;
-  S.long_cta = (int32_t)ceil_div(d->long_warps, 8);
+  S.long_cta = (int32_t)ceil_div(d->long_groups, 8);
   S.reg_cta = (int32_t)ceil_div(ceil_div(d->row_block, 8), 8);
-  S.s1_cta = (int32_t)ceil_div(d->short_row_1, 256);
-  S.t13_cta = (int32_t)ceil_div(ceil_div(d->short_block13, 2), 8);
-  S.t34_cta = (int32_t)ceil_div(ceil_div(d->short_row_34, 32), 8);
-  S.t22_cta = (int32_t)ceil_div(ceil_div(d->short_row_2, 32), 8);
+  S.s1_cta = (int32_t)ceil_div(d->short_row_1, 256 * kS1PerThread);
+  S.t13_cta = (int32_t)ceil_div(2 * (int64_t)d->common_13, 256 * kShortPerThread);
+  S.t34_cta = (int32_t)ceil_div(d->short_row_34, 256 * kShortPerThread);
+  S.t22_cta = (int32_t)ceil_div(d->short_row_2, 256 * kShortPerThread);
   S.zero_cta = (int32_t)ceil_div(d->row_zero, 256);
   const int64_t grid = (int64_t)S.long_cta + S.reg_cta + S.s1_cta + S.t13_cta + S.t34_cta + S.t22_cta + S.zero_cta;
   if (grid == 0) return BSP_OK;
@@ -698,6 +866,8 @@ extern "C" bsp_status bsp_dasp_free(bsp_dasp *d) {
   dfree(d->order_rid, s);
   dfree(d->sorted_rid, s);
   dfree(d->row_len_sorted, s);
+  dfree(d->long_group_ptr, s);
+  dfree(d->long_group_info, s);
   BSP_CUDA(cudaStreamSynchronize(s));
   return BSP_OK;
 }

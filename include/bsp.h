@@ -297,6 +297,13 @@ typedef struct {
   int32_t *order_rid;                          /* [rows] y slot -> row */
   int32_t *sorted_rid;                         /* [row_block] row-block rows, sorted */
   int32_t *row_len_sorted;                     /* [row_block+1] prefix of their lengths */
+  /* SpMV work split of the long rows: groups of up to 8 consecutive chunks
+   * of one row, one warp each */
+  int32_t long_groups;
+  int32_t *long_group_ptr;                     /* [row_long+1] group prefix */
+  int32_t *long_group_info;                    /* [4*long_groups] per group: long-row
+                                                  index, first chunk, first group of
+                                                  the row, chunks | row's groups << 4 */
 } bsp_dasp;
 
 /* CSR -> DASP on the device, arrays bit-identical to spmv_all's host

@@ -89,6 +89,8 @@ def test_dasp_spmv(cuda, golden, kind):
     tol = pyoracle.spmv_tolerance(A.rowptr, A.colidx, A.values, x)
     rp, ci, va, xx = _dev(cuda, A.rowptr, A.colidx, A.values, x)
     D = bsp.csr2dasp(rp, ci, va, rows=A.rows, cols=A.cols)
+    chunks = np.diff(D.arrays()["long_ptr_warp"])
+    assert D.long_groups == int(np.sum((chunks + 3) // 4))   # up to 4 chunks of a row per warp
     for _ in range(3):  # repeated calls reuse the long-row counters
         y = D.spmv(xx).cpu().numpy()
         assert np.all(np.abs(y - ref) <= tol)
