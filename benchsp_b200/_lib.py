@@ -111,6 +111,8 @@ _PROTOS = {
     "bsp_memcpy_d2h": (C.c_int, [_P, _P, C.c_size_t]),
     "bsp_memcpy_h2d": (C.c_int, [_P, _P, C.c_size_t]),
     "bsp_device_sync": (C.c_int, []),
+    "bsp_device_alloc": (C.c_int, [C.POINTER(C.c_void_p), C.c_size_t]),
+    "bsp_device_free": (C.c_int, [_P]),
     "bsp_csr_spmv": (C.c_int, [_I32, _I32, _I32, _P, _P, _P, C.c_int, _P, _P, _D, _D, _I32, _I32, _P]),
     "bsp_csr_merge_workspace": (C.c_size_t, [_I32, _I32]),
     "bsp_csr_spmv_merge_f64": (C.c_int, [_I32, _I32, _I32, _P, _P, _P, _P, _P, _D, _D, _P, C.c_size_t, _P]),
