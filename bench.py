@@ -52,6 +52,24 @@ def algorithmic_bytes_bsr(nb: int, blc_row: int, n: int, bs: int = 4) -> int:
     return nb * bs * bs * 8 + nb * 4 + (blc_row + 1) * 4 + n * 8 + n * 8
 
 
+def max_over_ranks(ms: float, ws: int, device) -> float:
+    """The slowest rank's time: every rank passes its own CUDA-event time;
+    all ranks return the maximum (a no-op for one rank)."""
+    if ws <= 1:
+        return ms
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_gflops(ws: int, flops_per_step: float, steps: int, ms: float) -> float:
+    """Whole-job throughput of `ws` replicas that each ran `steps` steps of
+    `flops_per_step`, over the slowest rank's time `ms` (weak scaling)."""
+    return ws * flops_per_step * steps / (ms / 1e3) / 1e9
+
+
 def dist_init():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -245,14 +263,11 @@ def run_ours(args, ws, rank, local):
             M.spmv(x, y)
         ev1.record(stream)
         torch.cuda.synchronize()
-    ms = ev0.elapsed_time(ev1)
+    ms = max_over_ranks(ev0.elapsed_time(ev1), ws, dev)
     if ws > 1:
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
         torch.distributed.barrier()
     ms_step = ms / args.steps
-    value = ws * flops * args.steps / (ms / 1e3) / 1e9
+    value = job_gflops(ws, flops, args.steps, ms)
 
     # e2e through the host-buffer C-ABI call: H2D x, SpMV, D2H y per step
     xh = torch.from_numpy(x_h).pin_memory()
@@ -271,12 +286,8 @@ def run_ours(args, ws, rank, local):
         M.spmv_host(xh_np, yh_np)
     e1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
-    if ws > 1:
-        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = ws * flops * e2e_steps / (e2e_ms / 1e3) / 1e9
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), ws, dev)
+    e2e_value = job_gflops(ws, flops, e2e_steps, e2e_ms)
 
     # correctness of the benchmarked result (cheap, outside the timed region)
     y_np = y.cpu().numpy()

@@ -1,0 +1,53 @@
+"""bench.py's multi-rank logic on CPU: two gloo ranks (127.0.0.1), each with
+its own step time; both see the slowest rank's time and the whole-job value
+counts the work of both replicas (weak scaling)."""
+import os
+import socket
+import sys
+from pathlib import Path
+
+import pytest
+import torch.multiprocessing as mp
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def _free_port() -> int:
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank(rank, ws, port, out):
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    sys.path.insert(0, str(ROOT))
+    import bench
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=ws, timeout=datetime.timedelta(seconds=60))
+    try:
+        ms = 10.0 * (rank + 1)                       # rank 1 is the slow one
+        m = bench.max_over_ranks(ms, ws, torch.device("cpu"))
+        out[rank] = (m, bench.job_gflops(ws, 2.0e9, 100, m))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_take_the_slowest_time():
+    ctx = mp.get_context("spawn")
+    out = ctx.Manager().dict()
+    port = _free_port()
+    mp.start_processes(_rank, args=(2, port, out), nprocs=2, join=True, start_method="spawn")
+    assert out[0][0] == out[1][0] == 20.0
+    # 2 replicas x 100 steps x 2 GFLOP in 20 ms
+    assert out[0][1] == pytest.approx(2 * 2.0 * 100 / 0.020)
+
+
+def test_single_rank_is_a_no_op():
+    sys.path.insert(0, str(ROOT))
+    import bench
+    assert bench.max_over_ranks(3.5, 1, None) == 3.5
+    assert bench.job_gflops(1, 1e9, 10, 1000.0) == pytest.approx(10.0)
