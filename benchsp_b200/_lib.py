@@ -222,6 +222,27 @@ _PROTOS.update({
 })
 
 
+class BspTuneResult(C.Structure):
+    """Mirror of bsp_tune_result (include/bsp.h)."""
+    _fields_ = [("format", C.c_int32), ("csr_algo", C.c_int32), ("lanes", C.c_int32), ("bs", C.c_int32),
+                ("bsr_algo", C.c_int32), ("from_cache", C.c_int32), ("spmv_us", C.c_double), ("key", C.c_uint64),
+                ("mean_len", C.c_double), ("cv_len", C.c_double), ("fill4", C.c_double), ("fill8", C.c_double),
+                ("max_len", C.c_int32), ("long_rows", C.c_int32)]
+
+
+FMT_CSR, FMT_BSR, FMT_DASP = 0, 1, 2
+
+_PROTOS.update({
+    "bsp_tune_spmv": (C.c_int, [_I32, _I32, _I32, _P, _P, _P, _I32, C.POINTER(BspTuneResult), _P]),
+    "bsp_matrix_key": (C.c_int, [_I32, _I32, _I32, _P, _P, C.POINTER(C.c_uint64), _P]),
+    "bsp_tune_cache_clear": (None, []),
+    "bsp_spmv_plan_create": (C.c_int, [_I32, _I32, _I32, _P, _P, _P, _I32, C.POINTER(C.c_void_p), _P]),
+    "bsp_spmv_plan_choice": (C.c_int, [C.c_void_p, C.POINTER(BspTuneResult)]),
+    "bsp_spmv_plan_run": (C.c_int, [C.c_void_p, _P, _P, _D, _D, _P]),
+    "bsp_spmv_plan_destroy": (C.c_int, [C.c_void_p]),
+})
+
+
 class BspSpmmPlan(C.Structure):
     """Mirror of bsp_spmm_plan (include/bsp.h)."""
     _fields_ = [("rows", C.c_int32), ("chunk", C.c_int32), ("nchunks", C.c_int64), ("nparts", C.c_int64),

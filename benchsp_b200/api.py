@@ -699,3 +699,74 @@ def gen_batch(count: int, seed: int, n_lo: int = 1000, n_hi: int = 65536) -> lis
             out.append(gen_powerlaw(n, 2.2, n, seed * 1000 + i))
     return out
 
+
+# ---------------------------------------------------------------------------
+# Format autotuner (no reference counterpart)
+
+_FMT_NAMES = {_lib.FMT_CSR: "csr", _lib.FMT_BSR: "bsr", _lib.FMT_DASP: "dasp"}
+
+
+def _tune_dict(r: "_lib.BspTuneResult") -> dict:
+    d = {k: getattr(r, k) for k, _ in _lib.BspTuneResult._fields_}
+    d["format_name"] = _FMT_NAMES.get(r.format, "?")
+    return d
+
+
+def tune_spmv(rowptr, colidx, values, *, cols: int, measure: bool = False, stream=None) -> dict:
+    """Chooses the FP64 SpMV format for a device CSR matrix (cached by structure)."""
+    r = _lib.BspTuneResult()
+    check(lib().bsp_tune_spmv(rowptr.numel() - 1, cols, colidx.numel(), _dptr(rowptr, "rowptr"),
+                              _dptr(colidx, "colidx"), _dptr(values, "values"), int(measure), C.byref(r),
+                              _stream(stream)))
+    return _tune_dict(r)
+
+
+def matrix_key(rowptr, colidx, *, cols: int, stream=None) -> int:
+    k = C.c_uint64()
+    check(lib().bsp_matrix_key(rowptr.numel() - 1, cols, colidx.numel(), _dptr(rowptr, "rowptr"),
+                               _dptr(colidx, "colidx"), C.byref(k), _stream(stream)))
+    return k.value
+
+
+def tune_cache_clear() -> None:
+    lib().bsp_tune_cache_clear()
+
+
+class SpmvPlan:
+    """Tuned FP64 SpMV: converts once to the chosen format and runs it (the
+    CSR tensors must stay alive)."""
+
+    def __init__(self, rowptr, colidx, values, *, cols: int, measure: bool = False, stream=None):
+        self._keep = (rowptr, colidx, values)
+        self.rows = rowptr.numel() - 1
+        self._h = C.c_void_p()
+        check(lib().bsp_spmv_plan_create(self.rows, cols, colidx.numel(), _dptr(rowptr, "rowptr"),
+                                         _dptr(colidx, "colidx"), _dptr(values, "values"), int(measure),
+                                         C.byref(self._h), _stream(stream)))
+
+    @property
+    def choice(self) -> dict:
+        r = _lib.BspTuneResult()
+        check(lib().bsp_spmv_plan_choice(self._h, C.byref(r)))
+        return _tune_dict(r)
+
+    def spmv(self, x, y=None, *, alpha: float = 1.0, beta: float = 0.0, stream=None):
+        torch = _torch()
+        if y is None:
+            y = torch.empty(self.rows, dtype=torch.float64, device=x.device)
+            beta = 0.0
+        check(lib().bsp_spmv_plan_run(self._h, _dptr(x, "x"), _dptr(y, "y"), float(alpha), float(beta),
+                                      _stream(stream)))
+        return y
+
+    def close(self) -> None:
+        if self._h:
+            check(lib().bsp_spmv_plan_destroy(self._h))
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+

@@ -454,6 +454,55 @@ bsp_status bsp_blockinfo(int32_t rows, int32_t cols, int32_t nnz,
                          bsp_stream_t stream);
 
 /* ---------------------------------------------------------------------- */
+/* Format autotuner for FP64 SpMV (no reference counterpart: the reference's
+ * drivers run every format on every matrix, bench/spmvfp64.cpp:135-177).
+ * Model mode decides from row-length statistics and exact 4x4 / 8x8 block
+ * counts; measure mode converts to each candidate that can pay off, times
+ * them and keeps the fastest.  Results are cached per process by a
+ * structural hash of (rows, cols, nnz, rowPtr, colIdx); with the environment
+ * variable BSP_TUNE_CACHE set to a file path, the cache is also read from
+ * and appended to that file. */
+typedef enum { BSP_FMT_CSR = 0, BSP_FMT_BSR = 1, BSP_FMT_DASP = 2 } bsp_format;
+
+typedef struct {
+  int32_t format;   /* bsp_format */
+  int32_t csr_algo; /* BSP_CSR_VECTOR or BSP_CSR_MERGE (format CSR) */
+  int32_t lanes;    /* lanes per row (CSR vector) */
+  int32_t bs;       /* 4 or 8 (format BSR) */
+  int32_t bsr_algo; /* BSP_BSR_FFMA / DMMA / ADAPTIVE (format BSR) */
+  int32_t from_cache;
+  double spmv_us;   /* measured time of the choice (measure mode), else 0 */
+  uint64_t key;     /* structural hash */
+  /* statistics the model used */
+  double mean_len, cv_len, fill4, fill8;
+  int32_t max_len;
+  int32_t long_rows; /* rows with >= 256 nonzeros */
+} bsp_tune_result;
+
+bsp_status bsp_tune_spmv(int32_t rows, int32_t cols, int32_t nnz,
+                         const int32_t *rowPtr, const int32_t *colIdx,
+                         const double *values, int32_t measure,
+                         bsp_tune_result *out, bsp_stream_t stream);
+/* Structural hash only. */
+bsp_status bsp_matrix_key(int32_t rows, int32_t cols, int32_t nnz,
+                          const int32_t *rowPtr, const int32_t *colIdx,
+                          uint64_t *key, bsp_stream_t stream);
+void bsp_tune_cache_clear(void);
+
+/* A tuned SpMV executor: holds the chosen format's arrays (the CSR arrays
+ * must stay alive for the CSR choice). */
+typedef struct bsp_spmv_plan_s *bsp_spmv_plan;
+bsp_status bsp_spmv_plan_create(int32_t rows, int32_t cols, int32_t nnz,
+                                const int32_t *rowPtr, const int32_t *colIdx,
+                                const double *values, int32_t measure,
+                                bsp_spmv_plan *plan, bsp_stream_t stream);
+bsp_status bsp_spmv_plan_choice(bsp_spmv_plan plan, bsp_tune_result *out);
+/* y = alpha*A*x + beta*y in the original row order. */
+bsp_status bsp_spmv_plan_run(bsp_spmv_plan plan, const double *x, double *y,
+                             double alpha, double beta, bsp_stream_t stream);
+bsp_status bsp_spmv_plan_destroy(bsp_spmv_plan plan);
+
+/* ---------------------------------------------------------------------- */
 /* Batched SpMV / SpMM over many independent CSR matrices (no reference
  * counterpart: the reference launches one matrix at a time, e.g.
  * src/csrspmv.cu:104-170).  One persistent kernel processes a work list
