@@ -4,13 +4,17 @@
 // benchmark's CG configuration: 3-D 7-point Poisson, tolerance 1e-10 on
 // ||b - A x|| / ||b|| checked in FP64.
 //
-// Mixed precision: the matrix is stored a second time with values in FP32,
-// FP16 or BF16.  FP16/BF16 values carry one power-of-two exponent per group of
-// 32 consecutive nonzeros (v = stored * 2^e, the group maximum scaled into
-// [1, 2)), and column indices are stored as int16 offsets from the row when
-// every |col - row| < 32768 (banded matrices), else int32.  A nonzero then
-// moves 4 bytes (FP16/BF16 + int16) instead of 12 (FP64 + int32).  CG
-// iterations run on that matrix with FP32 vectors (dot products in FP64).
+// Mixed precision: the matrix is stored a second time, in SELL-32 layout
+// (slices of 32 consecutive rows padded to the slice's longest row; entry k of
+// the slice's row l at slice_off + 32 k + l, so the 32 rows of a warp read
+// each k with one coalesced access), with values in FP32, FP16 or BF16.
+// FP16/BF16 values carry one power-of-two exponent per row (v = stored * 2^e,
+// the row's largest magnitude scaled into [1, 2); the row sum is scaled once),
+// and column indices are stored as int16 offsets from the row
+// when every |col - row| < 32768 (banded matrices), else int32.  FP16/BF16
+// values with int16 offsets are packed into one 32-bit word per entry.  A
+// nonzero then moves 4 bytes instead of 12 (FP64 + int32).  CG iterations
+// run on that matrix with FP32 vectors (dot products in FP64).
 // The FP64 state is the solution x64 and the true residual: whenever the
 // iterated residual has dropped by `reliable_delta` since the last update,
 // x64 += x32, r = b - A x64 is recomputed in FP64 with the FP64 matrix and
@@ -29,6 +33,11 @@
 // denominators freeze the iteration (alpha = beta = 0), so iterations run
 // after convergence inside a captured graph are harmless.
 #include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <type_traits>
+#include <vector>
 
 #include "bsp_internal.cuh"
 #include "util.cuh"
@@ -36,7 +45,6 @@
 namespace bsp {
 
 constexpr int kCgThreads = 256;
-constexpr int kScaleGroup = 32;
 constexpr int kRowFirst = 8;  // row entries loaded together per lane
 
 template <typename V> __device__ __forceinline__ float lp_to_float(V v);
@@ -74,25 +82,22 @@ __device__ __forceinline__ double reduce_partials(const double *__restrict__ par
 
 // Matrix access: values V with optional group exponents, columns int32 or
 // int16 offsets from the row.
+// kPacked (FP16/BF16 values with int16 offsets): one 32-bit word per entry,
+// value bits low, offset high, so one load gives both.
 template <typename V, typename VT, bool SCALED, bool DELTA16>
 struct CgMat {
-  const int32_t *rowPtr;
+  static constexpr bool kPacked = SCALED && DELTA16 && sizeof(V) == 2;
+  const int32_t *rowPtr;  // CSR row pointers (FP64 mode)
   const void *cols;
-  const V *val;
+  const V *val;           // SELL values, or the packed words when kPacked
   const int8_t *exps;
+  const int32_t *slice_len;  // SELL-32 (mixed modes)
+  const int64_t *slice_off;
   __device__ __forceinline__ int64_t col(int64_t r, int32_t j) const {
     if (DELTA16) return r + (int64_t) reinterpret_cast<const int16_t *>(cols)[j];
     return reinterpret_cast<const int32_t *>(cols)[j];
   }
-  __device__ __forceinline__ VT value(int32_t j) const {
-    if constexpr (sizeof(V) == 8) {
-      return (VT)val[j];
-    } else {
-      float af = lp_to_float<V>(val[j]);
-      if (SCALED) af *= pow2f(exps[j / kScaleGroup]);
-      return (VT)af;
-    }
-  }
+  __device__ __forceinline__ VT value(int32_t j) const { return (VT)val[j]; }  // CSR (FP64) path
 };
 
 // Kernel A: p_k = r + beta p_prev (own row stored, gathered columns formed on
@@ -114,6 +119,63 @@ __global__ void __launch_bounds__(kCgThreads) cg_dir_spmv_kernel(int32_t n, CgMa
   const VT bt = (VT)beta;
   double dot = 0.0;
   const int64_t stride = (int64_t)gridDim.x * kCgThreads;
+  if constexpr (sizeof(V) < 8) {
+    // SELL-32: warp = slice (the grid stride is a multiple of 32 rows); the
+    // row's power-of-two scale is applied once to its sum; offsets are 32-bit
+    // (the padded matrix has < 2^31 entries).
+    using Mat = CgMat<V, VT, SCALED, DELTA16>;
+    const int lane = threadIdx.x & 31;
+    for (int64_t i = (int64_t)blockIdx.x * kCgThreads + threadIdx.x; i - lane < n; i += stride) {
+      const int32_t sl = (int32_t)(i >> 5);
+      const int32_t len = A.slice_len[sl];
+      const uint32_t base = (uint32_t)A.slice_off[sl];
+      const uint32_t off = base + lane;
+      const bool live = i < n;
+      const int32_t row = (int32_t)i;
+      VT acc = VT(0);
+      const float row_scale = (SCALED && live) ? pow2f(A.exps[i]) : 1.f;
+      {
+        const int32_t kb = 0, kn = len;
+        for (int32_t k0 = 0; k0 < kn; k0 += kRowFirst) {
+          int32_t c[kRowFirst];
+          float a[kRowFirst];
+#pragma unroll
+          for (int k = 0; k < kRowFirst; ++k) {
+            c[k] = row;
+            a[k] = 0.f;
+            if (k0 + k < kn) {
+              const uint32_t j = off + (uint32_t)(kb + k0 + k) * 32u;
+              if constexpr (Mat::kPacked) {
+                const uint32_t w = __ldg(reinterpret_cast<const uint32_t *>(A.val) + j);
+                const unsigned short vb = (unsigned short)(w & 0xffffu);
+                if constexpr (std::is_same<V, __half>::value)
+                  a[k] = __half2float(__ushort_as_half(vb));
+                else
+                  a[k] = __bfloat162float(__ushort_as_bfloat16(vb));
+                c[k] = row + (int32_t)(int16_t)(w >> 16);
+              } else {
+                a[k] = lp_to_float<V>(__ldg(A.val + j));
+                if (DELTA16)
+                  c[k] = row + (int32_t)__ldg(reinterpret_cast<const int16_t *>(A.cols) + j);
+                else
+                  c[k] = __ldg(reinterpret_cast<const int32_t *>(A.cols) + j);
+              }
+            }
+          }
+#pragma unroll
+          for (int k = 0; k < kRowFirst; ++k)
+            if (k0 + k < kn && live) acc = fma((VT)a[k], fma(bt, __ldg(p_prev + c[k]), __ldg(r + c[k])), acc);
+        }
+      }
+      acc *= row_scale;
+      if (live) {
+        const VT pi = fma(bt, p_prev[i], r[i]);
+        p[i] = pi;
+        q[i] = acc;
+        dot += (double)acc * (double)pi;
+      }
+    }
+  } else
   for (int64_t i = (int64_t)blockIdx.x * kCgThreads + threadIdx.x; i < n; i += stride) {
     const int32_t s = A.rowPtr[i], e = A.rowPtr[i + 1];
     int64_t c[kRowFirst];
@@ -145,41 +207,75 @@ __global__ void __launch_bounds__(kCgThreads) cg_dir_spmv_kernel(int32_t n, CgMa
 }
 
 // Kernel B: alpha = rr_k / p.q; x += alpha p; r -= alpha q; partials of r.r.
+// 16-byte vector accesses (4 floats or 2 doubles per load), two in flight
+// per thread; the scalar tail covers n not divisible by the vector width.
+template <typename VT> struct Vec16;
+template <> struct Vec16<float> { using T = float4; static constexpr int W = 4; };
+template <> struct Vec16<double> { using T = double2; static constexpr int W = 2; };
+
+__device__ __forceinline__ float vget(const float4 &v, int k) { return k == 0 ? v.x : k == 1 ? v.y : k == 2 ? v.z : v.w; }
+__device__ __forceinline__ double vget(const double2 &v, int k) { return k == 0 ? v.x : v.y; }
+__device__ __forceinline__ void vset(float4 &v, int k, float a) {
+  if (k == 0) v.x = a; else if (k == 1) v.y = a; else if (k == 2) v.z = a; else v.w = a;
+}
+__device__ __forceinline__ void vset(double2 &v, int k, double a) {
+  if (k == 0) v.x = a; else v.y = a;
+}
+
 template <typename VT>
 __global__ void __launch_bounds__(kCgThreads) cg_update_kernel(int32_t n, const double *__restrict__ pq_part,
                                                                int npart, const double *__restrict__ rr_slot,
                                                                VT *__restrict__ x, VT *__restrict__ r,
                                                                const VT *__restrict__ p, const VT *__restrict__ q,
                                                                double *__restrict__ rr_part) {
+  using V = typename Vec16<VT>::T;
+  constexpr int W = Vec16<VT>::W;
+  constexpr int U = 2;
   __shared__ double smem[kCgThreads / 32];
   const double pq = reduce_partials(pq_part, npart, smem);
   const double rr = *rr_slot;
   const double alpha = (pq != 0.0 && rr != 0.0 && isfinite(pq)) ? rr / pq : 0.0;
   const VT a = (VT)alpha;
   double s = 0.0;
+  const int64_t nv = n / W;
   const int64_t stride = (int64_t)gridDim.x * kCgThreads;
-  for (int64_t i0 = (int64_t)blockIdx.x * kCgThreads + threadIdx.x; i0 < n; i0 += 4 * stride) {
-    VT pv[4], qv[4], xv[4], rv[4];
+  V *xv = reinterpret_cast<V *>(x);
+  V *rv = reinterpret_cast<V *>(r);
+  const V *pv = reinterpret_cast<const V *>(p);
+  const V *qv = reinterpret_cast<const V *>(q);
+  for (int64_t i0 = (int64_t)blockIdx.x * kCgThreads + threadIdx.x; i0 < nv; i0 += U * stride) {
+    V P[U], Q[U], X[U], R[U];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const int64_t i = i0 + k * stride;
-      if (i < n) {
-        pv[k] = p[i];
-        qv[k] = q[i];
-        xv[k] = x[i];
-        rv[k] = r[i];
+    for (int u = 0; u < U; ++u) {
+      const int64_t i = i0 + u * stride;
+      if (i < nv) {
+        P[u] = pv[i];
+        Q[u] = qv[i];
+        X[u] = xv[i];
+        R[u] = rv[i];
       }
     }
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const int64_t i = i0 + k * stride;
-      if (i < n) {
-        x[i] = fma(a, pv[k], xv[k]);
-        const VT ri = fma(-a, qv[k], rv[k]);
-        r[i] = ri;
-        s += (double)ri * (double)ri;
+    for (int u = 0; u < U; ++u) {
+      const int64_t i = i0 + u * stride;
+      if (i < nv) {
+#pragma unroll
+        for (int k = 0; k < W; ++k) {
+          vset(X[u], k, fma(a, vget(P[u], k), vget(X[u], k)));
+          const VT ri = fma(-a, vget(Q[u], k), vget(R[u], k));
+          vset(R[u], k, ri);
+          s += (double)ri * (double)ri;
+        }
+        xv[i] = X[u];
+        rv[i] = R[u];
       }
     }
+  }
+  for (int64_t i = nv * W + (int64_t)blockIdx.x * kCgThreads + threadIdx.x; i < n; i += stride) {
+    x[i] = fma(a, p[i], x[i]);
+    const VT ri = fma(-a, q[i], r[i]);
+    r[i] = ri;
+    s += (double)ri * (double)ri;
   }
   const double t = block_sum(s, smem);
   if (threadIdx.x == 0) rr_part[blockIdx.x] = t;
@@ -246,19 +342,28 @@ __global__ void sum_partials_kernel(const double *__restrict__ part, int npart, 
 }
 
 // ---------------------------------------------------------------------------
-// Low-precision copy of the matrix.
-__global__ void cg_group_exp_kernel(int64_t nnz, const double *__restrict__ val, int8_t *__restrict__ exps) {
-  const int64_t ng = (nnz + kScaleGroup - 1) / kScaleGroup;
-  for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < ng; g += (int64_t)gridDim.x * blockDim.x) {
+// Low-precision SELL-32 copy of the matrix.
+__global__ void sell_len_kernel(int32_t n, const int32_t *__restrict__ rowPtr, int32_t *__restrict__ slice_len) {
+  const int64_t ns = ((int64_t)n + 31) / 32;
+  for (int64_t sl = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; sl < ns; sl += (int64_t)gridDim.x * blockDim.x) {
+    int32_t m = 0;
+    for (int64_t r = sl * 32; r < n && r < sl * 32 + 32; ++r) m = max(m, rowPtr[r + 1] - rowPtr[r]);
+    slice_len[sl] = m;
+  }
+}
+
+// One power-of-two exponent per row: the row's largest magnitude scaled into [1, 2).
+__global__ void row_exp_kernel(int32_t n, const int32_t *__restrict__ rowPtr, const double *__restrict__ val,
+                               int8_t *__restrict__ exps) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
     double m = 0.0;
-    for (int64_t j = g * kScaleGroup; j < nnz && j < (g + 1) * kScaleGroup; ++j) m = fmax(m, fabs(val[j]));
+    for (int32_t j = rowPtr[r]; j < rowPtr[r + 1]; ++j) m = fmax(m, fabs(val[j]));
     int e = 0;
     if (m > 0.0) {
       frexp(m, &e);  // m = f * 2^e, f in [0.5, 1)
-      e -= 1;        // scaled group maximum in [1, 2)
+      e -= 1;
     }
-    e = e < -100 ? -100 : (e > 100 ? 100 : e);
-    exps[g] = (int8_t)e;
+    exps[r] = (int8_t)(e < -100 ? -100 : (e > 100 ? 100 : e));
   }
 }
 
@@ -268,13 +373,42 @@ template <> __device__ __forceinline__ float from_float_lp<float>(float f) { ret
 template <> __device__ __forceinline__ __half from_float_lp<__half>(float f) { return __float2half_rn(f); }
 template <> __device__ __forceinline__ __nv_bfloat16 from_float_lp<__nv_bfloat16>(float f) { return __float2bfloat16_rn(f); }
 
-template <typename V, bool SCALED>
-__global__ void cg_quantize_kernel(int64_t nnz, const double *__restrict__ val, const int8_t *__restrict__ exps,
-                                   V *__restrict__ out) {
-  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < nnz; j += (int64_t)gridDim.x * blockDim.x) {
-    double v = val[j];
-    if (SCALED) v = ldexp(v, -(int)exps[j / kScaleGroup]);
-    out[j] = from_float_lp<V>((float)v);
+// Thread per (slice row): its entries (scaled, converted) and columns (int16
+// offsets or int32) into the slice; padding = value 0, column = the row
+// itself (rows past n in the last slice: column 0, never gathered).
+template <typename V, bool SCALED, bool D16, bool PACKED>
+__global__ void sell_fill_kernel(int32_t n, const int32_t *__restrict__ rowPtr, const int32_t *__restrict__ colIdx,
+                                 const double *__restrict__ val, const int32_t *__restrict__ slice_len,
+                                 const int64_t *__restrict__ slice_off, const int8_t *__restrict__ exps,
+                                 V *__restrict__ out, void *__restrict__ cols) {
+  const int64_t ns = ((int64_t)n + 31) / 32;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < ns * 32; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t sl = t >> 5, lane = t & 31;
+    const int64_t self = t < n ? t : 0;
+    const int32_t s0 = t < n ? rowPtr[t] : 0, e0 = t < n ? rowPtr[t + 1] : 0;
+    for (int32_t k = 0; k < slice_len[sl]; ++k) {
+      const int64_t j = slice_off[sl] + (int64_t)k * 32 + lane;
+      double v = 0.0;
+      int64_t c = self;
+      if (s0 + k < e0) {
+        v = val[s0 + k];
+        c = colIdx[s0 + k];
+        if (SCALED) v = ldexp(v, -(int)exps[t]);
+      }
+      const V lv = from_float_lp<V>((float)v);
+      const int64_t d = c - self;
+      if (PACKED) {
+        unsigned short vb;
+        memcpy(&vb, &lv, sizeof(vb));
+        reinterpret_cast<uint32_t *>(out)[j] = (uint32_t)vb | ((uint32_t)(uint16_t)(int16_t)d << 16);
+      } else {
+        out[j] = lv;
+        if (D16)
+          reinterpret_cast<int16_t *>(cols)[j] = (int16_t)d;
+        else
+          reinterpret_cast<int32_t *>(cols)[j] = (int32_t)c;
+      }
+    }
   }
 }
 
@@ -288,12 +422,6 @@ __global__ void cg_delta_check_kernel(int32_t n, const int32_t *__restrict__ row
         break;
       }
     }
-}
-
-__global__ void cg_delta_fill_kernel(int32_t n, const int32_t *__restrict__ rowPtr,
-                                     const int32_t *__restrict__ colIdx, int16_t *__restrict__ out) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    for (int32_t j = rowPtr[i]; j < rowPtr[i + 1]; ++j) out[j] = (int16_t)((int64_t)colIdx[j] - i);
 }
 
 __global__ void f64_to_f32_kernel(int64_t n, const double *__restrict__ a, float *__restrict__ b) {
@@ -313,7 +441,9 @@ struct bsp_cg_plan_s {
   // low-precision copy of the matrix (mixed modes)
   void *lp_val = nullptr;
   int8_t *exps = nullptr;
-  int16_t *lp_cols = nullptr;  // int16 offsets, or nullptr (then colIdx)
+  void *lp_cols = nullptr;     // int16 offsets or int32 columns (unpacked SELL)
+  int32_t *slice_len = nullptr;
+  int64_t *slice_off = nullptr;
   bool delta16 = false;
   // FP64 state
   double *x64 = nullptr, *r64 = nullptr;
@@ -321,7 +451,8 @@ struct bsp_cg_plan_s {
   void *x = nullptr, *r = nullptr, *p[2] = {nullptr, nullptr}, *q = nullptr;
   double *part_pq = nullptr, *part_rr = nullptr, *part_res = nullptr;
   double *sc = nullptr, *h_sc = nullptr;  // [0],[1] rr slots, [2] ||b-Ax||^2, [3] ||b||^2, [4] rr after a chunk
-  int grid = 0;
+  int grid = 0;    // update, residual and reduction kernels (writers of the rr partials)
+  int grid_a = 0;  // direction/SpMV kernel (writer of the p.q partials)
   cudaGraphExec_t graph = nullptr;
   cudaStream_t graph_stream = nullptr;
   int64_t bytes_iter = 0, bytes_residual = 0;
@@ -329,9 +460,25 @@ struct bsp_cg_plan_s {
 
 namespace bsp {
 
-static int cg_grid(int32_t n) {
+constexpr int kCgMaxCtasPerSm = 2048 / kCgThreads;
+
+// Resident CTAs per SM of the direction/SpMV kernel (a) and of the update
+// kernel (b).
+template <typename V, typename VT, bool SC, bool D16>
+static void cg_occupancy(int &a, int &b) {
+  a = b = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, cg_dir_spmv_kernel<V, VT, SC, D16>, kCgThreads, 0) !=
+      cudaSuccess)
+    a = 4;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, cg_update_kernel<VT>, kCgThreads, 0) != cudaSuccess) b = 4;
+  a = a < 1 ? 1 : (a > kCgMaxCtasPerSm ? kCgMaxCtasPerSm : a);
+  b = b < 1 ? 1 : (b > kCgMaxCtasPerSm ? kCgMaxCtasPerSm : b);
+}
+
+// One resident wave (grid-stride loops inside).
+static int cg_grid(int32_t n, int occ) {
   int64_t g = ceil_div(n, kCgThreads);
-  const int64_t cap = (int64_t)sm_count() * 4;  // one wave at <= 64 registers per thread
+  const int64_t cap = (int64_t)sm_count() * occ;
   if (g > cap) g = cap;
   if (g < 1) g = 1;
   return (int)g;
@@ -339,17 +486,33 @@ static int cg_grid(int32_t n) {
 
 static bool cg_mixed(const bsp_cg_plan_s *P) { return P->opt.mode != BSP_CG_FP64; }
 
+static void cg_plan_occupancy(const bsp_cg_plan_s *P, int &a, int &b) {
+  const bool d = P->delta16;
+  switch (P->opt.mode) {
+    case BSP_CG_FP64:
+      return cg_occupancy<double, double, false, false>(a, b);
+    case BSP_CG_MIXED_F32:
+      return d ? cg_occupancy<float, float, false, true>(a, b) : cg_occupancy<float, float, false, false>(a, b);
+    case BSP_CG_MIXED_F16:
+      return d ? cg_occupancy<__half, float, true, true>(a, b) : cg_occupancy<__half, float, true, false>(a, b);
+    default:
+      return d ? cg_occupancy<__nv_bfloat16, float, true, true>(a, b)
+               : cg_occupancy<__nv_bfloat16, float, true, false>(a, b);
+  }
+}
+
 template <typename V, typename VT, bool SC, bool D16>
 static void launch_iter(bsp_cg_plan_s *P, int k, cudaStream_t s) {
-  CgMat<V, VT, SC, D16> A{P->rowPtr, D16 ? (const void *)P->lp_cols : (const void *)P->colIdx,
-                           (const V *)(sizeof(V) == 8 ? (const void *)P->val : P->lp_val), P->exps};
+  CgMat<V, VT, SC, D16> A{P->rowPtr, sizeof(V) == 8 ? (const void *)P->colIdx : (const void *)P->lp_cols,
+                           (const V *)(sizeof(V) == 8 ? (const void *)P->val : P->lp_val), P->exps,
+                           P->slice_len, P->slice_off};
   VT *r = (VT *)P->r, *x = (VT *)P->x, *q = (VT *)P->q;
   VT *pp = (VT *)P->p[k & 1], *pn = (VT *)P->p[(k + 1) & 1];
-  const int g = P->grid;
-  cg_dir_spmv_kernel<V, VT, SC, D16><<<g, kCgThreads, 0, s>>>(P->n, A, r, pp, pn, q, P->part_rr, g,
-                                                               P->sc + ((k + 1) & 1), P->sc + (k & 1),
-                                                               P->part_pq);
-  cg_update_kernel<VT><<<g, kCgThreads, 0, s>>>(P->n, P->part_pq, g, P->sc + (k & 1), x, r, pn, q, P->part_rr);
+  const int g = P->grid, ga = P->grid_a;
+  cg_dir_spmv_kernel<V, VT, SC, D16><<<ga, kCgThreads, 0, s>>>(P->n, A, r, pp, pn, q, P->part_rr, g,
+                                                                P->sc + ((k + 1) & 1), P->sc + (k & 1),
+                                                                P->part_pq);
+  cg_update_kernel<VT><<<g, kCgThreads, 0, s>>>(P->n, P->part_pq, ga, P->sc + (k & 1), x, r, pn, q, P->part_rr);
 }
 
 static bsp_status cg_iteration(bsp_cg_plan_s *P, int k, cudaStream_t s) {
@@ -451,8 +614,10 @@ extern "C" bsp_status bsp_cg_destroy(bsp_cg_plan P) {
   dfree(P->r64, s);
   for (void *v : {P->x, P->r, P->p[0], P->p[1], P->q, P->lp_val})
     if (v) cudaFreeAsync(v, s);
-  dfree(P->lp_cols, s);
+  if (P->lp_cols) cudaFreeAsync(P->lp_cols, s);
   dfree(P->exps, s);
+  dfree(P->slice_len, s);
+  dfree(P->slice_off, s);
   dfree(P->part_pq, s);
   dfree(P->part_rr, s);
   dfree(P->part_res, s);
@@ -481,7 +646,7 @@ extern "C" bsp_status bsp_cg_create(int32_t n, int32_t nnz, const int32_t *rowPt
   P->rowPtr = rowPtr;
   P->colIdx = colIdx;
   P->val = values;
-  P->grid = cg_grid(n);
+  P->grid = (int)std::min<int64_t>(ceil_div(n, kCgThreads), (int64_t)sm_count() * kCgMaxCtasPerSm);
   const bool mixed = cg_mixed(P);
   const size_t vt = mixed ? 4 : 8;
   bsp_status st = BSP_OK;
@@ -519,25 +684,27 @@ extern "C" bsp_status bsp_cg_create(int32_t n, int32_t nnz, const int32_t *rowPt
   if (mixed) {
     const bool scaled = opt->mode != BSP_CG_MIXED_F32;
     const size_t vsz = opt->mode == BSP_CG_MIXED_F32 ? 4 : 2;
-    BSP_CG_CUDA(cudaMallocAsync(&P->lp_val, vsz * (size_t)(nnz > 0 ? nnz : 1), s));
-    int64_t gq = ceil_div(nnz, 256);
-    if (gq > (int64_t)sm_count() * 32) gq = (int64_t)sm_count() * 32;
-    if (gq < 1) gq = 1;
-    const int64_t ng = ceil_div(nnz, kScaleGroup);
-    if (scaled) {
-      BSP_CG_TRY(dalloc(&P->exps, (size_t)(ng > 0 ? ng : 1), s));
-      cg_group_exp_kernel<<<(unsigned)ceil_div(ng > 0 ? ng : 1, 256), 256, 0, s>>>(nnz, values, P->exps);
+    // SELL-32 slices: lengths on the device, offsets summed on the host
+    const int64_t ns = ceil_div(n, 32);
+    BSP_CG_TRY(dalloc(&P->slice_len, (size_t)ns, s));
+    BSP_CG_TRY(dalloc(&P->slice_off, (size_t)ns + 1, s));
+    const unsigned gs = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div(ns, 256), (int64_t)sm_count() * 16));
+    sell_len_kernel<<<gs, 256, 0, s>>>(n, rowPtr, P->slice_len);
+    std::vector<int32_t> hlen((size_t)ns);
+    std::vector<int64_t> hoff((size_t)ns + 1, 0);
+    BSP_CG_CUDA(cudaMemcpyAsync(hlen.data(), P->slice_len, sizeof(int32_t) * ns, cudaMemcpyDeviceToHost, s));
+    BSP_CG_CUDA(cudaStreamSynchronize(s));
+    for (int64_t k = 0; k < ns; ++k) hoff[k + 1] = hoff[k] + 32 * (int64_t)hlen[k];
+    const int64_t padded = hoff[ns];
+    if (padded >= ((int64_t)1 << 31)) {
+      set_error("bsp_cg_create: the padded low-precision matrix needs >= 2^31 entries");
+      return fail(BSP_ERR_UNSUPPORTED);
     }
-    if (opt->mode == BSP_CG_MIXED_F32)
-      cg_quantize_kernel<float, false><<<(unsigned)gq, 256, 0, s>>>(nnz, values, nullptr, (float *)P->lp_val);
-    else if (opt->mode == BSP_CG_MIXED_F16)
-      cg_quantize_kernel<__half, true><<<(unsigned)gq, 256, 0, s>>>(nnz, values, P->exps, (__half *)P->lp_val);
-    else
-      cg_quantize_kernel<__nv_bfloat16, true><<<(unsigned)gq, 256, 0, s>>>(nnz, values, P->exps,
-                                                                           (__nv_bfloat16 *)P->lp_val);
-    if (cudaGetLastError() != cudaSuccess) {
-      set_error("bsp_cg_create: quantization kernel launch failed");
-      return fail(BSP_ERR_CUDA);
+    BSP_CG_CUDA(cudaMemcpyAsync(P->slice_off, hoff.data(), sizeof(int64_t) * (ns + 1), cudaMemcpyHostToDevice, s));
+    if (scaled) {
+      BSP_CG_TRY(dalloc(&P->exps, (size_t)n, s));
+      const unsigned ge = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div(n, 256), (int64_t)sm_count() * 16));
+      row_exp_kernel<<<ge, 256, 0, s>>>(n, rowPtr, values, P->exps);
     }
     int32_t *bad = nullptr;
     BSP_CG_TRY(dalloc(&bad, 1, s));
@@ -548,19 +715,45 @@ extern "C" bsp_status bsp_cg_create(int32_t n, int32_t nnz, const int32_t *rowPt
     int32_t h_bad = 1;
     BSP_CG_TRY(read_i32(bad, &h_bad, s));
     dfree(bad, s);
-    if (!h_bad) {
-      BSP_CG_TRY(dalloc(&P->lp_cols, (size_t)(nnz > 0 ? nnz : 1), s));
-      cg_delta_fill_kernel<<<(unsigned)gr, 256, 0, s>>>(n, rowPtr, colIdx, P->lp_cols);
-      P->delta16 = true;
+    P->delta16 = !h_bad;
+    const bool packed = scaled && P->delta16;
+    BSP_CG_CUDA(cudaMallocAsync(&P->lp_val, (packed ? 4 : vsz) * (size_t)(padded > 0 ? padded : 1), s));
+    if (!packed)
+      BSP_CG_CUDA(cudaMallocAsync(&P->lp_cols, (P->delta16 ? 2 : 4) * (size_t)(padded > 0 ? padded : 1), s));
+    int64_t gf = ceil_div(ns * 32, 256);
+    if (gf > (int64_t)sm_count() * 32) gf = (int64_t)sm_count() * 32;
+#define BSP_SELL_FILL(V, SC, D, PK)                                                                          \
+  sell_fill_kernel<V, SC, D, PK><<<(unsigned)gf, 256, 0, s>>>(n, rowPtr, colIdx, values, P->slice_len,           \
+                                                              P->slice_off, P->exps, (V *)P->lp_val, P->lp_cols)
+    if (opt->mode == BSP_CG_MIXED_F32) {
+      if (P->delta16) BSP_SELL_FILL(float, false, true, false); else BSP_SELL_FILL(float, false, false, false);
+    } else if (opt->mode == BSP_CG_MIXED_F16) {
+      if (P->delta16) BSP_SELL_FILL(__half, true, true, true); else BSP_SELL_FILL(__half, true, false, false);
+    } else {
+      if (P->delta16)
+        BSP_SELL_FILL(__nv_bfloat16, true, true, true);
+      else
+        BSP_SELL_FILL(__nv_bfloat16, true, false, false);
     }
-    mat_bytes = (int64_t)nnz * ((int64_t)vsz + (P->delta16 ? 2 : 4)) + (scaled ? ng : 0);
+#undef BSP_SELL_FILL
+    if (cudaGetLastError() != cudaSuccess) {
+      set_error("bsp_cg_create: building the low-precision matrix failed");
+      return fail(BSP_ERR_CUDA);
+    }
+    mat_bytes = padded * (packed ? 4 : (int64_t)vsz + (P->delta16 ? 2 : 4)) + (scaled ? (int64_t)n : 0) + 12 * ns;
+  }
+  {  // partials were sized for the largest grid
+    int oa = 4, ob = 4;
+    cg_plan_occupancy(P, oa, ob);
+    P->grid_a = cg_grid(n, oa);
+    P->grid = cg_grid(n, ob);
   }
 #undef BSP_CG_TRY
 #undef BSP_CG_CUDA
   // algorithmic bytes: kernel A reads the matrix, r and p_prev (own rows;
   // gathers counted once) and writes p and q; kernel B reads p, q, x, r and
   // writes x, r.
-  P->bytes_iter = mat_bytes + 4 * ((int64_t)n + 1) + 10 * (int64_t)vt * n;
+  P->bytes_iter = mat_bytes + (mixed ? 0 : 4 * ((int64_t)n + 1)) + 10 * (int64_t)vt * n;
   P->bytes_residual = (int64_t)nnz * 12 + 4 * ((int64_t)n + 1) + 3 * 8 * (int64_t)n;
   if (cudaStreamSynchronize(s) != cudaSuccess) {
     set_error("bsp_cg_create: preparing the matrix failed");
