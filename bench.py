@@ -547,6 +547,57 @@ def run_suite(args) -> None:
     _emit("batch_512_banded_and_zipf2.2", matrices=len(mats), rows=rows, nnz=nnz, variants=res)
 
 
+# ---------------------------------------------------------------------------
+# --profile W: a few calls of one workload's kernels, for ncu captures (small
+# enough to capture, inputs still larger than L2).  Prints one line.
+
+def run_profile(args) -> None:
+    import torch
+
+    import benchsp_b200 as bsp
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    reps = max(1, min(args.steps, 5))
+
+    def up(*arrs):
+        return [torch.from_numpy(np.ascontiguousarray(a)).to(dev) for a in arrs]
+
+    w = args.profile
+    if w == "dasp":   # power-law rows, Zipf 2.0 capped at 10k, n = 2^21 (190 MB of CSR)
+        A = bsp.gen_powerlaw(1 << 21, 2.0, 10000, SEED + 13)
+        rp, ci, va, x = up(A.rowptr, A.colidx, A.values, bsp.gen_uniform(A.cols, SEED + 14))
+        D = bsp.csr2dasp(rp, ci, va, rows=A.rows, cols=A.cols)
+        y = torch.empty(A.rows, dtype=torch.float64, device=dev)
+        for _ in range(reps):
+            D.spmv(x, y)
+    elif w in ("cg_fp64", "cg_f16"):   # 7-point Poisson 128^3, 32 iterations, no graphs
+        A = bsp.gen_poisson3d(128)
+        rp, ci, va, b = up(A.rowptr, A.colidx, A.values, bsp.gen_uniform(A.rows, SEED + 3))
+        S = bsp.CgSolver(rp, ci, va, mode=w[3:], max_iters=32, check_every=16, use_graphs=False)
+        S.solve(b, raise_on_stall=False)
+    elif w == "spmm":   # power-law graph 2^20, FP16, N = 128, row-split CSR
+        A = bsp.gen_graph(1 << 20, 1.8, 32, SEED + 4)
+        rp, ci, v64 = up(A.rowptr, A.colidx, A.values)
+        v = v64.half()
+        P = bsp.SpmmPlan(rp, ci, v, cols=A.cols, chunk=256)
+        B = (torch.rand(A.cols, 128, generator=torch.Generator().manual_seed(1)) * 2 - 1).half().to(dev)
+        for _ in range(reps):
+            P.spmm(B)
+    elif w == "batch":   # the 512-matrix batch, FP64, one RHS
+        mats = bsp.gen_batch(512, SEED + 6)
+        d = []
+        for m in mats:
+            rp, ci, va, x = up(m.rowptr, m.colidx, m.values, bsp.gen_uniform(m.cols, 1))
+            d.append((rp, ci, va, x, torch.empty(m.rows, dtype=torch.float64, device=dev)))
+        P = bsp.BatchPlan(d, use_graph=False)
+        for _ in range(reps):
+            P.run()
+    else:
+        raise SystemExit(f"unknown profile workload {w}")
+    torch.cuda.synchronize()
+    print(json.dumps({"profile": w, "calls": reps}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -557,7 +608,12 @@ def main():
     ap.add_argument("--suite", action="store_true", help="one JSON line per further workload (1 GPU)")
     ap.add_argument("--grid", type=int, default=GRID, help="stencil grid edge (64 = the benchmark config; "
                     "smaller values only for profiling captures)")
+    ap.add_argument("--profile", choices=["dasp", "cg_fp64", "cg_f16", "spmm", "batch"],
+                    help="a few calls of one workload's kernels (for ncu captures)")
     args = ap.parse_args()
+    if args.profile:
+        run_profile(args)
+        return
     if args.suite:
         run_suite(args)
         return
