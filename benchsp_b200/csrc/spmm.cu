@@ -116,6 +116,135 @@ __global__ void __launch_bounds__(256) spmm_csr_kernel(int32_t rows, int32_t N, 
 }
 
 // ---------------------------------------------------------------------------
+// Grouped CSR SpMM engine.  Every lane moves 16 bytes (VEC elements) of a
+// gathered B row; LPR lanes cover LPR*VEC columns of one row, so one warp step
+// handles G = 32/LPR nonzeros at once (N = 32 FP16: 8 nonzeros of 64 bytes
+// each), and kSpmmU steps are in flight.  The row's 32 column indices and
+// values are loaded once per chunk of 32 and broadcast by shuffle.  After the
+// segment the G groups' partial sums are added with a fixed shuffle tree, so
+// every lane holds the totals (deterministic).
+constexpr int kSpmmU = 4;
+
+template <typename T> struct SpmmVec { static constexpr int VEC = 16 / (int)sizeof(T); };
+
+template <typename T>
+__device__ __forceinline__ void unpack16(const uint4 &u, float (&o)[SpmmVec<T>::VEC]);
+template <>
+__device__ __forceinline__ void unpack16<float>(const uint4 &u, float (&o)[4]) {
+  o[0] = __uint_as_float(u.x);
+  o[1] = __uint_as_float(u.y);
+  o[2] = __uint_as_float(u.z);
+  o[3] = __uint_as_float(u.w);
+}
+template <>
+__device__ __forceinline__ void unpack16<__half>(const uint4 &u, float (&o)[8]) {
+  const unsigned w[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    __half2 h;
+    memcpy(&h, &w[k], 4);
+    const float2 f = __half22float2(h);
+    o[2 * k] = f.x;
+    o[2 * k + 1] = f.y;
+  }
+}
+template <>
+__device__ __forceinline__ void unpack16<__nv_bfloat16>(const uint4 &u, float (&o)[8]) {
+  const unsigned w[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    __nv_bfloat162 h;
+    memcpy(&h, &w[k], 4);
+    const float2 f = __bfloat1622float2(h);
+    o[2 * k] = f.x;
+    o[2 * k + 1] = f.y;
+  }
+}
+
+// acc (this lane's VEC columns starting at cl) += sum over nonzeros [s, e).
+template <typename T, int LPR>
+__device__ __forceinline__ void spmm_segment(int32_t s, int32_t e, const int32_t *__restrict__ colIdx,
+                                             const T *__restrict__ val, const T *__restrict__ B, int64_t ldb,
+                                             int32_t cl, int lane, float (&acc)[SpmmVec<T>::VEC]) {
+  constexpr int VEC = SpmmVec<T>::VEC;
+  constexpr int G = 32 / LPR;
+  const int g = lane / LPR;
+  for (int32_t j0 = s; j0 < e; j0 += 32) {
+    const int32_t j = j0 + lane;
+    const int32_t cj = j < e ? __ldg(colIdx + j) : 0;
+    const float vj = j < e ? sp_to_float<T>(__ldg(val + j)) : 0.f;
+    const int cnt = e - j0 < 32 ? e - j0 : 32;
+    for (int t = 0; t < cnt; t += G * kSpmmU) {  // warp-uniform bounds
+      uint4 raw[kSpmmU];
+      float v[kSpmmU];
+#pragma unroll
+      for (int u = 0; u < kSpmmU; ++u) {
+        const int src = t + u * G + g;
+        const int32_t c = __shfl_sync(0xffffffffu, cj, src & 31);
+        const float vv = __shfl_sync(0xffffffffu, vj, src & 31);
+        const bool ok = src < cnt;
+        v[u] = ok ? vv : 0.f;
+        raw[u] = ok ? __ldg(reinterpret_cast<const uint4 *>(B + (int64_t)c * ldb + cl)) : make_uint4(0, 0, 0, 0);
+      }
+#pragma unroll
+      for (int u = 0; u < kSpmmU; ++u) {
+        float b[VEC];
+        unpack16<T>(raw[u], b);
+#pragma unroll
+        for (int k = 0; k < VEC; ++k) acc[k] = fmaf(v[u], b[k], acc[k]);
+      }
+    }
+  }
+#pragma unroll
+  for (int o = LPR; o < 32; o <<= 1)
+#pragma unroll
+    for (int k = 0; k < VEC; ++k) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
+}
+
+// Warp per row; column passes of LPR*VEC columns.
+template <typename T, int LPR>
+__global__ void __launch_bounds__(256) spmm_grouped_kernel(int32_t rows, int32_t N, const int32_t *__restrict__ rowPtr,
+                                                           const int32_t *__restrict__ colIdx,
+                                                           const T *__restrict__ val, const T *__restrict__ B,
+                                                           int64_t ldb, float *__restrict__ C, int64_t ldc,
+                                                           float alpha, float beta) {
+  constexpr int VEC = SpmmVec<T>::VEC;
+  const int lane = threadIdx.x & 31;
+  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < rows; r += nwarps) {
+    const int32_t s = rowPtr[r], e = rowPtr[r + 1];
+    for (int32_t c0 = 0; c0 < N; c0 += LPR * VEC) {
+      const int32_t cl = c0 + (lane % LPR) * VEC;
+      float acc[VEC];
+#pragma unroll
+      for (int k = 0; k < VEC; ++k) acc[k] = 0.f;
+      spmm_segment<T, LPR>(s, e, colIdx, val, B, ldb, cl, lane, acc);
+      if (lane < LPR) {
+        float *cp = C + r * ldc + cl;
+#pragma unroll
+        for (int k = 0; k < VEC; ++k) {
+          float o = alpha * acc[k];
+          if (beta != 0.f) o += beta * cp[k];
+          cp[k] = o;
+        }
+      }
+    }
+  }
+}
+
+// Lanes per B row for the grouped kernels: the largest power of two <= 32
+// with LPR * VEC dividing N; 0 when B's rows are not 16-byte aligned or N is
+// not a multiple of VEC (then the scalar-column kernels run).
+template <typename T>
+static int grouped_lpr(int32_t N, const void *B, int64_t ldb) {
+  constexpr int VEC = SpmmVec<T>::VEC;
+  if ((uintptr_t)B % 16 != 0 || (ldb * (int64_t)sizeof(T)) % 16 != 0 || N % VEC != 0) return 0;
+  int l = 32;
+  while (l > 1 && (N % (l * VEC) != 0)) l >>= 1;
+  return l;
+}
+
+// ---------------------------------------------------------------------------
 // Block (16x16) tensor-core SpMM.
 constexpr int kTS = 16;            // tile side
 constexpr int kStages = 4;         // shared-memory ring depth per warp
@@ -333,10 +462,33 @@ static bsp_status launch_spmm_csr(int32_t rows, int32_t N, const int32_t *rp, co
   return BSP_OK;
 }
 
+template <typename T, int LPR>
+static bsp_status launch_grouped(int32_t rows, int32_t N, const int32_t *rp, const int32_t *ci, const void *val,
+                                 const void *B, int64_t ldb, float *C, int64_t ldc, float a, float b,
+                                 cudaStream_t s) {
+  int64_t blocks = ceil_div(rows, 8);
+  const int64_t cap = (int64_t)sm_count() * 32;
+  if (blocks > cap) blocks = cap;
+  if (blocks < 1) blocks = 1;
+  spmm_grouped_kernel<T, LPR><<<(unsigned)blocks, 256, 0, s>>>(rows, N, rp, ci, (const T *)val, (const T *)B, ldb,
+                                                               C, ldc, a, b);
+  BSP_LAUNCH_CHECK();
+  return BSP_OK;
+}
+
 template <typename T>
 static bsp_status spmm_csr_typed(int32_t rows, int32_t N, const int32_t *rp, const int32_t *ci, const void *val,
                                  const void *B, int64_t ldb, float *C, int64_t ldc, float a, float b,
                                  cudaStream_t s) {
+  switch (grouped_lpr<T>(N, B, ldb)) {
+    case 32: return launch_grouped<T, 32>(rows, N, rp, ci, val, B, ldb, C, ldc, a, b, s);
+    case 16: return launch_grouped<T, 16>(rows, N, rp, ci, val, B, ldb, C, ldc, a, b, s);
+    case 8: return launch_grouped<T, 8>(rows, N, rp, ci, val, B, ldb, C, ldc, a, b, s);
+    case 4: return launch_grouped<T, 4>(rows, N, rp, ci, val, B, ldb, C, ldc, a, b, s);
+    case 2: return launch_grouped<T, 2>(rows, N, rp, ci, val, B, ldb, C, ldc, a, b, s);
+    case 1: return launch_grouped<T, 1>(rows, N, rp, ci, val, B, ldb, C, ldc, a, b, s);
+    default: break;
+  }
   // widest per-lane vector that divides N/32 and keeps B loads aligned
   const size_t es = sizeof(T);
   const bool al16 = ((uintptr_t)B % 16 == 0) && ((ldb * es) % 16 == 0);
@@ -670,6 +822,63 @@ extern "C" bsp_status bsp_spmm_plan_free(bsp_spmm_plan *p) {
 }
 
 namespace bsp {
+// Warp per chunk (see spmm_chunk_kernel) with the grouped engine.
+template <typename T, int LPR>
+__global__ void __launch_bounds__(256) spmm_grouped_chunk_kernel(
+    int64_t nchunks, int32_t N, int32_t chunk, const int32_t *__restrict__ chunk_row,
+    const int32_t *__restrict__ chunk_ptr, const int32_t *__restrict__ part_ptr, const int32_t *__restrict__ rowPtr,
+    const int32_t *__restrict__ colIdx, const T *__restrict__ val, const T *__restrict__ B, int64_t ldb,
+    float *__restrict__ C, int64_t ldc, float *__restrict__ part, float alpha, float beta) {
+  constexpr int VEC = SpmmVec<T>::VEC;
+  const int lane = threadIdx.x & 31;
+  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < nchunks; w += nwarps) {
+    const int32_t r = chunk_row[w];
+    const int32_t ci = (int32_t)(w - chunk_ptr[r]);
+    const bool split = chunk_ptr[r + 1] - chunk_ptr[r] > 1;
+    const int32_t s0 = rowPtr[r], e0 = rowPtr[r + 1];
+    const int32_t s = split ? s0 + ci * chunk : s0;
+    const int32_t e = split ? min(s + chunk, e0) : e0;
+    for (int32_t c0 = 0; c0 < N; c0 += LPR * VEC) {
+      const int32_t cl = c0 + (lane % LPR) * VEC;
+      float acc[VEC];
+#pragma unroll
+      for (int k = 0; k < VEC; ++k) acc[k] = 0.f;
+      spmm_segment<T, LPR>(s, e, colIdx, val, B, ldb, cl, lane, acc);
+      if (lane < LPR) {
+        if (split) {
+          float *pp = part + ((int64_t)part_ptr[r] + ci) * N + cl;
+#pragma unroll
+          for (int k = 0; k < VEC; ++k) pp[k] = acc[k];
+        } else {
+          float *cp = C + (int64_t)r * ldc + cl;
+#pragma unroll
+          for (int k = 0; k < VEC; ++k) {
+            float o = alpha * acc[k];
+            if (beta != 0.f) o += beta * cp[k];
+            cp[k] = o;
+          }
+        }
+      }
+    }
+  }
+}
+
+template <typename T, int LPR>
+static bsp_status launch_grouped_chunked(const bsp_spmm_plan *p, int32_t N, const int32_t *rp, const int32_t *ci,
+                                         const void *val, const void *B, int64_t ldb, float *C, int64_t ldc,
+                                         float *part, float a, float b, cudaStream_t s) {
+  int64_t blocks = ceil_div(p->nchunks, 8);
+  const int64_t cap = (int64_t)sm_count() * 32;
+  if (blocks > cap) blocks = cap;
+  if (blocks < 1) blocks = 1;
+  spmm_grouped_chunk_kernel<T, LPR><<<(unsigned)blocks, 256, 0, s>>>(
+      p->nchunks, N, p->chunk, p->chunk_row, p->chunk_ptr, p->part_ptr, rp, ci, (const T *)val, (const T *)B, ldb, C,
+      ldc, part, a, b);
+  BSP_LAUNCH_CHECK();
+  return BSP_OK;
+}
+
 template <typename T, int CPL>
 static bsp_status launch_chunked(const bsp_spmm_plan *p, int32_t N, const int32_t *rp, const int32_t *ci,
                                  const void *val, const void *B, int64_t ldb, float *C, int64_t ldc, float *part,
@@ -689,6 +898,17 @@ template <typename T>
 static bsp_status chunked_typed(const bsp_spmm_plan *p, int32_t N, const int32_t *rp, const int32_t *ci,
                                 const void *val, const void *B, int64_t ldb, float *C, int64_t ldc, float *part,
                                 float a, float b, cudaStream_t s) {
+#define BSP_GC(L) launch_grouped_chunked<T, L>(p, N, rp, ci, val, B, ldb, C, ldc, part, a, b, s)
+  switch (grouped_lpr<T>(N, B, ldb)) {
+    case 32: return BSP_GC(32);
+    case 16: return BSP_GC(16);
+    case 8: return BSP_GC(8);
+    case 4: return BSP_GC(4);
+    case 2: return BSP_GC(2);
+    case 1: return BSP_GC(1);
+    default: break;
+  }
+#undef BSP_GC
   const size_t es = sizeof(T);
   const bool al16 = ((uintptr_t)B % 16 == 0) && ((ldb * es) % 16 == 0);
   const bool al8 = ((uintptr_t)B % 8 == 0) && ((ldb * es) % 8 == 0);
