@@ -262,5 +262,7 @@ _PROTOS.update({
     "bsp_smat_free": (C.c_int, [C.POINTER(BspSmat)]),
     "bsp_smat_spmm": (C.c_int, [C.POINTER(BspSmat), _P, _I32, _I64, _P, _I64, C.c_float, C.c_float, _P]),
     "bsp_smat_check": (C.c_int, [C.POINTER(BspSmat), _P]),
+    "bsp_smat_spmm_path": (C.c_int, [C.POINTER(BspSmat), _P, _I32, _I64, _P, _I64, C.c_float, C.c_float, _I32,
+                                     _P]),
     "bsp_gen_graph": (C.c_int, [_I32, _D, _D, _U64, _PI32, _PI64, _P, _P, _P]),
 })

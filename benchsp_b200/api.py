@@ -582,14 +582,17 @@ class SmatMatrix:
     def tiles(self) -> int:
         return self._d.tiles.nonzeroBlocks
 
-    def spmm(self, B, C=None, *, alpha: float = 1.0, beta: float = 0.0, stream=None):
+    _PATHS = {"auto": 0, "mma_sync": 1, "tcgen05": 2}
+
+    def spmm(self, B, C=None, *, alpha: float = 1.0, beta: float = 0.0, path: str = "auto", stream=None):
+        """path: "auto" (tcgen05 when N % 128 == 0), "mma_sync" or "tcgen05"."""
         torch = _torch()
         N = B.shape[1]
         if C is None:
             C = torch.empty(self._d.rows, N, dtype=torch.float32, device=B.device)
             beta = 0.0
-        check(lib().bsp_smat_spmm(C_byref(self._d), _dptr(B, "B"), N, B.stride(0),
-                                  _dptr(C, "C"), C.stride(0), float(alpha), float(beta), _stream(stream)))
+        check(lib().bsp_smat_spmm_path(C_byref(self._d), _dptr(B, "B"), N, B.stride(0), _dptr(C, "C"),
+                                       C.stride(0), float(alpha), float(beta), self._PATHS[path], _stream(stream)))
         return C
 
     def check(self, stream=None) -> None:

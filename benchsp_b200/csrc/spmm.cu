@@ -19,6 +19,11 @@
 //    mma.sync.m16n8k16 with FP32 accumulators.  Every wait is bounded: on
 //    timeout the kernel records an error, waits (bounded) for its own copies
 //    and returns.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <mutex>
+
 #include "bsp_internal.cuh"
 #include "util.cuh"
 
@@ -244,6 +249,16 @@ static int grouped_lpr(int32_t N, const void *B, int64_t ldb) {
   return l;
 }
 
+// Position of tile element (row n, column k) in the stored tile: four 8x8
+// core matrices of 128 contiguous bytes, core (n/8, k/8) at (2*(n/8) + k/8)
+// * 64 elements, row n%8 of it at 8*(n%8).  This is the no-swizzle K-major
+// operand layout of tcgen05.mma (rows 16 bytes apart inside a core matrix,
+// K halves 128 bytes apart, 8-row groups 256 bytes apart); ldmatrix reads
+// the same 16-byte rows.
+__host__ __device__ __forceinline__ int tile_pos(int n, int k) {
+  return ((n >> 3) * 2 + (k >> 3)) * 64 + (n & 7) * 8 + (k & 7);
+}
+
 // ---------------------------------------------------------------------------
 // Block (16x16) tensor-core SpMM.
 constexpr int kTS = 16;            // tile side
@@ -391,7 +406,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) spmm_block_kernel(
       uses[slot]++;
       SpmmStage<NT> &S = st[slot];
       uint32_t a[4];
-      ldm_x4(a, S.a + ((lane & 15) * kTS + (lane >> 4) * 8) * 2);
+      ldm_x4(a, S.a + tile_pos(lane & 15, (lane >> 4) * 8) * 2);
 #pragma unroll
       for (int j = 0; j < NT; j += 2) {
         uint32_t b[4];
@@ -434,18 +449,242 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) spmm_block_kernel(
   }
 }
 
-template <typename T>
-__global__ void tiles_to_lp_kernel(int64_t n, const double *__restrict__ v, T *__restrict__ out);
-template <>
-__global__ void tiles_to_lp_kernel<__half>(int64_t n, const double *__restrict__ v, __half *__restrict__ out) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    out[i] = __double2half(v[i]);
+
+// ---------------------------------------------------------------------------
+// Block SpMM on the 5th-generation tensor cores (tcgen05), for N % 128 == 0.
+//
+// Transposed product: for a 16-row block br and a 128-column slab n0 of C,
+//   D (128 x 16, FP32, in tensor memory) = sum over the block-row's tiles of
+//   Bslab^T (128 x 16: rows bc*16.. of B, columns n0..n0+127) * Atile^T.
+// D's row m is C column n0+m, its column j is C row br*16+j.  One
+// tcgen05.mma (kind::f16, M = 128, N = 16, K = 16) per tile:
+//   * A operand = the B slab, MN-major, loaded by TMA (two 64-column boxes,
+//     128-byte swizzle) into a 4 KB stage aligned to 1 KB;
+//   * B operand = the stored tile (512 B, no swizzle, K-major core matrices,
+//     see tile_pos) copied with cp.async.bulk.
+// Thread 0 runs a kTcStages-deep pipeline (a typical block-row fits whole): wait for a stage's bytes, issue
+// the MMA, commit it to the stage's "empty" barrier, refill the stage when
+// that MMA has read it.  A final commit signals the epilogue: every warp
+// reads its 32 TMEM lanes (tcgen05.ld 32x32b, 16 columns) and writes 16 C
+// rows for its 32 columns.  Waits are bounded; on a timeout the kernel
+// records an error, waits (bounded) for its own copies, frees its TMEM and
+// returns.  Rows of B past K come back as zeros from TMA.
+constexpr int kTcStages = 8;
+constexpr int kTcSlab = 128;                       // UMMA M = C columns per CTA
+constexpr int kTcBBytes = kTcSlab * kTS * 2;       // 4096
+constexpr int kTcABytes = kTS * kTS * 2;           // 512
+constexpr int kTcThreads = 128;
+constexpr int kTcTmemCols = 32;                    // >= N = 16, power of two
+constexpr int kTcSmem = 1024 + kTcStages * (kTcBBytes + kTcABytes) + 128;
+
+__device__ __forceinline__ uint64_t umma_smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo, uint32_t layout) {
+  uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;  // sm100 descriptor version
+  d |= (uint64_t)(layout & 7u) << 61;
+  return d;
 }
-template <>
-__global__ void tiles_to_lp_kernel<__nv_bfloat16>(int64_t n, const double *__restrict__ v,
-                                                  __nv_bfloat16 *__restrict__ out) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    out[i] = __float2bfloat16_rn((float)v[i]);
+
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int32_t c0, int32_t c1,
+                                            uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void umma_f16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                         uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n}" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t *bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kTcThreads) spmm_tc_kernel(const __grid_constant__ CUtensorMap tmB, int32_t M,
+                                                             int32_t nbr, const int32_t *__restrict__ bptr,
+                                                             const int32_t *__restrict__ bcol,
+                                                             const T *__restrict__ tiles, float *__restrict__ C,
+                                                             int64_t ldc, float alpha, float beta,
+                                                             int32_t *__restrict__ err) {
+  extern __shared__ unsigned char smem_raw[];
+  const uint32_t raw = smem_u32(smem_raw);
+  unsigned char *sm = smem_raw + ((1024u - (raw & 1023u)) & 1023u);  // 1 KB aligned for the swizzle atoms
+  unsigned char *bslab = sm;
+  unsigned char *atile = sm + kTcStages * kTcBBytes;
+  uint64_t *full = reinterpret_cast<uint64_t *>(atile + kTcStages * kTcABytes);
+  uint64_t *empty = full + kTcStages;
+  uint64_t *done = empty + kTcStages;
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int32_t br = blockIdx.x;
+  const int32_t n0 = blockIdx.y * kTcSlab;
+  const int32_t k0 = bptr[br], nk = bptr[br + 1] - k0;
+
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < kTcStages; ++i) {
+      mbar_init(&full[i], 1);
+      mbar_init(&empty[i], 1);
+    }
+    mbar_init(done, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"((uint32_t)kTcTmemCols)
+                 : "memory");
+    // this CTA allocates only once: let the other CTAs on the SM allocate
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  int ok = 1;
+  if (threadIdx.x == 0 && nk > 0) {
+    constexpr uint32_t fmt = std::is_same<T, __nv_bfloat16>::value ? 1u : 0u;
+    // kind::f16 instruction descriptor: D FP32, A and B in `fmt`, A MN-major,
+    // B K-major, N = 16, M = 128
+    constexpr uint32_t idesc = (1u << 4) | (fmt << 7) | (fmt << 10) | (1u << 15) | ((16u >> 3) << 17) |
+                               ((uint32_t)(kTcSlab >> 4) << 24);
+    int issued = 0, waited = 0;
+    auto load = [&](int i) {
+      const int st = i % kTcStages;
+      const int32_t bc = bcol[k0 + i];
+      mbar_expect_tx(&full[st], kTcBBytes + kTcABytes);
+      tma_load_2d(bslab + st * kTcBBytes, &tmB, n0, bc * kTS, &full[st]);
+      tma_load_2d(bslab + st * kTcBBytes + kTcBBytes / 2, &tmB, n0 + 64, bc * kTS, &full[st]);
+      bulk_g2s(atile + st * kTcABytes, tiles + (int64_t)(k0 + i) * kTS * kTS, kTcABytes, &full[st]);
+      ++issued;
+    };
+    for (int i = 0; i < nk && i < kTcStages; ++i) load(i);
+    for (int i = 0; i < nk; ++i) {
+      const int st = i % kTcStages;
+      const unsigned ph = (unsigned)(i / kTcStages) & 1u;
+      if (!mbar_wait(&full[st], ph)) {
+        ok = 0;
+        break;
+      }
+      ++waited;
+      // A: the B slab, 128-byte swizzle, 64-column halves 2 KB apart (LBO),
+      // 8-row K groups 1 KB apart (SBO).  B: the tile, no swizzle, K halves
+      // 128 B apart (LBO), 8-row groups 256 B apart (SBO).
+      const uint64_t adesc = umma_smem_desc(smem_u32(bslab + st * kTcBBytes), 2048u, 1024u, 2u);
+      const uint64_t bdesc = umma_smem_desc(smem_u32(atile + st * kTcABytes), 128u, 256u, 0u);
+      umma_f16(tmem, adesc, bdesc, idesc, i > 0 ? 1u : 0u);
+      umma_commit(&empty[st]);
+      if (i + kTcStages < nk) {
+        if (!mbar_wait(&empty[st], ph)) {  // this stage's MMA has read it
+          ok = 0;
+          break;
+        }
+        load(i + kTcStages);
+      }
+    }
+    umma_commit(done);  // arrives when every MMA issued above has completed
+    if (!ok) {
+      // let the copies still in flight land before the CTA goes away
+      for (int j = waited; j < issued; ++j) (void)mbar_wait(&full[j % kTcStages], (unsigned)(j / kTcStages) & 1u);
+    }
+  }
+  __syncwarp();
+  int good = ok;
+  if (nk > 0) good = good && mbar_wait(done, 0u);
+  const int all_good = __syncthreads_and(good);
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  float v[16];
+#pragma unroll
+  for (int j = 0; j < 16; ++j) v[j] = 0.f;
+  if (all_good && nk > 0) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(tmem + ((uint32_t)(warp * 32) << 16)));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
+  }
+  if (all_good) {
+    const int64_t col = (int64_t)n0 + warp * 32 + lane;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const int64_t row = (int64_t)br * kTS + j;
+      if (row < M) {
+        float *cp = C + row * ldc + col;
+        float o = alpha * v[j];
+        if (beta != 0.f) o += beta * *cp;
+        *cp = o;
+      }
+    }
+  } else if (threadIdx.x == 0) {
+    atomicExch(err, 1);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)kTcTmemCols)
+                 : "memory");
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against libcuda).
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static std::once_flag once;
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+// B (K rows x N columns, row stride ldb elements) as a 2-D tensor map with
+// 64-column x 16-row boxes and 128-byte swizzle.
+static bsp_status make_b_map(CUtensorMap *map, const void *B, int32_t K, int32_t N, int64_t ldb, bool bf16) {
+  auto enc = tensor_map_encoder();
+  if (!enc) BSP_FAIL(BSP_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+  const cuuint64_t dims[2] = {(cuuint64_t)N, (cuuint64_t)K};
+  const cuuint64_t strides[1] = {(cuuint64_t)ldb * 2};
+  const cuuint32_t box[2] = {64, (cuuint32_t)kTS};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = enc(map, bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2,
+                         const_cast<void *>(B), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                         CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) BSP_FAIL(BSP_ERR_INVALID, "cuTensorMapEncodeTiled rejected B (code " + std::to_string((int)r) + ")");
+  return BSP_OK;
+}
+
+template <typename T>
+__device__ __forceinline__ T tile_cvt(double v);
+template <> __device__ __forceinline__ __half tile_cvt<__half>(double v) { return __double2half(v); }
+template <> __device__ __forceinline__ __nv_bfloat16 tile_cvt<__nv_bfloat16>(double v) {
+  return __float2bfloat16_rn((float)v);
+}
+
+// Row-major FP64 tiles -> stored low-precision tiles.
+template <typename T>
+__global__ void tiles_to_lp_kernel(int64_t n, const double *__restrict__ v, T *__restrict__ out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int e = (int)(i & 255);
+    out[(i & ~(int64_t)255) + tile_pos(e >> 4, e & 15)] = tile_cvt<T>(v[i]);
+  }
 }
 
 template <typename T, int CPL>
@@ -577,8 +816,32 @@ extern "C" bsp_status bsp_smat_free(bsp_smat *m) {
   return BSP_OK;
 }
 
+static bsp_status smat_spmm_tc(const bsp_smat *m, const void *B, int32_t N, int64_t ldb, float *C, int64_t ldc,
+                               float alpha, float beta, cudaStream_t s) {
+  CUtensorMap map;
+  BSP_TRY(make_b_map(&map, B, m->cols, N, ldb, m->dtype == BSP_BF16));
+  const dim3 grid((unsigned)m->tiles.rowRegions, (unsigned)(N / kTcSlab));
+  if (m->dtype == BSP_F16)
+    spmm_tc_kernel<__half><<<grid, kTcThreads, kTcSmem, s>>>(map, m->rows, m->tiles.rowRegions,
+                                                             m->tiles.bcsrRowPtr, m->tiles.bcsrcolIdx,
+                                                             (const __half *)m->tile_val, C, ldc, alpha, beta,
+                                                             m->err);
+  else
+    spmm_tc_kernel<__nv_bfloat16><<<grid, kTcThreads, kTcSmem, s>>>(
+        map, m->rows, m->tiles.rowRegions, m->tiles.bcsrRowPtr, m->tiles.bcsrcolIdx,
+        (const __nv_bfloat16 *)m->tile_val, C, ldc, alpha, beta, m->err);
+  BSP_LAUNCH_CHECK();
+  return BSP_OK;
+}
+
 extern "C" bsp_status bsp_smat_spmm(const bsp_smat *m, const void *B, int32_t N, int64_t ldb, float *C,
                                     int64_t ldc, float alpha, float beta, bsp_stream_t stream) {
+  return bsp_smat_spmm_path(m, B, N, ldb, C, ldc, alpha, beta, BSP_SMAT_AUTO, stream);
+}
+
+extern "C" bsp_status bsp_smat_spmm_path(const bsp_smat *m, const void *B, int32_t N, int64_t ldb, float *C,
+                                         int64_t ldc, float alpha, float beta, int32_t path,
+                                         bsp_stream_t stream) {
   clear_error();
   BSP_CHECK_ARG(m && B && C, "null pointer");
   BSP_CHECK_ARG(N > 0 && N % 32 == 0, "N must be a positive multiple of 32");
@@ -586,8 +849,12 @@ extern "C" bsp_status bsp_smat_spmm(const bsp_smat *m, const void *B, int32_t N,
   // cp.async.bulk needs 16-byte aligned sources and sizes
   BSP_CHECK_ARG((uintptr_t)B % 16 == 0 && (ldb * 2) % 16 == 0, "B must be 16-byte aligned with ldb % 8 == 0");
   BSP_CHECK_ARG((uintptr_t)m->tile_val % 16 == 0, "tile values must be 16-byte aligned");
+  BSP_CHECK_ARG(path >= BSP_SMAT_AUTO && path <= BSP_SMAT_TCGEN05, "unknown path");
+  BSP_CHECK_ARG(path != BSP_SMAT_TCGEN05 || N % kTcSlab == 0, "the tcgen05 path needs N % 128 == 0");
   if (m->tiles.rowRegions == 0) return BSP_OK;
   cudaStream_t s = as_stream(stream);
+  if (path == BSP_SMAT_TCGEN05 || (path == BSP_SMAT_AUTO && N % kTcSlab == 0))
+    return smat_spmm_tc(m, B, N, ldb, C, ldc, alpha, beta, s);
   const int nt = (N % 64 == 0) ? 8 : 4;
   const int64_t items = (int64_t)m->tiles.rowRegions * (N / (8 * nt));
   int64_t blocks = ceil_div(items, kWarpsPerCta);

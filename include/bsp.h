@@ -373,7 +373,8 @@ typedef struct {
   int32_t rows, cols, nnz;
   int32_t dtype;      /* BSP_F16 or BSP_BF16 */
   bsp_bcsr tiles;     /* 16x16 structure (tiles.values released) */
-  void *tile_val;     /* [tiles.nonzeroBlocks*256] F16/BF16 row-major tiles */
+  void *tile_val;     /* [tiles.nonzeroBlocks*256] F16/BF16 tiles, each as four
+                         8x8 core matrices (tcgen05 K-major operand order) */
   int32_t *err;       /* device flag: a bounded wait timed out */
   double fill;
 } bsp_smat;
@@ -383,10 +384,20 @@ bsp_status bsp_smat_create(int32_t rows, int32_t cols, int32_t nnz,
                            const double *values, bsp_dtype dtype, bsp_smat *out,
                            bsp_stream_t stream);
 bsp_status bsp_smat_free(bsp_smat *m);
-/* B: dtype of the matrix, 16-byte aligned, ldb % 8 == 0; N % 32 == 0. */
+/* B: dtype of the matrix, 16-byte aligned, ldb % 8 == 0; N % 32 == 0.
+ * N % 128 == 0 runs on the tcgen05 tensor cores (TMEM accumulator, TMA
+ * staging of B), otherwise on mma.sync. */
 bsp_status bsp_smat_spmm(const bsp_smat *m, const void *B, int32_t N,
                          int64_t ldb, float *C, int64_t ldc, float alpha,
                          float beta, bsp_stream_t stream);
+typedef enum {
+  BSP_SMAT_AUTO = 0,
+  BSP_SMAT_MMA_SYNC = 1, /* warp mma.sync.m16n8k16, FP32 accumulators in registers */
+  BSP_SMAT_TCGEN05 = 2   /* tcgen05.mma M=128 N=16 K=16 per tile; N % 128 == 0 */
+} bsp_smat_path;
+bsp_status bsp_smat_spmm_path(const bsp_smat *m, const void *B, int32_t N,
+                              int64_t ldb, float *C, int64_t ldc, float alpha,
+                              float beta, int32_t path, bsp_stream_t stream);
 /* Reads the device error flag (waits for `stream`): BSP_ERR_TIMEOUT when a
  * bounded copy wait gave up. */
 bsp_status bsp_smat_check(const bsp_smat *m, bsp_stream_t stream);

@@ -171,3 +171,34 @@ def test_smat_alpha_beta_and_argument_errors(cuda):
     with pytest.raises(ValueError):
         bsp.spmm_csr(rp, ci, vals_t.to(cuda), B_t.to(cuda).to(torch.bfloat16))
     M.free()
+
+
+@pytest.mark.parametrize("name", ["f16", "bf16"])
+@pytest.mark.parametrize("N", [128, 256])
+@pytest.mark.parametrize("kind", ["dense_tiles", "ragged"])
+def test_smat_tcgen05_and_mma_sync_paths(cuda, name, N, kind):
+    """The tcgen05 path (TMEM accumulator, TMA-staged B) and the mma.sync path
+    against the FP64 oracle; both deterministic across calls."""
+    import torch
+    A = bsp.gen_random_bsr(96, 16, 6, 1.0, 1.0, 4) if kind == "dense_tiles" else bsp.gen_powerlaw(1003, 1.7, 400, 12)
+    vals_t, vals64, B_t, B64 = _case(A, N, name, N + 7)
+    rp, ci, v64 = _dev(cuda, A.rowptr, A.colidx, vals64)
+    M = bsp.SmatMatrix(rp, ci, v64, rows=A.rows, cols=A.cols, dtype=name)
+    Bd = B_t.to(cuda)
+    Cref, absC = pyoracle.spmm_f64(A.rowptr, A.colidx, vals64, B64)
+    L = np.full((A.rows, 1), 16.0 * ((A.cols + 15) // 16) + 2.0)
+    u = 2.0 ** -24
+    tol = 2.0 * (L * u / (1 - L * u)) * absC + 1e-30
+    for path in ("tcgen05", "mma_sync"):
+        C1 = M.spmm(Bd, path=path).cpu().numpy()
+        C2 = M.spmm(Bd, path=path).cpu().numpy()
+        M.check()
+        assert np.array_equal(C1, C2), path
+        assert np.all(np.abs(C1.astype(np.float64) - Cref) <= tol), path
+    Cin = torch.from_numpy(np.random.default_rng(5).uniform(-1, 1, (A.rows, N)).astype(np.float32)).to(cuda)
+    Cb = M.spmm(Bd, Cin.clone(), alpha=0.5, beta=2.0, path="tcgen05").cpu().numpy().astype(np.float64)
+    want = 0.5 * Cref + 2.0 * Cin.cpu().numpy().astype(np.float64)
+    assert np.all(np.abs(Cb - want) <= tol + 4 * u * (0.5 * absC + 2.0 * np.abs(Cin.cpu().numpy())))
+    with pytest.raises(bsp.BspError):
+        M.spmm(torch.zeros(A.cols, 96, dtype=Bd.dtype, device=cuda), path="tcgen05")   # N % 128 != 0
+    M.free()
