@@ -462,14 +462,14 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) spmm_block_kernel(
 //     128-byte swizzle) into a 4 KB stage aligned to 1 KB;
 //   * B operand = the stored tile (512 B, no swizzle, K-major core matrices,
 //     see tile_pos) copied with cp.async.bulk.
-// Thread 0 runs a kTcStages-deep pipeline (a typical block-row fits whole): wait for a stage's bytes, issue
+// Thread 0 runs a kTcStages-deep pipeline (4 stages keep ~11 CTAs per SM): wait for a stage's bytes, issue
 // the MMA, commit it to the stage's "empty" barrier, refill the stage when
 // that MMA has read it.  A final commit signals the epilogue: every warp
 // reads its 32 TMEM lanes (tcgen05.ld 32x32b, 16 columns) and writes 16 C
 // rows for its 32 columns.  Waits are bounded; on a timeout the kernel
 // records an error, waits (bounded) for its own copies, frees its TMEM and
 // returns.  Rows of B past K come back as zeros from TMA.
-constexpr int kTcStages = 8;
+constexpr int kTcStages = 4;
 constexpr int kTcSlab = 128;                       // UMMA M = C columns per CTA
 constexpr int kTcBBytes = kTcSlab * kTS * 2;       // 4096
 constexpr int kTcABytes = kTS * kTS * 2;           // 512
