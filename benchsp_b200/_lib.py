@@ -233,6 +233,13 @@ class BspTuneResult(C.Structure):
 FMT_CSR, FMT_BSR, FMT_DASP = 0, 1, 2
 
 _PROTOS.update({
+    "bsp_reorder_rcm": (C.c_int, [_I32, _I32, _P, _P, _P, _P]),
+    "bsp_permute_csr": (C.c_int, [_I32, _I32, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "bsp_reorder_rcm_host": (C.c_int, [_I32, _I32, _P, _P, _P]),
+    "bsp_permute_csr_host": (C.c_int, [_I32, _I32, _P, _P, _P, _P, _P, _P, _P]),
+})
+
+_PROTOS.update({
     "bsp_tune_spmv": (C.c_int, [_I32, _I32, _I32, _P, _P, _P, _I32, C.POINTER(BspTuneResult), _P]),
     "bsp_matrix_key": (C.c_int, [_I32, _I32, _I32, _P, _P, C.POINTER(C.c_uint64), _P]),
     "bsp_tune_cache_clear": (None, []),

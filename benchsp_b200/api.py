@@ -773,3 +773,53 @@ class SpmvPlan:
         except Exception:
             pass
 
+
+# ---------------------------------------------------------------------------
+# Reordering (no reference counterpart)
+
+def _np_ptr(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def reorder_rcm_host(rowptr: np.ndarray, colidx: np.ndarray) -> np.ndarray:
+    """Reverse Cuthill-McKee permutation (perm[new] = old) of host CSR arrays."""
+    rowptr = np.ascontiguousarray(rowptr, np.int32)
+    colidx = np.ascontiguousarray(colidx, np.int32)
+    perm = np.empty(rowptr.size - 1, np.int32)
+    check(lib().bsp_reorder_rcm_host(perm.size, colidx.size, _np_ptr(rowptr), _np_ptr(colidx), _np_ptr(perm)))
+    return perm
+
+
+def permute_csr_host(A: "HostCSR", perm: np.ndarray) -> "HostCSR":
+    """P A P^T of a square host CSR matrix."""
+    perm = np.ascontiguousarray(perm, np.int32)
+    rp = np.empty(A.rows + 1, np.int32)
+    ci = np.empty(A.nnz, np.int32)
+    va = np.empty(A.nnz, np.float64)
+    check(lib().bsp_permute_csr_host(A.rows, A.nnz, _np_ptr(np.ascontiguousarray(A.rowptr, np.int32)),
+                                     _np_ptr(np.ascontiguousarray(A.colidx, np.int32)),
+                                     _np_ptr(np.ascontiguousarray(A.values, np.float64)), _np_ptr(perm),
+                                     _np_ptr(rp), _np_ptr(ci), _np_ptr(va)))
+    return HostCSR(A.rows, A.cols, rp, ci, va)
+
+
+def reorder_rcm(rowptr, colidx, stream=None):
+    """Device form: returns perm as an int32 tensor on the same device."""
+    torch = _torch()
+    perm = torch.empty(rowptr.numel() - 1, dtype=torch.int32, device=rowptr.device)
+    check(lib().bsp_reorder_rcm(perm.numel(), colidx.numel(), _dptr(rowptr, "rowptr"), _dptr(colidx, "colidx"),
+                                _dptr(perm, "perm"), _stream(stream)))
+    return perm
+
+
+def permute_csr(rowptr, colidx, values, perm, stream=None):
+    """Device form of P A P^T; returns (rowptr, colidx, values) tensors."""
+    torch = _torch()
+    rp = torch.empty_like(rowptr)
+    ci = torch.empty_like(colidx)
+    va = torch.empty_like(values)
+    check(lib().bsp_permute_csr(perm.numel(), colidx.numel(), _dptr(rowptr, "rowptr"), _dptr(colidx, "colidx"),
+                                _dptr(values, "values"), _dptr(perm, "perm"), _dptr(rp, "out_rowptr"),
+                                _dptr(ci, "out_colidx"), _dptr(va, "out_values"), _stream(stream)))
+    return rp, ci, va
+

@@ -1,0 +1,262 @@
+// Matrix reordering (no reference counterpart: the reference's SMaT path
+// blocks the matrix in its given order, src/smat.cu:116-120, so scattered
+// nonzeros give one nonzero per 16x16 tile).  Reverse Cuthill-McKee on the
+// symmetrized pattern gathers nonzeros near the diagonal, which raises the
+// fill of BSR blocks and SMaT tiles for matrices whose rows were numbered
+// without locality.  Host code (a one-time preprocessing step); the device
+// entry points copy in, reorder on the host and copy back.
+//
+// RCM: for every connected component, start from a pseudo-peripheral vertex
+// (the George-Liu search: repeat a BFS from the farthest, lowest-degree
+// vertex of the last level while the eccentricity grows), visit the BFS
+// levels taking each vertex's unvisited neighbours in increasing degree
+// (ties by index), and reverse the whole order at the end.
+#include <cuda_runtime.h>
+#include <omp.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "../../include/bsp.h"
+
+namespace bsp {
+void set_error(const std::string &msg);
+void clear_error();
+}  // namespace bsp
+
+namespace {
+
+bsp_status fail(bsp_status st, const char *msg) {
+  bsp::set_error(msg);
+  return st;
+}
+
+struct Graph {
+  std::vector<int64_t> ptr;
+  std::vector<int32_t> adj;
+};
+
+// Pattern of A + A^T without the diagonal, neighbours sorted and distinct.
+Graph symmetrize(int32_t n, const int32_t *rp, const int32_t *ci) {
+  std::vector<int64_t> deg(n + 1, 0);
+  for (int32_t i = 0; i < n; ++i)
+    for (int32_t j = rp[i]; j < rp[i + 1]; ++j) {
+      const int32_t c = ci[j];
+      if (c == i || c < 0 || c >= n) continue;
+      ++deg[i];
+      ++deg[c];
+    }
+  Graph g;
+  g.ptr.assign(n + 1, 0);
+  for (int32_t i = 0; i < n; ++i) g.ptr[i + 1] = g.ptr[i] + deg[i];
+  g.adj.resize(g.ptr[n]);
+  std::vector<int64_t> fill(g.ptr.begin(), g.ptr.end() - 1);
+  for (int32_t i = 0; i < n; ++i)
+    for (int32_t j = rp[i]; j < rp[i + 1]; ++j) {
+      const int32_t c = ci[j];
+      if (c == i || c < 0 || c >= n) continue;
+      g.adj[fill[i]++] = c;
+      g.adj[fill[c]++] = i;
+    }
+  // sort + unique each list, then compact
+  std::vector<int64_t> np(n + 1, 0);
+#pragma omp parallel for schedule(dynamic, 1024)
+  for (int32_t i = 0; i < n; ++i) {
+    auto b = g.adj.begin() + g.ptr[i], e = g.adj.begin() + g.ptr[i + 1];
+    std::sort(b, e);
+    np[i + 1] = std::unique(b, e) - b;
+  }
+  for (int32_t i = 0; i < n; ++i) np[i + 1] += np[i];
+  std::vector<int32_t> adj(np[n]);
+#pragma omp parallel for schedule(static)
+  for (int32_t i = 0; i < n; ++i)
+    std::copy(g.adj.begin() + g.ptr[i], g.adj.begin() + g.ptr[i] + (np[i + 1] - np[i]), adj.begin() + np[i]);
+  g.ptr.swap(np);
+  g.adj.swap(adj);
+  return g;
+}
+
+// BFS from s over unvisited-by-order vertices of s's component; returns the
+// last level's vertices and the number of levels.
+int bfs_levels(const Graph &g, int32_t s, std::vector<int32_t> &level, std::vector<int32_t> &queue,
+               std::vector<int32_t> &last) {
+  queue.clear();
+  queue.push_back(s);
+  level[s] = 0;
+  int depth = 0;
+  size_t head = 0;
+  while (head < queue.size()) {
+    const int32_t v = queue[head++];
+    for (int64_t k = g.ptr[v]; k < g.ptr[v + 1]; ++k) {
+      const int32_t w = g.adj[k];
+      if (level[w] < 0) {
+        level[w] = level[v] + 1;
+        depth = std::max(depth, level[w]);
+        queue.push_back(w);
+      }
+    }
+  }
+  last.clear();
+  for (int32_t v : queue)
+    if (level[v] == depth) last.push_back(v);
+  for (int32_t v : queue) level[v] = -1;  // reset for the next search
+  return depth;
+}
+
+void rcm(int32_t n, const int32_t *rp, const int32_t *ci, int32_t *perm) {
+  const Graph g = symmetrize(n, rp, ci);
+  auto degree = [&](int32_t v) { return g.ptr[v + 1] - g.ptr[v]; };
+  std::vector<int32_t> level(n, -1), queue, last, order;
+  order.reserve(n);
+  std::vector<char> placed(n, 0);
+  std::vector<int32_t> nb;
+  for (int32_t seed = 0; seed < n; ++seed) {
+    if (placed[seed]) continue;
+    // pseudo-peripheral start (a few George-Liu steps)
+    int32_t s = seed;
+    int depth = bfs_levels(g, s, level, queue, last);
+    for (int it = 0; it < 8; ++it) {
+      int32_t best = last[0];
+      for (int32_t v : last)
+        if (degree(v) < degree(best) || (degree(v) == degree(best) && v < best)) best = v;
+      const int d2 = bfs_levels(g, best, level, queue, last);
+      if (d2 <= depth) break;
+      s = best;
+      depth = d2;
+    }
+    // Cuthill-McKee BFS from s
+    size_t head = order.size();
+    order.push_back(s);
+    placed[s] = 1;
+    while (head < order.size()) {
+      const int32_t v = order[head++];
+      nb.clear();
+      for (int64_t k = g.ptr[v]; k < g.ptr[v + 1]; ++k)
+        if (!placed[g.adj[k]]) nb.push_back(g.adj[k]);
+      std::sort(nb.begin(), nb.end(), [&](int32_t a, int32_t b) {
+        return degree(a) != degree(b) ? degree(a) < degree(b) : a < b;
+      });
+      for (int32_t w : nb) {
+        placed[w] = 1;
+        order.push_back(w);
+      }
+    }
+  }
+  for (int32_t i = 0; i < n; ++i) perm[i] = order[n - 1 - i];
+}
+
+// P A P^T: new row i = old row perm[i], columns renumbered by the inverse and
+// sorted.
+void permute(int32_t n, const int32_t *rp, const int32_t *ci, const double *va, const int32_t *perm,
+             int32_t *orp, int32_t *oci, double *ova) {
+  std::vector<int32_t> inv(n);
+  for (int32_t i = 0; i < n; ++i) inv[perm[i]] = i;
+  orp[0] = 0;
+  for (int32_t i = 0; i < n; ++i) orp[i + 1] = orp[i] + (rp[perm[i] + 1] - rp[perm[i]]);
+#pragma omp parallel
+  {
+    std::vector<std::pair<int32_t, double>> row;
+#pragma omp for schedule(dynamic, 512)
+    for (int32_t i = 0; i < n; ++i) {
+      const int32_t o = perm[i];
+      row.clear();
+      for (int32_t j = rp[o]; j < rp[o + 1]; ++j) row.emplace_back(inv[ci[j]], va ? va[j] : 0.0);
+      std::sort(row.begin(), row.end(), [](const auto &a, const auto &b) { return a.first < b.first; });
+      for (size_t k = 0; k < row.size(); ++k) {
+        oci[orp[i] + k] = row[k].first;
+        if (ova) ova[orp[i] + k] = row[k].second;
+      }
+    }
+  }
+}
+
+bool valid_csr(int32_t n, int32_t nnz, const int32_t *rp) {
+  if (rp[0] != 0 || rp[n] != nnz) return false;
+  for (int32_t i = 0; i < n; ++i)
+    if (rp[i + 1] < rp[i]) return false;
+  return true;
+}
+
+bool valid_perm(int32_t n, const int32_t *perm) {
+  std::vector<char> seen(n, 0);
+  for (int32_t i = 0; i < n; ++i) {
+    if (perm[i] < 0 || perm[i] >= n || seen[perm[i]]) return false;
+    seen[perm[i]] = 1;
+  }
+  return true;
+}
+
+template <typename T>
+bool d2h(std::vector<T> &h, const T *d, size_t n) {
+  h.resize(n);
+  return n == 0 || cudaMemcpy(h.data(), d, n * sizeof(T), cudaMemcpyDeviceToHost) == cudaSuccess;
+}
+
+template <typename T>
+bool h2d(T *d, const std::vector<T> &h) {
+  return h.empty() || cudaMemcpy(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice) == cudaSuccess;
+}
+
+}  // namespace
+
+extern "C" bsp_status bsp_reorder_rcm_host(int32_t rows, int32_t nnz, const int32_t *rowPtr,
+                                           const int32_t *colIdx, int32_t *perm) {
+  bsp::clear_error();
+  if (rows < 0 || nnz < 0 || !rowPtr || !perm || (nnz > 0 && !colIdx))
+    return fail(BSP_ERR_INVALID, "bsp_reorder_rcm: bad argument");
+  if (!valid_csr(rows, nnz, rowPtr)) return fail(BSP_ERR_INVALID, "bsp_reorder_rcm: malformed row pointers");
+  if (rows > 0) rcm(rows, rowPtr, colIdx, perm);
+  return BSP_OK;
+}
+
+extern "C" bsp_status bsp_permute_csr_host(int32_t rows, int32_t nnz, const int32_t *rowPtr, const int32_t *colIdx,
+                                           const double *values, const int32_t *perm, int32_t *outRowPtr,
+                                           int32_t *outColIdx, double *outValues) {
+  bsp::clear_error();
+  if (rows < 0 || nnz < 0 || !rowPtr || !perm || !outRowPtr || (nnz > 0 && (!colIdx || !outColIdx)))
+    return fail(BSP_ERR_INVALID, "bsp_permute_csr: bad argument");
+  if (!valid_csr(rows, nnz, rowPtr)) return fail(BSP_ERR_INVALID, "bsp_permute_csr: malformed row pointers");
+  if (!valid_perm(rows, perm)) return fail(BSP_ERR_INVALID, "bsp_permute_csr: perm is not a permutation");
+  for (int32_t j = 0; j < nnz; ++j)
+    if (colIdx[j] < 0 || colIdx[j] >= rows)
+      return fail(BSP_ERR_INVALID, "bsp_permute_csr: column out of range (square matrices only)");
+  permute(rows, rowPtr, colIdx, values, perm, outRowPtr, outColIdx, outValues);
+  return BSP_OK;
+}
+
+extern "C" bsp_status bsp_reorder_rcm(int32_t rows, int32_t nnz, const int32_t *rowPtr, const int32_t *colIdx,
+                                      int32_t *perm, bsp_stream_t stream) {
+  bsp::clear_error();
+  if (rows < 0 || nnz < 0) return fail(BSP_ERR_INVALID, "bsp_reorder_rcm: negative size");
+  if (cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(stream)) != cudaSuccess)
+    return fail(BSP_ERR_CUDA, "bsp_reorder_rcm: stream synchronize failed");
+  std::vector<int32_t> rp, ci, p(rows > 0 ? rows : 0);
+  if (!d2h(rp, rowPtr, (size_t)rows + 1) || !d2h(ci, colIdx, (size_t)nnz))
+    return fail(BSP_ERR_CUDA, "bsp_reorder_rcm: copy to the host failed");
+  const bsp_status st = bsp_reorder_rcm_host(rows, nnz, rp.data(), ci.data(), p.data());
+  if (st != BSP_OK) return st;
+  return h2d(perm, p) ? BSP_OK : fail(BSP_ERR_CUDA, "bsp_reorder_rcm: copy to the device failed");
+}
+
+extern "C" bsp_status bsp_permute_csr(int32_t rows, int32_t nnz, const int32_t *rowPtr, const int32_t *colIdx,
+                                      const double *values, const int32_t *perm, int32_t *outRowPtr,
+                                      int32_t *outColIdx, double *outValues, bsp_stream_t stream) {
+  bsp::clear_error();
+  if (rows < 0 || nnz < 0) return fail(BSP_ERR_INVALID, "bsp_permute_csr: negative size");
+  if (cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(stream)) != cudaSuccess)
+    return fail(BSP_ERR_CUDA, "bsp_permute_csr: stream synchronize failed");
+  std::vector<int32_t> rp, ci, p, orp((size_t)rows + 1), oci(nnz);
+  std::vector<double> va, ova(values ? nnz : 0);
+  if (!d2h(rp, rowPtr, (size_t)rows + 1) || !d2h(ci, colIdx, (size_t)nnz) || !d2h(p, perm, (size_t)rows) ||
+      (values && !d2h(va, values, (size_t)nnz)))
+    return fail(BSP_ERR_CUDA, "bsp_permute_csr: copy to the host failed");
+  const bsp_status st = bsp_permute_csr_host(rows, nnz, rp.data(), ci.data(), values ? va.data() : nullptr,
+                                             p.data(), orp.data(), oci.data(), values ? ova.data() : nullptr);
+  if (st != BSP_OK) return st;
+  if (!h2d(outRowPtr, orp) || !h2d(outColIdx, oci) || (values && outValues && !h2d(outValues, ova)))
+    return fail(BSP_ERR_CUDA, "bsp_permute_csr: copy to the device failed");
+  return BSP_OK;
+}

@@ -465,6 +465,31 @@ bsp_status bsp_blockinfo(int32_t rows, int32_t cols, int32_t nnz,
                          bsp_stream_t stream);
 
 /* ---------------------------------------------------------------------- */
+/* Reordering (no reference counterpart; the reference blocks matrices in the
+ * order given, src/smat.cu:116-120).  Reverse Cuthill-McKee on the pattern
+ * of A + A^T: perm[new] = old.  Gathers nonzeros near the diagonal, which
+ * raises BSR block and SMaT tile fill for matrices numbered without
+ * locality.  Runs on the host (a one-time preprocessing step); the device
+ * forms copy in and out and wait for `stream`. */
+bsp_status bsp_reorder_rcm(int32_t rows, int32_t nnz, const int32_t *rowPtr,
+                           const int32_t *colIdx, int32_t *perm,
+                           bsp_stream_t stream);
+/* P A P^T of a square CSR matrix (new row i = old row perm[i], columns
+ * renumbered and sorted); values may be NULL (pattern only). */
+bsp_status bsp_permute_csr(int32_t rows, int32_t nnz, const int32_t *rowPtr,
+                           const int32_t *colIdx, const double *values,
+                           const int32_t *perm, int32_t *outRowPtr,
+                           int32_t *outColIdx, double *outValues,
+                           bsp_stream_t stream);
+/* The same on host arrays. */
+bsp_status bsp_reorder_rcm_host(int32_t rows, int32_t nnz, const int32_t *rowPtr,
+                                const int32_t *colIdx, int32_t *perm);
+bsp_status bsp_permute_csr_host(int32_t rows, int32_t nnz, const int32_t *rowPtr,
+                                const int32_t *colIdx, const double *values,
+                                const int32_t *perm, int32_t *outRowPtr,
+                                int32_t *outColIdx, double *outValues);
+
+/* ---------------------------------------------------------------------- */
 /* Format autotuner for FP64 SpMV (no reference counterpart: the reference's
  * drivers run every format on every matrix, bench/spmvfp64.cpp:135-177).
  * Model mode decides from row-length statistics and exact 4x4 / 8x8 block
