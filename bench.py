@@ -516,6 +516,31 @@ def run_suite(args) -> None:
     _emit("spmm_graph_1M_zipf1.8_deg32", n=A.rows, nnz=A.nnz, max_row=int(np.diff(A.rowptr).max()), variants=res)
     del rp, ci, v64, A64
 
+    # --- block SpMM on dense 16x16 tiles: tcgen05 vs mma.sync vs CSR
+    A = bsp.gen_random_bsr(32768, 16, 8, 1.0, 1.0, SEED + 5)
+    rp, ci, v64 = up(A.rowptr, A.colidx, A.values)
+    res = {}
+    for name, tdt in (("f16", torch.float16), ("bf16", torch.bfloat16)):
+        M = bsp.SmatMatrix(rp, ci, v64, rows=A.rows, cols=A.cols, dtype=name)
+        v = v64.to(tdt)
+        for N in (128, 256):
+            B = (torch.rand(A.cols, N, generator=torch.Generator().manual_seed(N)) * 2 - 1).to(tdt).to(dev)
+            Cref = torch.sparse_csr_tensor(rp.long(), ci.long(), v64, size=(A.rows, A.cols)) @ B.double()
+            row = {}
+            for path in ("tcgen05", "mma_sync"):
+                Cm = M.spmm(B, path=path)
+                err = float(torch.linalg.norm(Cm.double() - Cref) / torch.linalg.norm(Cref))
+                t = _timed(lambda: M.spmm(B, Cm, path=path), 10)
+                row[path] = {"ms": round(t * 1e3, 4), "tflops": round(2 * A.nnz * N / t / 1e12, 2),
+                             "rel_err_vs_fp64": err}
+            t = _timed(lambda: bsp.spmm_csr(rp, ci, v, B), 5)
+            row["csr_grouped"] = {"ms": round(t * 1e3, 4), "tflops": round(2 * A.nnz * N / t / 1e12, 2)}
+            res[f"{name}_N{N}"] = row
+        M.check()
+        M.free()
+    _emit("smat_dense16_tiles_524k_rows_8_per_row", rows=A.rows, nnz=A.nnz, tiles=A.nnz // 256, variants=res)
+    del rp, ci, v64
+
     # --- 512 independent SpMVs (and 8-RHS SpMMs) in one persistent launch
     mats = bsp.gen_batch(512, SEED + 6)
     nnz = sum(int(m.rowptr[-1]) for m in mats)
@@ -583,6 +608,14 @@ def run_profile(args) -> None:
         B = (torch.rand(A.cols, 128, generator=torch.Generator().manual_seed(1)) * 2 - 1).half().to(dev)
         for _ in range(reps):
             P.spmm(B)
+    elif w in ("smat_tc", "smat_mma"):   # dense 16x16 tiles, 8 per block-row, 524,288 rows, N = 256, FP16
+        A = bsp.gen_random_bsr(32768, 16, 8, 1.0, 1.0, SEED + 5)
+        rp, ci, va = up(A.rowptr, A.colidx, A.values)
+        M = bsp.SmatMatrix(rp, ci, va, rows=A.rows, cols=A.cols, dtype="f16")
+        B = (torch.rand(A.cols, 256, generator=torch.Generator().manual_seed(1)) * 2 - 1).half().to(dev)
+        for _ in range(reps):
+            M.spmm(B, path="tcgen05" if w == "smat_tc" else "mma_sync")
+        M.check()
     elif w == "batch":   # the 512-matrix batch, FP64, one RHS
         mats = bsp.gen_batch(512, SEED + 6)
         d = []
@@ -608,7 +641,7 @@ def main():
     ap.add_argument("--suite", action="store_true", help="one JSON line per further workload (1 GPU)")
     ap.add_argument("--grid", type=int, default=GRID, help="stencil grid edge (64 = the benchmark config; "
                     "smaller values only for profiling captures)")
-    ap.add_argument("--profile", choices=["dasp", "cg_fp64", "cg_f16", "spmm", "batch"],
+    ap.add_argument("--profile", choices=["dasp", "cg_fp64", "cg_f16", "spmm", "batch", "smat_tc", "smat_mma"],
                     help="a few calls of one workload's kernels (for ncu captures)")
     args = ap.parse_args()
     if args.profile:
