@@ -36,6 +36,7 @@ sys.path.insert(0, str(ROOT))
 GRID, DOF, SEED = 64, 4, 20261203 + 1
 METRIC = "SpMV GFLOP/s (FP64 BSR 4x4, 27-pt stencil 64^3 x 4 dof)"
 WORKLOAD = "bsr4_fp64_spmv_stencil27_64cubed_4dof"
+E2E_CHUNKS = 4
 
 
 def peaks() -> dict:
@@ -274,8 +275,9 @@ def run_ours(args, ws, rank, local):
     yh = torch.empty(A.rows, dtype=torch.float64).pin_memory()
     xh_np, yh_np = xh.numpy(), yh.numpy()
     e2e_steps = max(3, min(args.steps, 200))
+    HP = M.host_plan(E2E_CHUNKS)   # overlapped x upload / SpMV / y download
     for _ in range(3):
-        M.spmv_host(xh_np, yh_np)
+        HP.spmv(xh_np, yh_np)
     if ws > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
@@ -283,7 +285,7 @@ def run_ours(args, ws, rank, local):
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(e2e_steps):
-        M.spmv_host(xh_np, yh_np)
+        HP.spmv(xh_np, yh_np)
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(e0.elapsed_time(e1), ws, dev)
@@ -321,7 +323,8 @@ def run_ours(args, ws, rank, local):
                      "peak_src": pk["src"], "algorithmic_bytes_per_launch": algo_bytes},
         "cpu_baseline": cpu,
         "e2e": {"value": round(e2e_value, 3), "unit": "GFLOP/s", "h2d_bytes_per_step": 8 * A.cols,
-                "d2h_bytes_per_step": 8 * A.rows, "steps": e2e_steps},
+                "d2h_bytes_per_step": 8 * A.rows, "steps": e2e_steps,
+                "call": f"bsp_bsr_spmv_host_pipelined ({E2E_CHUNKS} chunks, pinned host x/y)"},
         "gpu_launches": args.steps,
         "clocks": clk.summary(),
         "extra": {"csr2bsr_seconds": round(convert_s, 4), "gbs": round(achieved, 1),

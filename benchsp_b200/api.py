@@ -164,6 +164,10 @@ class BsrMatrix:
                                       _stream(stream)))
         return y_host
 
+    def host_plan(self, chunks: int = 8, stream=None) -> "BsrHostPlan":
+        """Overlapped host-buffer SpMV plan (see BsrHostPlan)."""
+        return BsrHostPlan(self, chunks, stream)
+
     def free(self) -> None:
         if self._live:
             self._live = False
@@ -172,6 +176,34 @@ class BsrMatrix:
     def __del__(self):
         try:
             self.free()
+        except Exception:
+            pass
+
+
+class BsrHostPlan:
+    """Host-buffer BSR SpMV with the x upload, the SpMV and the y download
+    overlapped in block-row chunks (keeps the matrix alive)."""
+
+    def __init__(self, M: "BsrMatrix", chunks: int = 8, stream=None):
+        self._m = M
+        self._h = C.c_void_p()
+        check(lib().bsp_bsr_host_plan_create(C.byref(M._d), chunks, C.byref(self._h), _stream(stream)))
+
+    def spmv(self, x_host: np.ndarray, y_host: np.ndarray, *, alpha: float = 1.0, beta: float = 0.0,
+             stream=None) -> np.ndarray:
+        check(lib().bsp_bsr_spmv_host_pipelined(self._h, x_host.ctypes.data_as(C.c_void_p),
+                                                y_host.ctypes.data_as(C.c_void_p), float(alpha), float(beta),
+                                                _stream(stream)))
+        return y_host
+
+    def close(self) -> None:
+        if self._h:
+            check(lib().bsp_bsr_host_plan_destroy(self._h))
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
         except Exception:
             pass
 

@@ -31,6 +31,8 @@
 //   * DMMA: FP64 mma.sync.m8n8k4 on block pairs (the reference's scheme,
 //     rows of two blocks stacked into the 8x4 A fragment) with deterministic
 //     extraction of the useful diagonal sub-blocks.
+#include <algorithm>
+
 #include "bsp_internal.cuh"
 #include "util.cuh"
 
@@ -514,6 +516,19 @@ bsp_status bsr_spmv_impl(const bsp_bsr *m, const double *x, double *y, double al
   if (algo != BSP_BSR_FFMA) BSP_FAIL(BSP_ERR_INVALID, "unknown BSR algo");
   if (m->bs != 4 && m->bs != 8) BSP_FAIL(BSP_ERR_UNSUPPORTED, "block size must be 4 or 8");
   return default_ffma(m)->fn(m, x, y, alpha, beta, s);
+}
+
+// FFMA SpMV of block rows [lo, hi) only (y given for the whole matrix), with
+// the kernel shape chosen for the whole matrix.
+bsp_status bsr_spmv_rows(const bsp_bsr *m, int32_t lo, int32_t hi, const double *x, double *y, double alpha,
+                         double beta, cudaStream_t s) {
+  if (hi <= lo) return BSP_OK;
+  if (((uintptr_t)m->blcVal & 31) != 0) BSP_FAIL(BSP_ERR_INVALID, "blcVal must be 32-byte aligned");
+  bsp_bsr sub = *m;
+  sub.blcPtr = m->blcPtr + lo;  // block offsets stay absolute
+  sub.blc_row = hi - lo;
+  sub.row = std::min<int64_t>((int64_t)m->row - (int64_t)lo * m->bs, (int64_t)(hi - lo) * m->bs);
+  return default_ffma(m)->fn(&sub, x, y + (int64_t)lo * m->bs, alpha, beta, s);
 }
 
 bsp_status bsr_spmv_variant(const bsp_bsr *m, const double *x, double *y, double alpha, double beta, int lanes,

@@ -187,6 +187,21 @@ bsp_status bsp_bsr_spmv_host(const bsp_bsr *m, const double *x_host, double *y_h
                              double alpha, double beta, int32_t algo,
                              bsp_stream_t stream);
 
+/* Host-buffer form with the copies overlapped (no reference counterpart).
+ * The plan cuts the block rows into `chunks` ranges (1..64) and keeps device
+ * x / y and three streams: x goes up in pieces, each range starts once the x
+ * it reads has arrived (its largest column, found at plan time), and its y
+ * goes down as soon as it is done.  Pays for matrices whose columns follow
+ * their rows (stencils, banded, reordered).  Host buffers should be pinned.
+ * The call returns when y_host is written; `m` must outlive the plan. */
+typedef struct bsp_bsr_host_plan_s *bsp_bsr_host_plan;
+bsp_status bsp_bsr_host_plan_create(const bsp_bsr *m, int32_t chunks,
+                                    bsp_bsr_host_plan *plan, bsp_stream_t stream);
+bsp_status bsp_bsr_spmv_host_pipelined(bsp_bsr_host_plan plan, const double *x_host,
+                                       double *y_host, double alpha, double beta,
+                                       bsp_stream_t stream);
+bsp_status bsp_bsr_host_plan_destroy(bsp_bsr_host_plan plan);
+
 /* ---------------------------------------------------------------------- */
 /* Fixed-tile BCSR (BCSRFormat<double,int32_t>, reference
  * include/matrixFormat.hpp:16-30).  blockNum is 64-bit (rowRegions *

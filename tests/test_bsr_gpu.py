@@ -123,3 +123,30 @@ def test_misaligned_x_uses_scalar_gathers(cuda):
     M = bsp.csr2bsr(rp, ci, va, rows=A.rows, cols=A.cols, bs=4)
     y = M.spmv(xx, algo="ffma").cpu().numpy()
     assert np.all(np.abs(y - ref) <= pyoracle.spmv_tolerance(A.rowptr, A.colidx, A.values, x[1:].copy()))
+
+
+@pytest.mark.parametrize("kind", ["stencil", "random", "ragged"])
+@pytest.mark.parametrize("chunks", [1, 3, 8, 64])
+def test_bsr_host_pipelined_matches_host_call(cuda, kind, chunks):
+    """The overlapped host-buffer SpMV returns exactly what the plain
+    host-buffer call returns (same kernel per row), with and without beta."""
+    import torch
+    A = {"stencil": lambda: bsp.gen_stencil27(10, 4, 2), "random": lambda: bsp.gen_random_bsr(300, 4, 5, 0.4, 1.0, 3),
+         "ragged": lambda: bsp.gen_powerlaw(1001, 1.9, 200, 4)}[kind]()
+    rp, ci, va = (torch.from_numpy(a).to(cuda) for a in (A.rowptr, A.colidx, A.values))
+    M = bsp.csr2bsr(rp, ci, va, rows=A.rows, cols=A.cols, bs=4)
+    x = torch.from_numpy(bsp.gen_uniform(A.cols, 5)).pin_memory().numpy()
+    y0 = torch.from_numpy(np.random.default_rng(2).uniform(-1, 1, A.rows)).pin_memory().numpy()
+    want = y0.copy()
+    M.spmv_host(x, want, alpha=1.5, beta=-0.5)
+    P = M.host_plan(chunks)
+    for _ in range(2):
+        got = y0.copy()
+        P.spmv(x, got, alpha=1.5, beta=-0.5)
+        assert np.array_equal(got, want)
+    got = np.empty(A.rows)
+    P.spmv(x, got)
+    ref = pyoracle.spmv_f64(A.rowptr, A.colidx, A.values, x)
+    assert np.all(np.abs(got - ref) <= pyoracle.spmv_tolerance(A.rowptr, A.colidx, A.values, x))
+    P.close()
+    M.free()
