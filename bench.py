@@ -574,6 +574,62 @@ def run_suite(args) -> None:
             P.close()
     _emit("batch_512_banded_and_zipf2.2", matrices=len(mats), rows=rows, nnz=nnz, variants=res)
 
+    # --- Matrix Market file -> CSR (stencil 32^3 x 4 dof written by the library)
+    run_mtx_read(bsp, dev)
+
+
+def run_mtx_read(bsp, dev) -> None:
+    """File -> device CSR through the library vs scipy.io.mmread (the
+    fast_matrix_market reader the reference's drivers use) + a stable
+    (row, col) sort, the reference's conversion; median of 3 each."""
+    import os
+    import tempfile
+    import time
+    import warnings
+
+    import scipy.io
+    import torch
+    A = bsp.gen_stencil27(32, 4, SEED + 20)
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "stencil.mtx")
+        bsp.write_mtx(path, A)
+        mb = os.path.getsize(path) / 1e6
+
+        def ours():
+            f = bsp.MtxFile(path)
+            t1 = time.perf_counter()
+            out = f.csr(dev)
+            torch.cuda.synchronize()
+            f.close()
+            return out, t1
+
+        def theirs():
+            with warnings.catch_warnings():
+                warnings.simplefilter("ignore")
+                m = scipy.io.mmread(path)
+            o = np.lexsort((m.col, m.row))
+            rp = np.zeros(m.shape[0] + 1, np.int64)
+            np.add.at(rp, m.row.astype(np.int64) + 1, 1)
+            return np.cumsum(rp), m.col[o], m.data[o]
+
+        t_ours, t_parse, t_ref = [], [], []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            (rp, ci, va), t1 = ours()
+            t2 = time.perf_counter()
+            t_ours.append(t2 - t0)
+            t_parse.append(t1 - t0)
+            t0 = time.perf_counter()
+            R = theirs()
+            t_ref.append(time.perf_counter() - t0)
+        same = (np.array_equal(rp.cpu().numpy(), R[0]) and np.array_equal(ci.cpu().numpy(), R[1])
+                and np.array_equal(va.cpu().numpy().view(np.uint64), R[2].astype(np.float64).view(np.uint64)))
+    to, tp, tr = (float(np.median(t)) for t in (t_ours, t_parse, t_ref))
+    _emit("mtx_read_stencil27_32cubed_4dof", nnz=A.nnz, file_mb=round(mb, 1), threads=os.cpu_count(),
+          ours={"file_to_device_csr_s": round(to, 4), "parse_s": round(tp, 4), "mb_per_s": round(mb / to, 1)},
+          scipy_fmm_plus_sort={"file_to_host_csr_s": round(tr, 4), "mb_per_s": round(mb / tr, 1)},
+          speedup=round(tr / to, 2), identical_csr=bool(same))
+
 
 # ---------------------------------------------------------------------------
 # --profile W: a few calls of one workload's kernels, for ncu captures (small

@@ -276,3 +276,22 @@ _PROTOS.update({
                                      _P]),
     "bsp_gen_graph": (C.c_int, [_I32, _D, _D, _U64, _PI32, _PI64, _P, _P, _P]),
 })
+
+
+class BspMtxInfo(C.Structure):
+    """Mirror of bsp_mtx_info (include/bsp.h)."""
+    _fields_ = [("rows", C.c_int64), ("cols", C.c_int64), ("entries", C.c_int64), ("nnz", C.c_int64),
+                ("format", C.c_int32), ("field", C.c_int32), ("symmetry", C.c_int32)]
+
+
+MTX_DIAG_ZERO = 1
+
+_PROTOS.update({
+    "bsp_mtx_read": (C.c_int, [C.c_char_p, _I32, _I32, C.POINTER(C.c_void_p)]),
+    "bsp_mtx_get_info": (C.c_int, [C.c_void_p, C.POINTER(BspMtxInfo)]),
+    "bsp_mtx_triplets": (C.c_int, [C.c_void_p, _P, _P, _P]),
+    "bsp_mtx_csr_host": (C.c_int, [C.c_void_p, _P, _P, _P]),
+    "bsp_mtx_csr": (C.c_int, [C.c_void_p, _P, _P, _P, _P]),
+    "bsp_mtx_free": (C.c_int, [C.c_void_p]),
+    "bsp_mtx_write_csr_host": (C.c_int, [C.c_char_p, _I32, _I32, _I64, _P, _P, _P, _I32]),
+})

@@ -9,6 +9,7 @@ synthetic inputs stand in for its .mtx matrices.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from dataclasses import dataclass
 
 import numpy as np
@@ -855,3 +856,84 @@ def permute_csr(rowptr, colidx, values, perm, stream=None):
                                 _dptr(ci, "out_colidx"), _dptr(va, "out_values"), _stream(stream)))
     return rp, ci, va
 
+
+
+# ---------------------------------------------------------------------------
+# Matrix Market files (replaces the drivers' read_triplet_file + triplet sort,
+# reference bench/spmvfp64.cpp:37-86)
+
+_MTX_FORMATS = {0: "coordinate", 1: "array"}
+_MTX_FIELDS = {0: "real", 1: "integer", 2: "pattern"}
+_MTX_SYMMETRIES = {0: "general", 1: "symmetric", 2: "skew-symmetric", 3: "hermitian"}
+
+
+class MtxFile:
+    """A parsed Matrix Market file (host triplets held by the library).
+
+    ``fmm_diag_zero`` adds an explicit 0.0 mirror for every diagonal entry of
+    a non-general file, fast_matrix_market's default element count."""
+
+    def __init__(self, path, *, fmm_diag_zero: bool = False, threads: int = 0):
+        h = C.c_void_p()
+        check(lib().bsp_mtx_read(os.fsencode(os.fspath(path)), _lib.MTX_DIAG_ZERO if fmm_diag_zero else 0,
+                                 int(threads), C.byref(h)))
+        self._h = h
+        info = _lib.BspMtxInfo()
+        check(lib().bsp_mtx_get_info(h, C.byref(info)))
+        self.rows, self.cols, self.entries, self.nnz = info.rows, info.cols, info.entries, info.nnz
+        self.format = _MTX_FORMATS[info.format]
+        self.field = _MTX_FIELDS[info.field]
+        self.symmetry = _MTX_SYMMETRIES[info.symmetry]
+
+    def triplets(self) -> tuple:
+        r = np.empty(self.nnz, np.int32)
+        c = np.empty(self.nnz, np.int32)
+        v = np.empty(self.nnz, np.float64)
+        check(lib().bsp_mtx_triplets(self._h, _np_ptr(r), _np_ptr(c), _np_ptr(v)))
+        return r, c, v
+
+    def csr_host(self) -> HostCSR:
+        rp = np.empty(self.rows + 1, np.int32)
+        ci = np.empty(self.nnz, np.int32)
+        va = np.empty(self.nnz, np.float64)
+        check(lib().bsp_mtx_csr_host(self._h, _np_ptr(rp), _np_ptr(ci), _np_ptr(va)))
+        return HostCSR(int(self.rows), int(self.cols), rp, ci, va)
+
+    def csr(self, device="cuda", stream=None) -> tuple:
+        """CSR built on the device: (rowptr, colidx, values) tensors."""
+        torch = _torch()
+        rp = torch.empty(self.rows + 1, dtype=torch.int32, device=device)
+        ci = torch.empty(max(1, self.nnz), dtype=torch.int32, device=device)
+        va = torch.empty(max(1, self.nnz), dtype=torch.float64, device=device)
+        check(lib().bsp_mtx_csr(self._h, _dptr(rp, "rowptr"), _dptr(ci, "colidx"), _dptr(va, "values"),
+                                _stream(stream)))
+        return rp, ci[:self.nnz], va[:self.nnz]
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().bsp_mtx_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def read_mtx(path, *, fmm_diag_zero: bool = False, threads: int = 0) -> HostCSR:
+    """Host CSR of a Matrix Market file (rows, then columns ascending)."""
+    f = MtxFile(path, fmm_diag_zero=fmm_diag_zero, threads=threads)
+    try:
+        return f.csr_host()
+    finally:
+        f.close()
+
+
+def write_mtx(path, A: HostCSR, *, pattern: bool = False, threads: int = 0) -> None:
+    """Writes host CSR as 'coordinate real general' (shortest round-trip values)."""
+    rp = np.ascontiguousarray(A.rowptr, np.int32)
+    ci = np.ascontiguousarray(A.colidx, np.int32)
+    va = None if pattern else np.ascontiguousarray(A.values, np.float64)
+    check(lib().bsp_mtx_write_csr_host(os.fsencode(os.fspath(path)), A.rows, A.cols, ci.size, _np_ptr(rp),
+                                       _np_ptr(ci), None if va is None else _np_ptr(va), int(threads)))

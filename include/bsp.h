@@ -645,6 +645,70 @@ bsp_status bsp_gen_banded(int32_t n, int32_t width, uint64_t seed,
 /* Uniform random x in [-1, 1]. */
 bsp_status bsp_gen_uniform(int64_t n, uint64_t seed, double *x);
 
+/* ---------------------------------------------------------------------- */
+/* Matrix Market files.  Replaces the reference drivers' read_triplet_file +
+ * triplet-to-CSR block (bench/spmvfp64.cpp:37-86, bench/spmvfp16.cpp:32-60,
+ * bench/spmmfp16.cpp:32-60), which read through the third-party
+ * fast_matrix_market header and then sort by (row, col).
+ *
+ * Accepted: "%%MatrixMarket matrix coordinate|array real|double|integer|pattern
+ * general|symmetric|skew-symmetric|hermitian" (complex is BSP_ERR_UNSUPPORTED;
+ * hermitian with a real field is symmetric).  Comment lines (%) and blank
+ * lines may appear anywhere after the banner; CR-LF line ends are accepted.
+ * Values are converted with correct rounding; pattern entries are 1.0.
+ * Array files give every stored element (zeros included), column-major.
+ *
+ * Triplets are the file's entries in file order (1-based -> 0-based), then,
+ * for a non-general file, one mirrored entry (j, i) per off-diagonal entry,
+ * in file order, negated for skew-symmetric.  With BSP_MTX_DIAG_ZERO every
+ * diagonal entry of a non-general file also gets an explicit 0.0 mirror,
+ * which is fast_matrix_market's default element count (2 x entries).
+ * CSR: rows ascending, columns ascending within a row, entries with the same
+ * (row, col) kept in triplet order (duplicates are not summed). */
+#define BSP_MTX_DIAG_ZERO 1
+
+typedef enum { BSP_MTX_COORDINATE = 0, BSP_MTX_ARRAY = 1 } bsp_mtx_format;
+typedef enum { BSP_MTX_REAL = 0, BSP_MTX_INTEGER = 1, BSP_MTX_PATTERN = 2 } bsp_mtx_field;
+typedef enum {
+  BSP_MTX_GENERAL = 0,
+  BSP_MTX_SYMMETRIC = 1,
+  BSP_MTX_SKEW_SYMMETRIC = 2,
+  BSP_MTX_HERMITIAN = 3
+} bsp_mtx_symmetry;
+
+typedef struct {
+  int64_t rows, cols;
+  int64_t entries;  /* stored entries in the file */
+  int64_t nnz;      /* triplets after the symmetry expansion */
+  int32_t format, field, symmetry;
+} bsp_mtx_info;
+
+typedef struct bsp_mtx_s *bsp_mtx;
+
+/* Maps and parses the whole file on `threads` host threads (0 = all).  The
+ * handle keeps the triplets; rows, cols <= 2^31-1 and nnz <= 2^31-1. */
+bsp_status bsp_mtx_read(const char *path, int32_t flags, int32_t threads,
+                        bsp_mtx *out);
+bsp_status bsp_mtx_get_info(bsp_mtx m, bsp_mtx_info *info);
+/* The expanded triplets (nnz each), as read_matrix_market_triplet returns
+ * them (any argument may be NULL to skip it). */
+bsp_status bsp_mtx_triplets(bsp_mtx m, int32_t *rows, int32_t *cols,
+                            double *values);
+/* CSR on the host: rowPtr[rows+1], colIdx[nnz], values[nnz]. */
+bsp_status bsp_mtx_csr_host(bsp_mtx m, int32_t *rowPtr, int32_t *colIdx,
+                            double *values);
+/* CSR in device memory (caller-allocated, same sizes): the triplets are
+ * copied up and ordered on the device by two stable radix sorts. */
+bsp_status bsp_mtx_csr(bsp_mtx m, int32_t *rowPtr, int32_t *colIdx,
+                       double *values, bsp_stream_t stream);
+bsp_status bsp_mtx_free(bsp_mtx m);
+/* Writes host CSR as "coordinate real general" (values == NULL: "pattern"),
+ * each value in its shortest round-trip decimal form. */
+bsp_status bsp_mtx_write_csr_host(const char *path, int32_t rows, int32_t cols,
+                                  int64_t nnz, const int32_t *rowPtr,
+                                  const int32_t *colIdx, const double *values,
+                                  int32_t threads);
+
 #ifdef __cplusplus
 }
 #endif
