@@ -284,10 +284,11 @@ class BspMtxInfo(C.Structure):
                 ("format", C.c_int32), ("field", C.c_int32), ("symmetry", C.c_int32)]
 
 
-MTX_DIAG_ZERO = 1
+MTX_DIAG_ZERO, MTX_DIAG_DUPLICATE, MTX_NO_EXPAND = 1, 2, 4
 
 _PROTOS.update({
     "bsp_mtx_read": (C.c_int, [C.c_char_p, _I32, _I32, C.POINTER(C.c_void_p)]),
+    "bsp_mtx_read_buffer": (C.c_int, [C.c_char_p, C.c_size_t, _I32, _I32, C.POINTER(C.c_void_p)]),
     "bsp_mtx_get_info": (C.c_int, [C.c_void_p, C.POINTER(BspMtxInfo)]),
     "bsp_mtx_triplets": (C.c_int, [C.c_void_p, _P, _P, _P]),
     "bsp_mtx_csr_host": (C.c_int, [C.c_void_p, _P, _P, _P]),

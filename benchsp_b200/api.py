@@ -873,10 +873,10 @@ class MtxFile:
     ``fmm_diag_zero`` adds an explicit 0.0 mirror for every diagonal entry of
     a non-general file, fast_matrix_market's default element count."""
 
-    def __init__(self, path, *, fmm_diag_zero: bool = False, threads: int = 0):
+    def __init__(self, path, *, fmm_diag_zero: bool = False, flags: int = 0, threads: int = 0):
         h = C.c_void_p()
-        check(lib().bsp_mtx_read(os.fsencode(os.fspath(path)), _lib.MTX_DIAG_ZERO if fmm_diag_zero else 0,
-                                 int(threads), C.byref(h)))
+        flags = int(flags) | (_lib.MTX_DIAG_ZERO if fmm_diag_zero else 0)
+        check(lib().bsp_mtx_read(os.fsencode(os.fspath(path)), flags, int(threads), C.byref(h)))
         self._h = h
         info = _lib.BspMtxInfo()
         check(lib().bsp_mtx_get_info(h, C.byref(info)))

@@ -370,21 +370,24 @@ bsp_status read_body(const char *b, const char *e, const Header &h, int T, int32
     csorted = general;
   }
   // symmetry expansion: mirrors after the stored entries, in file order
-  const bool diag_zero = !general && (flags & BSP_MTX_DIAG_ZERO);
+  const bool expand = !general && !(flags & BSP_MTX_NO_EXPAND);
+  const bool diag_zero = expand && (flags & BSP_MTX_DIAG_ZERO);
+  const bool diag_dup = expand && (flags & BSP_MTX_DIAG_DUPLICATE);
+  const bool diag_copy = diag_zero || diag_dup;
   std::vector<int64_t> moff(T + 1, 0);
   const auto tcut = [&](int t) { return got * t / T; };
-  if (!general) {
+  if (expand) {
 #pragma omp parallel for num_threads(T) schedule(static, 1)
     for (int t = 0; t < T; ++t) {
       int64_t m = 0;
-      for (int64_t k = tcut(t); k < tcut(t + 1); ++k) m += (R[k] != Cc[k]) || diag_zero;
+      for (int64_t k = tcut(t); k < tcut(t + 1); ++k) m += (R[k] != Cc[k]) || diag_copy;
       moff[t + 1] = m;
     }
     for (int t = 0; t < T; ++t) moff[t + 1] += moff[t];
   }
   const int64_t nnz = got + moff[T];
   if (nnz > INT32_MAX) return fail(BSP_ERR_UNSUPPORTED, "more than 2^31-1 entries after the symmetry expansion");
-  if (!general) {
+  if (expand) {
     const double sign = skew ? -1.0 : 1.0;
 #pragma omp parallel for num_threads(T) schedule(static, 1)
     for (int t = 0; t < T; ++t) {
@@ -395,10 +398,10 @@ bsp_status read_body(const char *b, const char *e, const Header &h, int T, int32
           Cc[o] = R[k];
           V[o] = sign * V[k];
           ++o;
-        } else if (diag_zero) {
+        } else if (diag_copy) {
           R[o] = R[k];
           Cc[o] = Cc[k];
-          V[o] = 0.0;
+          V[o] = diag_zero ? 0.0 : V[k];
           ++o;
         }
       }
@@ -419,21 +422,18 @@ bsp_status read_body(const char *b, const char *e, const Header &h, int T, int32
 
 }  // namespace
 
-extern "C" bsp_status bsp_mtx_read(const char *path, int32_t flags, int32_t threads, bsp_mtx *out) {
-  bsp::clear_error();
-  if (!path || !out) return fail(BSP_ERR_INVALID, "bsp_mtx_read: null pointer");
-  if (flags & ~BSP_MTX_DIAG_ZERO) return fail(BSP_ERR_INVALID, "bsp_mtx_read: unknown flags");
-  *out = nullptr;
-  Mapped f;
-  bsp_status st = map_file(path, f);
-  if (st != BSP_OK) return st;
+static bsp_status read_text(const char *p, size_t n, int32_t flags, int32_t threads, bsp_mtx *out) {
+  if (flags & ~(BSP_MTX_DIAG_ZERO | BSP_MTX_DIAG_DUPLICATE | BSP_MTX_NO_EXPAND))
+    return fail(BSP_ERR_INVALID, "bsp_mtx_read: unknown flags");
+  if ((flags & BSP_MTX_DIAG_ZERO) && (flags & BSP_MTX_DIAG_DUPLICATE))
+    return fail(BSP_ERR_INVALID, "bsp_mtx_read: DIAG_ZERO and DIAG_DUPLICATE exclude each other");
   Header h;
-  st = parse_header(f.p, f.p + f.n, h);
+  bsp_status st = parse_header(p, p + n, h);
   if (st != BSP_OK) return st;
   auto *M = new (std::nothrow) bsp_mtx_s();
   if (!M) return fail(BSP_ERR_ALLOC, "bsp_mtx_read: out of host memory");
   try {
-    st = read_body(h.body, f.p + f.n, h, nthreads(threads), flags, *M);
+    st = read_body(h.body, p + n, h, nthreads(threads), flags, *M);
   } catch (const std::bad_alloc &) {
     st = fail(BSP_ERR_ALLOC, "bsp_mtx_read: out of host memory");
   }
@@ -443,6 +443,25 @@ extern "C" bsp_status bsp_mtx_read(const char *path, int32_t flags, int32_t thre
   }
   *out = M;
   return BSP_OK;
+}
+
+extern "C" bsp_status bsp_mtx_read(const char *path, int32_t flags, int32_t threads, bsp_mtx *out) {
+  bsp::clear_error();
+  if (!path || !out) return fail(BSP_ERR_INVALID, "bsp_mtx_read: null pointer");
+  *out = nullptr;
+  Mapped f;
+  const bsp_status st = map_file(path, f);
+  if (st != BSP_OK) return st;
+  return read_text(f.p, f.n, flags, threads, out);
+}
+
+extern "C" bsp_status bsp_mtx_read_buffer(const char *data, size_t bytes, int32_t flags, int32_t threads,
+                                          bsp_mtx *out) {
+  bsp::clear_error();
+  if (!data || !out) return fail(BSP_ERR_INVALID, "bsp_mtx_read_buffer: null pointer");
+  *out = nullptr;
+  if (bytes == 0) return fail(BSP_ERR_INVALID, "bsp_mtx_read_buffer: empty buffer");
+  return read_text(data, bytes, flags, threads, out);
 }
 
 extern "C" bsp_status bsp_mtx_get_info(bsp_mtx m, bsp_mtx_info *info) {

@@ -662,10 +662,15 @@ bsp_status bsp_gen_uniform(int64_t n, uint64_t seed, double *x);
  * for a non-general file, one mirrored entry (j, i) per off-diagonal entry,
  * in file order, negated for skew-symmetric.  With BSP_MTX_DIAG_ZERO every
  * diagonal entry of a non-general file also gets an explicit 0.0 mirror,
- * which is fast_matrix_market's default element count (2 x entries).
+ * which is fast_matrix_market's default element count (2 x entries);
+ * BSP_MTX_DIAG_DUPLICATE repeats the diagonal value instead, and
+ * BSP_MTX_NO_EXPAND keeps the stored entries only (its
+ * generalize_symmetry = false).
  * CSR: rows ascending, columns ascending within a row, entries with the same
  * (row, col) kept in triplet order (duplicates are not summed). */
-#define BSP_MTX_DIAG_ZERO 1
+#define BSP_MTX_DIAG_ZERO 1      /* explicit 0.0 mirror per diagonal entry */
+#define BSP_MTX_DIAG_DUPLICATE 2 /* a copy of each diagonal entry instead */
+#define BSP_MTX_NO_EXPAND 4      /* stored entries only, no mirrors */
 
 typedef enum { BSP_MTX_COORDINATE = 0, BSP_MTX_ARRAY = 1 } bsp_mtx_format;
 typedef enum { BSP_MTX_REAL = 0, BSP_MTX_INTEGER = 1, BSP_MTX_PATTERN = 2 } bsp_mtx_field;
@@ -689,6 +694,9 @@ typedef struct bsp_mtx_s *bsp_mtx;
  * handle keeps the triplets; rows, cols <= 2^31-1 and nnz <= 2^31-1. */
 bsp_status bsp_mtx_read(const char *path, int32_t flags, int32_t threads,
                         bsp_mtx *out);
+/* The same on file contents already in memory. */
+bsp_status bsp_mtx_read_buffer(const char *data, size_t bytes, int32_t flags,
+                               int32_t threads, bsp_mtx *out);
 bsp_status bsp_mtx_get_info(bsp_mtx m, bsp_mtx_info *info);
 /* The expanded triplets (nnz each), as read_matrix_market_triplet returns
  * them (any argument may be NULL to skip it). */

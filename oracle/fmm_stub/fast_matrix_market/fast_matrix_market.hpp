@@ -1,13 +1,11 @@
 // Minimal stand-in for the fast_matrix_market header the reference's bench
 // drivers include (fetched from the network by its CMakeLists.txt:15-21, not
 // available here).  TEST INFRASTRUCTURE ONLY: it lets oracle/Makefile compile
-// the reference's bench drivers unchanged (bench/blockinfo.cpp for its block
-// statistics; bench/spmvfp64.cpp, spmvfp16.cpp and spmmfp16.cpp linked
-// against libbspmv_compat to show the drop-in).  Reads Matrix Market coordinate files (real / integer /
-// pattern, general or symmetric) into triplet vectors, 1-based -> 0-based.
-// Drivers that open a fixed path of the reference author's machine
-// (bench/spmvfp16.cpp:41, bench/spmmfp16.cpp:37) read the file named by the
-// environment variable FMM_STUB_FILE when their stream did not open.
+// the reference's bench/blockinfo.cpp unchanged as an oracle of its block
+// statistics, independent of the library's own reader (the bench drivers
+// linked against libbspmv_compat use the library's drop-in header instead).
+// Reads Matrix Market coordinate files (real / integer / pattern, general or
+// symmetric) into triplet vectors, 1-based -> 0-based.
 #pragma once
 #include <cstdint>
 #include <cstdlib>
@@ -27,14 +25,7 @@ struct read_options {
 template <typename IT, typename VT, typename DIM>
 void read_matrix_market_triplet(std::istream &in0, DIM &nrows, DIM &ncols, std::vector<IT> &rows,
                                 std::vector<IT> &cols, std::vector<VT> &vals, const read_options & = {}) {
-  std::ifstream redirect;
-  std::istream *src = &in0;
-  if (!in0.good())
-    if (const char *p = std::getenv("FMM_STUB_FILE")) {
-      redirect.open(p);
-      src = &redirect;
-    }
-  std::istream &in = *src;
+  std::istream &in = in0;
   std::string line;
   if (!std::getline(in, line) || line.rfind("%%MatrixMarket", 0) != 0) throw std::runtime_error("not a MatrixMarket file");
   const bool pattern = line.find("pattern") != std::string::npos;

@@ -162,7 +162,7 @@ def test_reference_fp16_drivers_run(cuda, tmp_path, name):
     A = bsp.gen_laplace2d(48, 48) if name == "spmvfp16" else bsp.gen_random_bsr(32, 4, 4, 0.5, 1.0, 3)
     p = tmp_path / "m.mtx"
     pyoracle.write_mtx(p, A.rows, A.cols, A.rowptr, A.colidx, A.values)
-    env = dict(os.environ, FMM_STUB_FILE=str(p))
+    env = dict(os.environ, BSP_MTX_FILE=str(p))
     r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=600, env=env)
     assert r.returncode == 0, r.stdout + r.stderr
     if name == "spmvfp16":

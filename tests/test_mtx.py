@@ -204,6 +204,29 @@ def test_symmetric_expansion_and_fmm_diag_zero(tmp_path):
     assert np.array_equal(A.values[:3], [2.0, 0.0, -1.0])
 
 
+def test_expansion_flags_and_buffer_entry(tmp_path):
+    import ctypes as C
+    text = CASES["skew"].encode()
+    p = _write(tmp_path, "k.mtx", CASES["skew"])
+    assert bsp.MtxFile(p, flags=bsp._lib.MTX_NO_EXPAND).nnz == 2
+    s = bsp.MtxFile(_write(tmp_path, "s.mtx", CASES["symmetric_crlf_comments"]), flags=bsp._lib.MTX_DIAG_DUPLICATE)
+    r, c, v = s.triplets()
+    assert np.array_equal(v[4:], [2.0, -1.0, -1.5, 4.0]) and s.nnz == 8
+    with pytest.raises(bsp.BspError):
+        bsp.MtxFile(p, flags=bsp._lib.MTX_DIAG_DUPLICATE | bsp._lib.MTX_DIAG_ZERO)
+    with pytest.raises(bsp.BspError):
+        bsp.MtxFile(p, flags=64)
+    h = C.c_void_p()
+    bsp._lib.check(bsp.lib().bsp_mtx_read_buffer(text, len(text), 0, 2, C.byref(h)))
+    info = bsp._lib.BspMtxInfo()
+    bsp._lib.check(bsp.lib().bsp_mtx_get_info(h, C.byref(info)))
+    assert (info.rows, info.entries, info.nnz, info.symmetry) == (3, 2, 4, 2)
+    v2 = np.empty(4)
+    bsp._lib.check(bsp.lib().bsp_mtx_triplets(h, None, None, v2.ctypes.data_as(C.c_void_p)))
+    assert np.array_equal(v2, [1.25, -4.0, -1.25, 4.0])
+    bsp.lib().bsp_mtx_free(h)
+
+
 @pytest.mark.parametrize("threads", [1, 3, 8])
 def test_thread_count_does_not_change_the_result(tmp_path, threads):
     A = bsp.gen_powerlaw(60000, 1.7, 3000, 2)
@@ -323,3 +346,51 @@ def test_device_csr_matches_host_csr(cuda, tmp_path, kind):
     if kind != "powerlaw_dups":
         assert np.array_equal(H.rowptr, A.rowptr) and np.array_equal(H.colidx, A.colidx)
         assert np.array_equal(_bits(H.values), _bits(A.values))
+
+
+PROBE = r"""
+#include <cstdio>
+#include <fstream>
+#include "fast_matrix_market/fast_matrix_market.hpp"
+int main(int argc, char **argv) {
+  struct { int64_t nrows = 0, ncols = 0; std::vector<int32_t> rows, cols; std::vector<double> vals; } t;
+  std::ifstream f(argv[1]);
+  fast_matrix_market::read_options o;
+  if (argc > 2) o.generalize_symmetry = false;
+  fast_matrix_market::read_matrix_market_triplet(f, t.nrows, t.ncols, t.rows, t.cols, t.vals, o);
+  printf("%lld %lld %zu\n", (long long)t.nrows, (long long)t.ncols, t.vals.size());
+  for (size_t k = 0; k < t.vals.size(); ++k) printf("%d %d %a\n", t.rows[k], t.cols[k], t.vals[k]);
+}
+"""
+
+
+def test_fast_matrix_market_dropin_header(tmp_path):
+    """The reference drivers' read_matrix_market_triplet call, compiled
+    against the library's drop-in header, returns the library's triplets
+    (with fast_matrix_market's explicit zero per mirrored diagonal)."""
+    import shutil
+    import subprocess
+    from pathlib import Path
+    if shutil.which("g++") is None:
+        pytest.skip("no g++")
+    root = Path(__file__).resolve().parents[1]
+    src = tmp_path / "probe.cpp"
+    src.write_text(PROBE)
+    exe = tmp_path / "probe"
+    libdir = root / "benchsp_b200" / "lib"
+    subprocess.run(["g++", "-std=c++17", "-O1", f"-I{root / 'benchsp_b200' / 'compat'}", f"-I{root / 'include'}",
+                    str(src), "-o", str(exe), f"-L{libdir}", "-lbspmv", f"-Wl,-rpath,{libdir}"], check=True)
+    p = _write(tmp_path, "s.mtx", CASES["symmetric_crlf_comments"])
+    for flag, fmm in ((["x"], None), ([], True)):
+        out = subprocess.run([str(exe), str(p), *flag], capture_output=True, text=True, check=True).stdout.split("\n")
+        rows, cols, n = map(int, out[0].split())
+        trip = [ln.split() for ln in out[1:1 + n]]
+        r = np.array([int(a) for a, _, _ in trip])
+        c = np.array([int(b) for _, b, _ in trip])
+        v = np.array([float.fromhex(x) for _, _, x in trip])
+        if fmm:
+            rr, cc, vv = bsp.MtxFile(p, fmm_diag_zero=True).triplets()
+        else:
+            rr, cc, vv = (a[:4] for a in bsp.MtxFile(p).triplets())   # stored entries only
+        assert (rows, cols) == (3, 3)
+        assert np.array_equal(r, rr) and np.array_equal(c, cc) and np.array_equal(_bits(v), _bits(vv))
