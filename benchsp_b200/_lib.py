@@ -173,14 +173,15 @@ def check(status: int) -> None:
 class BspCgOptions(C.Structure):
     """Mirror of bsp_cg_options (include/bsp.h)."""
     _fields_ = [("mode", C.c_int32), ("tol", C.c_double), ("max_iters", C.c_int32), ("check_every", C.c_int32),
-                ("reliable_delta", C.c_double), ("use_graphs", C.c_int32)]
+                ("reliable_delta", C.c_double), ("use_graphs", C.c_int32), ("precond", C.c_int32),
+                ("precond_block", C.c_int32), ("refine", C.c_int32)]
 
 
 class BspCgResult(C.Structure):
     """Mirror of bsp_cg_result (include/bsp.h)."""
     _fields_ = [("iterations", C.c_int32), ("reliable_updates", C.c_int32), ("rel_residual", C.c_double),
                 ("seconds", C.c_double), ("converged", C.c_int32), ("bytes_moved", C.c_int64),
-                ("delta16", C.c_int32)]
+                ("delta16", C.c_int32), ("outer_steps", C.c_int32)]
 
 
 CG_FP64, CG_MIXED_F32, CG_MIXED_F16, CG_MIXED_BF16 = 0, 1, 2, 3
@@ -222,6 +223,8 @@ _PROTOS.update({
     "bsp_batch_stats": (C.c_int, [C.c_void_p, _PI64, _PI64, _PI64]),
     "bsp_batch_destroy": (C.c_int, [C.c_void_p]),
     "bsp_gen_banded": (C.c_int, [_I32, _I32, _U64, _PI32, _PI64, _P, _P, _P]),
+    "bsp_gen_diffusion3d": (C.c_int, [_I32, _D, _U64, _PI32, _PI64, _P, _P, _P]),
+    "bsp_gen_block_laplace3d": (C.c_int, [_I32, _I32, _D, _U64, _PI32, _PI64, _P, _P, _P]),
 })
 
 

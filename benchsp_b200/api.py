@@ -462,6 +462,16 @@ def gen_poisson3d(n: int) -> HostCSR:
     return _two_phase(lib().bsp_gen_poisson3d, n)
 
 
+def gen_diffusion3d(n: int, contrast: float, seed: int) -> HostCSR:
+    """SPD 7-point diffusion, face coefficients exp(contrast * U[-1, 1])."""
+    return _two_phase(lib().bsp_gen_diffusion3d, n, float(contrast), seed)
+
+
+def gen_block_laplace3d(n: int, dof: int, cond: float, seed: int) -> HostCSR:
+    """SPD L (x) S with a dof x dof coupling S of condition number `cond`."""
+    return _two_phase(lib().bsp_gen_block_laplace3d, n, dof, float(cond), seed)
+
+
 def gen_stencil27(n: int, dof: int, seed: int) -> HostCSR:
     return _two_phase(lib().bsp_gen_stencil27, n, dof, seed)
 
@@ -486,15 +496,23 @@ def gen_uniform(n: int, seed: int) -> np.ndarray:
 _CG_MODES = {"fp64": _lib.CG_FP64, "f32": _lib.CG_MIXED_F32, "f16": _lib.CG_MIXED_F16, "bf16": _lib.CG_MIXED_BF16}
 
 
+_CG_PRECONDS = {"none": 0, "jacobi": 1, "block_jacobi": 2}
+
+
 class CgSolver:
     """Solver plan for an SPD CSR matrix on the device (arrays must stay alive)."""
 
     def __init__(self, rowptr, colidx, values, *, mode: str = "f16", tol: float = 1e-10, max_iters: int = 20000,
-                 check_every: int = 16, reliable_delta: float = 0.1, use_graphs: bool = True, stream=None):
+                 check_every: int = 16, reliable_delta: float = 0.1, use_graphs: bool = True,
+                 precond: str = "none", block: int = 4, refine: str = "auto", stream=None):
+        """precond: "none", "jacobi" or "block_jacobi" (diagonal blocks of `block` rows, 4 or 8);
+        refine (mixed modes): "auto", "reliable" or "flexible"."""
         o = _lib.BspCgOptions()
         check(lib().bsp_cg_default_options(C.byref(o)))
         o.mode, o.tol, o.max_iters, o.check_every = _CG_MODES[mode], tol, max_iters, check_every
         o.reliable_delta, o.use_graphs = reliable_delta, int(use_graphs)
+        o.precond, o.precond_block = _CG_PRECONDS[precond], int(block)
+        o.refine = {"auto": 0, "reliable": 1, "flexible": 2}[refine]
         self._keep = (rowptr, colidx, values)
         self.n = rowptr.numel() - 1
         self._plan = C.c_void_p()

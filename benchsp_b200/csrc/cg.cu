@@ -281,8 +281,255 @@ __global__ void __launch_bounds__(kCgThreads) cg_update_kernel(int32_t n, const 
   if (threadIdx.x == 0) rr_part[blockIdx.x] = t;
 }
 
+// ---------------------------------------------------------------------------
+// Preconditioned CG (Jacobi: BS = 1; block-Jacobi: BS = 4 or 8 consecutive
+// rows).  M^{-1} is stored in the iteration precision: dinv[n] for BS = 1,
+// else the inverted diagonal blocks, BS*BS row-major per block (the last block
+// padded with identity rows).  The preconditioned iteration keeps the two
+// kernels: kernel A gathers z = M^{-1} r where it gathered r and reduces the
+// r.z partials where it reduced r.r; the update kernel below also applies
+// M^{-1} to the new residual and writes both the r.r partials (convergence
+// checks) and the r.z partials (the next direction).
+//
+// One thread per group of 8 rows (BS divides 8, so blocks never straddle
+// groups): 16-byte vector accesses for full groups, bounds-checked scalars for
+// the last partial group.
+template <typename VT>
+__device__ __forceinline__ void ld8(const VT *__restrict__ p, VT (&v)[8]) {
+  using V = typename Vec16<VT>::T;
+  constexpr int W = Vec16<VT>::W;
+  const V *pv = reinterpret_cast<const V *>(p);
+#pragma unroll
+  for (int u = 0; u < 8 / W; ++u) {
+    const V t = pv[u];
+#pragma unroll
+    for (int k = 0; k < W; ++k) v[u * W + k] = vget(t, k);
+  }
+}
+
+template <typename VT>
+__device__ __forceinline__ void st8(VT *__restrict__ p, const VT (&v)[8]) {
+  using V = typename Vec16<VT>::T;
+  constexpr int W = Vec16<VT>::W;
+  V *pv = reinterpret_cast<V *>(p);
+#pragma unroll
+  for (int u = 0; u < 8 / W; ++u) {
+    V t;
+#pragma unroll
+    for (int k = 0; k < W; ++k) vset(t, k, v[u * W + k]);
+    pv[u] = t;
+  }
+}
+
+// z = M^{-1} r for the 8-row group starting at row i0 (rows >= n hold r = 0).
+template <typename VT, int BS>
+__device__ __forceinline__ void apply_minv(const VT *__restrict__ minv, int64_t i0, int32_t n, const VT (&r)[8],
+                                           VT (&z)[8]) {
+  if constexpr (BS == 1) {
+    if (i0 + 8 <= n) {
+      VT d[8];
+      ld8(minv + i0, d);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) z[k] = d[k] * r[k];
+    } else {
+#pragma unroll
+      for (int k = 0; k < 8; ++k) z[k] = i0 + k < n ? minv[i0 + k] * r[k] : VT(0);
+    }
+  } else {
+    const int64_t nb = ((int64_t)n + BS - 1) / BS;
+#pragma unroll
+    for (int b = 0; b < 8 / BS; ++b) {
+      const int64_t blk = i0 / BS + b;
+      if (blk >= nb) {
+#pragma unroll
+        for (int i = 0; i < BS; ++i) z[b * BS + i] = VT(0);
+        continue;
+      }
+      const VT *Mb = minv + blk * BS * BS;
+#pragma unroll
+      for (int i = 0; i < BS; ++i) {
+        VT row[8];
+        if constexpr (BS == 8) {
+          ld8(Mb + i * BS, row);
+        } else {
+          using V = typename Vec16<VT>::T;
+          constexpr int W = Vec16<VT>::W;
+#pragma unroll
+          for (int u = 0; u < BS / W; ++u) {
+            const V t = reinterpret_cast<const V *>(Mb + i * BS)[u];
+#pragma unroll
+            for (int k = 0; k < W; ++k) row[u * W + k] = vget(t, k);
+          }
+        }
+        VT acc = VT(0);
+#pragma unroll
+        for (int j = 0; j < BS; ++j) acc = fma(row[j], r[b * BS + j], acc);
+        z[b * BS + i] = acc;
+      }
+    }
+  }
+}
+
+// UPDATE: alpha = rz / p.q; x += alpha p; r -= alpha q; then z = M^{-1} r,
+// partials of r.r and r.z.  !UPDATE: z = M^{-1} r and r.z partials only
+// (after the residual was replaced).
+template <typename VT, int BS, bool UPDATE>
+__global__ void __launch_bounds__(kCgThreads) cg_update_prec_kernel(int32_t n, const double *__restrict__ pq_part,
+                                                                    int npart, const double *__restrict__ rz_slot,
+                                                                    VT *__restrict__ x, VT *__restrict__ r,
+                                                                    VT *__restrict__ z, const VT *__restrict__ p,
+                                                                    const VT *__restrict__ q,
+                                                                    const VT *__restrict__ minv,
+                                                                    double *__restrict__ rr_part,
+                                                                    double *__restrict__ rz_part) {
+  __shared__ double smem[kCgThreads / 32];
+  VT a = VT(0);
+  if constexpr (UPDATE) {
+    const double pq = reduce_partials(pq_part, npart, smem);
+    const double rz = *rz_slot;
+    const double alpha = (pq != 0.0 && rz != 0.0 && isfinite(pq)) ? rz / pq : 0.0;
+    a = (VT)alpha;
+  }
+  double srr = 0.0, srz = 0.0;
+  const int64_t ng = ((int64_t)n + 7) / 8;
+  const int64_t stride = (int64_t)gridDim.x * kCgThreads;
+  for (int64_t g = (int64_t)blockIdx.x * kCgThreads + threadIdx.x; g < ng; g += stride) {
+    const int64_t i0 = g * 8;
+    const bool full = i0 + 8 <= n;
+    VT R[8], Z[8];
+    if (full) {
+      ld8(r + i0, R);
+    } else {
+#pragma unroll
+      for (int k = 0; k < 8; ++k) R[k] = i0 + k < n ? r[i0 + k] : VT(0);
+    }
+    if constexpr (UPDATE) {
+      VT P[8], Q[8], X[8];
+      if (full) {
+        ld8(p + i0, P);
+        ld8(q + i0, Q);
+        ld8(x + i0, X);
+      } else {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const bool in = i0 + k < n;
+          P[k] = in ? p[i0 + k] : VT(0);
+          Q[k] = in ? q[i0 + k] : VT(0);
+          X[k] = in ? x[i0 + k] : VT(0);
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        X[k] = fma(a, P[k], X[k]);
+        R[k] = fma(-a, Q[k], R[k]);
+        srr += (double)R[k] * (double)R[k];
+      }
+      if (full) {
+        st8(x + i0, X);
+        st8(r + i0, R);
+      } else {
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+          if (i0 + k < n) {
+            x[i0 + k] = X[k];
+            r[i0 + k] = R[k];
+          }
+      }
+    }
+    apply_minv<VT, BS>(minv, i0, n, R, Z);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) srz += (double)R[k] * (double)Z[k];
+    if (full) {
+      st8(z + i0, Z);
+    } else {
+#pragma unroll
+      for (int k = 0; k < 8; ++k)
+        if (i0 + k < n) z[i0 + k] = Z[k];
+    }
+  }
+  if constexpr (UPDATE) {
+    const double t = block_sum(srr, smem);
+    if (threadIdx.x == 0) rr_part[blockIdx.x] = t;
+  }
+  const double t2 = block_sum(srz, smem);
+  if (threadIdx.x == 0) rz_part[blockIdx.x] = t2;
+}
+
+// M^{-1} from the CSR matrix: thread per block of BS rows; the block's
+// entries (columns in the block's own range, found by binary search in the
+// sorted row, duplicates summed) inverted by Gauss-Jordan elimination with
+// partial pivoting in FP64.  A zero or non-finite pivot sets *bad.
+template <typename VT, int BS>
+__global__ void cg_minv_kernel(int32_t n, const int32_t *__restrict__ rowPtr, const int32_t *__restrict__ colIdx,
+                               const double *__restrict__ val, VT *__restrict__ minv, int32_t *__restrict__ bad) {
+  const int64_t nb = ((int64_t)n + BS - 1) / BS;
+  for (int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += (int64_t)gridDim.x * blockDim.x) {
+    double M[BS][BS], I[BS][BS];
+    const int64_t lo = b * BS;
+    for (int i = 0; i < BS; ++i)
+      for (int j = 0; j < BS; ++j) {
+        M[i][j] = 0.0;
+        I[i][j] = i == j ? 1.0 : 0.0;
+      }
+    for (int i = 0; i < BS; ++i) {
+      const int64_t row = lo + i;
+      if (row >= n) {
+        M[i][i] = 1.0;  // padding of the last block
+        continue;
+      }
+      int32_t s = rowPtr[row], e = rowPtr[row + 1];
+      while (s < e) {  // first column >= lo
+        const int32_t m = s + ((e - s) >> 1);
+        if (colIdx[m] < lo)
+          s = m + 1;
+        else
+          e = m;
+      }
+      for (int32_t j = s; j < rowPtr[row + 1] && colIdx[j] < lo + BS; ++j) M[i][colIdx[j] - lo] += val[j];
+    }
+    bool ok = true;
+    for (int c = 0; c < BS && ok; ++c) {
+      int piv = c;
+      for (int i = c + 1; i < BS; ++i)
+        if (fabs(M[i][c]) > fabs(M[piv][c])) piv = i;
+      if (!(fabs(M[piv][c]) > 0.0) || !isfinite(M[piv][c])) {
+        ok = false;
+        break;
+      }
+      if (piv != c)
+        for (int j = 0; j < BS; ++j) {
+          double t = M[c][j];
+          M[c][j] = M[piv][j];
+          M[piv][j] = t;
+          t = I[c][j];
+          I[c][j] = I[piv][j];
+          I[piv][j] = t;
+        }
+      const double inv = 1.0 / M[c][c];
+      for (int j = 0; j < BS; ++j) {
+        M[c][j] *= inv;
+        I[c][j] *= inv;
+      }
+      for (int i = 0; i < BS; ++i)
+        if (i != c) {
+          const double f = M[i][c];
+          if (f != 0.0)
+            for (int j = 0; j < BS; ++j) {
+              M[i][j] -= f * M[c][j];
+              I[i][j] -= f * I[c][j];
+            }
+        }
+    }
+    if (!ok) atomicExch(bad, 1);
+    for (int i = 0; i < BS; ++i)
+      for (int j = 0; j < BS; ++j) minv[b * BS * BS + i * BS + j] = (VT)(ok ? I[i][j] : (i == j ? 1.0 : 0.0));
+  }
+}
+
 // FP64 true residual r = b - A x, partials of ||r||^2; optionally also the
-// inner-precision copy r_lp = (VT) r and its partials (reliable update).
+// inner-precision copy r_lp = (VT) r and its partials (reliable update), and
+// the partials of ||r - r_lp_old||^2, the distance of the true residual from
+// the iterated one it replaces (part_dev, may be null).
 template <typename VT>
 __global__ void __launch_bounds__(kCgThreads) cg_residual_kernel(int32_t n, const int32_t *__restrict__ rowPtr,
                                                                  const int32_t *__restrict__ colIdx,
@@ -291,9 +538,10 @@ __global__ void __launch_bounds__(kCgThreads) cg_residual_kernel(int32_t n, cons
                                                                  const double *__restrict__ x,
                                                                  double *__restrict__ r, VT *__restrict__ r_lp,
                                                                  double *__restrict__ part,
-                                                                 double *__restrict__ part_lp) {
+                                                                 double *__restrict__ part_lp,
+                                                                 double *__restrict__ part_dev = nullptr) {
   __shared__ double smem[kCgThreads / 32];
-  double nrm = 0.0, nrm_lp = 0.0;
+  double nrm = 0.0, nrm_lp = 0.0, dev = 0.0;
   const int64_t stride = (int64_t)gridDim.x * kCgThreads;
   for (int64_t i = (int64_t)blockIdx.x * kCgThreads + threadIdx.x; i < n; i += stride) {
     const int32_t s = rowPtr[i], e = rowPtr[i + 1];
@@ -313,6 +561,10 @@ __global__ void __launch_bounds__(kCgThreads) cg_residual_kernel(int32_t n, cons
     if (r) r[i] = ri;
     nrm += ri * ri;
     if (r_lp) {
+      if (part_dev) {
+        const double d = ri - (double)r_lp[i];
+        dev += d * d;
+      }
       const VT v = (VT)ri;
       r_lp[i] = v;
       nrm_lp += (double)v * (double)v;
@@ -324,6 +576,10 @@ __global__ void __launch_bounds__(kCgThreads) cg_residual_kernel(int32_t n, cons
     t = block_sum(nrm_lp, smem);
     if (threadIdx.x == 0) part_lp[blockIdx.x] = t;
   }
+  if (part_dev) {
+    t = block_sum(dev, smem);
+    if (threadIdx.x == 0) part_dev[blockIdx.x] = t;
+  }
 }
 
 // x64 += x_lp; x_lp = 0 (reliable update of the solution).
@@ -332,6 +588,112 @@ __global__ void cg_fold_kernel(int32_t n, VT *__restrict__ x_lp, double *__restr
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     x[i] += (double)x_lp[i];
     x_lp[i] = VT(0);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Flexible outer iteration for the mixed modes (FCG(1), one previous
+// direction): the inner low-precision (P)CG, run until its residual has
+// dropped by reliable_delta, is the preconditioner z = B(r) of an FP64 CG on
+// the FP64 matrix.  Because B changes from step to step (and the inner matrix
+// is only an approximation of A), the new direction is A-orthogonalised
+// against the previous one explicitly: p = z - (z.q_prev / p_prev.q_prev) p_prev,
+// q = A p, alpha = p.r / p.q.  Unlike residual replacement, the outer Krylov
+// step keeps converging when the low-precision matrix is far from A.
+//
+// F1: z = (double) x_lp; x_lp = 0; partials of z.q_prev.
+__global__ void __launch_bounds__(kCgThreads) fcg_z_kernel(int32_t n, float *__restrict__ x_lp,
+                                                           double *__restrict__ z, const double *__restrict__ q_prev,
+                                                           double *__restrict__ part) {
+  __shared__ double smem[kCgThreads / 32];
+  double s = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * kCgThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kCgThreads) {
+    const double zi = (double)x_lp[i];
+    x_lp[i] = 0.f;
+    z[i] = zi;
+    s += zi * q_prev[i];
+  }
+  const double t = block_sum(s, smem);
+  if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+
+// F2: p = z - gamma p_prev, gamma = z.q_prev / pq_prev (0 on the first step).
+__global__ void __launch_bounds__(kCgThreads) fcg_dir_kernel(int32_t n, const double *__restrict__ part, int npart,
+                                                             const double *__restrict__ pq_prev_slot,
+                                                             const double *__restrict__ z, double *__restrict__ p) {
+  __shared__ double smem[kCgThreads / 32];
+  const double zq = reduce_partials(part, npart, smem);
+  const double pq_prev = *pq_prev_slot;
+  const double gamma = (pq_prev != 0.0 && isfinite(zq)) ? zq / pq_prev : 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * kCgThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kCgThreads)
+    p[i] = gamma != 0.0 ? fma(-gamma, p[i], z[i]) : z[i];
+}
+
+// F3: q = A p (FP64 CSR); partials of p.q and p.r.
+__global__ void __launch_bounds__(kCgThreads) fcg_spmv_kernel(int32_t n, const int32_t *__restrict__ rowPtr,
+                                                              const int32_t *__restrict__ colIdx,
+                                                              const double *__restrict__ val,
+                                                              const double *__restrict__ p, double *__restrict__ q,
+                                                              const double *__restrict__ r,
+                                                              double *__restrict__ part_pq,
+                                                              double *__restrict__ part_pr) {
+  __shared__ double smem[kCgThreads / 32];
+  double spq = 0.0, spr = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * kCgThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kCgThreads) {
+    const int32_t s0 = rowPtr[i], e0 = rowPtr[i + 1];
+    int32_t c[kRowFirst];
+    double a[kRowFirst];
+#pragma unroll
+    for (int k = 0; k < kRowFirst; ++k) {
+      c[k] = s0 + k < e0 ? colIdx[s0 + k] : -1;
+      a[k] = s0 + k < e0 ? val[s0 + k] : 0.0;
+    }
+    double acc = 0.0;
+#pragma unroll
+    for (int k = 0; k < kRowFirst; ++k)
+      if (c[k] >= 0) acc = fma(a[k], __ldg(p + c[k]), acc);
+    for (int32_t j = s0 + kRowFirst; j < e0; ++j) acc = fma(val[j], __ldg(p + colIdx[j]), acc);
+    q[i] = acc;
+    spq += p[i] * acc;
+    spr += p[i] * r[i];
+  }
+  double t = block_sum(spq, smem);
+  if (threadIdx.x == 0) part_pq[blockIdx.x] = t;
+  t = block_sum(spr, smem);
+  if (threadIdx.x == 0) part_pr[blockIdx.x] = t;
+}
+
+// F4: alpha = p.r / p.q; x += alpha p; r -= alpha q; r_lp = (float) r;
+// partials of r.r and r_lp.r_lp; p.q kept in *pq_slot for the next F2.
+__global__ void __launch_bounds__(kCgThreads) fcg_update_kernel(int32_t n, const double *__restrict__ part_pq,
+                                                                const double *__restrict__ part_pr, int npart,
+                                                                double *__restrict__ pq_slot,
+                                                                double *__restrict__ x, double *__restrict__ r,
+                                                                const double *__restrict__ p,
+                                                                const double *__restrict__ q,
+                                                                float *__restrict__ r_lp,
+                                                                double *__restrict__ part_rr,
+                                                                double *__restrict__ part_rr_lp) {
+  __shared__ double smem[kCgThreads / 32];
+  const double pq = reduce_partials(part_pq, npart, smem);
+  const double pr = reduce_partials(part_pr, npart, smem);
+  const double alpha = (pq > 0.0 && isfinite(pq) && isfinite(pr)) ? pr / pq : 0.0;
+  double s = 0.0, sl = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * kCgThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kCgThreads) {
+    x[i] = fma(alpha, p[i], x[i]);
+    const double ri = fma(-alpha, q[i], r[i]);
+    r[i] = ri;
+    const float rl = (float)ri;
+    r_lp[i] = rl;
+    s += ri * ri;
+    sl += (double)rl * (double)rl;
+  }
+  double t = block_sum(s, smem);
+  if (threadIdx.x == 0) part_rr[blockIdx.x] = t;
+  t = block_sum(sl, smem);
+  if (threadIdx.x == 0) {
+    part_rr_lp[blockIdx.x] = t;
+    if (blockIdx.x == 0) *pq_slot = (pq > 0.0 && isfinite(pq)) ? pq : 0.0;
   }
 }
 
@@ -450,6 +812,15 @@ struct bsp_cg_plan_s {
   // iteration vectors: FP64 (mode FP64) or FP32 (mixed); p ping-pongs
   void *x = nullptr, *r = nullptr, *p[2] = {nullptr, nullptr}, *q = nullptr;
   double *part_pq = nullptr, *part_rr = nullptr, *part_res = nullptr;
+  // preconditioning: prec_bs = 0 (none), 1 (Jacobi), 4 or 8 (block-Jacobi)
+  int prec_bs = 0;
+  void *z = nullptr, *minv = nullptr;
+  double *part_rz = nullptr;
+  // flexible outer iteration (mixed modes): FP64 p, q, z; r64 holds the
+  // FP64 residual; partials of z.q_prev and p.r
+  double *p64 = nullptr, *q64 = nullptr, *z64 = nullptr;
+  double *part_zq = nullptr, *part_pr = nullptr;
+  int64_t bytes_outer = 0;
   double *sc = nullptr, *h_sc = nullptr;  // [0],[1] rr slots, [2] ||b-Ax||^2, [3] ||b||^2, [4] rr after a chunk
   int grid = 0;    // update, residual and reduction kernels (writers of the rr partials)
   int grid_a = 0;  // direction/SpMV kernel (writer of the p.q partials)
@@ -461,6 +832,20 @@ struct bsp_cg_plan_s {
 namespace bsp {
 
 constexpr int kCgMaxCtasPerSm = 2048 / kCgThreads;
+// Mixed modes: a replaced (true) residual whose distance from the iterated
+// one exceeds kCgDeviation x its norm, or an iterated residual above kCgGrowth
+// x the last true one, marks the low-precision matrix as too far from A for
+// residual replacement (AUTO then switches to the flexible outer iteration).
+// Measured: <= 0.006 where replacement keeps the FP64 iteration count, >= 0.13
+// where it costs 1.5x-30x more iterations.
+constexpr double kCgDeviation = 0.1;
+constexpr double kCgGrowth = 1e4;
+// Mixed modes: this many residual replacements in a row without a new lowest
+// true residual end the solve (BSP_ERR_NOT_CONVERGED).
+constexpr int kCgNoProgress = 6;
+// Mixed modes: this many chunks without the inner drop force a residual
+// replacement / outer step (an inner iteration that stagnates).
+constexpr int kCgInnerChunks = 32;
 
 // Resident CTAs per SM of the direction/SpMV kernel (a) and of the update
 // kernel (b).
@@ -509,10 +894,54 @@ static void launch_iter(bsp_cg_plan_s *P, int k, cudaStream_t s) {
   VT *r = (VT *)P->r, *x = (VT *)P->x, *q = (VT *)P->q;
   VT *pp = (VT *)P->p[k & 1], *pn = (VT *)P->p[(k + 1) & 1];
   const int g = P->grid, ga = P->grid_a;
-  cg_dir_spmv_kernel<V, VT, SC, D16><<<ga, kCgThreads, 0, s>>>(P->n, A, r, pp, pn, q, P->part_rr, g,
+  if (P->prec_bs == 0) {
+    cg_dir_spmv_kernel<V, VT, SC, D16><<<ga, kCgThreads, 0, s>>>(P->n, A, r, pp, pn, q, P->part_rr, g,
+                                                                  P->sc + ((k + 1) & 1), P->sc + (k & 1),
+                                                                  P->part_pq);
+    cg_update_kernel<VT><<<g, kCgThreads, 0, s>>>(P->n, P->part_pq, ga, P->sc + (k & 1), x, r, pn, q, P->part_rr);
+    return;
+  }
+  // preconditioned: directions from z, r.z in the scalar slots
+  VT *z = (VT *)P->z;
+  const VT *mi = (const VT *)P->minv;
+  cg_dir_spmv_kernel<V, VT, SC, D16><<<ga, kCgThreads, 0, s>>>(P->n, A, z, pp, pn, q, P->part_rz, g,
                                                                 P->sc + ((k + 1) & 1), P->sc + (k & 1),
                                                                 P->part_pq);
-  cg_update_kernel<VT><<<g, kCgThreads, 0, s>>>(P->n, P->part_pq, ga, P->sc + (k & 1), x, r, pn, q, P->part_rr);
+  const double *sl = P->sc + (k & 1);
+  switch (P->prec_bs) {
+    case 1:
+      cg_update_prec_kernel<VT, 1, true><<<g, kCgThreads, 0, s>>>(P->n, P->part_pq, ga, sl, x, r, z, pn, q, mi,
+                                                                   P->part_rr, P->part_rz);
+      break;
+    case 4:
+      cg_update_prec_kernel<VT, 4, true><<<g, kCgThreads, 0, s>>>(P->n, P->part_pq, ga, sl, x, r, z, pn, q, mi,
+                                                                   P->part_rr, P->part_rz);
+      break;
+    default:
+      cg_update_prec_kernel<VT, 8, true><<<g, kCgThreads, 0, s>>>(P->n, P->part_pq, ga, sl, x, r, z, pn, q, mi,
+                                                                   P->part_rr, P->part_rz);
+  }
+}
+
+// z = M^{-1} r and the r.z partials, after the residual was replaced.
+template <typename VT>
+static void launch_prec(bsp_cg_plan_s *P, cudaStream_t s) {
+  VT *r = (VT *)P->r, *z = (VT *)P->z;
+  const VT *mi = (const VT *)P->minv;
+  const int g = P->grid;
+  switch (P->prec_bs) {
+    case 1:
+      cg_update_prec_kernel<VT, 1, false><<<g, kCgThreads, 0, s>>>(P->n, nullptr, 0, nullptr, nullptr, r, z, nullptr,
+                                                                    nullptr, mi, nullptr, P->part_rz);
+      break;
+    case 4:
+      cg_update_prec_kernel<VT, 4, false><<<g, kCgThreads, 0, s>>>(P->n, nullptr, 0, nullptr, nullptr, r, z, nullptr,
+                                                                    nullptr, mi, nullptr, P->part_rz);
+      break;
+    default:
+      cg_update_prec_kernel<VT, 8, false><<<g, kCgThreads, 0, s>>>(P->n, nullptr, 0, nullptr, nullptr, r, z, nullptr,
+                                                                    nullptr, mi, nullptr, P->part_rz);
+  }
 }
 
 static bsp_status cg_iteration(bsp_cg_plan_s *P, int k, cudaStream_t s) {
@@ -570,11 +999,13 @@ static bsp_status read_scalars(bsp_cg_plan_s *P, cudaStream_t s) {
 
 // True FP64 residual of x64 -> sc[2]; the iterated residual (and its r.r
 // partials for the next iteration) is replaced by it.
-static bsp_status cg_true_residual(bsp_cg_plan_s *P, const double *b, cudaStream_t s) {
+// measure_dev (mixed modes): also ||r_true - r_iterated||^2 -> sc[7].
+static bsp_status cg_true_residual(bsp_cg_plan_s *P, const double *b, cudaStream_t s, bool measure_dev = false) {
   const int g = P->grid;
   if (cg_mixed(P))
-    cg_residual_kernel<float><<<g, kCgThreads, 0, s>>>(P->n, P->rowPtr, P->colIdx, P->val, b, P->x64, nullptr,
-                                                        (float *)P->r, P->part_res, P->part_rr);
+    cg_residual_kernel<float><<<g, kCgThreads, 0, s>>>(P->n, P->rowPtr, P->colIdx, P->val, b, P->x64, P->r64,
+                                                        (float *)P->r, P->part_res, P->part_rr,
+                                                        measure_dev ? P->part_zq : nullptr);
   else
     cg_residual_kernel<double><<<g, kCgThreads, 0, s>>>(P->n, P->rowPtr, P->colIdx, P->val, b, P->x64,
                                                          (double *)P->r, nullptr, P->part_res, nullptr);
@@ -584,6 +1015,76 @@ static bsp_status cg_true_residual(bsp_cg_plan_s *P, const double *b, cudaStream
   }
   sum_partials_kernel<<<1, kCgThreads, 0, s>>>(P->part_res, g, P->sc + 2);
   BSP_LAUNCH_CHECK();
+  if (measure_dev && cg_mixed(P)) {
+    sum_partials_kernel<<<1, kCgThreads, 0, s>>>(P->part_zq, g, P->sc + 7);
+    BSP_LAUNCH_CHECK();
+  }
+  if (P->prec_bs) {
+    if (cg_mixed(P))
+      launch_prec<float>(P, s);
+    else
+      launch_prec<double>(P, s);
+    BSP_LAUNCH_CHECK();
+  }
+  return BSP_OK;
+}
+
+// M^{-1} (Jacobi or block-Jacobi) of the CSR matrix in the iteration precision.
+template <typename VT>
+static bsp_status build_minv(bsp_cg_plan_s *P, cudaStream_t s) {
+  const int bs = P->prec_bs;
+  const int64_t nb = ((int64_t)P->n + bs - 1) / bs;
+  BSP_CUDA(cudaMallocAsync(&P->minv, sizeof(VT) * (size_t)(nb * bs * bs), s));
+  int32_t *bad = nullptr;
+  BSP_TRY(dalloc(&bad, 1, s));
+  BSP_CUDA(cudaMemsetAsync(bad, 0, sizeof(int32_t), s));
+  const unsigned gr = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div(nb, 128), (int64_t)sm_count() * 16));
+  VT *mi = (VT *)P->minv;
+  if (bs == 1)
+    cg_minv_kernel<VT, 1><<<gr, 128, 0, s>>>(P->n, P->rowPtr, P->colIdx, P->val, mi, bad);
+  else if (bs == 4)
+    cg_minv_kernel<VT, 4><<<gr, 128, 0, s>>>(P->n, P->rowPtr, P->colIdx, P->val, mi, bad);
+  else
+    cg_minv_kernel<VT, 8><<<gr, 128, 0, s>>>(P->n, P->rowPtr, P->colIdx, P->val, mi, bad);
+  BSP_LAUNCH_CHECK();
+  int32_t h_bad = 0;
+  const bsp_status st = read_i32(bad, &h_bad, s);
+  dfree(bad, s);
+  BSP_TRY(st);
+  if (h_bad)
+    BSP_FAIL(BSP_ERR_INVALID, bs == 1 ? "a diagonal entry is zero or not finite"
+                                      : "a diagonal block is singular or not finite");
+  return BSP_OK;
+}
+
+// Enters the flexible outer iteration from a folded state (x_lp = 0, r64 and
+// r_lp = b - A x64): no previous direction, inner direction restarted.
+static bsp_status fcg_begin(bsp_cg_plan_s *P, cudaStream_t s) {
+  BSP_CUDA(cudaMemsetAsync(P->p64, 0, sizeof(double) * P->n, s));
+  BSP_CUDA(cudaMemsetAsync(P->q64, 0, sizeof(double) * P->n, s));
+  BSP_CUDA(cudaMemsetAsync(P->sc, 0, 2 * sizeof(double), s));
+  BSP_CUDA(cudaMemsetAsync(P->sc + 5, 0, sizeof(double), s));
+  return BSP_OK;
+}
+
+// One outer step with z = the inner solution since the last step; then the
+// inner iteration restarts on the new residual.  ||r64||^2 -> sc[6].
+static bsp_status fcg_step(bsp_cg_plan_s *P, cudaStream_t s) {
+  const int g = P->grid;
+  fcg_z_kernel<<<g, kCgThreads, 0, s>>>(P->n, (float *)P->x, P->z64, P->q64, P->part_zq);
+  fcg_dir_kernel<<<g, kCgThreads, 0, s>>>(P->n, P->part_zq, g, P->sc + 5, P->z64, P->p64);
+  fcg_spmv_kernel<<<g, kCgThreads, 0, s>>>(P->n, P->rowPtr, P->colIdx, P->val, P->p64, P->q64, P->r64,
+                                           P->part_pq, P->part_pr);
+  fcg_update_kernel<<<g, kCgThreads, 0, s>>>(P->n, P->part_pq, P->part_pr, g, P->sc + 5, P->x64, P->r64, P->p64,
+                                             P->q64, (float *)P->r, P->part_res, P->part_rr);
+  BSP_LAUNCH_CHECK();
+  sum_partials_kernel<<<1, kCgThreads, 0, s>>>(P->part_res, g, P->sc + 6);
+  BSP_LAUNCH_CHECK();
+  BSP_CUDA(cudaMemsetAsync(P->sc, 0, 2 * sizeof(double), s));  // inner restart: beta = 0
+  if (P->prec_bs) {
+    launch_prec<float>(P, s);
+    BSP_LAUNCH_CHECK();
+  }
   return BSP_OK;
 }
 
@@ -600,6 +1101,9 @@ extern "C" bsp_status bsp_cg_default_options(bsp_cg_options *o) {
   o->check_every = 16;
   o->reliable_delta = 0.1;
   o->use_graphs = 1;
+  o->precond = BSP_CG_PRECOND_NONE;
+  o->precond_block = 4;
+  o->refine = BSP_CG_REFINE_AUTO;
   return BSP_OK;
 }
 
@@ -612,8 +1116,14 @@ extern "C" bsp_status bsp_cg_destroy(bsp_cg_plan P) {
   if (P->x == P->x64) P->x = nullptr;  // FP64 mode iterates on x64 itself
   dfree(P->x64, s);
   dfree(P->r64, s);
-  for (void *v : {P->x, P->r, P->p[0], P->p[1], P->q, P->lp_val})
+  for (void *v : {P->x, P->r, P->p[0], P->p[1], P->q, P->lp_val, P->z, P->minv})
     if (v) cudaFreeAsync(v, s);
+  dfree(P->part_rz, s);
+  dfree(P->p64, s);
+  dfree(P->q64, s);
+  dfree(P->z64, s);
+  dfree(P->part_zq, s);
+  dfree(P->part_pr, s);
   if (P->lp_cols) cudaFreeAsync(P->lp_cols, s);
   dfree(P->exps, s);
   dfree(P->slice_len, s);
@@ -637,6 +1147,11 @@ extern "C" bsp_status bsp_cg_create(int32_t n, int32_t nnz, const int32_t *rowPt
   BSP_CHECK_ARG(opt->mode >= BSP_CG_FP64 && opt->mode <= BSP_CG_MIXED_BF16, "unknown mode");
   BSP_CHECK_ARG(opt->tol > 0 && opt->check_every >= 1 && opt->max_iters >= 1, "bad options");
   BSP_CHECK_ARG(opt->reliable_delta > 0 && opt->reliable_delta < 1, "reliable_delta must be in (0, 1)");
+  BSP_CHECK_ARG(opt->precond >= BSP_CG_PRECOND_NONE && opt->precond <= BSP_CG_PRECOND_BLOCK_JACOBI,
+                "unknown preconditioner");
+  BSP_CHECK_ARG(opt->precond != BSP_CG_PRECOND_BLOCK_JACOBI || opt->precond_block == 4 || opt->precond_block == 8,
+                "precond_block must be 4 or 8");
+  BSP_CHECK_ARG(opt->refine >= BSP_CG_REFINE_AUTO && opt->refine <= BSP_CG_REFINE_FLEXIBLE, "unknown refine");
   cudaStream_t s = as_stream(stream);
   bsp_cg_plan_s *P = new bsp_cg_plan_s();
   P->n = n;
@@ -676,6 +1191,21 @@ extern "C" bsp_status bsp_cg_create(int32_t n, int32_t nnz, const int32_t *rowPt
     P->x = nullptr;  // x32 allocated below
   }
   for (void **v : {&P->x, &P->r, &P->p[0], &P->p[1], &P->q}) BSP_CG_CUDA(cudaMallocAsync(v, vt * (size_t)n, s));
+  P->prec_bs = opt->precond == BSP_CG_PRECOND_JACOBI ? 1
+               : opt->precond == BSP_CG_PRECOND_BLOCK_JACOBI ? opt->precond_block : 0;
+  if (mixed) {
+    BSP_CG_TRY(dalloc(&P->r64, (size_t)n, s));
+    BSP_CG_TRY(dalloc(&P->p64, (size_t)n, s));
+    BSP_CG_TRY(dalloc(&P->q64, (size_t)n, s));
+    BSP_CG_TRY(dalloc(&P->z64, (size_t)n, s));
+    BSP_CG_TRY(dalloc(&P->part_zq, (size_t)P->grid, s));
+    BSP_CG_TRY(dalloc(&P->part_pr, (size_t)P->grid, s));
+  }
+  if (P->prec_bs) {
+    BSP_CG_CUDA(cudaMallocAsync(&P->z, vt * (size_t)n, s));
+    BSP_CG_TRY(dalloc(&P->part_rz, (size_t)P->grid, s));
+    BSP_CG_TRY(mixed ? build_minv<float>(P, s) : build_minv<double>(P, s));
+  }
   if (!mixed) {  // FP64 mode iterates directly on x64
     cudaFreeAsync(P->x, s);
     P->x = P->x64;
@@ -753,8 +1283,13 @@ extern "C" bsp_status bsp_cg_create(int32_t n, int32_t nnz, const int32_t *rowPt
   // algorithmic bytes: kernel A reads the matrix, r and p_prev (own rows;
   // gathers counted once) and writes p and q; kernel B reads p, q, x, r and
   // writes x, r.
+  // Preconditioned: the update kernel also reads M^{-1} and writes z.
   P->bytes_iter = mat_bytes + (mixed ? 0 : 4 * ((int64_t)n + 1)) + 10 * (int64_t)vt * n;
+  if (P->prec_bs)
+    P->bytes_iter += (int64_t)vt * (ceil_div(n, P->prec_bs) * P->prec_bs * P->prec_bs + (int64_t)n);
   P->bytes_residual = (int64_t)nnz * 12 + 4 * ((int64_t)n + 1) + 3 * 8 * (int64_t)n;
+  // flexible outer step: F1 8n+8n+8n, F2 24n, F3 matrix + 4(n+1) + 32n, F4 52n
+  P->bytes_outer = (int64_t)nnz * 12 + 4 * ((int64_t)n + 1) + 132 * (int64_t)n;
   if (cudaStreamSynchronize(s) != cudaSuccess) {
     set_error("bsp_cg_create: preparing the matrix failed");
     return fail(BSP_ERR_CUDA);
@@ -794,30 +1329,87 @@ extern "C" bsp_status bsp_cg_solve(bsp_cg_plan P, const double *b, double *x, bs
   const double delta2 = P->opt.reliable_delta * P->opt.reliable_delta;
   double rmax2 = P->h_sc[2];
   int64_t residuals = 2, iters = 0;
-  int32_t updates = 0;
+  int32_t updates = 0, no_progress = 0;
+  double best_true = P->h_sc[2];
+  bool coarse = false;
   bool done = bb == 0.0 || P->h_sc[2] <= target;
+  bool flex = mixed && P->opt.refine == BSP_CG_REFINE_FLEXIBLE;
+  int32_t outer = 0;
+  if (flex) BSP_TRY(fcg_begin(P, s));
+  // replacements / outer steps that stop lowering the residual: the
+  // low-precision copy is too coarse for this matrix
+  auto progress = [&](double r2) {
+    if (r2 < best_true) {
+      best_true = r2;
+      no_progress = 0;
+    } else if (++no_progress >= kCgNoProgress) {
+      coarse = true;
+    }
+  };
+  int chunks = 0;  // since the last replacement / outer step
   while (!done && iters < P->opt.max_iters) {
     BSP_TRY(cg_run_chunk(P, s));
     iters += P->opt.check_every;
+    ++chunks;
     BSP_TRY(read_scalars(P, s));
     const double rr = P->h_sc[4];
     const bool stalled = !(rr == rr);  // NaN
-    if (rr <= target || (mixed && rr <= delta2 * rmax2) || stalled) {
-      // reliable update: fold the inner solution, replace the residual
-      if (mixed) {
-        cg_fold_kernel<float><<<g, kCgThreads, 0, s>>>(P->n, (float *)P->x, P->x64);
-        BSP_LAUNCH_CHECK();
-      }
-      BSP_TRY(cg_true_residual(P, b, s));
+    const bool growing = mixed && (rr > kCgGrowth * rmax2 || chunks >= kCgInnerChunks);
+    if (!(rr <= target || (mixed && rr <= delta2 * rmax2) || stalled || growing)) continue;
+    chunks = 0;
+    if (flex) {
+      if (stalled) break;
+      BSP_TRY(fcg_step(P, s));
       BSP_TRY(read_scalars(P, s));
-      ++residuals;
-      ++updates;
-      rmax2 = P->h_sc[2];
-      done = P->h_sc[2] <= target || stalled;
+      ++outer;
+      double r2 = P->h_sc[6];
+      if (r2 <= target) {  // confirm with the true residual (which also restarts the inner iteration)
+        BSP_TRY(cg_true_residual(P, b, s));
+        BSP_CUDA(cudaMemsetAsync(P->sc, 0, 2 * sizeof(double), s));
+        BSP_TRY(read_scalars(P, s));
+        ++residuals;
+        r2 = P->h_sc[2];
+      }
+      rmax2 = r2;
+      progress(r2);
+      done = r2 <= target || coarse;
+      continue;
     }
+    // reliable update: fold the inner solution, replace the residual
+    if (mixed) {
+      cg_fold_kernel<float><<<g, kCgThreads, 0, s>>>(P->n, (float *)P->x, P->x64);
+      BSP_LAUNCH_CHECK();
+    }
+    BSP_TRY(cg_true_residual(P, b, s, mixed));
+    BSP_TRY(read_scalars(P, s));
+    ++residuals;
+    ++updates;
+    // A true residual far (in direction, not only in norm) from the iterated
+    // one it replaces: the low-precision matrix is far from A (a large
+    // condition number times the storage rounding) and the kept direction no
+    // longer fits the replaced residual.  AUTO switches to the flexible outer
+    // iteration; RELIABLE restarts the direction (beta = 0, i.e. iterative
+    // refinement with CG as the inner solver).
+    if (mixed && (growing || P->h_sc[7] > kCgDeviation * kCgDeviation * rr)) {
+      if (P->opt.refine == BSP_CG_REFINE_AUTO) {
+        flex = true;
+        BSP_TRY(fcg_begin(P, s));
+      } else {
+        BSP_CUDA(cudaMemsetAsync(P->sc, 0, 2 * sizeof(double), s));
+      }
+    }
+    rmax2 = P->h_sc[2];
+    progress(P->h_sc[2]);
+    done = P->h_sc[2] <= target || stalled || coarse;
   }
-  if (!done && mixed) {  // iteration budget spent: fold what the inner solve has
-    cg_fold_kernel<float><<<g, kCgThreads, 0, s>>>(P->n, (float *)P->x, P->x64);
+  if (!done && mixed) {  // budget spent: apply what the inner solve has
+    if (flex) {
+      BSP_TRY(fcg_step(P, s));
+      ++outer;
+    } else {
+      cg_fold_kernel<float><<<g, kCgThreads, 0, s>>>(P->n, (float *)P->x, P->x64);
+      BSP_LAUNCH_CHECK();
+    }
     BSP_TRY(cg_true_residual(P, b, s));
     ++residuals;
   }
@@ -830,13 +1422,17 @@ extern "C" bsp_status bsp_cg_solve(bsp_cg_plan P, const double *b, double *x, bs
   cudaEventDestroy(e1);
   res->iterations = (int32_t)iters;
   res->reliable_updates = updates;
+  res->outer_steps = outer;
   res->seconds = ms * 1e-3;
   res->rel_residual = bb > 0 ? sqrt(P->h_sc[2] / bb) : 0.0;
   res->converged = res->rel_residual <= P->opt.tol;
-  res->bytes_moved = residuals * P->bytes_residual + iters * P->bytes_iter;
+  res->bytes_moved = residuals * P->bytes_residual + iters * P->bytes_iter + (int64_t)outer * P->bytes_outer;
   res->delta16 = P->delta16 ? 1 : 0;
   if (!res->converged) {
-    set_error("CG stopped at relative residual " + std::to_string(res->rel_residual));
+    set_error("CG stopped at relative residual " + std::to_string(res->rel_residual) +
+              (coarse ? ": the low-precision matrix is too coarse for this matrix's condition number "
+                        "(residual replacements stopped reducing the residual); use mode f32 or fp64"
+                      : ""));
     return BSP_ERR_NOT_CONVERGED;
   }
   return BSP_OK;

@@ -384,3 +384,118 @@ extern "C" bsp_status bsp_gen_banded(int32_t n, int32_t width, uint64_t seed, in
   }
   return BSP_OK;
 }
+
+// ---------------------------------------------------------------------------
+// SPD test matrices for preconditioned CG.
+namespace {
+
+// Coefficient of the face of node i towards direction d (0..5: -z,-y,-x,+x,+y,+z),
+// shared by the two nodes it joins: keyed by the lower node and the axis.
+inline double face_coef(uint64_t seed, double contrast, int64_t lower, int axis) {
+  return exp(contrast * (2.0 * u01(h3(seed, 40 + axis, (uint64_t)lower)) - 1.0));
+}
+
+// Row i of the weighted 7-point Laplacian on an m^3 grid with Dirichlet
+// boundary faces: neighbours in ascending order, diagonal = sum of the six
+// face coefficients.  put(col, value).
+template <typename Put>
+void laplace_row(int64_t i, int64_t m, uint64_t seed, double contrast, Put put) {
+  const int64_t m2 = m * m, x = i % m, y = (i / m) % m, z = i / m2;
+  // lower node and axis of each face: -z, -y, -x, +x, +y, +z
+  const int64_t lo[6] = {i - m2, i - m, i - 1, i, i, i};
+  const int ax[6] = {2, 1, 0, 0, 1, 2};
+  const bool in[6] = {z > 0, y > 0, x > 0, x < m - 1, y < m - 1, z < m - 1};
+  const int64_t nb[6] = {i - m2, i - m, i - 1, i + 1, i + m, i + m2};
+  double k[6], diag = 0.0;
+  for (int f = 0; f < 6; ++f) {
+    // boundary faces get their own draw (lower node = -1 - i keeps the keys distinct)
+    k[f] = in[f] ? face_coef(seed, contrast, lo[f], ax[f]) : face_coef(seed, contrast, -1 - i, 3 + f);
+    diag += k[f];
+  }
+  for (int f = 0; f < 3; ++f)
+    if (in[f]) put(nb[f], -k[f]);
+  put(i, diag);
+  for (int f = 3; f < 6; ++f)
+    if (in[f]) put(nb[f], -k[f]);
+}
+
+}  // namespace
+
+extern "C" bsp_status bsp_gen_diffusion3d(int32_t m, double contrast, uint64_t seed, int32_t *rows, int64_t *nnz,
+                                          int32_t *rowPtr, int32_t *colIdx, double *values) {
+  if (m <= 0 || !rows || !nnz || !(contrast >= 0.0)) return BSP_ERR_INVALID;
+  const int64_t n = (int64_t)m * m * m;
+  if (n > INT32_MAX) return BSP_ERR_INVALID;
+  std::vector<int32_t> cnt(n);
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < n; ++i) {
+    const int64_t x = i % m, y = (i / m) % m, z = i / ((int64_t)m * m);
+    cnt[i] = 1 + (x > 0) + (x < m - 1) + (y > 0) + (y < m - 1) + (z > 0) + (z < m - 1);
+  }
+  *rows = (int32_t)n;
+  *nnz = prefix(cnt, rowPtr);
+  if (!rowPtr) return BSP_OK;
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < n; ++i) {
+    int64_t k = rowPtr[i];
+    laplace_row(i, m, seed, contrast, [&](int64_t c, double v) {
+      colIdx[k] = (int32_t)c;
+      values[k] = v;
+      ++k;
+    });
+  }
+  return BSP_OK;
+}
+
+extern "C" bsp_status bsp_gen_block_laplace3d(int32_t m, int32_t dof, double cond, uint64_t seed, int32_t *rows,
+                                              int64_t *nnz, int32_t *rowPtr, int32_t *colIdx, double *values) {
+  if (m <= 0 || dof <= 0 || dof > 16 || !rows || !nnz || !(cond >= 1.0)) return BSP_ERR_INVALID;
+  const int64_t nodes = (int64_t)m * m * m, n = nodes * dof;
+  if (n > INT32_MAX) return BSP_ERR_INVALID;
+  // S = Q diag(lambda) Q^T: Q from Gram-Schmidt of a seeded normal matrix,
+  // lambda log-spaced in [1, cond]
+  std::vector<double> Q((size_t)dof * dof), S((size_t)dof * dof, 0.0);
+  for (int a = 0; a < dof * dof; ++a) Q[a] = normal(seed, 50, (uint64_t)a);
+  for (int c = 0; c < dof; ++c) {
+    for (int p = 0; p < c; ++p) {
+      double d = 0.0;
+      for (int r = 0; r < dof; ++r) d += Q[r * dof + c] * Q[r * dof + p];
+      for (int r = 0; r < dof; ++r) Q[r * dof + c] -= d * Q[r * dof + p];
+    }
+    double nrm = 0.0;
+    for (int r = 0; r < dof; ++r) nrm += Q[r * dof + c] * Q[r * dof + c];
+    nrm = sqrt(nrm);
+    for (int r = 0; r < dof; ++r) Q[r * dof + c] /= nrm;
+  }
+  for (int c = 0; c < dof; ++c) {
+    const double lam = dof > 1 ? pow(cond, (double)c / (dof - 1)) : 1.0;
+    for (int a = 0; a < dof; ++a)
+      for (int b = 0; b < dof; ++b) S[a * dof + b] += Q[a * dof + c] * lam * Q[b * dof + c];
+  }
+  for (int a = 0; a < dof; ++a)  // exactly symmetric
+    for (int b = 0; b < a; ++b) S[a * dof + b] = S[b * dof + a];
+  std::vector<int32_t> cnt(n);
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < nodes; ++i) {
+    const int64_t x = i % m, y = (i / m) % m, z = i / ((int64_t)m * m);
+    const int32_t deg = 1 + (x > 0) + (x < m - 1) + (y > 0) + (y < m - 1) + (z > 0) + (z < m - 1);
+    for (int a = 0; a < dof; ++a) cnt[i * dof + a] = deg * dof;
+  }
+  *rows = (int32_t)n;
+  *nnz = prefix(cnt, rowPtr);
+  if (!rowPtr) return BSP_OK;
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < nodes; ++i) {
+    for (int a = 0; a < dof; ++a) {
+      int64_t k = rowPtr[i * dof + a];
+      laplace_row(i, m, seed, 1.0, [&](int64_t c, double v) {
+        for (int b = 0; b < dof; ++b) {
+          colIdx[k] = (int32_t)(c * dof + b);
+          values[k] = v * S[a * dof + b];
+          ++k;
+        }
+      });
+    }
+  }
+  return BSP_OK;
+}

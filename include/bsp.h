@@ -433,6 +433,33 @@ typedef enum {
   BSP_CG_MIXED_BF16 = 3
 } bsp_cg_mode;
 
+/* Preconditioner (applied in the iteration precision): none; Jacobi (the
+ * inverse diagonal); block-Jacobi (the inverses of the diagonal blocks of
+ * precond_block consecutive rows, e.g. the dof blocks of a BSR matrix; the last
+ * block is padded with identity rows).  create fails with BSP_ERR_INVALID on a
+ * zero diagonal entry or a singular block. */
+/* How the mixed modes reach the FP64 tolerance.  RELIABLE: one CG on the
+ * low-precision matrix whose residual is replaced by the FP64 one (and the
+ * solution folded into x64) each time it has dropped by reliable_delta; the
+ * search direction is kept, so the count stays that of FP64 CG while the
+ * low-precision matrix is close to A.  FLEXIBLE: an FP64 flexible CG (one
+ * previous direction, FP64 matrix) whose preconditioner is the low-precision
+ * (P)CG run until its residual has dropped by reliable_delta; it keeps
+ * converging when the low-precision matrix is far from A (large condition
+ * number times storage rounding).  AUTO: RELIABLE, switching to FLEXIBLE when
+ * a replaced residual is far above the iterated one. */
+typedef enum {
+  BSP_CG_REFINE_AUTO = 0,
+  BSP_CG_REFINE_RELIABLE = 1,
+  BSP_CG_REFINE_FLEXIBLE = 2
+} bsp_cg_refine;
+
+typedef enum {
+  BSP_CG_PRECOND_NONE = 0,
+  BSP_CG_PRECOND_JACOBI = 1,
+  BSP_CG_PRECOND_BLOCK_JACOBI = 2
+} bsp_cg_precond;
+
 typedef struct {
   int32_t mode;          /* bsp_cg_mode */
   double tol;            /* relative residual target (1e-10) */
@@ -440,6 +467,9 @@ typedef struct {
   int32_t check_every;   /* iterations per CUDA graph between host checks (rounded up to even) */
   double reliable_delta; /* mixed modes: residual drop that triggers an FP64 update (0.1) */
   int32_t use_graphs;    /* 1: replay captured iteration chunks */
+  int32_t precond;       /* bsp_cg_precond */
+  int32_t precond_block; /* BLOCK_JACOBI: rows per diagonal block, 4 or 8 */
+  int32_t refine;        /* bsp_cg_refine (mixed modes) */
 } bsp_cg_options;
 
 typedef struct {
@@ -450,6 +480,8 @@ typedef struct {
   int32_t converged;
   int64_t bytes_moved;      /* algorithmic bytes of all kernels */
   int32_t delta16;          /* int16 column offsets were used */
+  int32_t outer_steps;      /* mixed modes: outer flexible steps taken (0 when
+                               residual replacement sufficed) */
 } bsp_cg_result;
 
 typedef struct bsp_cg_plan_s *bsp_cg_plan;
@@ -644,6 +676,20 @@ bsp_status bsp_gen_banded(int32_t n, int32_t width, uint64_t seed,
                           int32_t *colIdx, double *values);
 /* Uniform random x in [-1, 1]. */
 bsp_status bsp_gen_uniform(int64_t n, uint64_t seed, double *x);
+/* SPD 7-point diffusion on an m^3 grid: face coefficients exp(contrast * u),
+ * u ~ U[-1, 1] per face (Dirichlet boundary faces included on the diagonal);
+ * contrast > 0 makes Jacobi preconditioning pay. */
+bsp_status bsp_gen_diffusion3d(int32_t m, double contrast, uint64_t seed,
+                               int32_t *rows, int64_t *nnz, int32_t *rowPtr,
+                               int32_t *colIdx, double *values);
+/* SPD block Laplacian L (x) S: L the 7-point diffusion with contrast 1, S a
+ * seeded dof x dof SPD coupling with eigenvalues log-spaced in [1, cond];
+ * node-major rows (dof consecutive rows per node), so block-Jacobi with
+ * blocks of dof rows inverts S exactly. */
+bsp_status bsp_gen_block_laplace3d(int32_t m, int32_t dof, double cond,
+                                   uint64_t seed, int32_t *rows, int64_t *nnz,
+                                   int32_t *rowPtr, int32_t *colIdx,
+                                   double *values);
 
 /* ---------------------------------------------------------------------- */
 /* Matrix Market files.  Replaces the reference drivers' read_triplet_file +

@@ -241,6 +241,128 @@ double orc_bsr_stand(int32_t blc_row, const int32_t *blcPtr) {
 /* FP64 CG on the CPU with orc_spmv_f64_i32 as the operator (the reference has
  * no solver; this is the FP64 oracle the GPU solves are compared against).
  * Returns iterations; x holds the solution. */
+/* Inverse of the diagonal blocks of bs consecutive rows (bs = 1: the inverse
+ * diagonal), row-major bs*bs per block, the last block padded with identity
+ * rows; Gauss-Jordan elimination with partial pivoting.  Returns 0, or -1 on
+ * a zero pivot.  No reference counterpart (the reference has no solver);
+ * plain FP64 restatement of block-Jacobi preconditioning. */
+int32_t orc_block_jacobi(int32_t n, const int32_t *rowPtr, const int32_t *colIdx, const double *val, int32_t bs,
+                         double *minv) {
+  const int64_t nb = ((int64_t)n + bs - 1) / bs;
+  double *M = (double *)malloc(sizeof(double) * bs * bs * 2);
+  double *I = M + bs * bs;
+  int32_t rc = 0;
+  for (int64_t b = 0; b < nb && rc == 0; b++) {
+    const int64_t lo = b * bs;
+    for (int32_t i = 0; i < bs * bs; i++) {
+      M[i] = 0.0;
+      I[i] = (i / bs == i % bs) ? 1.0 : 0.0;
+    }
+    for (int32_t i = 0; i < bs; i++) {
+      if (lo + i >= n) {
+        M[i * bs + i] = 1.0;
+        continue;
+      }
+      for (int32_t j = rowPtr[lo + i]; j < rowPtr[lo + i + 1]; j++)
+        if (colIdx[j] >= lo && colIdx[j] < lo + bs) M[i * bs + (colIdx[j] - lo)] += val[j];
+    }
+    for (int32_t c = 0; c < bs; c++) {
+      int32_t piv = c;
+      for (int32_t i = c + 1; i < bs; i++)
+        if (fabs(M[i * bs + c]) > fabs(M[piv * bs + c])) piv = i;
+      if (!(fabs(M[piv * bs + c]) > 0.0)) {
+        rc = -1;
+        break;
+      }
+      for (int32_t j = 0; j < bs && piv != c; j++) {
+        double t = M[c * bs + j];
+        M[c * bs + j] = M[piv * bs + j];
+        M[piv * bs + j] = t;
+        t = I[c * bs + j];
+        I[c * bs + j] = I[piv * bs + j];
+        I[piv * bs + j] = t;
+      }
+      const double inv = 1.0 / M[c * bs + c];
+      for (int32_t j = 0; j < bs; j++) {
+        M[c * bs + j] *= inv;
+        I[c * bs + j] *= inv;
+      }
+      for (int32_t i = 0; i < bs; i++) {
+        const double f = M[i * bs + c];
+        if (i == c || f == 0.0) continue;
+        for (int32_t j = 0; j < bs; j++) {
+          M[i * bs + j] -= f * M[c * bs + j];
+          I[i * bs + j] -= f * I[c * bs + j];
+        }
+      }
+    }
+    for (int32_t i = 0; i < bs * bs; i++) minv[b * bs * bs + i] = I[i];
+  }
+  free(M);
+  return rc;
+}
+
+/* Preconditioned CG in FP64 (x0 given), M^{-1} = block-Jacobi with blocks of
+ * bs rows (bs = 1: Jacobi); stops at ||r|| <= tol ||b||.  Returns the
+ * iteration count, or -1 when a diagonal block is singular. */
+int32_t orc_pcg(int32_t n, const int32_t *rowPtr, const int32_t *colIdx, const double *val, const double *b,
+                double *x, double tol, int32_t max_iters, int32_t bs) {
+  const int64_t nb = ((int64_t)n + bs - 1) / bs;
+  double *minv = (double *)malloc(sizeof(double) * nb * bs * bs);
+  if (orc_block_jacobi(n, rowPtr, colIdx, val, bs, minv) != 0) {
+    free(minv);
+    return -1;
+  }
+  double *r = (double *)calloc((size_t)nb * bs, sizeof(double)), *z = (double *)calloc((size_t)nb * bs, sizeof(double));
+  double *p = (double *)malloc(sizeof(double) * n), *q = (double *)malloc(sizeof(double) * n);
+  orc_spmv_f64_i32(n, rowPtr, colIdx, val, x, q);
+  double bb = 0, rr = 0, rz = 0;
+  for (int32_t i = 0; i < n; i++) {
+    r[i] = b[i] - q[i];
+    bb += b[i] * b[i];
+    rr += r[i] * r[i];
+  }
+#define ORC_APPLY_MINV()                                                   \
+  do {                                                                     \
+    rz = 0;                                                                \
+    for (int64_t blk = 0; blk < nb; blk++)                                 \
+      for (int32_t i = 0; i < bs; i++) {                                   \
+        double acc = 0;                                                    \
+        for (int32_t j = 0; j < bs; j++)                                   \
+          acc += minv[blk * bs * bs + i * bs + j] * r[blk * bs + j];       \
+        z[blk * bs + i] = acc;                                             \
+      }                                                                    \
+    for (int32_t i = 0; i < n; i++) rz += r[i] * z[i];                     \
+  } while (0)
+  ORC_APPLY_MINV();
+  for (int32_t i = 0; i < n; i++) p[i] = z[i];
+  int32_t it = 0;
+  while (it < max_iters && rr > tol * tol * bb) {
+    orc_spmv_f64_i32(n, rowPtr, colIdx, val, p, q);
+    double pq = 0;
+    for (int32_t i = 0; i < n; i++) pq += p[i] * q[i];
+    const double a = rz / pq;
+    rr = 0;
+    for (int32_t i = 0; i < n; i++) {
+      x[i] += a * p[i];
+      r[i] -= a * q[i];
+      rr += r[i] * r[i];
+    }
+    const double rz_old = rz;
+    ORC_APPLY_MINV();
+    const double bt = rz / rz_old;
+    for (int32_t i = 0; i < n; i++) p[i] = z[i] + bt * p[i];
+    it++;
+  }
+#undef ORC_APPLY_MINV
+  free(minv);
+  free(r);
+  free(z);
+  free(p);
+  free(q);
+  return it;
+}
+
 int32_t orc_cg(int32_t n, const int32_t *rowPtr, const int32_t *colIdx, const double *val, const double *b,
                double *x, double tol, int32_t max_iters) {
   double *r = (double *)malloc(sizeof(double) * n), *p = (double *)malloc(sizeof(double) * n);

@@ -46,6 +46,10 @@ void orc_abs_rowsum(int32_t rows, const int32_t *rowPtr, const int32_t *colIdx, 
 
 /* FP64 CG with orc_spmv_f64_i32 (the CPU oracle of the GPU solves).  x holds
  * the initial guess on entry and the solution on exit; returns iterations. */
+int32_t orc_block_jacobi(int32_t n, const int32_t *rowPtr, const int32_t *colIdx, const double *val, int32_t bs,
+                         double *minv);
+int32_t orc_pcg(int32_t n, const int32_t *rowPtr, const int32_t *colIdx, const double *val, const double *b,
+                double *x, double tol, int32_t max_iters, int32_t bs);
 int32_t orc_cg(int32_t n, const int32_t *rowPtr, const int32_t *colIdx, const double *val, const double *b,
                double *x, double tol, int32_t max_iters);
 

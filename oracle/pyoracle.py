@@ -326,6 +326,31 @@ def cg(rowptr, colidx, val, b, tol=1e-10, max_iters=100000) -> tuple:
     return x, int(it)
 
 
+def pcg(rowptr, colidx, val, b, bs, tol=1e-10, max_iters=100000) -> tuple:
+    """FP64 block-Jacobi PCG on the CPU (bs = 1: Jacobi; x0 = 0); returns
+    (x, iterations)."""
+    L = orc()
+    L.orc_pcg.restype = _I32
+    L.orc_pcg.argtypes = [_I32, _P, _P, _P, _P, _P, C.c_double, _I32, _I32]
+    n = rowptr.size - 1
+    x = np.zeros(n)
+    it = L.orc_pcg(n, _p(rowptr), _p(colidx), _p(val), _p(np.ascontiguousarray(b, np.float64)), _p(x), tol,
+                   max_iters, bs)
+    return x, int(it)
+
+
+def block_jacobi(rowptr, colidx, val, bs) -> np.ndarray:
+    """Inverted diagonal blocks of bs rows, [nblocks, bs, bs] (None if singular)."""
+    L = orc()
+    L.orc_block_jacobi.restype = _I32
+    L.orc_block_jacobi.argtypes = [_I32, _P, _P, _P, _I32, _P]
+    n = rowptr.size - 1
+    nb = (n + bs - 1) // bs
+    out = np.zeros((nb, bs, bs))
+    rc = L.orc_block_jacobi(n, _p(rowptr), _p(colidx), _p(val), bs, _p(out))
+    return None if rc != 0 else out
+
+
 def rel_residual(rowptr, colidx, val, b, x) -> float:
     """||b - A x|| / ||b|| with the oracle SpMV."""
     r = b - spmv_f64(rowptr, colidx, val, np.ascontiguousarray(x, np.float64))
