@@ -548,6 +548,17 @@ def run_suite(args) -> None:
     del rp, ci, v64
 
     # --- 512 independent SpMVs (and 8-RHS SpMMs) in one persistent launch
+    run_batch(bsp, dev, pk, up)
+
+    # --- Matrix Market file -> CSR (stencil 32^3 x 4 dof written by the library)
+    run_mtx_read(bsp, dev)
+
+
+def run_batch(bsp, dev, pk, up) -> None:
+    """512 independent CSR matrices (half banded, half Zipf 2.2 rows), F64 and
+    F32, 1 and 8 right-hand sides: one persistent graph launch vs one launch
+    per matrix vs one cuSPARSE call per matrix."""
+    import torch
     mats = bsp.gen_batch(512, SEED + 6)
     nnz = sum(int(m.rowptr[-1]) for m in mats)
     rows = sum(m.rows for m in mats)
@@ -565,20 +576,22 @@ def run_suite(args) -> None:
             P = bsp.BatchPlan(d, nrhs=nrhs, tune=1)
             tb = _timed(P.run, 50)
             ts = _timed(P.run_separate, 5)
+            choice = {int(k): int(v) for k, v in zip(*np.unique(P.lanes(), return_counts=True))}
+            Pm = bsp.BatchPlan(d, nrhs=nrhs, tune=0)
+            tm = _timed(Pm.run, 50)
+            Pm.close()
             nb = nnz * (es + 4) + (rows + len(mats)) * 4 + 2 * rows * nrhs * es
             res[f"{dname}_rhs{nrhs}"] = {"batched_us": round(tb * 1e6, 1), "separate_us": round(ts * 1e6, 1),
                                          "speedup": round(ts / tb, 2), "gbs": round(nb / tb / 1e9, 1),
                                          "frac": round(nb / tb / 1e9 / pk, 4),
                                          "gflops": round(2 * nnz * nrhs / tb / 1e9, 1), "launches_batched": 1,
-                                         "launches_separate": len(mats)}
+                                         "launches_separate": len(mats), "model_plan_us": round(tm * 1e6, 1),
+                                         "lanes_chosen": choice}
             if nrhs == 1:
                 fns = [_cusparse_spmv(rp, ci, va, xx, m.rows, m.cols) for m, (rp, ci, va, xx, _) in zip(mats, d)]
                 res[f"{dname}_rhs1"]["cusparse_separate_us"] = round(_timed(lambda: [f() for f in fns], 5) * 1e6, 1)
             P.close()
     _emit("batch_512_banded_and_zipf2.2", matrices=len(mats), rows=rows, nnz=nnz, variants=res)
-
-    # --- Matrix Market file -> CSR (stencil 32^3 x 4 dof written by the library)
-    run_mtx_read(bsp, dev)
 
 
 def run_pcg(bsp, up) -> None:
