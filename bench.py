@@ -736,6 +736,26 @@ def run_profile(args) -> None:
         for _ in range(reps):
             M.spmm(B, path="tcgen05" if w == "smat_tc" else "mma_sync")
         M.check()
+    elif w == "csr":   # CSR FP64 vector kernel, 2-D Laplacian 512x512 (21 MB; ncu replays cold-cache)
+        A = bsp.gen_laplace2d(512, 512)
+        rp, ci, va, x = up(A.rowptr, A.colidx, A.values, bsp.gen_uniform(A.cols, SEED + 10))
+        y = torch.empty(A.rows, dtype=torch.float64, device=dev)
+        for _ in range(reps):
+            bsp.csr_spmv(rp, ci, va, x, y)
+    elif w == "pcg_bj":   # block-Jacobi PCG, block Laplacian 48^3 x 4 dof (145 MB of CSR), 32 iterations
+        A = bsp.gen_block_laplace3d(48, 4, 1e3, SEED + 30)
+        rp, ci, va, b = up(A.rowptr, A.colidx, A.values, bsp.gen_uniform(A.rows, SEED + 32))
+        S = bsp.CgSolver(rp, ci, va, mode="fp64", precond="block_jacobi", block=4, max_iters=32, check_every=16,
+                         use_graphs=False)
+        S.solve(b, raise_on_stall=False)
+    elif w == "spmm_grouped":   # power-law graph 2^20, FP16, N = 128, grouped CSR engine
+        A = bsp.gen_graph(1 << 20, 1.8, 32, SEED + 4)
+        rp, ci, v64 = up(A.rowptr, A.colidx, A.values)
+        v = v64.half()
+        B = (torch.rand(A.cols, 128, generator=torch.Generator().manual_seed(1)) * 2 - 1).half().to(dev)
+        C_out = torch.empty(A.rows, 128, dtype=torch.float32, device=dev)
+        for _ in range(reps):
+            bsp.spmm_csr(rp, ci, v, B, C_out)
     elif w == "batch":   # the 512-matrix batch, FP64, one RHS
         mats = bsp.gen_batch(512, SEED + 6)
         d = []
@@ -761,7 +781,8 @@ def main():
     ap.add_argument("--suite", action="store_true", help="one JSON line per further workload (1 GPU)")
     ap.add_argument("--grid", type=int, default=GRID, help="stencil grid edge (64 = the benchmark config; "
                     "smaller values only for profiling captures)")
-    ap.add_argument("--profile", choices=["dasp", "cg_fp64", "cg_f16", "spmm", "batch", "smat_tc", "smat_mma"],
+    ap.add_argument("--profile", choices=["dasp", "cg_fp64", "cg_f16", "spmm", "batch", "smat_tc", "smat_mma", "csr",
+                                          "pcg_bj", "spmm_grouped"],
                     help="a few calls of one workload's kernels (for ncu captures)")
     args = ap.parse_args()
     if args.profile:

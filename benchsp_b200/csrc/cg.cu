@@ -103,7 +103,10 @@ struct CgMat {
 // Kernel A: p_k = r + beta p_prev (own row stored, gathered columns formed on
 // the fly), q = A p_k, partials of p_k.q.  rr_part = partials of rr_k;
 // rr_prev_slot = rr_{k-1}; rr_slot receives rr_k (written by CTA 0).
-template <typename V, typename VT, bool SCALED, bool DELTA16>
+// LPR (FP64 CSR path only): lanes per row; rows longer than ~10 entries
+// get 2, 4 or 8 lanes that split the row's entries (4 loads in flight each)
+// and combine by shuffle, instead of one thread walking the row.
+template <typename V, typename VT, bool SCALED, bool DELTA16, int LPR = 1>
 __global__ void __launch_bounds__(kCgThreads) cg_dir_spmv_kernel(int32_t n, CgMat<V, VT, SCALED, DELTA16> A,
                                                                  const VT *__restrict__ r,
                                                                  const VT *__restrict__ p_prev,
@@ -169,6 +172,42 @@ __global__ void __launch_bounds__(kCgThreads) cg_dir_spmv_kernel(int32_t n, CgMa
       }
       acc *= row_scale;
       if (live) {
+        const VT pi = fma(bt, p_prev[i], r[i]);
+        p[i] = pi;
+        q[i] = acc;
+        dot += (double)acc * (double)pi;
+      }
+    }
+  } else if constexpr (LPR > 1) {
+    // warp-uniform loop: each pass covers 32 / LPR consecutive rows per warp
+    const int lane = threadIdx.x & 31, sub = lane & (LPR - 1);
+    const int64_t rstride = stride / LPR;
+    for (int64_t base = ((int64_t)blockIdx.x * kCgThreads + (threadIdx.x & ~31)) / LPR; base < n; base += rstride) {
+      const int64_t i = base + lane / LPR;
+      const bool live = i < n;
+      VT acc = VT(0);
+      if (live) {
+        const int32_t e = A.rowPtr[i + 1];
+        int32_t j = A.rowPtr[i] + sub;
+        for (; j + 3 * LPR < e; j += 4 * LPR) {
+          int64_t c[4];
+          VT a[4];
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            c[k] = A.col(i, j + k * LPR);
+            a[k] = A.value(j + k * LPR);
+          }
+#pragma unroll
+          for (int k = 0; k < 4; ++k) acc = fma(a[k], fma(bt, __ldg(p_prev + c[k]), __ldg(r + c[k])), acc);
+        }
+        for (; j < e; j += LPR) {
+          const int64_t cj = A.col(i, j);
+          acc = fma(A.value(j), fma(bt, __ldg(p_prev + cj), __ldg(r + cj)), acc);
+        }
+      }
+#pragma unroll
+      for (int o = LPR / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+      if (live && sub == 0) {
         const VT pi = fma(bt, p_prev[i], r[i]);
         p[i] = pi;
         q[i] = acc;
@@ -291,29 +330,33 @@ __global__ void __launch_bounds__(kCgThreads) cg_update_kernel(int32_t n, const 
 // M^{-1} to the new residual and writes both the r.r partials (convergence
 // checks) and the r.z partials (the next direction).
 //
-// One thread per group of 8 rows (BS divides 8, so blocks never straddle
-// groups): 16-byte vector accesses for full groups, bounds-checked scalars for
-// the last partial group.
-template <typename VT>
-__device__ __forceinline__ void ld8(const VT *__restrict__ p, VT (&v)[8]) {
+// One thread per group of G rows, G = 8 for 8x8 blocks and 4 otherwise (BS
+// divides G, so blocks never straddle groups; 4 rows keep the FP64 kernel
+// near 60 registers, 8 rows of five vectors needed 100 and halved the
+// resident warps): 16-byte vector accesses for full groups, bounds-checked
+// scalars for the last partial group.
+template <int BS> struct PrecGroup { static constexpr int G = BS == 8 ? 8 : 4; };
+
+template <typename VT, int G>
+__device__ __forceinline__ void ldg_rows(const VT *__restrict__ p, VT (&v)[G]) {
   using V = typename Vec16<VT>::T;
   constexpr int W = Vec16<VT>::W;
   const V *pv = reinterpret_cast<const V *>(p);
 #pragma unroll
-  for (int u = 0; u < 8 / W; ++u) {
+  for (int u = 0; u < G / W; ++u) {
     const V t = pv[u];
 #pragma unroll
     for (int k = 0; k < W; ++k) v[u * W + k] = vget(t, k);
   }
 }
 
-template <typename VT>
-__device__ __forceinline__ void st8(VT *__restrict__ p, const VT (&v)[8]) {
+template <typename VT, int G>
+__device__ __forceinline__ void stg_rows(VT *__restrict__ p, const VT (&v)[G]) {
   using V = typename Vec16<VT>::T;
   constexpr int W = Vec16<VT>::W;
   V *pv = reinterpret_cast<V *>(p);
 #pragma unroll
-  for (int u = 0; u < 8 / W; ++u) {
+  for (int u = 0; u < G / W; ++u) {
     V t;
 #pragma unroll
     for (int k = 0; k < W; ++k) vset(t, k, v[u * W + k]);
@@ -321,24 +364,24 @@ __device__ __forceinline__ void st8(VT *__restrict__ p, const VT (&v)[8]) {
   }
 }
 
-// z = M^{-1} r for the 8-row group starting at row i0 (rows >= n hold r = 0).
-template <typename VT, int BS>
-__device__ __forceinline__ void apply_minv(const VT *__restrict__ minv, int64_t i0, int32_t n, const VT (&r)[8],
-                                           VT (&z)[8]) {
+// z = M^{-1} r for the G-row group starting at row i0 (rows >= n hold r = 0).
+template <typename VT, int BS, int G>
+__device__ __forceinline__ void apply_minv(const VT *__restrict__ minv, int64_t i0, int32_t n, const VT (&r)[G],
+                                           VT (&z)[G]) {
   if constexpr (BS == 1) {
-    if (i0 + 8 <= n) {
-      VT d[8];
-      ld8(minv + i0, d);
+    if (i0 + G <= n) {
+      VT d[G];
+      ldg_rows<VT, G>(minv + i0, d);
 #pragma unroll
-      for (int k = 0; k < 8; ++k) z[k] = d[k] * r[k];
+      for (int k = 0; k < G; ++k) z[k] = d[k] * r[k];
     } else {
 #pragma unroll
-      for (int k = 0; k < 8; ++k) z[k] = i0 + k < n ? minv[i0 + k] * r[k] : VT(0);
+      for (int k = 0; k < G; ++k) z[k] = i0 + k < n ? minv[i0 + k] * r[k] : VT(0);
     }
   } else {
     const int64_t nb = ((int64_t)n + BS - 1) / BS;
 #pragma unroll
-    for (int b = 0; b < 8 / BS; ++b) {
+    for (int b = 0; b < G / BS; ++b) {
       const int64_t blk = i0 / BS + b;
       if (blk >= nb) {
 #pragma unroll
@@ -348,19 +391,8 @@ __device__ __forceinline__ void apply_minv(const VT *__restrict__ minv, int64_t 
       const VT *Mb = minv + blk * BS * BS;
 #pragma unroll
       for (int i = 0; i < BS; ++i) {
-        VT row[8];
-        if constexpr (BS == 8) {
-          ld8(Mb + i * BS, row);
-        } else {
-          using V = typename Vec16<VT>::T;
-          constexpr int W = Vec16<VT>::W;
-#pragma unroll
-          for (int u = 0; u < BS / W; ++u) {
-            const V t = reinterpret_cast<const V *>(Mb + i * BS)[u];
-#pragma unroll
-            for (int k = 0; k < W; ++k) row[u * W + k] = vget(t, k);
-          }
-        }
+        VT row[BS];
+        ldg_rows<VT, BS>(Mb + i * BS, row);
         VT acc = VT(0);
 #pragma unroll
         for (int j = 0; j < BS; ++j) acc = fma(row[j], r[b * BS + j], acc);
@@ -374,7 +406,7 @@ __device__ __forceinline__ void apply_minv(const VT *__restrict__ minv, int64_t 
 // partials of r.r and r.z.  !UPDATE: z = M^{-1} r and r.z partials only
 // (after the residual was replaced).
 template <typename VT, int BS, bool UPDATE>
-__global__ void __launch_bounds__(kCgThreads) cg_update_prec_kernel(int32_t n, const double *__restrict__ pq_part,
+__global__ void __launch_bounds__(kCgThreads, 4) cg_update_prec_kernel(int32_t n, const double *__restrict__ pq_part,
                                                                     int npart, const double *__restrict__ rz_slot,
                                                                     VT *__restrict__ x, VT *__restrict__ r,
                                                                     VT *__restrict__ z, const VT *__restrict__ p,
@@ -390,28 +422,29 @@ __global__ void __launch_bounds__(kCgThreads) cg_update_prec_kernel(int32_t n, c
     const double alpha = (pq != 0.0 && rz != 0.0 && isfinite(pq)) ? rz / pq : 0.0;
     a = (VT)alpha;
   }
+  constexpr int G = PrecGroup<BS>::G;
   double srr = 0.0, srz = 0.0;
-  const int64_t ng = ((int64_t)n + 7) / 8;
+  const int64_t ng = ((int64_t)n + G - 1) / G;
   const int64_t stride = (int64_t)gridDim.x * kCgThreads;
   for (int64_t g = (int64_t)blockIdx.x * kCgThreads + threadIdx.x; g < ng; g += stride) {
-    const int64_t i0 = g * 8;
-    const bool full = i0 + 8 <= n;
-    VT R[8], Z[8];
+    const int64_t i0 = g * G;
+    const bool full = i0 + G <= n;
+    VT R[G], Z[G];
     if (full) {
-      ld8(r + i0, R);
+      ldg_rows<VT, G>(r + i0, R);
     } else {
 #pragma unroll
-      for (int k = 0; k < 8; ++k) R[k] = i0 + k < n ? r[i0 + k] : VT(0);
+      for (int k = 0; k < G; ++k) R[k] = i0 + k < n ? r[i0 + k] : VT(0);
     }
     if constexpr (UPDATE) {
-      VT P[8], Q[8], X[8];
+      VT P[G], Q[G], X[G];
       if (full) {
-        ld8(p + i0, P);
-        ld8(q + i0, Q);
-        ld8(x + i0, X);
+        ldg_rows<VT, G>(p + i0, P);
+        ldg_rows<VT, G>(q + i0, Q);
+        ldg_rows<VT, G>(x + i0, X);
       } else {
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
+        for (int k = 0; k < G; ++k) {
           const bool in = i0 + k < n;
           P[k] = in ? p[i0 + k] : VT(0);
           Q[k] = in ? q[i0 + k] : VT(0);
@@ -419,31 +452,31 @@ __global__ void __launch_bounds__(kCgThreads) cg_update_prec_kernel(int32_t n, c
         }
       }
 #pragma unroll
-      for (int k = 0; k < 8; ++k) {
+      for (int k = 0; k < G; ++k) {
         X[k] = fma(a, P[k], X[k]);
         R[k] = fma(-a, Q[k], R[k]);
         srr += (double)R[k] * (double)R[k];
       }
       if (full) {
-        st8(x + i0, X);
-        st8(r + i0, R);
+        stg_rows<VT, G>(x + i0, X);
+        stg_rows<VT, G>(r + i0, R);
       } else {
 #pragma unroll
-        for (int k = 0; k < 8; ++k)
+        for (int k = 0; k < G; ++k)
           if (i0 + k < n) {
             x[i0 + k] = X[k];
             r[i0 + k] = R[k];
           }
       }
     }
-    apply_minv<VT, BS>(minv, i0, n, R, Z);
+    apply_minv<VT, BS, G>(minv, i0, n, R, Z);
 #pragma unroll
-    for (int k = 0; k < 8; ++k) srz += (double)R[k] * (double)Z[k];
+    for (int k = 0; k < G; ++k) srz += (double)R[k] * (double)Z[k];
     if (full) {
-      st8(z + i0, Z);
+      stg_rows<VT, G>(z + i0, Z);
     } else {
 #pragma unroll
-      for (int k = 0; k < 8; ++k)
+      for (int k = 0; k < G; ++k)
         if (i0 + k < n) z[i0 + k] = Z[k];
     }
   }
@@ -814,6 +847,7 @@ struct bsp_cg_plan_s {
   double *part_pq = nullptr, *part_rr = nullptr, *part_res = nullptr;
   // preconditioning: prec_bs = 0 (none), 1 (Jacobi), 4 or 8 (block-Jacobi)
   int prec_bs = 0;
+  int lpr = 1;  // FP64 mode: lanes per row of the direction/SpMV kernel
   void *z = nullptr, *minv = nullptr;
   double *part_rz = nullptr;
   // flexible outer iteration (mixed modes): FP64 p, q, z; r64 holds the
@@ -886,7 +920,7 @@ static void cg_plan_occupancy(const bsp_cg_plan_s *P, int &a, int &b) {
   }
 }
 
-template <typename V, typename VT, bool SC, bool D16>
+template <typename V, typename VT, bool SC, bool D16, int LPR = 1>
 static void launch_iter(bsp_cg_plan_s *P, int k, cudaStream_t s) {
   CgMat<V, VT, SC, D16> A{P->rowPtr, sizeof(V) == 8 ? (const void *)P->colIdx : (const void *)P->lp_cols,
                            (const V *)(sizeof(V) == 8 ? (const void *)P->val : P->lp_val), P->exps,
@@ -895,7 +929,7 @@ static void launch_iter(bsp_cg_plan_s *P, int k, cudaStream_t s) {
   VT *pp = (VT *)P->p[k & 1], *pn = (VT *)P->p[(k + 1) & 1];
   const int g = P->grid, ga = P->grid_a;
   if (P->prec_bs == 0) {
-    cg_dir_spmv_kernel<V, VT, SC, D16><<<ga, kCgThreads, 0, s>>>(P->n, A, r, pp, pn, q, P->part_rr, g,
+    cg_dir_spmv_kernel<V, VT, SC, D16, LPR><<<ga, kCgThreads, 0, s>>>(P->n, A, r, pp, pn, q, P->part_rr, g,
                                                                   P->sc + ((k + 1) & 1), P->sc + (k & 1),
                                                                   P->part_pq);
     cg_update_kernel<VT><<<g, kCgThreads, 0, s>>>(P->n, P->part_pq, ga, P->sc + (k & 1), x, r, pn, q, P->part_rr);
@@ -904,7 +938,7 @@ static void launch_iter(bsp_cg_plan_s *P, int k, cudaStream_t s) {
   // preconditioned: directions from z, r.z in the scalar slots
   VT *z = (VT *)P->z;
   const VT *mi = (const VT *)P->minv;
-  cg_dir_spmv_kernel<V, VT, SC, D16><<<ga, kCgThreads, 0, s>>>(P->n, A, z, pp, pn, q, P->part_rz, g,
+  cg_dir_spmv_kernel<V, VT, SC, D16, LPR><<<ga, kCgThreads, 0, s>>>(P->n, A, z, pp, pn, q, P->part_rz, g,
                                                                 P->sc + ((k + 1) & 1), P->sc + (k & 1),
                                                                 P->part_pq);
   const double *sl = P->sc + (k & 1);
@@ -946,7 +980,12 @@ static void launch_prec(bsp_cg_plan_s *P, cudaStream_t s) {
 
 static bsp_status cg_iteration(bsp_cg_plan_s *P, int k, cudaStream_t s) {
   if (!cg_mixed(P)) {
-    launch_iter<double, double, false, false>(P, k, s);
+    switch (P->lpr) {
+      case 2: launch_iter<double, double, false, false, 2>(P, k, s); break;
+      case 4: launch_iter<double, double, false, false, 4>(P, k, s); break;
+      case 8: launch_iter<double, double, false, false, 8>(P, k, s); break;
+      default: launch_iter<double, double, false, false, 1>(P, k, s);
+    }
   } else {
     const bool d = P->delta16;
     switch (P->opt.mode) {
@@ -1191,6 +1230,10 @@ extern "C" bsp_status bsp_cg_create(int32_t n, int32_t nnz, const int32_t *rowPt
     P->x = nullptr;  // x32 allocated below
   }
   for (void **v : {&P->x, &P->r, &P->p[0], &P->p[1], &P->q}) BSP_CG_CUDA(cudaMallocAsync(v, vt * (size_t)n, s));
+  if (!mixed) {  // lanes per row from the mean row length
+    const double mean = (double)nnz / n;
+    P->lpr = mean <= 10.0 ? 1 : mean <= 20.0 ? 2 : mean <= 40.0 ? 4 : 8;
+  }
   P->prec_bs = opt->precond == BSP_CG_PRECOND_JACOBI ? 1
                : opt->precond == BSP_CG_PRECOND_BLOCK_JACOBI ? opt->precond_block : 0;
   if (mixed) {

@@ -744,6 +744,21 @@ static bsp_status spmm_csr_typed(int32_t rows, int32_t N, const int32_t *rp, con
   return launch_spmm_csr<T, 1>(rows, N, rp, ci, val, B, ldb, C, ldc, a, b, s);
 }
 
+// Longest row (atomicMax of the row lengths).
+__global__ void spmm_max_row_kernel(int32_t rows, const int32_t *__restrict__ rowPtr, int32_t *__restrict__ out) {
+  int32_t m = 0;
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += (int64_t)gridDim.x * blockDim.x)
+    m = max(m, rowPtr[r + 1] - rowPtr[r]);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
+// A row this long keeps one warp busy far past the rest of the launch: the
+// plan-free call routes such matrices through a temporary row-split plan.
+constexpr int32_t kSpmmLongRow = 8192;
+constexpr int32_t kSpmmTempChunk = 256;
+
 }  // namespace bsp
 
 using namespace bsp;
@@ -758,6 +773,39 @@ extern "C" bsp_status bsp_spmm_csr(int32_t rows, int32_t cols, int32_t nnz, cons
   BSP_CHECK_ARG(rowPtr && C && (nnz == 0 || (colIdx && values && B)), "null pointer");
   BSP_CHECK_ARG(ldb >= N && ldc >= N, "leading dimension smaller than N");
   cudaStream_t s = as_stream(stream);
+  BSP_CHECK_ARG(dtype == BSP_F16 || dtype == BSP_BF16 || dtype == BSP_F32, "SpMM takes F16, BF16 or F32 values");
+  // Rows far longer than the mean (power-law graphs) would serialize on one
+  // warp: look up the longest row (skipped while the stream is captured,
+  // since it reads a value back) and split such rows with a temporary plan.
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  BSP_CUDA(cudaStreamIsCapturing(s, &cap));
+  if (cap == cudaStreamCaptureStatusNone && nnz > kSpmmLongRow) {
+    int32_t *d_max = nullptr, h_max = 0;
+    BSP_TRY(dalloc(&d_max, 1, s));
+    BSP_CUDA(cudaMemsetAsync(d_max, 0, sizeof(int32_t), s));
+    const unsigned g = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div(rows, 256), (int64_t)sm_count() * 8));
+    spmm_max_row_kernel<<<g, 256, 0, s>>>(rows, rowPtr, d_max);
+    const bsp_status st = read_i32(d_max, &h_max, s);
+    dfree(d_max, s);
+    BSP_TRY(st);
+    if (h_max > kSpmmLongRow && (int64_t)h_max > 64 * ((int64_t)nnz / rows + 1)) {
+      bsp_spmm_plan plan{};
+      BSP_TRY(bsp_spmm_plan_create(rows, nnz, rowPtr, kSpmmTempChunk, &plan, stream));
+      const size_t ws = bsp_spmm_plan_workspace(&plan, N);
+      void *work = nullptr;
+      bsp_status r2 = BSP_OK;
+      if (ws > 0 && cudaMallocAsync(&work, ws, s) != cudaSuccess) {
+        set_error("bsp_spmm_csr: allocating the row-split workspace failed");
+        r2 = BSP_ERR_ALLOC;
+      }
+      if (r2 == BSP_OK)
+        r2 = bsp_spmm_csr_planned(&plan, cols, nnz, rowPtr, colIdx, values, dtype, B, N, ldb, C, ldc, alpha, beta,
+                                  work, ws, stream);
+      if (work) cudaFreeAsync(work, s);
+      bsp_spmm_plan_free(&plan);
+      return r2;
+    }
+  }
   switch (dtype) {
     case BSP_F16:
       return spmm_csr_typed<__half>(rows, N, rowPtr, colIdx, values, B, ldb, C, ldc, alpha, beta, s);

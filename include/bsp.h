@@ -346,7 +346,12 @@ bsp_status bsp_dasp_spmv(const bsp_dasp *d, const double *x, double *y,
  * include/smat.h:1), whose kernel accumulates in FP16 and never writes its
  * output; here the accumulation is FP32.
  *
- * CSR form: values and B share `dtype` (F16, BF16 or F32), any sparsity. */
+ * CSR form: values and B share `dtype` (F16, BF16 or F32), any sparsity.
+ * Outside stream capture the call first reads back the longest row length
+ * (one small kernel; it waits for the stream); when a row exceeds 8192
+ * nonzeros and 64x the mean, a temporary row-split plan (below) is built,
+ * used and freed.  Callers that repeat the product on such a matrix should
+ * keep their own plan (bsp_spmm_plan_create + bsp_spmm_csr_planned). */
 bsp_status bsp_spmm_csr(int32_t rows, int32_t cols, int32_t nnz,
                         const int32_t *rowPtr, const int32_t *colIdx,
                         const void *values, bsp_dtype dtype, const void *B,

@@ -97,6 +97,33 @@ def test_spmm_planned_matches_fp64_and_is_deterministic(cuda, chunk, N):
     P.free()
 
 
+@pytest.mark.parametrize("name", ["f16", "f32"])
+def test_spmm_csr_long_row_goes_through_a_temporary_plan(cuda, name):
+    """A row of 20,000 nonzeros among rows of ~4: the plan-free call splits it
+    (a temporary row-split plan with 256-nonzero chunks), giving exactly the
+    planned result, within the FP32 accumulation bound of the FP64 oracle."""
+    import torch
+    rng = np.random.default_rng(8)
+    n = 30000
+    lens = rng.integers(0, 8, n)
+    lens[123] = 20000
+    rp = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    ci = np.concatenate([np.sort(rng.choice(n, int(l), replace=False)) for l in lens]).astype(np.int32)
+    A = bsp.HostCSR(n, n, rp, ci, rng.uniform(-1, 1, int(rp[-1])))
+    N = 64
+    vals_t, vals64, B_t, B64 = _case(A, N, name, 5)
+    ref, absC = pyoracle.spmm_f64(A.rowptr, A.colidx, vals64, B64)
+    rpd, cid = _dev(cuda, A.rowptr, A.colidx)
+    vd, Bd = vals_t.to(cuda), B_t.to(cuda)
+    C1 = bsp.spmm_csr(rpd, cid, vd, Bd)
+    P = bsp.SpmmPlan(rpd, cid, vd, cols=A.cols, chunk=256)
+    C2 = P.spmm(Bd)
+    torch.cuda.synchronize()
+    assert torch.equal(C1, C2)
+    assert np.all(np.abs(C1.cpu().numpy().astype(np.float64) - ref) <= _tol(A, absC))
+    P.free()
+
+
 def test_spmm_planned_empty_rows_and_beta(cuda):
     import torch
     # every third row empty
