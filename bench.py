@@ -496,6 +496,9 @@ def run_suite(args) -> None:
     # --- preconditioned CG: Jacobi / block-Jacobi on SPD matrices that need them
     run_pcg(bsp, up)
 
+    # --- CG with 8 right-hand sides at once vs 8 single solves
+    run_cg_multi(bsp, up, dev)
+
     # --- SpMM on a power-law graph (n = 2^20, Zipf 1.8, mean degree 32)
     A = bsp.gen_graph(1 << 20, 1.8, 32, SEED + 4)
     rp, ci, v64 = up(A.rowptr, A.colidx, A.values)
@@ -592,6 +595,39 @@ def run_batch(bsp, dev, pk, up) -> None:
                 res[f"{dname}_rhs1"]["cusparse_separate_us"] = round(_timed(lambda: [f() for f in fns], 5) * 1e6, 1)
             P.close()
     _emit("batch_512_banded_and_zipf2.2", matrices=len(mats), rows=rows, nnz=nnz, variants=res)
+
+
+def run_cg_multi(bsp, up, dev) -> None:
+    """FP64 CG to 1e-10 for 8 right-hand sides: one multi-RHS solve (the
+    matrix read once per iteration for all columns) vs 8 single solves; the
+    7-point Poisson 128^3 and the 4-dof block Laplacian 48^3 (28 entries per
+    row) with Jacobi."""
+    import torch
+    for name, A, pc in (("cg_multi8_poisson3d_128", bsp.gen_poisson3d(128), "none"),
+                        ("cg_multi8_block_laplace3d_48_4dof_jacobi", bsp.gen_block_laplace3d(48, 4, 10.0, SEED + 33),
+                         "jacobi")):
+        rp, ci, va = up(A.rowptr, A.colidx, A.values)
+        g = torch.Generator(device="cpu").manual_seed(8)
+        B = (torch.rand(A.rows, 8, generator=g, dtype=torch.float64) * 2 - 1).to(dev)
+        S = bsp.CgSolver(rp, ci, va, mode="fp64", precond=pc, max_iters=50000)
+        S.solve_multi(B)                                            # warm-up
+        _, rel, rm = S.solve_multi(B)
+        single = 0.0
+        its = []
+        for j in range(8):
+            bj = B[:, j].contiguous()
+            S.solve(bj)
+            _, r1 = S.solve(bj)
+            single += r1["seconds"]
+            its.append(r1["iterations"])
+        S.close()
+        _emit(name, n=A.rows, nnz=A.nnz, k=8, precond=pc,
+              multi={"ms": round(rm["seconds"] * 1e3, 3), "iterations": rm["iterations"],
+                     "worst_rel_residual": float(rel.max()),
+                     "gbs": round(rm["bytes_moved"] / rm["seconds"] / 1e9, 1)},
+              eight_single={"ms": round(single * 1e3, 3), "iterations": its},
+              speedup=round(single / rm["seconds"], 2))
+        del rp, ci, va, B
 
 
 def run_pcg(bsp, up) -> None:

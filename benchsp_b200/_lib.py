@@ -299,3 +299,7 @@ _PROTOS.update({
     "bsp_mtx_free": (C.c_int, [C.c_void_p]),
     "bsp_mtx_write_csr_host": (C.c_int, [C.c_char_p, _I32, _I32, _I64, _P, _P, _P, _I32]),
 })
+
+_PROTOS.update({
+    "bsp_cg_solve_multi": (C.c_int, [C.c_void_p, _I32, _P, _I64, _P, _I64, _P, C.POINTER(BspCgResult), _P]),
+})

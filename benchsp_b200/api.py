@@ -529,6 +529,29 @@ class CgSolver:
             check(st)
         return x, {k: getattr(r, k) for k, _ in _lib.BspCgResult._fields_}
 
+    def solve_multi(self, B, X=None, *, stream=None, raise_on_stall: bool = True) -> tuple:
+        """A X = B for the k columns of B (n x k, FP64, row-major); FP64
+        plans with no or Jacobi preconditioning.  Returns (X, per-column
+        relative residuals, aggregate result)."""
+        torch = _torch()
+        k = B.shape[1]
+        if X is None:
+            X = torch.zeros(self.n, k, dtype=torch.float64, device=B.device)
+        for t, nm in ((B, "B"), (X, "X")):
+            if not t.is_cuda or t.dtype != torch.float64 or t.dim() != 2 or t.shape[0] != self.n or \
+                    (t.shape[1] > 1 and t.stride(1) != 1):
+                raise ValueError(f"{nm} must be a row-major n x k FP64 CUDA tensor (column stride 1)")
+        if X.shape[1] != k:
+            raise ValueError("X must have as many columns as B")
+        rel = np.zeros(k)
+        r = _lib.BspCgResult()
+        st = lib().bsp_cg_solve_multi(self._plan, k, C.c_void_p(B.data_ptr()), max(B.stride(0), k),
+                                      C.c_void_p(X.data_ptr()), max(X.stride(0), k),
+                                      rel.ctypes.data_as(C.c_void_p), C.byref(r), _stream(stream))
+        if st != _lib.BSP_ERR_NOT_CONVERGED or raise_on_stall:
+            check(st)
+        return X, rel, {k2: getattr(r, k2) for k2, _ in _lib.BspCgResult._fields_}
+
     def close(self) -> None:
         if self._plan:
             check(lib().bsp_cg_destroy(self._plan))

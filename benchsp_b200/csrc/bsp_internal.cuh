@@ -152,3 +152,19 @@ __device__ __forceinline__ T warp_sum(T v, unsigned mask = 0xffffffffu) {
 }
 
 }  // namespace bsp
+
+// What the multi-right-hand-side CG (cg_multi.cu) reads from a CG plan (cg.cu).
+struct bsp_cg_plan_s;
+namespace bsp {
+struct CgPlanView {
+  int32_t n, nnz;
+  const int32_t *rowPtr, *colIdx;
+  const double *val;
+  bool mixed;
+  int prec_bs;
+  const void *minv;
+  int32_t check_every, max_iters;
+  double tol;
+};
+void cg_plan_view(const bsp_cg_plan_s *P, CgPlanView *v);
+}  // namespace bsp

@@ -1341,6 +1341,22 @@ extern "C" bsp_status bsp_cg_create(int32_t n, int32_t nnz, const int32_t *rowPt
   return BSP_OK;
 }
 
+namespace bsp {
+void cg_plan_view(const bsp_cg_plan_s *P, CgPlanView *v) {
+  v->n = P->n;
+  v->nnz = P->nnz;
+  v->rowPtr = P->rowPtr;
+  v->colIdx = P->colIdx;
+  v->val = P->val;
+  v->mixed = cg_mixed(P);
+  v->prec_bs = P->prec_bs;
+  v->minv = P->minv;
+  v->check_every = P->opt.check_every;
+  v->max_iters = P->opt.max_iters;
+  v->tol = P->opt.tol;
+}
+}  // namespace bsp
+
 extern "C" bsp_status bsp_cg_solve(bsp_cg_plan P, const double *b, double *x, bsp_cg_result *res,
                                    bsp_stream_t stream) {
   clear_error();

@@ -504,6 +504,19 @@ bsp_status bsp_cg_create(int32_t n, int32_t nnz, const int32_t *rowPtr,
 bsp_status bsp_cg_solve(bsp_cg_plan plan, const double *b, double *x,
                         bsp_cg_result *res, bsp_stream_t stream);
 bsp_status bsp_cg_destroy(bsp_cg_plan plan);
+/* k right-hand sides at once: A X = B with B, X device arrays, row-major with
+ * leading dimensions ldb, ldx >= k (row i, column j at B[i*ldb + j]); X holds
+ * the initial guesses on entry.  Every column runs its own FP64 CG (same
+ * iterates as k separate solves) but each iteration reads the matrix once
+ * for up to 8 columns.  Needs a plan with mode BSP_CG_FP64 and precond NONE
+ * or JACOBI (else BSP_ERR_UNSUPPORTED).  rel_residuals (k entries, may be
+ * NULL) receives each column's final ||b - A x|| / ||b||; res aggregates
+ * (iterations = the most any column group ran, rel_residual = the worst).
+ * BSP_ERR_NOT_CONVERGED when a column stops above the tolerance. */
+bsp_status bsp_cg_solve_multi(bsp_cg_plan plan, int32_t k, const double *B,
+                              int64_t ldb, double *X, int64_t ldx,
+                              double *rel_residuals, bsp_cg_result *res,
+                              bsp_stream_t stream);
 
 /* ---------------------------------------------------------------------- */
 /* 4x4 block statistics of bench/blockinfo.cpp:96-119 (reference): the number
