@@ -133,11 +133,26 @@ __device__ __forceinline__ void rows_item(const BatchMatDev &M, int32_t r0, int3
   const V *val = static_cast<const V *>(M.val);
   const V *x = static_cast<const V *>(M.x);
   V *y = static_cast<V *>(M.y);
+  // one vector: the next group's row pointers are loaded while this group's
+  // entries are summed (one dependent round trip fewer per group; with 8
+  // vectors the extra registers cost more than it saves)
+  int32_t ns = 0, ne = 0;
+  if (NRHS == 1 && r0 + rl < r1) {
+    ns = __ldg(M.rp + r0 + rl);
+    ne = __ldg(M.rp + r0 + rl + 1);
+  }
   for (int32_t base = r0; base < r1; base += RPP) {
     const int32_t row = base + rl;
     const bool active = row < r1;
     int32_t s = 0, e = 0;
-    if (active) {
+    if constexpr (NRHS == 1) {
+      s = ns;
+      e = ne;
+      if (row + RPP < r1) {
+        ns = __ldg(M.rp + row + RPP);
+        ne = __ldg(M.rp + row + RPP + 1);
+      }
+    } else if (active) {
       s = __ldg(M.rp + row);
       e = __ldg(M.rp + row + 1);
     }
