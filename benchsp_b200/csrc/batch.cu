@@ -148,6 +148,7 @@ __device__ __forceinline__ void rows_item(const BatchMatDev &M, int32_t r0, int3
     if constexpr (NRHS == 1) {
       s = ns;
       e = ne;
+      ns = ne = 0;  // a row past the item stays empty
       if (row + RPP < r1) {
         ns = __ldg(M.rp + row + RPP);
         ne = __ldg(M.rp + row + RPP + 1);
