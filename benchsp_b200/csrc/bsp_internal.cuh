@@ -136,6 +136,7 @@ __device__ __forceinline__ int ld_stream_s32(const int *p, uint64_t pol) {
 }
 // Gathers of x: read-only path, default caching.
 __device__ __forceinline__ double ld_x(const double *p) { return __ldg(p); }
+
 __device__ __forceinline__ double2 ld_x2(const double *p) {
   return __ldg(reinterpret_cast<const double2 *>(p));
 }

@@ -530,7 +530,7 @@ bsp_status csr2dasp_impl(int32_t rows, int32_t cols, int32_t nnz, const int32_t 
 struct DaspSections {
   int32_t long_cta, reg_cta, s1_cta, t13_cta, t34_cta, t22_cta, zero_cta;
 };
-constexpr int kS1PerThread = 8;
+constexpr int kS1PerThread = 4;
 constexpr int kShortPerThread = 2;
 
 // Device-scope atomic add with acquire-release ordering: the caller's earlier
@@ -543,11 +543,11 @@ __device__ __forceinline__ int32_t atomic_add_acq_rel(int32_t *p, int32_t v) {
 }
 
 // y slot k -> element index (order_rid when the output is not permuted)
-__device__ __forceinline__ int64_t dasp_yidx(const int32_t *outIdx, int64_t k) {
-  return outIdx ? (int64_t)__ldg(outIdx + k) : k;
+__device__ __forceinline__ int32_t dasp_yidx(const int32_t *outIdx, int64_t k) {
+  return outIdx ? __ldg(outIdx + k) : (int32_t)k;
 }
 
-__device__ __forceinline__ void dasp_put(double *y, int64_t yi, double v, double alpha, double beta) {
+__device__ __forceinline__ void dasp_put(double *y, int32_t yi, double v, double alpha, double beta) {
   double r = alpha * v;
   if (beta != 0.0) r += beta * y[yi];
   y[yi] = r;
@@ -559,8 +559,12 @@ __device__ __forceinline__ f64x4 dasp_ld4(const double *p) {
   return f64x4{__ldg(p), __ldg(p + 1), __ldg(p + 2), __ldg(p + 3)};
 }
 
+// 32 registers (8 CTAs of 256 per SM): every section waits on dependent
+// gathers, so resident warps matter more than per-thread batching; at 64
+// registers (4 CTAs) the kernel kept half the warps and took 82-84 us on the
+// 2M-row power-law matrix.
 template <bool SHORT_ALIGNED>
-__global__ void __launch_bounds__(256) dasp_spmv_kernel(bsp_dasp D, DaspSections S, const double *__restrict__ x,
+__global__ void __launch_bounds__(256, 6) dasp_spmv_kernel(bsp_dasp D, DaspSections S, const double *__restrict__ x,
                                                         double *__restrict__ y, const int32_t *__restrict__ outIdx,
                                                         double alpha, double beta) {
   const int lane = threadIdx.x & 31;
@@ -572,7 +576,7 @@ __global__ void __launch_bounds__(256) dasp_spmv_kernel(bsp_dasp D, DaspSections
     const int4 gi = __ldg(reinterpret_cast<const int4 *>(D.long_group_info) + g);
     const int32_t row = gi.x, c0 = gi.y, g0 = gi.z, nc = gi.w & 15, ng = gi.w >> 4;
     const uint64_t pol = evict_first_policy();
-    const int64_t yi = lane == 0 ? dasp_yidx(outIdx, row) : 0;
+    const int32_t yi = lane == 0 ? dasp_yidx(outIdx, row) : 0;
     double2 v[kLongGroup];
     int2 c[kLongGroup];
 #pragma unroll
@@ -621,7 +625,7 @@ __global__ void __launch_bounds__(256) dasp_spmv_kernel(bsp_dasp D, DaspSections
     const bool live = row < D.row_block;
     const int32_t p0 = D.block_ptr[bid], p1 = D.block_ptr[bid + 1];
     const int32_t i0 = live ? __ldg(D.irreg_rpt + row) : 0, i1 = live ? __ldg(D.irreg_rpt + row + 1) : 0;
-    const int64_t yi = (live && t == 0) ? dasp_yidx(outIdx, D.row_long + row) : 0;
+    const int32_t yi = (live && t == 0) ? dasp_yidx(outIdx, D.row_long + row) : 0;
     double acc = 0.0;
     int32_t o = p0 + t * kTile;
     int32_t j = i0 + t;
@@ -673,7 +677,7 @@ __global__ void __launch_bounds__(256) dasp_spmv_kernel(bsp_dasp D, DaspSections
     const int64_t i0 = (int64_t)b * 256 * kS1PerThread + threadIdx.x;
     double v[kS1PerThread];
     int32_t c[kS1PerThread];
-    int64_t yi[kS1PerThread];
+    int32_t yi[kS1PerThread];
     const uint64_t pol = evict_first_policy();
 #pragma unroll
     for (int k = 0; k < kS1PerThread; ++k) {
@@ -701,7 +705,7 @@ __global__ void __launch_bounds__(256) dasp_spmv_kernel(bsp_dasp D, DaspSections
     const int64_t ns = 2 * (int64_t)D.common_13;
     double v[kShortPerThread][3];
     int32_t c[kShortPerThread][3];
-    int64_t yi[kShortPerThread];
+    int32_t yi[kShortPerThread];
 #pragma unroll
     for (int k = 0; k < kShortPerThread; ++k) {
       const int64_t s = s0 + k * 256;
@@ -743,7 +747,7 @@ __global__ void __launch_bounds__(256) dasp_spmv_kernel(bsp_dasp D, DaspSections
     const int64_t s0 = (int64_t)b * 256 * kShortPerThread + threadIdx.x;
     f64x4 v[kShortPerThread];
     int4 c[kShortPerThread];
-    int64_t yi[kShortPerThread];
+    int32_t yi[kShortPerThread];
 #pragma unroll
     for (int k = 0; k < kShortPerThread; ++k) {
       const int64_t s = s0 + k * 256;
@@ -775,7 +779,7 @@ __global__ void __launch_bounds__(256) dasp_spmv_kernel(bsp_dasp D, DaspSections
     const int64_t s0 = (int64_t)b * 256 * kShortPerThread + threadIdx.x;
     double2 v[kShortPerThread];
     int2 c[kShortPerThread];
-    int64_t yi[kShortPerThread];
+    int32_t yi[kShortPerThread];
 #pragma unroll
     for (int k = 0; k < kShortPerThread; ++k) {
       const int64_t s = s0 + k * 256;

@@ -137,3 +137,51 @@ def test_reference_csr_kernels_agree_and_are_timed(cuda):
     rec["case"] = "csr_laplace2d_512_l2_flushed"
     rec["n"], rec["nnz"] = A.rows, A.nnz
     print(json.dumps(rec))
+
+
+def dasp_case(cuda, A, reps=50):
+    """Runs the reference's DASP kernels (dasp_spmv2<1> + longPart_sum) on the
+    arguments its spmv_all builds for A (captured by oracle/_ref/dasp_capture)
+    and the library's DASP SpMV on its own packing (bit-identical to those
+    arrays); returns the record, x, the reference's y (original row order)
+    and the library's y."""
+    import torch
+    x = bsp.gen_uniform(A.cols, 13)
+    with tempfile.TemporaryDirectory() as td:
+        fin, fcap, fout = (os.path.join(td, n) for n in ("in.bin", "cap.bin", "y.bin"))
+        pyoracle.write_csr_bin(fin, A.rows, A.cols, A.rowptr, A.colidx, A.values, x)
+        r = subprocess.run([_exe("dasp_capture"), fin, fcap], capture_output=True, text=True, timeout=1200)
+        assert r.returncode == 0, r.stderr
+        order = np.frombuffer(pyoracle.read_records(fcap)["arr:order_rid"], np.int32)
+        r = subprocess.run([_exe("ref_dasp_time"), fcap, fout, str(reps)], capture_output=True, text=True,
+                           timeout=600)
+        assert r.returncode == 0, r.stderr
+        times = json.loads(r.stdout.strip().splitlines()[-1])
+        y_perm = np.fromfile(fout, np.float64)[:A.rows]
+    y_ref = np.empty(A.rows)
+    y_ref[order] = y_perm                          # output position k holds row order_rid[k]
+    rp, ci, va, xd = (torch.from_numpy(a).to(cuda) for a in (A.rowptr, A.colidx, A.values, x))
+    D = bsp.csr2dasp(rp, ci, va, rows=A.rows, cols=A.cols)
+    y = torch.empty(A.rows, dtype=torch.float64, device=cuda)
+    # the reference writes y in order_rid order: time that form too
+    ours_perm = _events(lambda: D.spmv(xd, y, permuted=True), reps)
+    ours = _events(lambda: D.spmv(xd, y), reps)
+    D.spmv(xd, y)
+    torch.cuda.synchronize()
+    rec = {"reference_us": times, "ours_us_permuted_output": round(ours_perm, 2),
+           "ours_us_row_order": round(ours, 2),
+           "speedup_same_output_order": round(times["dasp_spmv2+longPart_sum"] / ours_perm, 2)}
+    D.free()
+    return rec, x, y_ref, y.cpu().numpy()
+
+
+def test_reference_dasp_kernels_agree_and_are_timed(cuda):
+    A = bsp.gen_powerlaw(1 << 17, 2.0, 4000, 21)
+    rec, x, y_ref, ours = dasp_case(cuda, A)
+    want = pyoracle.spmv_f64(A.rowptr, A.colidx, A.values, x)
+    tol = pyoracle.spmv_tolerance(A.rowptr, A.colidx, A.values, x)
+    assert np.all(np.abs(y_ref - want) <= tol)
+    assert np.all(np.abs(ours - want) <= tol)
+    rec["case"] = "dasp_powerlaw_2^17_zipf2"
+    rec["n"], rec["nnz"] = A.rows, A.nnz
+    print(json.dumps(rec))
