@@ -106,8 +106,11 @@ struct CgMat {
 // LPR (FP64 CSR path only): lanes per row; rows longer than ~10 entries
 // get 2, 4 or 8 lanes that split the row's entries (4 loads in flight each)
 // and combine by shuffle, instead of one thread walking the row.
+// The FP64 CSR path fits 40 registers without spills: 6 resident CTAs per SM
+// instead of 4 (Poisson 128^3 FP64 CG 37.0 -> 35.9 ms); the SELL paths keep
+// the default (the same cap cost them 15%).
 template <typename V, typename VT, bool SCALED, bool DELTA16, int LPR = 1>
-__global__ void __launch_bounds__(kCgThreads) cg_dir_spmv_kernel(int32_t n, CgMat<V, VT, SCALED, DELTA16> A,
+__global__ void __launch_bounds__(kCgThreads, sizeof(V) == 8 ? 6 : 0) cg_dir_spmv_kernel(int32_t n, CgMat<V, VT, SCALED, DELTA16> A,
                                                                  const VT *__restrict__ r,
                                                                  const VT *__restrict__ p_prev,
                                                                  VT *__restrict__ p, VT *__restrict__ q,

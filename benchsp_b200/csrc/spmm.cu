@@ -210,9 +210,11 @@ __device__ __forceinline__ void spmm_segment(int32_t s, int32_t e, const int32_t
 // Wide B rows (8+ lanes per row, N >= 64 in FP16) are gather-latency bound:
 // capping registers at 40 keeps 6 CTAs per SM resident instead of 4 (graph
 // 2^20, FP16: N = 128 2.43 -> 2.16 ms, N = 256 4.43 -> 3.99 ms); narrow rows
-// lose 1% with the cap and keep the default.
+// lose 1% with the cap and keep the compiler's default (a minimum of 0 CTAs
+// leaves the register choice unconstrained, like no second bound; an explicit
+// 1 would let it take more registers than the default).
 template <typename T, int LPR>
-__global__ void __launch_bounds__(256, LPR >= 8 ? 6 : 1) spmm_grouped_kernel(int32_t rows, int32_t N, const int32_t *__restrict__ rowPtr,
+__global__ void __launch_bounds__(256, LPR >= 8 ? 6 : 0) spmm_grouped_kernel(int32_t rows, int32_t N, const int32_t *__restrict__ rowPtr,
                                                            const int32_t *__restrict__ colIdx,
                                                            const T *__restrict__ val, const T *__restrict__ B,
                                                            int64_t ldb, float *__restrict__ C, int64_t ldc,
@@ -1143,7 +1145,7 @@ extern "C" bsp_status bsp_spmm_plan_free(bsp_spmm_plan *p) {
 namespace bsp {
 // Warp per chunk (see spmm_chunk_kernel) with the grouped engine.
 template <typename T, int LPR>
-__global__ void __launch_bounds__(256, LPR >= 8 ? 6 : 1) spmm_grouped_chunk_kernel(
+__global__ void __launch_bounds__(256, LPR >= 8 ? 6 : 0) spmm_grouped_chunk_kernel(
     int64_t nchunks, int32_t N, int32_t chunk, const int32_t *__restrict__ chunk_row,
     const int32_t *__restrict__ chunk_ptr, const int32_t *__restrict__ part_ptr, const int32_t *__restrict__ rowPtr,
     const int32_t *__restrict__ colIdx, const T *__restrict__ val, const T *__restrict__ B, int64_t ldb,
