@@ -80,7 +80,7 @@ __device__ __forceinline__ void st2(double *p, double a, double b) {
 
 // Kernel A.  src = Z (or R); rz_part [K][npart]; rz_prev [K]; rz_out [K].
 template <int K>
-__global__ void __launch_bounds__(kMcgThreads) mcg_dir_kernel(int32_t n, const int32_t *__restrict__ rowPtr,
+__global__ void __launch_bounds__(kMcgThreads, 6) mcg_dir_kernel(int32_t n, const int32_t *__restrict__ rowPtr,
                                                               const int32_t *__restrict__ colIdx,
                                                               const double *__restrict__ val,
                                                               const double *__restrict__ src,
@@ -239,12 +239,17 @@ template <int K>
 bsp_status mcg_group(const CgPlanView &v, int32_t k, const double *Bu, int64_t ldb, double *Xu, int64_t ldx,
                      double *rel, int32_t *iters_out, bool *conv_out, int64_t *bytes, cudaStream_t s) {
   const int32_t n = v.n;
-  int occ = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, mcg_dir_kernel<K>, kMcgThreads, 0) != cudaSuccess ||
-      occ < 1)
-    occ = 1;
-  const int grid = (int)std::max<int64_t>(
-      1, std::min<int64_t>(ceil_div((int64_t)n * McgLayout<K>::CPL, kMcgThreads), (int64_t)sm_count() * occ));
+  // one wave of each kernel: the direction kernel (a gather, capped at 40
+  // registers for 6 CTAs/SM) and the streaming update / residual kernels
+  // each get their own resident-CTA count; a partial array's length is its
+  // writer's grid
+  auto wave = [&](auto kern) {
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kMcgThreads, 0) != cudaSuccess || occ < 1) occ = 1;
+    return (int)std::max<int64_t>(
+        1, std::min<int64_t>(ceil_div((int64_t)n * McgLayout<K>::CPL, kMcgThreads), (int64_t)sm_count() * occ));
+  };
+  const int grid_d = wave(mcg_dir_kernel<K>), grid = wave(mcg_update_kernel<K>);
   const double *dinv = v.prec_bs == 1 ? static_cast<const double *>(v.minv) : nullptr;
   McgBuffers m;
   const size_t nk = (size_t)n * K;
@@ -256,7 +261,8 @@ bsp_status mcg_group(const CgPlanView &v, int32_t k, const double *Bu, int64_t l
   for (double **p : {&m.X, &m.B, &m.R, &m.P0, &m.P1, &m.Q})
     if ((st = dalloc(p, nk, s)) != BSP_OK) return fail(st);
   if (dinv && (st = dalloc(&m.Z, nk, s)) != BSP_OK) return fail(st);
-  for (double **p : {&m.pq, &m.rr, &m.rz, &m.bb})
+  if ((st = dalloc(&m.pq, (size_t)K * grid_d, s)) != BSP_OK) return fail(st);
+  for (double **p : {&m.rr, &m.rz, &m.bb})
     if ((st = dalloc(p, (size_t)K * grid, s)) != BSP_OK) return fail(st);
   if ((st = dalloc(&m.slots, 2 * K, s)) != BSP_OK || (st = dalloc(&m.sums, 2 * K, s)) != BSP_OK) return fail(st);
   std::vector<double> h(2 * K);
@@ -307,9 +313,9 @@ bsp_status mcg_group(const CgPlanView &v, int32_t k, const double *Bu, int64_t l
     for (int c = 0; c < v.check_every; ++c, ++it) {
       double *pp = (it & 1) ? m.P1 : m.P0, *pn = (it & 1) ? m.P0 : m.P1;
       double *slot = m.slots + (it & 1) * K, *prev = m.slots + ((it + 1) & 1) * K;
-      mcg_dir_kernel<K><<<grid, kMcgThreads, 0, s>>>(n, v.rowPtr, v.colIdx, v.val, src, pp, pn, m.Q, m.rz, grid,
-                                                     prev, slot, m.pq);
-      mcg_update_kernel<K><<<grid, kMcgThreads, 0, s>>>(n, m.pq, grid, slot, m.X, m.R, m.Z, pn, m.Q, dinv, m.rr,
+      mcg_dir_kernel<K><<<grid_d, kMcgThreads, 0, s>>>(n, v.rowPtr, v.colIdx, v.val, src, pp, pn, m.Q, m.rz, grid,
+                                                       prev, slot, m.pq);
+      mcg_update_kernel<K><<<grid, kMcgThreads, 0, s>>>(n, m.pq, grid_d, slot, m.X, m.R, m.Z, pn, m.Q, dinv, m.rr,
                                                         m.rz);
     }
     mcg_sum_kernel<<<1, kMcgThreads, 0, s>>>(m.rr, grid, K, m.sums);
