@@ -274,19 +274,14 @@ __global__ void __launch_bounds__(kCgThreads) cg_update_kernel(int32_t n, const 
   constexpr int W = Vec16<VT>::W;
   constexpr int U = 2;
   __shared__ double smem[kCgThreads / 32];
-  const double pq = reduce_partials(pq_part, npart, smem);
-  const double rr = *rr_slot;
-  const double alpha = (pq != 0.0 && rr != 0.0 && isfinite(pq)) ? rr / pq : 0.0;
-  const VT a = (VT)alpha;
-  double s = 0.0;
   const int64_t nv = n / W;
   const int64_t stride = (int64_t)gridDim.x * kCgThreads;
   V *xv = reinterpret_cast<V *>(x);
   V *rv = reinterpret_cast<V *>(r);
   const V *pv = reinterpret_cast<const V *>(p);
   const V *qv = reinterpret_cast<const V *>(q);
-  for (int64_t i0 = (int64_t)blockIdx.x * kCgThreads + threadIdx.x; i0 < nv; i0 += U * stride) {
-    V P[U], Q[U], X[U], R[U];
+  V P[U], Q[U], X[U], R[U];
+  auto load = [&](int64_t i0) {
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const int64_t i = i0 + u * stride;
@@ -297,6 +292,18 @@ __global__ void __launch_bounds__(kCgThreads) cg_update_kernel(int32_t n, const 
         R[u] = rv[i];
       }
     }
+  };
+  // the first pass's vectors do not depend on alpha: their loads are in
+  // flight while the CTA sums the p.q partials
+  const int64_t first = (int64_t)blockIdx.x * kCgThreads + threadIdx.x;
+  load(first);
+  const double pq = reduce_partials(pq_part, npart, smem);
+  const double rr = *rr_slot;
+  const double alpha = (pq != 0.0 && rr != 0.0 && isfinite(pq)) ? rr / pq : 0.0;
+  const VT a = (VT)alpha;
+  double s = 0.0;
+  for (int64_t i0 = first; i0 < nv; i0 += U * stride) {
+    if (i0 != first) load(i0);
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const int64_t i = i0 + u * stride;
