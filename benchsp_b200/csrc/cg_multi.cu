@@ -38,16 +38,39 @@ __device__ __forceinline__ double mcg_block_sum(double v, double *smem) {
   return t;
 }
 
-// K column sums of [K][npart] partials, in index order, into out[K] (shared).
+// Warp sum of v (xor shuffle) into smem[warp * K + j]: the first half of
+// mcg_block_sum for column j, K columns sharing one barrier.
 template <int K>
-__device__ __forceinline__ void mcg_reduce(const double *__restrict__ part, int npart, double *smem, double *out) {
+__device__ __forceinline__ void mcg_warp_slot(double v, int j, double *smemk) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) smemk[(threadIdx.x >> 5) * K + j] = v;
+}
+
+// The second half for all K columns: out[j] = the warps' sums in index order
+// (threads j < K), then a barrier so smemk can be reused.
+template <int K>
+__device__ __forceinline__ void mcg_slots_sum(const double *smemk, double *out) {
+  __syncthreads();
+  if (threadIdx.x < K) {
+    double t = 0.0;
+    for (int w = 0; w < kMcgThreads / 32; ++w) t += smemk[w * K + threadIdx.x];
+    out[threadIdx.x] = t;
+  }
+  __syncthreads();
+}
+
+// K column sums of [K][npart] partials, in index order, into out[K] (shared;
+// smemk: K doubles per warp).
+template <int K>
+__device__ __forceinline__ void mcg_reduce(const double *__restrict__ part, int npart, double *smemk, double *out) {
+#pragma unroll
   for (int j = 0; j < K; ++j) {
     double s = 0.0;
     for (int i = threadIdx.x; i < npart; i += kMcgThreads) s += __ldcg(part + (int64_t)j * npart + i);
-    s = mcg_block_sum(s, smem);
-    if (threadIdx.x == 0) out[j] = s;
+    mcg_warp_slot<K>(s, j, smemk);
   }
-  __syncthreads();
+  mcg_slots_sum<K>(smemk, out);
 }
 
 // Thread layout: CPL = K / 2 lanes per row, lane `pr` of a row owning the
@@ -59,17 +82,17 @@ template <int K> struct McgLayout {
   static constexpr int CPL = K / 2;
 };
 
-// Per-column partials: thread (row, pr) holds columns 2 pr, 2 pr + 1.
+// Per-column partials: thread (row, pr) holds columns 2 pr, 2 pr + 1
+// (smemk: K doubles per warp; sums[K] shared).
 template <int K>
-__device__ __forceinline__ void write_pair_partials(double d0, double d1, double *smem, double *__restrict__ part) {
+__device__ __forceinline__ void write_pair_partials(double d0, double d1, double *smemk, double *sums,
+                                                    double *__restrict__ part) {
   constexpr int CPL = McgLayout<K>::CPL;
   const int pr = threadIdx.x % CPL;
 #pragma unroll
-  for (int j = 0; j < K; ++j) {
-    const double v = (pr == j / 2) ? ((j & 1) ? d1 : d0) : 0.0;
-    const double t = mcg_block_sum(v, smem);
-    if (threadIdx.x == 0) part[(int64_t)j * gridDim.x + blockIdx.x] = t;
-  }
+  for (int j = 0; j < K; ++j) mcg_warp_slot<K>((pr == j / 2) ? ((j & 1) ? d1 : d0) : 0.0, j, smemk);
+  mcg_slots_sum<K>(smemk, sums);
+  if (threadIdx.x < K) part[(int64_t)threadIdx.x * gridDim.x + blockIdx.x] = sums[threadIdx.x];
 }
 
 __device__ __forceinline__ double2 ld2(const double *p) { return __ldg(reinterpret_cast<const double2 *>(p)); }
@@ -91,7 +114,8 @@ __global__ void __launch_bounds__(kMcgThreads, 6) mcg_dir_kernel(int32_t n, cons
                                                               double *__restrict__ rz_out,
                                                               double *__restrict__ pq_part) {
   constexpr int CPL = McgLayout<K>::CPL;
-  __shared__ double smem[kMcgThreads / 32];
+  __shared__ double smem[kMcgThreads / 32 * K];
+  __shared__ double sums[K];
   __shared__ double rz[K];
   mcg_reduce<K>(rz_part, npart, smem, rz);
   if (blockIdx.x == 0 && threadIdx.x < K) rz_out[threadIdx.x] = rz[threadIdx.x];
@@ -129,13 +153,13 @@ __global__ void __launch_bounds__(kMcgThreads, 6) mcg_dir_kernel(int32_t n, cons
     d0 += a0 * p0;
     d1 += a1 * p1;
   }
-  write_pair_partials<K>(d0, d1, smem, pq_part);
+  write_pair_partials<K>(d0, d1, smem, sums, pq_part);
 }
 
 // Kernel B.  rz_slot [K] (written by kernel A); dinv null = no preconditioner
 // (then z is not written and the r.z partials are the r.r ones).
 template <int K>
-__global__ void __launch_bounds__(kMcgThreads) mcg_update_kernel(int32_t n, const double *__restrict__ pq_part,
+__global__ void __launch_bounds__(kMcgThreads, K == 4 ? 4 : 0) mcg_update_kernel(int32_t n, const double *__restrict__ pq_part,
                                                                  int npart, const double *__restrict__ rz_slot,
                                                                  double *__restrict__ x, double *__restrict__ r,
                                                                  double *__restrict__ z,
@@ -145,7 +169,8 @@ __global__ void __launch_bounds__(kMcgThreads) mcg_update_kernel(int32_t n, cons
                                                                  double *__restrict__ rr_part,
                                                                  double *__restrict__ rz_part) {
   constexpr int CPL = McgLayout<K>::CPL;
-  __shared__ double smem[kMcgThreads / 32];
+  __shared__ double smem[kMcgThreads / 32 * K];
+  __shared__ double sums[K];
   __shared__ double pq[K];
   mcg_reduce<K>(pq_part, npart, smem, pq);
   const int pr = threadIdx.x % CPL, c0 = 2 * pr;
@@ -168,8 +193,8 @@ __global__ void __launch_bounds__(kMcgThreads) mcg_update_kernel(int32_t n, cons
     z1s += r1 * (d * r1);
     if (dinv) st2(z + o, d * r0, d * r1);
   }
-  write_pair_partials<K>(rr0, rr1, smem, rr_part);
-  write_pair_partials<K>(z0s, z1s, smem, rz_part);
+  write_pair_partials<K>(rr0, rr1, smem, sums, rr_part);
+  write_pair_partials<K>(z0s, z1s, smem, sums, rz_part);
 }
 
 // R = B - A X (and Z = D^{-1} R); partials of r.r, r.z and b.b.
@@ -185,7 +210,8 @@ __global__ void __launch_bounds__(kMcgThreads) mcg_residual_kernel(int32_t n, co
                                                                    double *__restrict__ rz_part,
                                                                    double *__restrict__ bb_part) {
   constexpr int CPL = McgLayout<K>::CPL;
-  __shared__ double smem[kMcgThreads / 32];
+  __shared__ double smem[kMcgThreads / 32 * K];
+  __shared__ double sums[K];
   const int pr = threadIdx.x % CPL, c0 = 2 * pr;
   double rr0 = 0.0, rr1 = 0.0, z0s = 0.0, z1s = 0.0, b0s = 0.0, b1s = 0.0;
   const int64_t rstride = (int64_t)gridDim.x * (kMcgThreads / CPL);
@@ -210,9 +236,9 @@ __global__ void __launch_bounds__(kMcgThreads) mcg_residual_kernel(int32_t n, co
     b0s += B.x * B.x;
     b1s += B.y * B.y;
   }
-  write_pair_partials<K>(rr0, rr1, smem, rr_part);
-  write_pair_partials<K>(z0s, z1s, smem, rz_part);
-  write_pair_partials<K>(b0s, b1s, smem, bb_part);
+  write_pair_partials<K>(rr0, rr1, smem, sums, rr_part);
+  write_pair_partials<K>(z0s, z1s, smem, sums, rz_part);
+  write_pair_partials<K>(b0s, b1s, smem, sums, bb_part);
 }
 
 // out[j] = sum of partials j (one CTA).
