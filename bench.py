@@ -784,6 +784,13 @@ def run_profile(args) -> None:
         S = bsp.CgSolver(rp, ci, va, mode="fp64", precond="block_jacobi", block=4, max_iters=32, check_every=16,
                          use_graphs=False)
         S.solve(b, raise_on_stall=False)
+    elif w == "cg_multi":   # FP64 CG for 8 right-hand sides, 7-point Poisson 128^3 (~1 GB), 32 iterations
+        A = bsp.gen_poisson3d(128)
+        rp, ci, va = up(A.rowptr, A.colidx, A.values)
+        g = torch.Generator(device="cpu").manual_seed(8)
+        B = (torch.rand(A.rows, 8, generator=g, dtype=torch.float64) * 2 - 1).to(dev)
+        S = bsp.CgSolver(rp, ci, va, mode="fp64", max_iters=32, check_every=16)
+        S.solve_multi(B, raise_on_stall=False)
     elif w == "spmm_grouped":   # power-law graph 2^20, FP16, N = 128, grouped CSR engine
         A = bsp.gen_graph(1 << 20, 1.8, 32, SEED + 4)
         rp, ci, v64 = up(A.rowptr, A.colidx, A.values)
@@ -818,7 +825,7 @@ def main():
     ap.add_argument("--grid", type=int, default=GRID, help="stencil grid edge (64 = the benchmark config; "
                     "smaller values only for profiling captures)")
     ap.add_argument("--profile", choices=["dasp", "cg_fp64", "cg_f16", "spmm", "batch", "smat_tc", "smat_mma", "csr",
-                                          "pcg_bj", "spmm_grouped"],
+                                          "pcg_bj", "spmm_grouped", "cg_multi"],
                     help="a few calls of one workload's kernels (for ncu captures)")
     args = ap.parse_args()
     if args.profile:
