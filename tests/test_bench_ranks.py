@@ -1,6 +1,8 @@
 """bench.py's multi-rank logic on CPU: two gloo ranks (127.0.0.1), each with
 its own step time; both see the slowest rank's time and the whole-job value
-counts the work of both replicas (weak scaling)."""
+counts the work of both replicas (weak scaling).  The reference arm on a
+small stencil: exactly K timed steps, a named row sample when K full SpMVs
+would exceed its time budget, and no line from other ranks."""
 import os
 import socket
 import sys
@@ -51,3 +53,32 @@ def test_single_rank_is_a_no_op():
     import bench
     assert bench.max_over_ranks(3.5, 1, None) == 3.5
     assert bench.job_gflops(1, 1e9, 10, 1000.0) == pytest.approx(10.0)
+
+
+def _reference_line(capsys, monkeypatch, budget, steps, warmup, rank=0):
+    import argparse
+    import json
+    sys.path.insert(0, str(ROOT))
+    import bench
+    monkeypatch.setattr(bench, "REF_ARM_SECONDS", budget)
+    bench.run_reference(argparse.Namespace(grid=8, warmup=warmup, steps=steps, gpus=1), 1, rank)
+    out = capsys.readouterr().out.strip()
+    return json.loads(out.splitlines()[-1]) if out else None
+
+
+def test_reference_arm_times_exactly_k_full_steps(capsys, monkeypatch):
+    d = _reference_line(capsys, monkeypatch, 120.0, 7, 2)
+    assert d["impl"] == "reference" and d["steps"] == 7 and d["warmup"] == 2
+    assert d["cpu_baseline"]["sample"].startswith("full matrix per step")
+    assert d["value"] > 0 and d["e2e"]["value"] == d["value"] == d["cpu_baseline"]["value"]
+    assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
+
+
+def test_reference_arm_samples_rows_when_k_steps_exceed_the_budget(capsys, monkeypatch):
+    d = _reference_line(capsys, monkeypatch, 1e-9, 5, 1)
+    assert d["steps"] == 5 and d["cpu_baseline"]["sample"].startswith("first ")
+    assert "5 timed steps after 1 untimed" in d["cpu_baseline"]["sample"]
+
+
+def test_reference_arm_other_ranks_print_nothing(capsys, monkeypatch):
+    assert _reference_line(capsys, monkeypatch, 120.0, 3, 1, rank=1) is None
