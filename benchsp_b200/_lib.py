@@ -243,6 +243,10 @@ _PROTOS.update({
     "bsp_permute_csr": (C.c_int, [_I32, _I32, _P, _P, _P, _P, _P, _P, _P, _P]),
     "bsp_reorder_rcm_host": (C.c_int, [_I32, _I32, _P, _P, _P]),
     "bsp_permute_csr_host": (C.c_int, [_I32, _I32, _P, _P, _P, _P, _P, _P, _P]),
+    "bsp_reorder_similarity": (C.c_int, [_I32, _I32, _I32, _P, _P, _I32, _I32, _P, _P]),
+    "bsp_reorder_similarity_host": (C.c_int, [_I32, _I32, _I32, _P, _P, _I32, _I32, _P]),
+    "bsp_permute_rows_csr": (C.c_int, [_I32, _I32, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "bsp_permute_rows_csr_host": (C.c_int, [_I32, _I32, _P, _P, _P, _P, _P, _P, _P]),
 })
 
 _PROTOS.update({

@@ -886,6 +886,53 @@ def reorder_rcm(rowptr, colidx, stream=None):
     return perm
 
 
+def reorder_similarity_host(rowptr: np.ndarray, colidx: np.ndarray, cols: int, group_rows: int = 16,
+                            block_cols: int = 16) -> np.ndarray:
+    """Row-similarity permutation (perm[new] = old) of host CSR arrays: rows
+    with similar column-block sets land in the same group of group_rows."""
+    rowptr = np.ascontiguousarray(rowptr, np.int32)
+    colidx = np.ascontiguousarray(colidx, np.int32)
+    perm = np.empty(rowptr.size - 1, np.int32)
+    check(lib().bsp_reorder_similarity_host(perm.size, cols, colidx.size, _np_ptr(rowptr), _np_ptr(colidx),
+                                            group_rows, block_cols, _np_ptr(perm)))
+    return perm
+
+
+def permute_rows_csr_host(A: "HostCSR", perm: np.ndarray) -> "HostCSR":
+    """P A (rows only) of a host CSR matrix."""
+    perm = np.ascontiguousarray(perm, np.int32)
+    rp = np.empty(A.rows + 1, np.int32)
+    ci = np.empty(A.nnz, np.int32)
+    va = np.empty(A.nnz, np.float64)
+    check(lib().bsp_permute_rows_csr_host(A.rows, A.nnz, _np_ptr(np.ascontiguousarray(A.rowptr, np.int32)),
+                                          _np_ptr(np.ascontiguousarray(A.colidx, np.int32)),
+                                          _np_ptr(np.ascontiguousarray(A.values, np.float64)), _np_ptr(perm),
+                                          _np_ptr(rp), _np_ptr(ci), _np_ptr(va)))
+    return HostCSR(A.rows, A.cols, rp, ci, va)
+
+
+def reorder_similarity(rowptr, colidx, cols: int, group_rows: int = 16, block_cols: int = 16, stream=None):
+    """Device form of reorder_similarity_host: perm as an int32 tensor."""
+    torch = _torch()
+    perm = torch.empty(rowptr.numel() - 1, dtype=torch.int32, device=rowptr.device)
+    check(lib().bsp_reorder_similarity(perm.numel(), cols, colidx.numel(), _dptr(rowptr, "rowptr"),
+                                       _dptr(colidx, "colidx"), group_rows, block_cols, _dptr(perm, "perm"),
+                                       _stream(stream)))
+    return perm
+
+
+def permute_rows_csr(rowptr, colidx, values, perm, stream=None):
+    """Device form of P A (rows only); returns (rowptr, colidx, values)."""
+    torch = _torch()
+    rp = torch.empty_like(rowptr)
+    ci = torch.empty_like(colidx)
+    va = torch.empty_like(values)
+    check(lib().bsp_permute_rows_csr(perm.numel(), colidx.numel(), _dptr(rowptr, "rowptr"), _dptr(colidx, "colidx"),
+                                     _dptr(values, "values"), _dptr(perm, "perm"), _dptr(rp, "out_rowptr"),
+                                     _dptr(ci, "out_colidx"), _dptr(va, "out_values"), _stream(stream)))
+    return rp, ci, va
+
+
 def permute_csr(rowptr, colidx, values, perm, stream=None):
     """Device form of P A P^T; returns (rowptr, colidx, values) tensors."""
     torch = _torch()

@@ -173,6 +173,153 @@ void permute(int32_t n, const int32_t *rp, const int32_t *ci, const double *va, 
   }
 }
 
+// Row-similarity order for tile formats: rows whose nonzeros fall in the
+// same column blocks are placed in the same group of `G` consecutive rows,
+// so a G x BC tiling of the reordered matrix needs few tiles.  Signature of
+// a row = its distinct column blocks (col / BC), ascending.  A group starts
+// at the first unplaced row (row order) and grows one row at a time: the
+// candidates are the unplaced rows that share a block with the group's
+// union of blocks U, found through an inverted index (block -> rows,
+// ascending).  The scans are bounded: a joining row's new blocks are read
+// shortest list first (rare blocks say the most), at most kScanBlocks blocks
+// and kScanEntries entries per block, until a group has kTouched
+// candidates.  The next row is the candidate of highest Jaccard similarity
+// |S_c & U| / |S_c | U| (ties by row index; compared by exact integer
+// cross-multiplication), and its blocks join U.  A group left short is
+// filled with the next unplaced rows in row order.  Empty rows go last.
+// Deterministic; O(nnz log) for the signatures plus O(rows * kTouched) for
+// the grouping.
+constexpr int32_t kScanBlocks = 64;
+constexpr int64_t kScanEntries = 1024;
+constexpr size_t kTouched = 2048;
+
+void similarity_order(int32_t n, int32_t cols, const int32_t *rp, const int32_t *ci, int32_t G, int32_t BC,
+                      int32_t *perm) {
+  const int32_t nb = (int32_t)(((int64_t)cols + BC - 1) / BC);
+  std::vector<int32_t> len(n);
+#pragma omp parallel
+  {
+    std::vector<int32_t> t;
+#pragma omp for schedule(dynamic, 1024)
+    for (int32_t i = 0; i < n; ++i) {
+      t.assign(ci + rp[i], ci + rp[i + 1]);
+      for (int32_t &c : t) c /= BC;
+      std::sort(t.begin(), t.end());
+      len[i] = (int32_t)(std::unique(t.begin(), t.end()) - t.begin());
+    }
+  }
+  std::vector<int64_t> sp(n + 1, 0);
+  for (int32_t i = 0; i < n; ++i) sp[i + 1] = sp[i] + len[i];
+  std::vector<int32_t> sig(sp[n]);
+#pragma omp parallel
+  {
+    std::vector<int32_t> t;
+#pragma omp for schedule(dynamic, 1024)
+    for (int32_t i = 0; i < n; ++i) {
+      t.assign(ci + rp[i], ci + rp[i + 1]);
+      for (int32_t &c : t) c /= BC;
+      std::sort(t.begin(), t.end());
+      t.erase(std::unique(t.begin(), t.end()), t.end());
+      std::copy(t.begin(), t.end(), sig.begin() + sp[i]);
+    }
+  }
+  // inverted index, rows ascending within a block
+  std::vector<int64_t> bp(nb + 1, 0);
+  for (int64_t k = 0; k < sp[n]; ++k) ++bp[sig[k] + 1];
+  for (int32_t b = 0; b < nb; ++b) bp[b + 1] += bp[b];
+  std::vector<int32_t> brow(sp[n]);
+  {
+    std::vector<int64_t> fill(bp.begin(), bp.end() - 1);
+    for (int32_t i = 0; i < n; ++i)
+      for (int64_t k = sp[i]; k < sp[i + 1]; ++k) brow[fill[sig[k]]++] = i;
+  }
+  std::vector<int64_t> head(bp.begin(), bp.end() - 1);
+  std::vector<char> placed(n, 0);
+  std::vector<int32_t> shared(n, 0), touched, fresh, in_u(nb, -1);
+  int32_t out = 0, next = 0, group = 0;
+  auto place = [&](int32_t r) {
+    placed[r] = 1;
+    perm[out++] = r;
+  };
+  auto next_unplaced = [&]() {
+    while (next < n && (placed[next] || len[next] == 0)) ++next;
+    return next;
+  };
+  while (next_unplaced() < n) {
+    int64_t ulen = 0;
+    int32_t scanned = 0, size = 0;
+    touched.clear();
+    // row r joins the group: its new blocks join U and bring their rows in
+    auto join = [&](int32_t r) {
+      place(r);
+      ++size;
+      fresh.clear();
+      for (int64_t k = sp[r]; k < sp[r + 1]; ++k) {
+        const int32_t b = sig[k];
+        if (in_u[b] == group) continue;
+        in_u[b] = group;
+        ++ulen;
+        fresh.push_back(b);
+      }
+      std::sort(fresh.begin(), fresh.end(), [&](int32_t a, int32_t b) {
+        const int64_t la = bp[a + 1] - head[a], lb = bp[b + 1] - head[b];
+        return la != lb ? la < lb : a < b;
+      });
+      for (int32_t b : fresh) {
+        if (scanned >= kScanBlocks || touched.size() >= kTouched) break;
+        ++scanned;
+        while (head[b] < bp[b + 1] && placed[brow[head[b]]]) ++head[b];
+        for (int64_t e = head[b], lim = std::min<int64_t>(bp[b + 1], head[b] + kScanEntries); e < lim; ++e) {
+          const int32_t c = brow[e];
+          if (placed[c]) continue;
+          if (shared[c]++ == 0) {
+            touched.push_back(c);
+            if (touched.size() >= kTouched) break;
+          }
+        }
+      }
+    };
+    join(next);
+    while (size < G) {
+      // highest |S_c & U| / (|U| + |S_c| - |S_c & U|), then lower index
+      int32_t best = -1;
+      for (int32_t c : touched) {
+        if (placed[c]) continue;
+        if (best < 0) {
+          best = c;
+          continue;
+        }
+        const int64_t sc = shared[c], sb = shared[best];
+        const int64_t lhs = sc * (ulen + len[best] - sb), rhs = sb * (ulen + len[c] - sc);
+        if (lhs > rhs || (lhs == rhs && c < best)) best = c;
+      }
+      if (best < 0) break;
+      join(best);
+    }
+    for (int32_t c : touched) shared[c] = 0;
+    while (size < G && next_unplaced() < n) {
+      place(next);
+      ++size;
+    }
+    ++group;
+  }
+  for (int32_t i = 0; i < n; ++i)
+    if (!placed[i]) place(i);  // the empty rows
+}
+
+// P A (rows only): new row i = old row perm[i], its entries as stored.
+void permute_rows(int32_t n, const int32_t *rp, const int32_t *ci, const double *va, const int32_t *perm,
+                  int32_t *orp, int32_t *oci, double *ova) {
+  orp[0] = 0;
+  for (int32_t i = 0; i < n; ++i) orp[i + 1] = orp[i] + (rp[perm[i] + 1] - rp[perm[i]]);
+#pragma omp parallel for schedule(dynamic, 1024)
+  for (int32_t i = 0; i < n; ++i) {
+    const int32_t o = perm[i], m = rp[o + 1] - rp[o];
+    std::copy(ci + rp[o], ci + rp[o] + m, oci + orp[i]);
+    if (ova) std::copy(va + rp[o], va + rp[o] + m, ova + orp[i]);
+  }
+}
+
 bool valid_csr(int32_t n, int32_t nnz, const int32_t *rp) {
   if (rp[0] != 0 || rp[n] != nnz) return false;
   for (int32_t i = 0; i < n; ++i)
@@ -258,5 +405,69 @@ extern "C" bsp_status bsp_permute_csr(int32_t rows, int32_t nnz, const int32_t *
   if (st != BSP_OK) return st;
   if (!h2d(outRowPtr, orp) || !h2d(outColIdx, oci) || (values && outValues && !h2d(outValues, ova)))
     return fail(BSP_ERR_CUDA, "bsp_permute_csr: copy to the device failed");
+  return BSP_OK;
+}
+
+extern "C" bsp_status bsp_reorder_similarity_host(int32_t rows, int32_t cols, int32_t nnz, const int32_t *rowPtr,
+                                                  const int32_t *colIdx, int32_t group_rows, int32_t block_cols,
+                                                  int32_t *perm) {
+  bsp::clear_error();
+  if (rows < 0 || cols < 0 || nnz < 0 || !rowPtr || !perm || (nnz > 0 && !colIdx))
+    return fail(BSP_ERR_INVALID, "bsp_reorder_similarity: bad argument");
+  if (group_rows < 1 || group_rows > 4096 || block_cols < 1)
+    return fail(BSP_ERR_INVALID, "bsp_reorder_similarity: group_rows must be in [1, 4096], block_cols >= 1");
+  if (!valid_csr(rows, nnz, rowPtr)) return fail(BSP_ERR_INVALID, "bsp_reorder_similarity: malformed row pointers");
+  for (int32_t j = 0; j < nnz; ++j)
+    if (colIdx[j] < 0 || colIdx[j] >= cols) return fail(BSP_ERR_INVALID, "bsp_reorder_similarity: column out of range");
+  if (rows > 0) similarity_order(rows, cols, rowPtr, colIdx, group_rows, block_cols, perm);
+  return BSP_OK;
+}
+
+extern "C" bsp_status bsp_permute_rows_csr_host(int32_t rows, int32_t nnz, const int32_t *rowPtr,
+                                                const int32_t *colIdx, const double *values, const int32_t *perm,
+                                                int32_t *outRowPtr, int32_t *outColIdx, double *outValues) {
+  bsp::clear_error();
+  if (rows < 0 || nnz < 0 || !rowPtr || !perm || !outRowPtr || (nnz > 0 && (!colIdx || !outColIdx)))
+    return fail(BSP_ERR_INVALID, "bsp_permute_rows_csr: bad argument");
+  if (!valid_csr(rows, nnz, rowPtr)) return fail(BSP_ERR_INVALID, "bsp_permute_rows_csr: malformed row pointers");
+  if (!valid_perm(rows, perm)) return fail(BSP_ERR_INVALID, "bsp_permute_rows_csr: perm is not a permutation");
+  permute_rows(rows, rowPtr, colIdx, values && outValues ? values : nullptr, perm, outRowPtr, outColIdx,
+               values && outValues ? outValues : nullptr);
+  return BSP_OK;
+}
+
+extern "C" bsp_status bsp_reorder_similarity(int32_t rows, int32_t cols, int32_t nnz, const int32_t *rowPtr,
+                                             const int32_t *colIdx, int32_t group_rows, int32_t block_cols,
+                                             int32_t *perm, bsp_stream_t stream) {
+  bsp::clear_error();
+  if (rows < 0 || nnz < 0) return fail(BSP_ERR_INVALID, "bsp_reorder_similarity: negative size");
+  if (cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(stream)) != cudaSuccess)
+    return fail(BSP_ERR_CUDA, "bsp_reorder_similarity: stream synchronize failed");
+  std::vector<int32_t> rp, ci, p(rows > 0 ? rows : 0);
+  if (!d2h(rp, rowPtr, (size_t)rows + 1) || !d2h(ci, colIdx, (size_t)nnz))
+    return fail(BSP_ERR_CUDA, "bsp_reorder_similarity: copy to the host failed");
+  const bsp_status st =
+      bsp_reorder_similarity_host(rows, cols, nnz, rp.data(), ci.data(), group_rows, block_cols, p.data());
+  if (st != BSP_OK) return st;
+  return h2d(perm, p) ? BSP_OK : fail(BSP_ERR_CUDA, "bsp_reorder_similarity: copy to the device failed");
+}
+
+extern "C" bsp_status bsp_permute_rows_csr(int32_t rows, int32_t nnz, const int32_t *rowPtr, const int32_t *colIdx,
+                                           const double *values, const int32_t *perm, int32_t *outRowPtr,
+                                           int32_t *outColIdx, double *outValues, bsp_stream_t stream) {
+  bsp::clear_error();
+  if (rows < 0 || nnz < 0) return fail(BSP_ERR_INVALID, "bsp_permute_rows_csr: negative size");
+  if (cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(stream)) != cudaSuccess)
+    return fail(BSP_ERR_CUDA, "bsp_permute_rows_csr: stream synchronize failed");
+  std::vector<int32_t> rp, ci, p, orp((size_t)rows + 1), oci(nnz);
+  std::vector<double> va, ova(values ? nnz : 0);
+  if (!d2h(rp, rowPtr, (size_t)rows + 1) || !d2h(ci, colIdx, (size_t)nnz) || !d2h(p, perm, (size_t)rows) ||
+      (values && !d2h(va, values, (size_t)nnz)))
+    return fail(BSP_ERR_CUDA, "bsp_permute_rows_csr: copy to the host failed");
+  const bsp_status st = bsp_permute_rows_csr_host(rows, nnz, rp.data(), ci.data(), values ? va.data() : nullptr,
+                                                  p.data(), orp.data(), oci.data(), values ? ova.data() : nullptr);
+  if (st != BSP_OK) return st;
+  if (!h2d(outRowPtr, orp) || !h2d(outColIdx, oci) || (values && outValues && !h2d(outValues, ova)))
+    return fail(BSP_ERR_CUDA, "bsp_permute_rows_csr: copy to the device failed");
   return BSP_OK;
 }

@@ -553,6 +553,34 @@ bsp_status bsp_permute_csr_host(int32_t rows, int32_t nnz, const int32_t *rowPtr
                                 const int32_t *colIdx, const double *values,
                                 const int32_t *perm, int32_t *outRowPtr,
                                 int32_t *outColIdx, double *outValues);
+/* Row-similarity order for tile formats (SMaT 16x16 tiles, BSR blocks): rows
+ * whose nonzeros fall in the same `block_cols`-wide column blocks are put in
+ * the same group of `group_rows` consecutive rows; perm[new] = old.  Rows are
+ * grouped greedily by the Jaccard similarity of their column-block sets
+ * (seeds in row order, candidates from an inverted index with bounded
+ * scans, ties by row index; empty rows last), so it is deterministic.  For
+ * rectangular matrices too: apply it with bsp_permute_rows_csr (P A) and
+ * read row i of the product as original row perm[i].  Host code; the device
+ * form copies in and out and waits for `stream`. */
+bsp_status bsp_reorder_similarity(int32_t rows, int32_t cols, int32_t nnz,
+                                  const int32_t *rowPtr, const int32_t *colIdx,
+                                  int32_t group_rows, int32_t block_cols,
+                                  int32_t *perm, bsp_stream_t stream);
+bsp_status bsp_reorder_similarity_host(int32_t rows, int32_t cols, int32_t nnz,
+                                       const int32_t *rowPtr, const int32_t *colIdx,
+                                       int32_t group_rows, int32_t block_cols,
+                                       int32_t *perm);
+/* P A, rows only (new row i = old row perm[i], its entries as stored; any
+ * column count); values may be NULL (pattern only). */
+bsp_status bsp_permute_rows_csr(int32_t rows, int32_t nnz, const int32_t *rowPtr,
+                                const int32_t *colIdx, const double *values,
+                                const int32_t *perm, int32_t *outRowPtr,
+                                int32_t *outColIdx, double *outValues,
+                                bsp_stream_t stream);
+bsp_status bsp_permute_rows_csr_host(int32_t rows, int32_t nnz, const int32_t *rowPtr,
+                                     const int32_t *colIdx, const double *values,
+                                     const int32_t *perm, int32_t *outRowPtr,
+                                     int32_t *outColIdx, double *outValues);
 
 /* ---------------------------------------------------------------------- */
 /* Format autotuner for FP64 SpMV (no reference counterpart: the reference's

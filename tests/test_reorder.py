@@ -95,3 +95,104 @@ def test_device_reorder_matches_host_and_raises_tile_fill(cuda):
     assert np.allclose(Y1, Y0[perm.cpu().numpy()], rtol=1e-4, atol=1e-4)
     before.free()
     after.free()
+
+
+# --- row-similarity order -------------------------------------------------
+
+def _grouped(groups, blocks, nblocks, seed, keep=1.0, G=16, BC=16):
+    """groups x G rows; the rows of a group draw from the same `blocks`
+    column blocks (each block kept with probability `keep`, at least one);
+    rows then shuffled.  Returns (scrambled, original) HostCSR."""
+    rng = np.random.default_rng(seed)
+    rows, cols, vals = [], [], []
+    for g in range(groups):
+        bset = np.sort(rng.choice(nblocks, blocks, replace=False))
+        for r in range(G):
+            kept = bset[rng.random(blocks) < keep]
+            if kept.size == 0:
+                kept = bset[:1]
+            c = (kept[:, None] * BC + np.arange(BC)[None, :]).ravel()
+            rows.append(np.full(c.size, g * G + r))
+            cols.append(c)
+            vals.append(rng.uniform(-1, 1, c.size))
+    M = sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
+                      shape=(groups * G, nblocks * BC))
+    M.sort_indices()
+    p = np.random.default_rng(seed + 1).permutation(M.shape[0])
+    S = M[p].tocsr()
+    S.sort_indices()
+    mk = lambda X: bsp.HostCSR(X.shape[0], X.shape[1], X.indptr.astype(np.int32), X.indices.astype(np.int32),
+                               X.data.copy())
+    return mk(S), mk(M)
+
+
+def _tiles(A, G=16, BC=16):
+    r = np.repeat(np.arange(A.rows), np.diff(A.rowptr)) // G
+    return np.unique(r.astype(np.int64) * (A.cols // BC + 1) + A.colidx // BC).size
+
+
+def test_similarity_regroups_scrambled_tiles_exactly():
+    S, M = _grouped(256, 6, 1024, 11)
+    assert _tiles(S) > 10 * _tiles(M)
+    perm = bsp.reorder_similarity_host(S.rowptr, S.colidx, S.cols)
+    assert np.array_equal(np.sort(perm), np.arange(S.rows))
+    R = bsp.permute_rows_csr_host(S, perm)
+    assert _tiles(R) == _tiles(M) == 256 * 6
+    assert np.array_equal(perm, bsp.reorder_similarity_host(S.rowptr, S.colidx, S.cols))   # deterministic
+
+
+def test_similarity_groups_noisy_rows():
+    S, M = _grouped(300, 8, 2048, 12, keep=0.7)
+    R = bsp.permute_rows_csr_host(S, bsp.reorder_similarity_host(S.rowptr, S.colidx, S.cols))
+    assert _tiles(R) <= 1.25 * _tiles(M) and _tiles(S) > 5 * _tiles(R), (_tiles(S), _tiles(R), _tiles(M))
+
+
+def test_permute_rows_is_row_indexing():
+    S, _ = _grouped(20, 3, 64, 13)
+    perm = np.random.default_rng(3).permutation(S.rows).astype(np.int32)
+    R = bsp.permute_rows_csr_host(S, perm)
+    ref = _scipy(S)[perm].tocsr()
+    assert np.array_equal(R.rowptr, ref.indptr) and np.array_equal(R.colidx, ref.indices)
+    assert np.array_equal(R.values, ref.data) and (R.rows, R.cols) == (S.rows, S.cols)
+
+
+def test_similarity_group_size_empty_rows_and_bad_input():
+    S, M = _grouped(40, 4, 100, 14, G=8, BC=8)
+    perm = bsp.reorder_similarity_host(S.rowptr, S.colidx, S.cols, group_rows=8, block_cols=8)
+    assert _tiles(bsp.permute_rows_csr_host(S, perm), 8, 8) == _tiles(M, 8, 8)
+    # empty rows (3 of them) are placed last, in row order
+    rp = np.array([0, 2, 2, 3, 3, 5, 5], np.int32)
+    ci = np.array([0, 17, 1, 16, 18], np.int32)
+    perm = bsp.reorder_similarity_host(rp, ci, 32, group_rows=2)
+    assert np.array_equal(np.sort(perm), np.arange(6)) and list(perm[3:]) == [1, 3, 5]
+    assert bsp.reorder_similarity_host(np.zeros(1, np.int32), np.zeros(0, np.int32), 0).size == 0
+    for bad in (dict(group_rows=0), dict(block_cols=0)):
+        with pytest.raises(bsp.BspError):
+            bsp.reorder_similarity_host(rp, ci, 32, **bad)
+    with pytest.raises(bsp.BspError):
+        bsp.reorder_similarity_host(rp, ci, 18)                                          # column 18 >= cols
+    with pytest.raises(bsp.BspError):
+        bsp.permute_rows_csr_host(S, np.zeros(S.rows, np.int32))                         # not a permutation
+
+
+@pytest.mark.gpu
+def test_device_similarity_matches_host_and_densifies_tiles(cuda):
+    import torch
+    S, M = _grouped(2048, 6, 4096, 15)                   # 32,768 rows, scrambled dense 16x16 tiles
+    rp, ci, va = (torch.from_numpy(a).to(cuda) for a in (S.rowptr, S.colidx, S.values))
+    perm = bsp.reorder_similarity(rp, ci, S.cols)
+    assert np.array_equal(perm.cpu().numpy(), bsp.reorder_similarity_host(S.rowptr, S.colidx, S.cols))
+    rp2, ci2, va2 = bsp.permute_rows_csr(rp, ci, va, perm)
+    R = bsp.permute_rows_csr_host(S, perm.cpu().numpy())
+    assert np.array_equal(rp2.cpu().numpy(), R.rowptr) and np.array_equal(ci2.cpu().numpy(), R.colidx)
+    assert np.array_equal(va2.cpu().numpy(), R.values)
+    before = bsp.SmatMatrix(rp, ci, va, rows=S.rows, cols=S.cols, dtype="f16")
+    after = bsp.SmatMatrix(rp2, ci2, va2, rows=S.rows, cols=S.cols, dtype="f16")
+    assert after.fill == 1.0 and after.fill > 10 * before.fill, (before.fill, after.fill)
+    # (P A) X = P (A X): row i of the reordered product is row perm[i]
+    X = (torch.rand(S.cols, 128, generator=torch.Generator().manual_seed(2)) * 2 - 1).half().to(cuda)
+    Y0 = before.spmm(X).cpu().numpy()
+    Y1 = after.spmm(X).cpu().numpy()
+    assert np.allclose(Y1, Y0[perm.cpu().numpy()], rtol=1e-4, atol=1e-4)
+    before.free()
+    after.free()
