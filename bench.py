@@ -732,6 +732,7 @@ def run_reorder_similarity(bsp, dev, up) -> None:
     reorder_s = time.perf_counter() - t0
     R = bsp.permute_rows_csr_host(S, perm)
     N = 128
+    choice, _ = bsp.choose_spmm_host(S, N)
     B = (torch.rand(S.cols, N, generator=torch.Generator().manual_seed(3)) * 2 - 1).half().to(dev)
     res, C = {}, {}
     for name, M in (("shuffled", S), ("reordered", R)):
@@ -755,7 +756,9 @@ def run_reorder_similarity(bsp, dev, up) -> None:
                                                        res["reordered"]["smat_tcgen05_ms"], 2),
           speedup_vs_shuffled_best=round(min(res["shuffled"]["smat_tcgen05_ms"], res["shuffled"]["csr_grouped_ms"]) /
                                          res["reordered"]["smat_tcgen05_ms"], 2),
-          product_rows_match=same)
+          product_rows_match=same,
+          engine_choice={k: choice[k] for k in ("engine", "smat_path", "reorder", "est_seconds_smat_given",
+                                                "est_seconds_smat_reordered", "est_seconds_csr")})
 
 
 def run_mtx_read(bsp, dev) -> None:

@@ -177,6 +177,16 @@ class BspCgOptions(C.Structure):
                 ("precond_block", C.c_int32), ("refine", C.c_int32)]
 
 
+class BspSpmmChoice(C.Structure):
+    _fields_ = [("engine", C.c_int32), ("smat_path", C.c_int32), ("reorder", C.c_int32), ("reserved", C.c_int32),
+                ("tiles_given", C.c_int64), ("tiles_reordered", C.c_int64),
+                ("est_seconds_smat_given", C.c_double), ("est_seconds_smat_reordered", C.c_double),
+                ("est_seconds_csr", C.c_double)]
+
+
+BSP_SPMM_ENGINE_CSR, BSP_SPMM_ENGINE_SMAT = 0, 1
+
+
 class BspCgResult(C.Structure):
     """Mirror of bsp_cg_result (include/bsp.h)."""
     _fields_ = [("iterations", C.c_int32), ("reliable_updates", C.c_int32), ("rel_residual", C.c_double),
@@ -247,6 +257,7 @@ _PROTOS.update({
     "bsp_reorder_similarity_host": (C.c_int, [_I32, _I32, _I32, _P, _P, _I32, _I32, _P]),
     "bsp_permute_rows_csr": (C.c_int, [_I32, _I32, _P, _P, _P, _P, _P, _P, _P, _P]),
     "bsp_permute_rows_csr_host": (C.c_int, [_I32, _I32, _P, _P, _P, _P, _P, _P, _P]),
+    "bsp_spmm_choose_host": (C.c_int, [_I32, _I32, _I32, _P, _P, _I32, _P, C.POINTER(BspSpmmChoice)]),
 })
 
 _PROTOS.update({

@@ -320,6 +320,38 @@ void permute_rows(int32_t n, const int32_t *rp, const int32_t *ci, const double 
   }
 }
 
+// 16 x 16 tiles of A with its rows in the order `perm` (null: as given):
+// the distinct column blocks of every 16-row block, summed.
+int64_t count_tiles(int32_t n, const int32_t *rp, const int32_t *ci, const int32_t *perm) {
+  const int32_t nbr = (int32_t)(((int64_t)n + 15) / 16);
+  int64_t total = 0;
+#pragma omp parallel reduction(+ : total)
+  {
+    std::vector<int32_t> t;
+#pragma omp for schedule(dynamic, 256)
+    for (int32_t br = 0; br < nbr; ++br) {
+      t.clear();
+      for (int32_t i = br * 16; i < std::min<int32_t>(n, br * 16 + 16); ++i) {
+        const int32_t r = perm ? perm[i] : i;
+        for (int32_t j = rp[r]; j < rp[r + 1]; ++j) t.push_back(ci[j] >> 4);
+      }
+      std::sort(t.begin(), t.end());
+      total += (int64_t)(std::unique(t.begin(), t.end()) - t.begin());
+    }
+  }
+  return total;
+}
+
+// SpMM engine cost model, seconds per unit per column of B, from the B200
+// measurements of the SMaT and grouped CSR SpMM at N = 128 (dense-tile and
+// row-shuffled 524,288-row matrices, power-law graph): tcgen05 tiles cost
+// 0.86-0.91 ns per tile (7.0e-12 s per tile-column), mma.sync tiles 1.6x
+// that, the grouped CSR kernel 1.93 ms for 67.1M nonzeros (2.3e-13 s per
+// nonzero-column).
+constexpr double kTileColSecTc = 7.0e-12;
+constexpr double kTileColSecMma = 1.12e-11;
+constexpr double kNnzColSecCsr = 2.3e-13;
+
 bool valid_csr(int32_t n, int32_t nnz, const int32_t *rp) {
   if (rp[0] != 0 || rp[n] != nnz) return false;
   for (int32_t i = 0; i < n; ++i)
@@ -469,5 +501,40 @@ extern "C" bsp_status bsp_permute_rows_csr(int32_t rows, int32_t nnz, const int3
   if (st != BSP_OK) return st;
   if (!h2d(outRowPtr, orp) || !h2d(outColIdx, oci) || (values && outValues && !h2d(outValues, ova)))
     return fail(BSP_ERR_CUDA, "bsp_permute_rows_csr: copy to the device failed");
+  return BSP_OK;
+}
+
+extern "C" bsp_status bsp_spmm_choose_host(int32_t rows, int32_t cols, int32_t nnz, const int32_t *rowPtr,
+                                           const int32_t *colIdx, int32_t N, int32_t *perm, bsp_spmm_choice *out) {
+  bsp::clear_error();
+  if (rows < 0 || cols < 0 || nnz < 0 || N <= 0 || !rowPtr || !out || (nnz > 0 && !colIdx))
+    return fail(BSP_ERR_INVALID, "bsp_spmm_choose: bad argument");
+  if (!valid_csr(rows, nnz, rowPtr)) return fail(BSP_ERR_INVALID, "bsp_spmm_choose: malformed row pointers");
+  for (int32_t j = 0; j < nnz; ++j)
+    if (colIdx[j] < 0 || colIdx[j] >= cols) return fail(BSP_ERR_INVALID, "bsp_spmm_choose: column out of range");
+  bsp_spmm_choice c{};
+  const bool smat_ok = N % 32 == 0;
+  c.smat_path = N % 128 == 0 ? BSP_SMAT_TCGEN05 : BSP_SMAT_MMA_SYNC;
+  const double per_tile = (N % 128 == 0 ? kTileColSecTc : kTileColSecMma) * N;
+  c.tiles_given = count_tiles(rows, rowPtr, colIdx, nullptr);
+  c.tiles_reordered = -1;
+  if (perm && rows > 0) {
+    similarity_order(rows, cols, rowPtr, colIdx, 16, 16, perm);
+    c.tiles_reordered = count_tiles(rows, rowPtr, colIdx, perm);
+  }
+  c.est_seconds_csr = kNnzColSecCsr * N * (double)nnz;
+  c.est_seconds_smat_given = smat_ok ? per_tile * (double)c.tiles_given : -1.0;
+  c.est_seconds_smat_reordered = smat_ok && c.tiles_reordered >= 0 ? per_tile * (double)c.tiles_reordered : -1.0;
+  c.engine = BSP_SPMM_ENGINE_CSR;
+  double best = c.est_seconds_csr;
+  if (smat_ok && c.est_seconds_smat_given < best) {
+    best = c.est_seconds_smat_given;
+    c.engine = BSP_SPMM_ENGINE_SMAT;
+  }
+  if (c.est_seconds_smat_reordered >= 0 && c.est_seconds_smat_reordered < best) {
+    c.engine = BSP_SPMM_ENGINE_SMAT;
+    c.reorder = 1;
+  }
+  *out = c;
   return BSP_OK;
 }

@@ -570,6 +570,28 @@ bsp_status bsp_reorder_similarity_host(int32_t rows, int32_t cols, int32_t nnz,
                                        const int32_t *rowPtr, const int32_t *colIdx,
                                        int32_t group_rows, int32_t block_cols,
                                        int32_t *perm);
+/* SpMM engine choice for C = A B with N columns of B, sharing the
+ * reordering with the SMaT path: counts the 16x16 tiles of A as given and,
+ * when `perm` (rows entries) is not NULL, after bsp_reorder_similarity
+ * (written to perm), and estimates each engine from B200 measurements
+ * (SMaT time per tile, grouped CSR time per nonzero, both per column of B).
+ * engine = BSP_SPMM_ENGINE_SMAT (build the SMaT matrix from the rows in
+ * perm order when reorder = 1, and read row i of C as original row perm[i];
+ * smat_path says which tile path) or BSP_SPMM_ENGINE_CSR (bsp_spmm_csr on A
+ * as given).  SMaT needs N % 32 == 0; the estimates are -1 where an engine
+ * does not apply.  Host code, a one-time decision per matrix. */
+enum { BSP_SPMM_ENGINE_CSR = 0, BSP_SPMM_ENGINE_SMAT = 1 };
+typedef struct bsp_spmm_choice {
+  int32_t engine;
+  int32_t smat_path;   /* BSP_SMAT_TCGEN05 (N % 128 == 0) or BSP_SMAT_MMA_SYNC */
+  int32_t reorder;     /* 1: the SMaT matrix is built from the rows in perm order */
+  int32_t reserved;
+  int64_t tiles_given, tiles_reordered;   /* tiles_reordered = -1 without perm */
+  double est_seconds_smat_given, est_seconds_smat_reordered, est_seconds_csr;
+} bsp_spmm_choice;
+bsp_status bsp_spmm_choose_host(int32_t rows, int32_t cols, int32_t nnz,
+                                const int32_t *rowPtr, const int32_t *colIdx,
+                                int32_t N, int32_t *perm, bsp_spmm_choice *out);
 /* P A, rows only (new row i = old row perm[i], its entries as stored; any
  * column count); values may be NULL (pattern only). */
 bsp_status bsp_permute_rows_csr(int32_t rows, int32_t nnz, const int32_t *rowPtr,

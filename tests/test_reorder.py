@@ -1,7 +1,11 @@
 """Reverse Cuthill-McKee reordering and symmetric permutation: valid
 permutations, bandwidth as small as scipy's RCM, P A P^T exact, components
 and edge cases on the host; on the GPU the device forms agree with the host
-forms and reordering a scrambled stencil raises the SMaT 16x16 tile fill."""
+forms and reordering a scrambled stencil raises the SMaT 16x16 tile fill.
+Row-similarity order: row-shuffled tile matrices regrouped to the original
+tile count, noisy groups, P A exact, group sizes, empty rows, bad input, and
+the SpMM engine choice that uses it; on the GPU the device forms agree and
+the reordered SMaT product is the shuffled one with rows permuted."""
 import numpy as np
 import pytest
 import scipy.sparse as sp
@@ -173,6 +177,40 @@ def test_similarity_group_size_empty_rows_and_bad_input():
         bsp.reorder_similarity_host(rp, ci, 18)                                          # column 18 >= cols
     with pytest.raises(bsp.BspError):
         bsp.permute_rows_csr_host(S, np.zeros(S.rows, np.int32))                         # not a permutation
+
+
+def _argmin_engine(d):
+    est = {"csr": d["est_seconds_csr"]}
+    if d["est_seconds_smat_given"] >= 0:
+        est["smat_given"] = d["est_seconds_smat_given"]
+    if d["est_seconds_smat_reordered"] >= 0:
+        est["smat_reordered"] = d["est_seconds_smat_reordered"]
+    return min(est, key=lambda k: (est[k], k))
+
+
+def test_spmm_choice_uses_the_similarity_order():
+    S, M = _grouped(256, 6, 1024, 11)
+    d, perm = bsp.choose_spmm_host(S, 128)
+    assert (d["engine"], d["reorder"], d["smat_path"]) == ("smat", True, "tcgen05")
+    assert np.array_equal(perm, bsp.reorder_similarity_host(S.rowptr, S.colidx, S.cols))
+    assert d["tiles_given"] == _tiles(S) and d["tiles_reordered"] == _tiles(M) == 256 * 6
+    assert _argmin_engine(d) == "smat_reordered"
+    d, _ = bsp.choose_spmm_host(M, 128)                        # already grouped: no reordering needed
+    assert (d["engine"], d["reorder"]) == ("smat", False) and _argmin_engine(d) == "smat_given"
+
+
+def test_spmm_choice_scattered_rows_and_n():
+    G = bsp.gen_graph(1 << 16, 1.8, 8, 7)                      # power-law graph: few nonzeros per tile
+    d, _ = bsp.choose_spmm_host(G, 128)
+    assert d["engine"] == "csr" and _argmin_engine(d) == "csr"
+    S, _ = _grouped(64, 4, 256, 16)
+    d, perm = bsp.choose_spmm_host(S, 96, reorder=False)        # N % 128 != 0: the mma.sync tile cost
+    assert perm is None and d["tiles_reordered"] == -1 and d["est_seconds_smat_reordered"] == -1.0
+    assert d["smat_path"] == "mma_sync" and d["engine"] == {"csr": "csr", "smat_given": "smat"}[_argmin_engine(d)]
+    d, _ = bsp.choose_spmm_host(S, 100)                         # SMaT needs N % 32 == 0
+    assert d["engine"] == "csr" and d["est_seconds_smat_given"] == -1.0
+    with pytest.raises(bsp.BspError):
+        bsp.choose_spmm_host(S, 0)
 
 
 @pytest.mark.gpu
