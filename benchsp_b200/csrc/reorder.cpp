@@ -191,7 +191,7 @@ void permute(int32_t n, const int32_t *rp, const int32_t *ci, const double *va, 
 // the grouping.
 constexpr int32_t kScanBlocks = 64;
 constexpr int64_t kScanEntries = 1024;
-constexpr size_t kTouched = 2048;
+constexpr size_t kTouched = 512;
 
 void similarity_order(int32_t n, int32_t cols, const int32_t *rp, const int32_t *ci, int32_t G, int32_t BC,
                       int32_t *perm) {
