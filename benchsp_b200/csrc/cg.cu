@@ -93,6 +93,7 @@ struct CgMat {
   const int8_t *exps;
   const int32_t *slice_len;  // SELL-32 (mixed modes)
   const int64_t *slice_off;
+  int32_t uniform_len;       // > 0: every slice has this length, offsets are sl * 32 * uniform_len
   __device__ __forceinline__ int64_t col(int64_t r, int32_t j) const {
     if (DELTA16) return r + (int64_t) reinterpret_cast<const int16_t *>(cols)[j];
     return reinterpret_cast<const int32_t *>(cols)[j];
@@ -107,10 +108,12 @@ struct CgMat {
 // get 2, 4 or 8 lanes that split the row's entries (4 loads in flight each)
 // and combine by shuffle, instead of one thread walking the row.
 // The FP64 CSR path fits 40 registers without spills: 6 resident CTAs per SM
-// instead of 4 (Poisson 128^3 FP64 CG 37.0 -> 35.9 ms); the SELL paths keep
-// the default (the same cap cost them 15%).
+// instead of 4 (Poisson 128^3 FP64 CG 37.0 -> 35.9 ms); so does the FP32
+// SELL form with 32-bit columns (its default since the uniform-slice field).
+// The other SELL forms keep the default (the same cap cost them 15%).
 template <typename V, typename VT, bool SCALED, bool DELTA16, int LPR = 1>
-__global__ void __launch_bounds__(kCgThreads, sizeof(V) == 8 ? 6 : 0) cg_dir_spmv_kernel(int32_t n, CgMat<V, VT, SCALED, DELTA16> A,
+__global__ void __launch_bounds__(kCgThreads, (sizeof(V) == 8 || (sizeof(V) == 4 && !DELTA16)) ? 6 : 0)
+    cg_dir_spmv_kernel(int32_t n, CgMat<V, VT, SCALED, DELTA16> A,
                                                                  const VT *__restrict__ r,
                                                                  const VT *__restrict__ p_prev,
                                                                  VT *__restrict__ p, VT *__restrict__ q,
@@ -133,8 +136,11 @@ __global__ void __launch_bounds__(kCgThreads, sizeof(V) == 8 ? 6 : 0) cg_dir_spm
     const int lane = threadIdx.x & 31;
     for (int64_t i = (int64_t)blockIdx.x * kCgThreads + threadIdx.x; i - lane < n; i += stride) {
       const int32_t sl = (int32_t)(i >> 5);
-      const int32_t len = A.slice_len[sl];
-      const uint32_t base = (uint32_t)A.slice_off[sl];
+      // uniform slices (16-bit offset forms; the 32-bit column form would
+      // need 8 more registers): length and offset without loads
+      const bool uni = DELTA16 && A.uniform_len > 0;
+      const int32_t len = uni ? A.uniform_len : A.slice_len[sl];
+      const uint32_t base = uni ? (uint32_t)sl * 32u * (uint32_t)A.uniform_len : (uint32_t)A.slice_off[sl];
       const uint32_t off = base + lane;
       const bool live = i < n;
       const int32_t row = (int32_t)i;
@@ -849,6 +855,7 @@ struct bsp_cg_plan_s {
   void *lp_cols = nullptr;     // int16 offsets or int32 columns (unpacked SELL)
   int32_t *slice_len = nullptr;
   int64_t *slice_off = nullptr;
+  int32_t sell_uniform = 0;    // > 0: all slices padded to this length
   bool delta16 = false;
   // FP64 state
   double *x64 = nullptr, *r64 = nullptr;
@@ -934,7 +941,7 @@ template <typename V, typename VT, bool SC, bool D16, int LPR = 1>
 static void launch_iter(bsp_cg_plan_s *P, int k, cudaStream_t s) {
   CgMat<V, VT, SC, D16> A{P->rowPtr, sizeof(V) == 8 ? (const void *)P->colIdx : (const void *)P->lp_cols,
                            (const V *)(sizeof(V) == 8 ? (const void *)P->val : P->lp_val), P->exps,
-                           P->slice_len, P->slice_off};
+                           P->slice_len, P->slice_off, P->sell_uniform};
   VT *r = (VT *)P->r, *x = (VT *)P->x, *q = (VT *)P->q;
   VT *pp = (VT *)P->p[k & 1], *pn = (VT *)P->p[(k + 1) & 1];
   const int g = P->grid, ga = P->grid_a;
@@ -1277,6 +1284,20 @@ extern "C" bsp_status bsp_cg_create(int32_t n, int32_t nnz, const int32_t *rowPt
     std::vector<int64_t> hoff((size_t)ns + 1, 0);
     BSP_CG_CUDA(cudaMemcpyAsync(hlen.data(), P->slice_len, sizeof(int32_t) * ns, cudaMemcpyDeviceToHost, s));
     BSP_CG_CUDA(cudaStreamSynchronize(s));
+    // When padding every slice to the longest costs at most 1/32 more
+    // storage (stencils, banded matrices), the direction kernel computes a
+    // slice's offset instead of loading its length and offset.
+    int32_t lmax = 0;
+    int64_t natural = 0;
+    for (int64_t k = 0; k < ns; ++k) {
+      lmax = std::max(lmax, hlen[k]);
+      natural += 32 * (int64_t)hlen[k];
+    }
+    if (lmax > 0 && ns * 32 * (int64_t)lmax <= natural + natural / 32) {
+      std::fill(hlen.begin(), hlen.end(), lmax);
+      BSP_CG_CUDA(cudaMemcpyAsync(P->slice_len, hlen.data(), sizeof(int32_t) * ns, cudaMemcpyHostToDevice, s));
+      P->sell_uniform = lmax;
+    }
     for (int64_t k = 0; k < ns; ++k) hoff[k + 1] = hoff[k] + 32 * (int64_t)hlen[k];
     const int64_t padded = hoff[ns];
     if (padded >= ((int64_t)1 << 31)) {
