@@ -27,6 +27,46 @@ def _permuted_laplace(nx, seed):
     return bsp.HostCSR(A.rows, A.rows, M.indptr.astype(np.int32), M.indices.astype(np.int32), M.data.copy())
 
 
+def _ragged_laplace(nx):
+    """2-D Laplacian plus symmetric couplings (-0.1) from every 97th row to
+    the rows 100, 200, ..., 1000 after it, diagonal raised to keep it
+    diagonally dominant: SPD, offsets within int16, and SELL-32 slices of
+    uneven length (padding all to the longest would cost far more than 1/32
+    extra storage, so the low-precision copy keeps per-slice lengths)."""
+    import scipy.sparse as sp
+    A = bsp.gen_laplace2d(nx, nx)
+    n = A.rows
+    M = sp.csr_matrix((A.values, A.colidx, A.rowptr), shape=(n, n)).tolil()
+    for i in range(0, n, 97):
+        for d in range(100, 1001, 100):
+            if i + d < n:
+                M[i, i + d] = M[i + d, i] = -0.1
+                M[i, i] += 0.1
+                M[i + d, i + d] += 0.1
+    M = M.tocsr()
+    M.sort_indices()
+    return bsp.HostCSR(n, n, M.indptr.astype(np.int32), M.indices.astype(np.int32), M.data.copy())
+
+
+@pytest.mark.parametrize("mode", ["f32", "f16", "bf16"])
+def test_cg_mixed_uneven_slices(cuda, mode):
+    A = _ragged_laplace(120)
+    lens = np.zeros(-(-A.rows // 32) * 32, np.int64)
+    lens[:A.rows] = np.diff(A.rowptr)
+    sl = lens.reshape(-1, 32).max(axis=1)
+    assert sl.size * 32 * sl.max() > 32 * sl.sum() * 33 // 32      # per-slice lengths are kept
+    b = bsp.gen_uniform(A.rows, 12)
+    rp, ci, va, bb = _dev(cuda, A.rowptr, A.colidx, A.values, b)
+    S = bsp.CgSolver(rp, ci, va, mode=mode, tol=1e-10)
+    x, res = S.solve(bb)
+    S.close()
+    x = x.cpu().numpy()
+    assert res["converged"] == 1 and res["delta16"] == 1
+    assert pyoracle.rel_residual(A.rowptr, A.colidx, A.values, b, x) <= 2e-10
+    xr, _ = pyoracle.cg(A.rowptr, A.colidx, A.values, b, 1e-12)
+    assert np.linalg.norm(x - xr) / np.linalg.norm(xr) < 1e-7
+
+
 @pytest.mark.parametrize("mode", ["fp64", "f32", "f16", "bf16"])
 @pytest.mark.parametrize("kind", ["poisson24", "permuted_laplace"])
 def test_cg_reaches_1e10(cuda, mode, kind):
