@@ -128,11 +128,13 @@ __global__ void __launch_bounds__(kCgThreads, (sizeof(V) == 8 || (sizeof(V) == 4
   const VT bt = (VT)beta;
   double dot = 0.0;
   const int64_t stride = (int64_t)gridDim.x * kCgThreads;
-  if constexpr (sizeof(V) < 8) {
+  if constexpr (sizeof(V) < 8 || DELTA16) {
     // SELL-32: warp = slice (the grid stride is a multiple of 32 rows); the
     // row's power-of-two scale is applied once to its sum; offsets are 32-bit
-    // (the padded matrix has < 2^31 entries).
+    // (the padded matrix has < 2^31 entries).  FP64 values (V = double, 16-bit
+    // column offsets) are loaded and multiplied in FP64.
     using Mat = CgMat<V, VT, SCALED, DELTA16>;
+    using AV = typename std::conditional<sizeof(V) == 8, double, float>::type;
     const int lane = threadIdx.x & 31;
     for (int64_t i = (int64_t)blockIdx.x * kCgThreads + threadIdx.x; i - lane < n; i += stride) {
       const int32_t sl = (int32_t)(i >> 5);
@@ -150,11 +152,11 @@ __global__ void __launch_bounds__(kCgThreads, (sizeof(V) == 8 || (sizeof(V) == 4
         const int32_t kb = 0, kn = len;
         for (int32_t k0 = 0; k0 < kn; k0 += kRowFirst) {
           int32_t c[kRowFirst];
-          float a[kRowFirst];
+          AV a[kRowFirst];
 #pragma unroll
           for (int k = 0; k < kRowFirst; ++k) {
             c[k] = row;
-            a[k] = 0.f;
+            a[k] = AV(0);
             if (k0 + k < kn) {
               const uint32_t j = off + (uint32_t)(kb + k0 + k) * 32u;
               if constexpr (Mat::kPacked) {
@@ -166,7 +168,10 @@ __global__ void __launch_bounds__(kCgThreads, (sizeof(V) == 8 || (sizeof(V) == 4
                   a[k] = __bfloat162float(__ushort_as_bfloat16(vb));
                 c[k] = row + (int32_t)(int16_t)(w >> 16);
               } else {
-                a[k] = lp_to_float<V>(__ldg(A.val + j));
+                if constexpr (sizeof(V) == 8)
+                  a[k] = __ldg(A.val + j);
+                else
+                  a[k] = lp_to_float<V>(__ldg(A.val + j));
                 if (DELTA16)
                   c[k] = row + (int32_t)__ldg(reinterpret_cast<const int16_t *>(A.cols) + j);
                 else
@@ -179,7 +184,7 @@ __global__ void __launch_bounds__(kCgThreads, (sizeof(V) == 8 || (sizeof(V) == 4
             if (k0 + k < kn && live) acc = fma((VT)a[k], fma(bt, __ldg(p_prev + c[k]), __ldg(r + c[k])), acc);
         }
       }
-      acc *= row_scale;
+      if constexpr (SCALED) acc *= row_scale;
       if (live) {
         const VT pi = fma(bt, p_prev[i], r[i]);
         p[i] = pi;
@@ -806,7 +811,11 @@ __global__ void sell_fill_kernel(int32_t n, const int32_t *__restrict__ rowPtr, 
         c = colIdx[s0 + k];
         if (SCALED) v = ldexp(v, -(int)exps[t]);
       }
-      const V lv = from_float_lp<V>((float)v);
+      V lv;
+      if constexpr (sizeof(V) == 8)
+        lv = v;  // the FP64 copy keeps the values exactly
+      else
+        lv = from_float_lp<V>((float)v);
       const int64_t d = c - self;
       if (PACKED) {
         unsigned short vb;
@@ -857,6 +866,7 @@ struct bsp_cg_plan_s {
   int64_t *slice_off = nullptr;
   int32_t sell_uniform = 0;    // > 0: all slices padded to this length
   bool delta16 = false;
+  bool sell64 = false;         // FP64 mode iterates on an FP64 SELL-32 copy
   // FP64 state
   double *x64 = nullptr, *r64 = nullptr;
   // iteration vectors: FP64 (mode FP64) or FP32 (mixed); p ping-pongs
@@ -926,7 +936,8 @@ static void cg_plan_occupancy(const bsp_cg_plan_s *P, int &a, int &b) {
   const bool d = P->delta16;
   switch (P->opt.mode) {
     case BSP_CG_FP64:
-      return cg_occupancy<double, double, false, false>(a, b);
+      return P->sell64 ? cg_occupancy<double, double, false, true>(a, b)
+                       : cg_occupancy<double, double, false, false>(a, b);
     case BSP_CG_MIXED_F32:
       return d ? cg_occupancy<float, float, false, true>(a, b) : cg_occupancy<float, float, false, false>(a, b);
     case BSP_CG_MIXED_F16:
@@ -939,8 +950,9 @@ static void cg_plan_occupancy(const bsp_cg_plan_s *P, int &a, int &b) {
 
 template <typename V, typename VT, bool SC, bool D16, int LPR = 1>
 static void launch_iter(bsp_cg_plan_s *P, int k, cudaStream_t s) {
-  CgMat<V, VT, SC, D16> A{P->rowPtr, sizeof(V) == 8 ? (const void *)P->colIdx : (const void *)P->lp_cols,
-                           (const V *)(sizeof(V) == 8 ? (const void *)P->val : P->lp_val), P->exps,
+  constexpr bool csr = sizeof(V) == 8 && !D16;  // FP64 CSR; the other forms read the SELL copy
+  CgMat<V, VT, SC, D16> A{P->rowPtr, csr ? (const void *)P->colIdx : (const void *)P->lp_cols,
+                           (const V *)(csr ? (const void *)P->val : P->lp_val), P->exps,
                            P->slice_len, P->slice_off, P->sell_uniform};
   VT *r = (VT *)P->r, *x = (VT *)P->x, *q = (VT *)P->q;
   VT *pp = (VT *)P->p[k & 1], *pn = (VT *)P->p[(k + 1) & 1];
@@ -996,7 +1008,9 @@ static void launch_prec(bsp_cg_plan_s *P, cudaStream_t s) {
 }
 
 static bsp_status cg_iteration(bsp_cg_plan_s *P, int k, cudaStream_t s) {
-  if (!cg_mixed(P)) {
+  if (P->sell64) {
+    launch_iter<double, double, false, true>(P, k, s);
+  } else if (!cg_mixed(P)) {
     switch (P->lpr) {
       case 2: launch_iter<double, double, false, false, 2>(P, k, s); break;
       case 4: launch_iter<double, double, false, false, 4>(P, k, s); break;
@@ -1271,9 +1285,13 @@ extern "C" bsp_status bsp_cg_create(int32_t n, int32_t nnz, const int32_t *rowPt
     P->x = P->x64;
   }
   int64_t mat_bytes = (int64_t)nnz * 12;
-  if (mixed) {
-    const bool scaled = opt->mode != BSP_CG_MIXED_F32;
-    const size_t vsz = opt->mode == BSP_CG_MIXED_F32 ? 4 : 2;
+  // FP64 mode with short rows: an FP64 SELL-32 copy with 16-bit column
+  // offsets (10 bytes per entry, coalesced, no row pointers) replaces the CSR
+  // walk when its slices are uniform; otherwise the CSR kernel runs.
+  const bool try64 = !mixed && P->lpr == 1;
+  int64_t padded = 0;
+  if (mixed || try64) {
+    const bool scaled = mixed && opt->mode != BSP_CG_MIXED_F32;
     // SELL-32 slices: lengths on the device, offsets summed on the host
     const int64_t ns = ceil_div(n, 32);
     BSP_CG_TRY(dalloc(&P->slice_len, (size_t)ns, s));
@@ -1299,7 +1317,7 @@ extern "C" bsp_status bsp_cg_create(int32_t n, int32_t nnz, const int32_t *rowPt
       P->sell_uniform = lmax;
     }
     for (int64_t k = 0; k < ns; ++k) hoff[k + 1] = hoff[k] + 32 * (int64_t)hlen[k];
-    const int64_t padded = hoff[ns];
+    padded = hoff[ns];
     if (padded >= ((int64_t)1 << 31)) {
       set_error("bsp_cg_create: the padded low-precision matrix needs >= 2^31 entries");
       return fail(BSP_ERR_UNSUPPORTED);
@@ -1320,6 +1338,19 @@ extern "C" bsp_status bsp_cg_create(int32_t n, int32_t nnz, const int32_t *rowPt
     BSP_CG_TRY(read_i32(bad, &h_bad, s));
     dfree(bad, s);
     P->delta16 = !h_bad;
+    P->sell64 = try64 && P->delta16 && P->sell_uniform > 0;
+    if (try64 && !P->sell64) {  // FP64 stays on the CSR arrays
+      dfree(P->slice_len, s);
+      dfree(P->slice_off, s);
+      P->slice_len = nullptr;
+      P->slice_off = nullptr;
+      P->sell_uniform = 0;
+    }
+  }
+  if (mixed || P->sell64) {
+    const bool scaled = mixed && opt->mode != BSP_CG_MIXED_F32;
+    const size_t vsz = !mixed ? 8 : opt->mode == BSP_CG_MIXED_F32 ? 4 : 2;
+    const int64_t ns = ceil_div(n, 32);
     const bool packed = scaled && P->delta16;
     BSP_CG_CUDA(cudaMallocAsync(&P->lp_val, (packed ? 4 : vsz) * (size_t)(padded > 0 ? padded : 1), s));
     if (!packed)
@@ -1329,7 +1360,9 @@ extern "C" bsp_status bsp_cg_create(int32_t n, int32_t nnz, const int32_t *rowPt
 #define BSP_SELL_FILL(V, SC, D, PK)                                                                          \
   sell_fill_kernel<V, SC, D, PK><<<(unsigned)gf, 256, 0, s>>>(n, rowPtr, colIdx, values, P->slice_len,           \
                                                               P->slice_off, P->exps, (V *)P->lp_val, P->lp_cols)
-    if (opt->mode == BSP_CG_MIXED_F32) {
+    if (!mixed) {
+      BSP_SELL_FILL(double, false, true, false);
+    } else if (opt->mode == BSP_CG_MIXED_F32) {
       if (P->delta16) BSP_SELL_FILL(float, false, true, false); else BSP_SELL_FILL(float, false, false, false);
     } else if (opt->mode == BSP_CG_MIXED_F16) {
       if (P->delta16) BSP_SELL_FILL(__half, true, true, true); else BSP_SELL_FILL(__half, true, false, false);
@@ -1358,7 +1391,7 @@ extern "C" bsp_status bsp_cg_create(int32_t n, int32_t nnz, const int32_t *rowPt
   // gathers counted once) and writes p and q; kernel B reads p, q, x, r and
   // writes x, r.
   // Preconditioned: the update kernel also reads M^{-1} and writes z.
-  P->bytes_iter = mat_bytes + (mixed ? 0 : 4 * ((int64_t)n + 1)) + 10 * (int64_t)vt * n;
+  P->bytes_iter = mat_bytes + (mixed || P->sell64 ? 0 : 4 * ((int64_t)n + 1)) + 10 * (int64_t)vt * n;
   if (P->prec_bs)
     P->bytes_iter += (int64_t)vt * (ceil_div(n, P->prec_bs) * P->prec_bs * P->prec_bs + (int64_t)n);
   P->bytes_residual = (int64_t)nnz * 12 + 4 * ((int64_t)n + 1) + 3 * 8 * (int64_t)n;
