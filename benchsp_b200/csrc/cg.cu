@@ -1319,8 +1319,11 @@ extern "C" bsp_status bsp_cg_create(int32_t n, int32_t nnz, const int32_t *rowPt
     for (int64_t k = 0; k < ns; ++k) hoff[k + 1] = hoff[k] + 32 * (int64_t)hlen[k];
     padded = hoff[ns];
     if (padded >= ((int64_t)1 << 31)) {
-      set_error("bsp_cg_create: the padded low-precision matrix needs >= 2^31 entries");
-      return fail(BSP_ERR_UNSUPPORTED);
+      if (mixed) {
+        set_error("bsp_cg_create: the padded low-precision matrix needs >= 2^31 entries");
+        return fail(BSP_ERR_UNSUPPORTED);
+      }
+      P->sell_uniform = 0;  // FP64 stays on the CSR arrays
     }
     BSP_CG_CUDA(cudaMemcpyAsync(P->slice_off, hoff.data(), sizeof(int64_t) * (ns + 1), cudaMemcpyHostToDevice, s));
     if (scaled) {
@@ -1350,11 +1353,34 @@ extern "C" bsp_status bsp_cg_create(int32_t n, int32_t nnz, const int32_t *rowPt
   if (mixed || P->sell64) {
     const bool scaled = mixed && opt->mode != BSP_CG_MIXED_F32;
     const size_t vsz = !mixed ? 8 : opt->mode == BSP_CG_MIXED_F32 ? 4 : 2;
+    const bool packed = scaled && P->delta16;
+    if (P->sell64) {
+      // the FP64 copy is an optimisation: without room for it, stay on CSR
+      const size_t ne = (size_t)(padded > 0 ? padded : 1);
+      if (cudaMallocAsync(&P->lp_val, 8 * ne, s) != cudaSuccess ||
+          cudaMallocAsync(&P->lp_cols, 2 * ne, s) != cudaSuccess) {
+        cudaGetLastError();
+        if (P->lp_val) cudaFreeAsync(P->lp_val, s);
+        if (P->lp_cols) cudaFreeAsync(P->lp_cols, s);
+        P->lp_val = P->lp_cols = nullptr;
+        dfree(P->slice_len, s);
+        dfree(P->slice_off, s);
+        P->slice_len = nullptr;
+        P->slice_off = nullptr;
+        P->sell_uniform = 0;
+        P->sell64 = false;
+      }
+    } else {
+      BSP_CG_CUDA(cudaMallocAsync(&P->lp_val, (packed ? 4 : vsz) * (size_t)(padded > 0 ? padded : 1), s));
+      if (!packed)
+        BSP_CG_CUDA(cudaMallocAsync(&P->lp_cols, (P->delta16 ? 2 : 4) * (size_t)(padded > 0 ? padded : 1), s));
+    }
+  }
+  if (mixed || P->sell64) {
+    const bool scaled = mixed && opt->mode != BSP_CG_MIXED_F32;
+    const size_t vsz = !mixed ? 8 : opt->mode == BSP_CG_MIXED_F32 ? 4 : 2;
     const int64_t ns = ceil_div(n, 32);
     const bool packed = scaled && P->delta16;
-    BSP_CG_CUDA(cudaMallocAsync(&P->lp_val, (packed ? 4 : vsz) * (size_t)(padded > 0 ? padded : 1), s));
-    if (!packed)
-      BSP_CG_CUDA(cudaMallocAsync(&P->lp_cols, (P->delta16 ? 2 : 4) * (size_t)(padded > 0 ? padded : 1), s));
     int64_t gf = ceil_div(ns * 32, 256);
     if (gf > (int64_t)sm_count() * 32) gf = (int64_t)sm_count() * 32;
 #define BSP_SELL_FILL(V, SC, D, PK)                                                                          \
