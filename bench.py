@@ -224,6 +224,62 @@ def make_matrix(grid: int = GRID):
     return A, x
 
 
+def make_matrix_reference(grid: int = GRID):
+    """The same matrix and x as make_matrix, built by the oracle's copy of the
+    generator (bit-identical, checked in tests/test_generators.py), so the
+    reference arm's process never loads the library."""
+    from types import SimpleNamespace
+
+    from oracle import pyoracle
+    rp, ci, va = pyoracle.gen_stencil27(grid, DOF, SEED)
+    n = rp.size - 1
+    A = SimpleNamespace(rows=n, cols=n, nnz=int(ci.size), rowptr=rp, colidx=ci, values=va)
+    return A, pyoracle.gen_uniform(n, SEED + 1)
+
+
+def headline_config(grid: int, n_gpus: int) -> dict:
+    """The workload's `config`, printed identically by both arms.  With 4
+    unknowns per node every node is one 4x4 block row and couples to each of
+    its neighbours by one dense block: (3*grid - 2)^3 blocks."""
+    blocks = (3 * grid - 2) ** 3
+    return {"workload": WORKLOAD if grid == GRID else f"bsr4_fp64_spmv_stencil27_{grid}cubed_4dof",
+            "n": grid ** 3 * DOF, "nnz": blocks * DOF * DOF, "blocks": blocks, "block": "4x4",
+            "parallelism": f"replicas{n_gpus}",
+            "l2": f"inputs larger than L2 ({algorithmic_bytes_bsr(blocks, grid ** 3, grid ** 3 * DOF) / 1e6:.0f} MB "
+                  f"working set)"}
+
+
+def cg_poisson128(bsp, dev, grid: int = 128, reps: int = 3) -> dict:
+    """CG to 1e-10 on the 7-point Poisson matrix 128^3 (b uniform [-1, 1]) in
+    FP64 and with FP32, FP16 and BF16 stored values (FP64 residual, dots and
+    update): per mode the median wall time of `reps` solves after one untimed
+    solve (CUDA events inside the solver), iterations, and ||b - A x|| / ||b||
+    recomputed in FP64 by cuSPARSE (torch.sparse), independent of the solver."""
+    import torch
+    A = bsp.gen_poisson3d(grid)
+    bh = bsp.gen_uniform(A.rows, SEED + 3)
+    rp, ci, va, b = (torch.from_numpy(a).to(dev) for a in (A.rowptr, A.colidx, A.values, bh))
+    T = torch.sparse_csr_tensor(rp.long(), ci.long(), va, size=(A.rows, A.cols))
+    out = {"n": A.rows, "nnz": A.nnz, "tol": 1e-10}
+    for mode in ("fp64", "f32", "f16", "bf16"):
+        S = bsp.CgSolver(rp, ci, va, mode=mode, tol=1e-10)
+        S.solve(b)
+        runs = []
+        for _ in range(reps):
+            xs, r = S.solve(b)
+            runs.append((r["seconds"], r, xs))
+        runs.sort(key=lambda t: t[0])
+        sec, r, xs = runs[len(runs) // 2]
+        res = float(torch.linalg.norm(b - T @ xs) / torch.linalg.norm(b))
+        out[mode] = {"ms": round(sec * 1e3, 3), "iterations": r["iterations"], "rel_residual_fp64": res,
+                     "converged": bool(r["converged"]) and res <= 1e-10}
+        S.close()
+    best = min(("f32", "f16", "bf16"), key=lambda m: out[m]["ms"])
+    out["fastest_mixed"] = best
+    out["mixed_over_fp64_time"] = round(out[best]["ms"] / out["fp64"]["ms"], 4)
+    return out
+
+
 REF_ARM_SECONDS = 120.0   # the reference arm's K timed steps together
 
 
@@ -234,7 +290,7 @@ def run_reference(args, ws, rank):
     (the sample is named in the line); GFLOP/s = 2 * sample nnz * K / time."""
     if rank != 0:
         return
-    A, x = make_matrix(args.grid)
+    A, x = make_matrix_reference(args.grid)
     step, cores, kind, _ = _cpu_spmv(A, x)
     warm = []
     for _ in range(max(1, args.warmup)):
@@ -259,8 +315,7 @@ def run_reference(args, ws, rank):
         "metric": METRIC, "value": round(v, 3), "unit": "GFLOP/s", "n_gpus": args.gpus, "steps": k,
         "warmup": args.warmup, "ms_per_step": round(total / k * 1e3, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-        "config": {"workload": WORKLOAD, "n": A.rows, "nnz": A.nnz, "block": "4x4",
-                   "l2": "working set > L2"},
+        "config": headline_config(args.grid, args.gpus),
         "impl": "reference",
         "cpu_baseline": {"value": round(v, 3), "unit": "GFLOP/s", "cores": cores, "kind": kind, "sample": sample},
         "e2e": {"value": round(v, 3), "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -337,8 +392,13 @@ def run_ours(args, ws, rank, local):
     y_np = y.cpu().numpy()
     ok = bool(np.allclose(y_np, yh_np, rtol=0, atol=0))
 
+    # the CG target (mixed precision vs FP64 to 1e-10), outside the timed region
+    cg = cg_poisson128(bsp, dev) if (ws == 1 and not args.no_cg) else None
+
     if rank != 0:
         return
+    cfg = headline_config(args.grid, ws)
+    assert (cfg["n"], cfg["nnz"], cfg["blocks"]) == (A.rows, A.nnz, M.blc_num), "config does not describe the matrix"
     pk = peaks()
     achieved = algo_bytes / (ms_step / 1e3) / 1e9
     traffic = None
@@ -356,10 +416,7 @@ def run_ours(args, ws, rank, local):
         "metric": METRIC, "value": round(value, 3), "unit": "GFLOP/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_step, 6), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-        "config": {"workload": WORKLOAD if args.grid == GRID else f"bsr4_fp64_spmv_stencil27_{args.grid}cubed_4dof",
-                   "n": A.rows, "nnz": A.nnz, "blocks": M.blc_num, "block": "4x4",
-                   "parallelism": f"replicas{ws}", "l2": "inputs larger than L2 (923 MB working set)",
-                   "kernel": "bsr_ffma_kernel<4,16,1>"},
+        "config": cfg,
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": pk["hbm_gbs"], "unit": "GB/s",
                      "frac": round(achieved / pk["hbm_gbs"], 4), "traffic": traffic,
                      "peak_src": pk["src"], "algorithmic_bytes_per_launch": algo_bytes},
@@ -369,8 +426,8 @@ def run_ours(args, ws, rank, local):
                 "call": f"bsp_bsr_spmv_host_pipelined ({E2E_CHUNKS} chunks, pinned host x/y)"},
         "gpu_launches": args.steps,
         "clocks": clk.summary(),
-        "extra": {"csr2bsr_seconds": round(convert_s, 4), "gbs": round(achieved, 1),
-                  "e2e_matches_device_result": ok},
+        "extra": {"kernel": "bsr_ffma_kernel<4,16,1>", "csr2bsr_seconds": round(convert_s, 4),
+                  "gbs": round(achieved, 1), "e2e_matches_device_result": ok, "cg_poisson128": cg},
     }
     print(json.dumps(line), flush=True)
 
@@ -913,6 +970,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cg", action="store_true", help="skip the CG figures in the headline line's extra")
     ap.add_argument("--suite", action="store_true", help="one JSON line per further workload (1 GPU)")
     ap.add_argument("--grid", type=int, default=GRID, help="stencil grid edge (64 = the benchmark config; "
                     "smaller values only for profiling captures)")

@@ -110,6 +110,15 @@ def _d2h(ptr: int, count: int, dtype) -> np.ndarray:
     return out
 
 
+def _host_vec(a, n: int, name: str) -> None:
+    """The host-buffer calls copy n doubles to or from `a`: it must be a
+    C-contiguous float64 numpy array of at least n entries."""
+    if not isinstance(a, np.ndarray) or a.dtype != np.float64 or not a.flags.c_contiguous:
+        raise ValueError(f"{name} must be a C-contiguous float64 numpy array")
+    if a.size < n:
+        raise ValueError(f"{name} has {a.size} entries, the matrix needs {n}")
+
+
 class BsrMatrix:
     """Device BSR matrix built by the library (bs = 4 reproduces bsrMAT)."""
 
@@ -160,6 +169,8 @@ class BsrMatrix:
                   algo: str = "auto", stream=None) -> np.ndarray:
         """Host-buffer SpMV (H2D x, SpMV, D2H y, wait); x_host/y_host are
         float64 numpy arrays, ideally in pinned memory."""
+        _host_vec(x_host, self._d.col, "x_host")
+        _host_vec(y_host, self._d.row, "y_host")
         check(lib().bsp_bsr_spmv_host(C.byref(self._d), C.c_void_p(x_host.ctypes.data),
                                       C.c_void_p(y_host.ctypes.data), float(alpha), float(beta), _ALGO_BSR[algo],
                                       _stream(stream)))
@@ -192,6 +203,8 @@ class BsrHostPlan:
 
     def spmv(self, x_host: np.ndarray, y_host: np.ndarray, *, alpha: float = 1.0, beta: float = 0.0,
              stream=None) -> np.ndarray:
+        _host_vec(x_host, self._m._d.col, "x_host")
+        _host_vec(y_host, self._m._d.row, "y_host")
         check(lib().bsp_bsr_spmv_host_pipelined(self._h, x_host.ctypes.data_as(C.c_void_p),
                                                 y_host.ctypes.data_as(C.c_void_p), float(alpha), float(beta),
                                                 _stream(stream)))

@@ -114,7 +114,10 @@ bsp_status bsp_csr_spmv_merge_f64(int32_t rows, int32_t cols, int32_t nnz,
  * process exits, so rows + nnz must be at most 67,108,864; larger inputs are
  * rejected with BSP_ERR_INVALID.  The array's device address is looked up on
  * the first call on each device (make that first call before any stream
- * capture).  All calls share the one array: calls that overlap on the GPU
+ * capture).  With CUDA's lazy module loading (the default) the array may only
+ * be placed in device memory at that first call, so a host that hands its
+ * GPU memory to its own pool should make one call per device at start-up,
+ * before taking the pool.  All calls share the one array: calls that overlap on the GPU
  * (concurrent streams, threads) race and must be serialized by the caller.
  * Results match bsp_csr_spmv_merge_f64. */
 bsp_status bsp_csr_spmv_merge_f64_noalloc(int32_t rows, int32_t cols, int32_t nnz,
@@ -193,7 +196,12 @@ bsp_status bsp_bsr_spmv_host(const bsp_bsr *m, const double *x_host, double *y_h
  * it reads has arrived (its largest column, found at plan time), and its y
  * goes down as soon as it is done.  Pays for matrices whose columns follow
  * their rows (stencils, banded, reordered).  Host buffers should be pinned.
- * The call returns when y_host is written; `m` must outlive the plan. */
+ * The call returns when y_host is written.  The plan records the copies and
+ * launches as a CUDA graph for the (x_host, y_host, alpha, beta) it is given
+ * and replays that graph while the four repeat, without looking at the
+ * buffers again: `m`, its arrays and both host buffers must stay allocated,
+ * at their sizes, as long as the plan may be called with those pointers
+ * (free `m` only after bsp_bsr_host_plan_destroy). */
 typedef struct bsp_bsr_host_plan_s *bsp_bsr_host_plan;
 bsp_status bsp_bsr_host_plan_create(const bsp_bsr *m, int32_t chunks,
                                     bsp_bsr_host_plan *plan, bsp_stream_t stream);

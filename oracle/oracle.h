@@ -107,6 +107,13 @@ void orc_dasp_free(orc_dasp *o);
 void orc_blockinfo(int32_t rows, const int32_t *rowPtr, const int32_t *colIdx, int64_t *blocks,
                    int64_t *blocks_recorder);
 
+/* Benchmark input generator (oracle_gen.c): the seeded 27-point stencil with
+ * `dof` unknowns per node and the seeded uniform vector, bit-identical to the
+ * library's generator.  orc_gen_stencil27 returns nnz (arrays may be NULL to
+ * count only; rowPtr alone fills the row pointers), or -1 when too large. */
+int64_t orc_gen_stencil27(int32_t m, int32_t dof, uint64_t seed, int32_t *rowPtr, int32_t *colIdx, double *val);
+void orc_gen_uniform(int64_t n, uint64_t seed, double *x);
+
 #ifdef __cplusplus
 }
 #endif

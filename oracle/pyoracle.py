@@ -355,3 +355,33 @@ def rel_residual(rowptr, colidx, val, b, x) -> float:
     """||b - A x|| / ||b|| with the oracle SpMV."""
     r = b - spmv_f64(rowptr, colidx, val, np.ascontiguousarray(x, np.float64))
     return float(np.linalg.norm(r) / np.linalg.norm(b))
+
+
+# ---------------------------------------------------------------------------
+# Benchmark inputs without the library (oracle_gen.c)
+
+def gen_stencil27(m: int, dof: int, seed: int) -> tuple:
+    """The seeded 27-point stencil (m^3 nodes x dof) as (rowptr, colidx,
+    values), bit-identical to the library's generator."""
+    L = orc()
+    L.orc_gen_stencil27.restype = _I64
+    L.orc_gen_stencil27.argtypes = [_I32, _I32, C.c_uint64, _P, _P, _P]
+    n = m * m * m * dof
+    rowptr = np.empty(n + 1, np.int32)
+    nnz = int(L.orc_gen_stencil27(m, dof, seed, _p(rowptr), None, None))
+    if nnz < 0:
+        raise ValueError("stencil too large for int32 indices")
+    colidx = np.empty(nnz, np.int32)
+    values = np.empty(nnz, np.float64)
+    L.orc_gen_stencil27(m, dof, seed, _p(rowptr), _p(colidx), _p(values))
+    return rowptr, colidx, values
+
+
+def gen_uniform(n: int, seed: int) -> np.ndarray:
+    """The seeded uniform [-1, 1) vector, bit-identical to the library's."""
+    L = orc()
+    L.orc_gen_uniform.restype = None
+    L.orc_gen_uniform.argtypes = [_I64, C.c_uint64, _P]
+    x = np.empty(n, np.float64)
+    L.orc_gen_uniform(n, seed, _p(x))
+    return x

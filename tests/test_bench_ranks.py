@@ -82,3 +82,25 @@ def test_reference_arm_samples_rows_when_k_steps_exceed_the_budget(capsys, monke
 
 def test_reference_arm_other_ranks_print_nothing(capsys, monkeypatch):
     assert _reference_line(capsys, monkeypatch, 120.0, 3, 1, rank=1) is None
+
+
+def test_reference_arm_never_loads_the_library():
+    """The reference arm builds its input with the oracle's generator: after a
+    full run, neither the package nor libbspmv.so is in the process, and its
+    config is the one the library's arm prints."""
+    import json
+    import subprocess
+    code = (
+        "import sys, json, argparse\n"
+        f"sys.path.insert(0, {str(ROOT)!r})\n"
+        "import bench\n"
+        "bench.run_reference(argparse.Namespace(grid=8, warmup=1, steps=2, gpus=1), 1, 0)\n"
+        "maps = open('/proc/self/maps').read()\n"
+        "print(json.dumps({'pkg': 'benchsp_b200' in sys.modules, 'so': 'libbspmv' in maps}))\n")
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, check=True).stdout
+    line, probe = [json.loads(s) for s in out.strip().splitlines()[-2:]]
+    assert probe == {"pkg": False, "so": False}
+    sys.path.insert(0, str(ROOT))
+    import bench
+    assert line["config"] == bench.headline_config(8, 1)
+    assert line["config"]["n"] == 8 ** 3 * 4 and line["config"]["nnz"] == 22 ** 3 * 16

@@ -47,15 +47,21 @@ def test_noalloc_matches_workspace_entry_point_on_two_calls(cuda, kind):
         y_new = torch.from_numpy(y0_h).to(cuda)
         _lib.check(L.bsp_csr_spmv_merge_f64(A.rows, A.cols, A.nnz, _p(rp), _p(ci), _p(va), _p(x), _p(y_ref),
                                             alpha, beta, _p(ws), ws.numel(), stream))
+        torch.cuda.synchronize()
+        free_before = torch.cuda.mem_get_info()[0]
         _lib.check(_noalloc(L, A.rows, A.cols, rp, ci, va, x, y_new, alpha, beta, stream))
         torch.cuda.synchronize()
+        if call > 0:
+            # after the first call has set the array up, a call takes no device memory
+            assert torch.cuda.mem_get_info()[0] == free_before, "the allocation-free call changed free memory"
         a, b = y_new.cpu().numpy(), y_ref.cpu().numpy()
-        # same tolerance as the other SpMV parity tests: the per-row rounding
-        # bound (both sides scaled by |alpha|) plus the beta*y rounding
+        # the same kernels in the same order as the workspace entry point: the same bits
+        assert np.array_equal(a, b), f"call {call}"
+        # against the oracle: the per-row rounding bound (scaled by |alpha|)
+        # plus the rounding of alpha*(A x) + beta*y
         ax = pyoracle.spmv_f64(A.rowptr, A.colidx, A.values, x_h)
         tol = abs(alpha) * pyoracle.spmv_tolerance(A.rowptr, A.colidx, A.values, x_h) + \
             4 * 2.0 ** -53 * (np.abs(alpha * ax) + np.abs(beta * y0_h))
-        assert np.all(np.abs(a - b) <= tol), f"call {call}"
         ref = alpha * ax + beta * y0_h
         assert np.all(np.abs(a - ref) <= 2 * tol), f"call {call} vs oracle"
 
