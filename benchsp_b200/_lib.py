@@ -275,7 +275,8 @@ class BspSpmmPlan(C.Structure):
     """Mirror of bsp_spmm_plan (include/bsp.h)."""
     _fields_ = [("rows", C.c_int32), ("chunk", C.c_int32), ("nchunks", C.c_int64), ("nparts", C.c_int64),
                 ("nsplit", C.c_int32), ("chunk_ptr", C.c_void_p), ("part_ptr", C.c_void_p),
-                ("chunk_row", C.c_void_p), ("split_rows", C.c_void_p)]
+                ("chunk_row", C.c_void_p), ("split_rows", C.c_void_p), ("nshort", C.c_int32),
+                ("short_rows", C.c_void_p), ("long_chunk", C.c_void_p)]
 
 
 _PROTOS.update({
@@ -284,6 +285,9 @@ _PROTOS.update({
     "bsp_spmm_plan_workspace": (C.c_size_t, [C.POINTER(BspSpmmPlan), _I32]),
     "bsp_spmm_csr_planned": (C.c_int, [C.POINTER(BspSpmmPlan), _I32, _I32, _P, _P, _P, C.c_int, _P, _I32, _I64, _P,
                                        _I64, C.c_float, C.c_float, _P, C.c_size_t, _P]),
+    "bsp_spmm_csr_planned_variant": (C.c_int, [C.POINTER(BspSpmmPlan), _I32, _I32, _P, _P, _P, C.c_int, _P, _I32,
+                                               _I64, _P, _I64, C.c_float, C.c_float, _P, C.c_size_t, _I32, _I32,
+                                               _P]),
     "bsp_spmm_csr": (C.c_int, [_I32, _I32, _I32, _P, _P, _P, C.c_int, _P, _I32, _I64, _P, _I64, C.c_float,
                                C.c_float, _P]),
     "bsp_smat_create": (C.c_int, [_I32, _I32, _I32, _P, _P, _P, C.c_int, C.POINTER(BspSmat), _P]),
@@ -317,4 +321,23 @@ _PROTOS.update({
 
 _PROTOS.update({
     "bsp_cg_solve_multi": (C.c_int, [C.c_void_p, _I32, _P, _I64, _P, _I64, _P, C.POINTER(BspCgResult), _P]),
+})
+
+
+class BspBsrScaled(C.Structure):
+    """Mirror of bsp_bsr_scaled (include/bsp.h): FP16/BF16 BSR with one
+    power-of-two scale per block."""
+    _fields_ = [
+        ("row", C.c_int32), ("col", C.c_int32), ("bs", C.c_int32),
+        ("blc_row", C.c_int32), ("blc_col", C.c_int32), ("blc_num", C.c_int32),
+        ("dtype", C.c_int32), ("blcPtr", C.c_void_p), ("blcKey", C.c_void_p), ("blcVal", C.c_void_p),
+    ]
+
+
+_PROTOS.update({
+    "bsp_bsr_scaled_create": (C.c_int, [C.POINTER(BspBsr), _I32, C.POINTER(BspBsrScaled), _P]),
+    "bsp_bsr_scaled_free": (C.c_int, [C.POINTER(BspBsrScaled)]),
+    "bsp_bsr_scaled_spmv": (C.c_int, [C.POINTER(BspBsrScaled), _P, _I32, _P, _I32, _D, _D, _P]),
+    "bsp_bsr_scaled_spmv_variant": (C.c_int, [C.POINTER(BspBsrScaled), _P, _I32, _P, _I32, _D, _D, _I32, _I32,
+                                              _P]),
 })

@@ -176,6 +176,10 @@ class BsrMatrix:
                                       _stream(stream)))
         return y_host
 
+    def scaled(self, dtype: str = "f16", stream=None) -> "BsrScaledMatrix":
+        """FP16/BF16 copy with one power-of-two scale per block."""
+        return BsrScaledMatrix(self, dtype, stream)
+
     def host_plan(self, chunks: int = 8, stream=None) -> "BsrHostPlan":
         """Overlapped host-buffer SpMV plan (see BsrHostPlan)."""
         return BsrHostPlan(self, chunks, stream)
@@ -218,6 +222,68 @@ class BsrHostPlan:
     def __del__(self):
         try:
             self.close()
+        except Exception:
+            pass
+
+
+class BsrScaledMatrix:
+    """FP16/BF16 BSR with one power-of-two scale per block (bsp_bsr_scaled),
+    built from a BsrMatrix; the source may be freed afterwards."""
+
+    _DT = {"f16": _lib.F16, "bf16": _lib.BF16}
+
+    def __init__(self, src: "BsrMatrix", dtype: str = "f16", stream=None):
+        self._d = _lib.BspBsrScaled()
+        check(lib().bsp_bsr_scaled_create(C.byref(src._d), self._DT[dtype], C.byref(self._d), _stream(stream)))
+        self._live = True
+
+    def __getattr__(self, name):
+        d = self.__dict__.get("_d")
+        if d is not None and name in dict(_lib.BspBsrScaled._fields_):
+            return getattr(d, name)
+        raise AttributeError(name)
+
+    def stored_bytes(self) -> int:
+        """Bytes of the matrix arrays (values, keys, block-row pointers)."""
+        d = self._d
+        return d.blc_num * d.bs * d.bs * 2 + d.blc_num * 4 + (d.blc_row + 1) * 4
+
+    def arrays(self) -> dict[str, np.ndarray]:
+        d = self._d
+        return {"blcPtr": _d2h(d.blcPtr, d.blc_row + 1, np.int32),
+                "blcKey": _d2h(d.blcKey, d.blc_num, np.uint32),
+                "blcVal": _d2h(d.blcVal, d.blc_num * d.bs * d.bs, np.uint16)}
+
+    def spmv(self, x, y=None, *, alpha: float = 1.0, beta: float = 0.0, lanes: int = 0, unroll: int = 1,
+             stream=None):
+        """y = alpha*A*x + beta*y; x and y float64 or float32 device tensors
+        (y defaults to x's dtype); FP32 products and sums."""
+        torch = _torch()
+        if y is None:
+            y = torch.empty(self._d.row, dtype=x.dtype, device=x.device)
+            beta = 0.0
+        codes = {torch.float64: _lib.F64, torch.float32: _lib.F32}
+        if x.dtype not in codes or y.dtype not in codes:
+            raise ValueError("x and y must be float64 or float32")
+        if x.numel() < self._d.col or y.numel() < self._d.row:
+            raise ValueError("x or y is shorter than the matrix")
+        if lanes:
+            check(lib().bsp_bsr_scaled_spmv_variant(C.byref(self._d), _dptr(x, "x"), codes[x.dtype], _dptr(y, "y"),
+                                                    codes[y.dtype], float(alpha), float(beta), lanes, unroll,
+                                                    _stream(stream)))
+        else:
+            check(lib().bsp_bsr_scaled_spmv(C.byref(self._d), _dptr(x, "x"), codes[x.dtype], _dptr(y, "y"),
+                                            codes[y.dtype], float(alpha), float(beta), _stream(stream)))
+        return y
+
+    def free(self) -> None:
+        if self._live:
+            self._live = False
+            check(lib().bsp_bsr_scaled_free(C.byref(self._d)))
+
+    def __del__(self):
+        try:
+            self.free()
         except Exception:
             pass
 
@@ -620,7 +686,13 @@ class SpmmPlan:
     def workspace_bytes(self, N: int) -> int:
         return lib().bsp_spmm_plan_workspace(C.byref(self._d), N)
 
-    def spmm(self, B, C_out=None, *, alpha: float = 1.0, beta: float = 0.0, stream=None):
+    _ENGINES = {"auto": 0, "grouped": 1, "slab": 2}
+
+    def spmm(self, B, C_out=None, *, alpha: float = 1.0, beta: float = 0.0, engine: str = "auto",
+             slab_cols: int = 0, stream=None):
+        """C = alpha*A*B + beta*C.  engine "grouped" (one pass over all
+        columns), "slab" (passes over column slabs that fit in L2; slab_cols
+        0 = from the L2 size) or "auto"."""
         torch = _torch()
         N = B.shape[1]
         if self.values.dtype != B.dtype:
@@ -632,11 +704,13 @@ class SpmmPlan:
         if need and (self._ws is None or self._ws.numel() < need):
             self._ws = torch.empty(need, dtype=torch.uint8, device=B.device)
         ws = self._ws if need else None
-        check(lib().bsp_spmm_csr_planned(C.byref(self._d), self.cols, self.colidx.numel(),
-                                         _dptr(self.rowptr, "rowptr"), _dptr(self.colidx, "colidx"),
-                                         _dptr(self.values, "values"), _dtype_code(self.values), _dptr(B, "B"), N,
-                                         B.stride(0), _dptr(C_out, "C"), C_out.stride(0), float(alpha), float(beta),
-                                         ws.data_ptr() if ws is not None else None, need, _stream(stream)))
+        check(lib().bsp_spmm_csr_planned_variant(C.byref(self._d), self.cols, self.colidx.numel(),
+                                                 _dptr(self.rowptr, "rowptr"), _dptr(self.colidx, "colidx"),
+                                                 _dptr(self.values, "values"), _dtype_code(self.values),
+                                                 _dptr(B, "B"), N, B.stride(0), _dptr(C_out, "C"), C_out.stride(0),
+                                                 float(alpha), float(beta),
+                                                 ws.data_ptr() if ws is not None else None, need,
+                                                 self._ENGINES[engine], slab_cols, _stream(stream)))
         return C_out
 
     def free(self) -> None:

@@ -1071,6 +1071,27 @@ __global__ void spmm_split_list_kernel(int32_t rows, const int32_t *__restrict__
     if (chunk_ptr[r + 1] - chunk_ptr[r] > 1) split_rows[split_pos[r]] = (int32_t)r;
 }
 
+__global__ void spmm_long_chunk_kernel(int32_t rows, const int32_t *__restrict__ chunk_ptr,
+                                       const int32_t *__restrict__ part_ptr, int32_t *__restrict__ long_chunk) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t c0 = chunk_ptr[r], nc = chunk_ptr[r + 1] - c0;
+    if (nc > 1)
+      for (int32_t c = 0; c < nc; ++c) long_chunk[part_ptr[r] + c] = c0 + c;
+  }
+}
+
+// Sort keys for the short-row list: chunk - length for rows of at most
+// `chunk` nonzeros (so a stable ascending sort puts the longest first),
+// chunk + 1 for split rows (sorted past the end of the list).
+__global__ void spmm_short_key_kernel(int32_t rows, const int32_t *__restrict__ rowPtr, int32_t chunk,
+                                      int32_t *__restrict__ key, int32_t *__restrict__ idx) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t len = rowPtr[r + 1] - rowPtr[r];
+    key[r] = len <= chunk ? chunk - len : chunk + 1;
+    idx[r] = (int32_t)r;
+  }
+}
+
 __global__ void spmm_split_flag_kernel(int32_t rows, const int32_t *__restrict__ chunk_ptr,
                                        int32_t *__restrict__ flag) {
   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r <= rows; r += (int64_t)gridDim.x * blockDim.x)
@@ -1125,6 +1146,21 @@ extern "C" bsp_status bsp_spmm_plan_create(int32_t rows, int32_t nnz, const int3
   }
   dfree(flag, s);
   dfree(tot, s);
+  // slab engine: the long chunks in partial-slot order, the short rows by length
+  p.nshort = rows - p.nsplit;
+  BSP_TRY(dalloc(&p.long_chunk, (size_t)(p.nparts > 0 ? p.nparts : 1), s));
+  BSP_TRY(dalloc(&p.short_rows, (size_t)(rows > 0 ? rows : 1), s));
+  if (rows > 0) {
+    spmm_long_chunk_kernel<<<g, 256, 0, s>>>(rows, p.chunk_ptr, p.part_ptr, p.long_chunk);
+    BSP_LAUNCH_CHECK();
+    int32_t *keys = nullptr;
+    BSP_TRY(dalloc(&keys, (size_t)rows, s));
+    spmm_short_key_kernel<<<g, 256, 0, s>>>(rows, rowPtr, chunk, keys, p.short_rows);
+    BSP_LAUNCH_CHECK();
+    const bsp_status st = radix_sort_pairs(keys, p.short_rows, rows, bits_for(chunk + 1), s);
+    dfree(keys, s);
+    BSP_TRY(st);
+  }
   BSP_CUDA(cudaStreamSynchronize(s));
   *out = p;
   return BSP_OK;
@@ -1138,6 +1174,8 @@ extern "C" bsp_status bsp_spmm_plan_free(bsp_spmm_plan *p) {
   dfree(p->part_ptr, s);
   dfree(p->chunk_row, s);
   dfree(p->split_rows, s);
+  dfree(p->short_rows, s);
+  dfree(p->long_chunk, s);
   BSP_CUDA(cudaStreamSynchronize(s));
   return BSP_OK;
 }
@@ -1241,11 +1279,178 @@ static bsp_status chunked_typed(const bsp_spmm_plan *p, int32_t N, const int32_t
   if (N % 128 == 0 && al16) return launch_chunked<T, 4>(p, N, rp, ci, val, B, ldb, C, ldc, part, a, b, s);
   return launch_chunked<T, 1>(p, N, rp, ci, val, B, ldb, C, ldc, part, a, b, s);
 }
+
+// ---------------------------------------------------------------------------
+// Slab engine.  One pass per slab of NS = LPR*VEC columns [col0, col0 + NS):
+// B's slab (B rows x NS) is small enough to stay in L2 for the whole pass, so
+// every gathered B row after the first touch is an L2 hit, at the price of
+// reading A once per slab.  Warp tasks [0, nlong) are the long rows' chunks,
+// a warp each (the grouped segment: G groups of LPR lanes split the chunk's
+// nonzeros, then a fixed shuffle tree), written to their partial-row slot;
+// the remaining tasks take G consecutive rows of the length-sorted short-row
+// list, one row per group of LPR lanes, so a warp has G rows' load chains in
+// flight at once instead of one.  A group issues the column index and value
+// loads of its next U nonzeros before the U gathers of the current ones are
+// consumed.
+template <typename T, int LPR, int U>
+__global__ void __launch_bounds__(256) spmm_slab_kernel(
+    int64_t nlong, const int32_t *__restrict__ long_chunk, const int32_t *__restrict__ chunk_row,
+    const int32_t *__restrict__ chunk_ptr, int32_t chunk, int32_t nshort, const int32_t *__restrict__ short_rows,
+    const int32_t *__restrict__ rowPtr, const int32_t *__restrict__ colIdx, const T *__restrict__ val,
+    const T *__restrict__ B, int64_t ldb, int32_t col0, float *__restrict__ C, int64_t ldc,
+    float *__restrict__ part, float alpha, float beta) {
+  constexpr int VEC = SpmmVec<T>::VEC;
+  constexpr int NS = LPR * VEC;
+  constexpr int G = 32 / LPR;
+  const int lane = threadIdx.x & 31;
+  const int li = lane % LPR;
+  const int32_t cl = col0 + li * VEC;
+  const int64_t ntasks = nlong + (nshort + G - 1) / G;
+  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t task = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; task < ntasks; task += nwarps) {
+    float acc[VEC];
+#pragma unroll
+    for (int k = 0; k < VEC; ++k) acc[k] = 0.f;
+    if (task < nlong) {   // warp-uniform
+      const int32_t w = long_chunk[task];
+      const int32_t r = chunk_row[w];
+      const int32_t s = rowPtr[r] + (w - chunk_ptr[r]) * chunk;
+      const int32_t e = min(s + chunk, rowPtr[r + 1]);
+      spmm_segment<T, LPR>(s, e, colIdx, val, B, ldb, cl, lane, acc);
+      if (lane < LPR) {
+        float *pp = part + task * NS + li * VEC;
+#pragma unroll
+        for (int k = 0; k < VEC; ++k) pp[k] = acc[k];
+      }
+      continue;
+    }
+    const int64_t i = (task - nlong) * G + lane / LPR;
+    if (i >= nshort) continue;
+    const int32_t r = short_rows[i];
+    const int32_t s = rowPtr[r], e = rowPtr[r + 1];
+    int32_t cn[U];
+    float vn[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const bool ok = s + u < e;
+      cn[u] = ok ? __ldg(colIdx + s + u) : 0;
+      vn[u] = ok ? sp_to_float<T>(__ldg(val + s + u)) : 0.f;
+    }
+    for (int32_t j = s; j < e; j += U) {
+      uint4 raw[U];
+      float v[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        v[u] = vn[u];
+        raw[u] = j + u < e ? __ldg(reinterpret_cast<const uint4 *>(B + (int64_t)cn[u] * ldb + cl))
+                           : make_uint4(0, 0, 0, 0);
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int32_t jj = j + U + u;
+        const bool ok = jj < e;
+        cn[u] = ok ? __ldg(colIdx + jj) : 0;
+        vn[u] = ok ? sp_to_float<T>(__ldg(val + jj)) : 0.f;
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        float b[VEC];
+        unpack16<T>(raw[u], b);
+#pragma unroll
+        for (int k = 0; k < VEC; ++k) acc[k] = fmaf(v[u], b[k], acc[k]);
+      }
+    }
+    float *cp = C + (int64_t)r * ldc + cl;
+#pragma unroll
+    for (int k = 0; k < VEC; ++k) {
+      float o = alpha * acc[k];
+      if (beta != 0.f) o += beta * cp[k];
+      cp[k] = o;
+    }
+  }
+}
+
+template <typename T, int LPR>
+static bsp_status launch_slab(const bsp_spmm_plan *p, const int32_t *rp, const int32_t *ci, const void *val,
+                              const void *B, int64_t ldb, int32_t col0, float *C, int64_t ldc, float *part, float a,
+                              float b, cudaStream_t s) {
+  constexpr int G = 32 / LPR;
+  const int64_t ntasks = p->nparts + (p->nshort + G - 1) / G;
+  int64_t blocks = ceil_div(ntasks, 8);
+  const int64_t cap = (int64_t)sm_count() * 32;
+  if (blocks > cap) blocks = cap;
+  if (blocks < 1) blocks = 1;
+  spmm_slab_kernel<T, LPR, 4><<<(unsigned)blocks, 256, 0, s>>>(
+      p->nparts, p->long_chunk, p->chunk_row, p->chunk_ptr, p->chunk, p->nshort, p->short_rows, rp, ci,
+      (const T *)val, (const T *)B, ldb, col0, C, ldc, part, a, b);
+  BSP_LAUNCH_CHECK();
+  return BSP_OK;
+}
+
+// Slab width (columns per pass) for the slab engine: the widest power-of-two
+// lane count (1..32 lanes of 16 bytes) whose slab divides N and, when
+// `want` == 0, keeps cols x slab of B within 60% of L2 (the rest holds the
+// streamed A and C lines in flight); 0 when the slab engine cannot run (B
+// rows not 16-byte aligned, N not a multiple of VEC).
+template <typename T>
+static int slab_width(int32_t N, int32_t cols, const void *B, int64_t ldb, int32_t want) {
+  constexpr int VEC = SpmmVec<T>::VEC;
+  if ((uintptr_t)B % 16 != 0 || (ldb * (int64_t)sizeof(T)) % 16 != 0 || N % VEC != 0) return 0;
+  if (want > 0) {
+    if (want % VEC != 0 || N % want != 0) return -1;
+    const int l = want / VEC;
+    if (l > 32 || (l & (l - 1)) != 0) return -1;
+    return want;
+  }
+  int dev = 0, l2 = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev) != cudaSuccess)
+    l2 = 126 << 20;
+  const double budget = 0.6 * (double)l2;
+  int l = 32;
+  while (l > 1 && (N % (l * VEC) != 0 || (double)cols * l * VEC * sizeof(T) > budget)) l >>= 1;
+  return l * VEC;
+}
+
+template <typename T>
+static bsp_status slab_typed(const bsp_spmm_plan *p, int32_t N, int32_t ns, const int32_t *rp, const int32_t *ci,
+                             const void *val, const void *B, int64_t ldb, float *C, int64_t ldc, float *part,
+                             float a, float b, cudaStream_t s) {
+  constexpr int VEC = SpmmVec<T>::VEC;
+  for (int32_t col0 = 0; col0 < N; col0 += ns) {
+    bsp_status st;
+    switch (ns / VEC) {
+      case 32: st = launch_slab<T, 32>(p, rp, ci, val, B, ldb, col0, C, ldc, part, a, b, s); break;
+      case 16: st = launch_slab<T, 16>(p, rp, ci, val, B, ldb, col0, C, ldc, part, a, b, s); break;
+      case 8: st = launch_slab<T, 8>(p, rp, ci, val, B, ldb, col0, C, ldc, part, a, b, s); break;
+      case 4: st = launch_slab<T, 4>(p, rp, ci, val, B, ldb, col0, C, ldc, part, a, b, s); break;
+      case 2: st = launch_slab<T, 2>(p, rp, ci, val, B, ldb, col0, C, ldc, part, a, b, s); break;
+      case 1: st = launch_slab<T, 1>(p, rp, ci, val, B, ldb, col0, C, ldc, part, a, b, s); break;
+      default: BSP_FAIL(BSP_ERR_UNSUPPORTED, "slab width");
+    }
+    BSP_TRY(st);
+    if (p->nsplit > 0) {
+      int64_t blocks = ceil_div(p->nsplit, 8);
+      if (blocks > (int64_t)sm_count() * 32) blocks = (int64_t)sm_count() * 32;
+      spmm_split_reduce_kernel<<<(unsigned)blocks, 256, 0, s>>>(p->nsplit, p->split_rows, p->chunk_ptr, p->part_ptr,
+                                                                ns, part, C + col0, ldc, a, b);
+      BSP_LAUNCH_CHECK();
+    }
+  }
+  return BSP_OK;
+}
 }  // namespace bsp
 
 extern "C" size_t bsp_spmm_plan_workspace(const bsp_spmm_plan *p, int32_t N) {
   return p ? (size_t)p->nparts * (size_t)(N > 0 ? N : 0) * sizeof(float) : 0;
 }
+
+namespace bsp {
+static bsp_status spmm_planned_impl(const bsp_spmm_plan *p, int32_t cols, int32_t nnz, const int32_t *rowPtr,
+                                    const int32_t *colIdx, const void *values, bsp_dtype dtype, const void *B,
+                                    int32_t N, int64_t ldb, float *C, int64_t ldc, float alpha, float beta,
+                                    void *workspace, size_t workspace_bytes, int32_t engine, int32_t slab_cols,
+                                    cudaStream_t s);
+}  // namespace bsp
 
 extern "C" bsp_status bsp_spmm_csr_planned(const bsp_spmm_plan *p, int32_t cols, int32_t nnz,
                                            const int32_t *rowPtr, const int32_t *colIdx, const void *values,
@@ -1253,15 +1458,66 @@ extern "C" bsp_status bsp_spmm_csr_planned(const bsp_spmm_plan *p, int32_t cols,
                                            int64_t ldc, float alpha, float beta, void *workspace,
                                            size_t workspace_bytes, bsp_stream_t stream) {
   clear_error();
+  return spmm_planned_impl(p, cols, nnz, rowPtr, colIdx, values, dtype, B, N, ldb, C, ldc, alpha, beta, workspace,
+                           workspace_bytes, BSP_SPMM_AUTO, 0, as_stream(stream));
+}
+
+extern "C" bsp_status bsp_spmm_csr_planned_variant(const bsp_spmm_plan *p, int32_t cols, int32_t nnz,
+                                                   const int32_t *rowPtr, const int32_t *colIdx,
+                                                   const void *values, bsp_dtype dtype, const void *B, int32_t N,
+                                                   int64_t ldb, float *C, int64_t ldc, float alpha, float beta,
+                                                   void *workspace, size_t workspace_bytes, int32_t engine,
+                                                   int32_t slab_cols, bsp_stream_t stream) {
+  clear_error();
+  BSP_CHECK_ARG(engine >= BSP_SPMM_AUTO && engine <= BSP_SPMM_SLAB, "unknown engine");
+  BSP_CHECK_ARG(slab_cols >= 0, "negative slab width");
+  return spmm_planned_impl(p, cols, nnz, rowPtr, colIdx, values, dtype, B, N, ldb, C, ldc, alpha, beta, workspace,
+                           workspace_bytes, engine, slab_cols, as_stream(stream));
+}
+
+namespace bsp {
+template <typename T>
+static int slab_choice(const bsp_spmm_plan *p, int32_t N, int32_t cols, const void *B, int64_t ldb, int32_t engine,
+                       int32_t slab_cols) {
+  if (engine == BSP_SPMM_GROUPED) return 0;
+  const int ns = slab_width<T>(N, cols, B, ldb, slab_cols);
+  if (engine == BSP_SPMM_SLAB || ns <= 0) return ns;
+  // automatic: the slab engine when all of B does not fit in 60% of L2
+  return ns < N ? ns : 0;
+}
+
+static bsp_status spmm_planned_impl(const bsp_spmm_plan *p, int32_t cols, int32_t nnz, const int32_t *rowPtr,
+                                    const int32_t *colIdx, const void *values, bsp_dtype dtype, const void *B,
+                                    int32_t N, int64_t ldb, float *C, int64_t ldc, float alpha, float beta,
+                                    void *workspace, size_t workspace_bytes, int32_t engine, int32_t slab_cols,
+                                    cudaStream_t s) {
   BSP_CHECK_ARG(p && rowPtr && C, "null pointer");
   BSP_CHECK_ARG(N >= 0 && ldb >= N && ldc >= N, "bad N / leading dimensions");
   if (p->rows == 0 || N == 0) return BSP_OK;
   BSP_CHECK_ARG(nnz == 0 || (colIdx && values && B), "null pointer");
   const size_t need = bsp_spmm_plan_workspace(p, N);
   BSP_CHECK_ARG(workspace_bytes >= need && (need == 0 || workspace), "workspace too small");
-  cudaStream_t s = as_stream(stream);
   float *part = reinterpret_cast<float *>(workspace);
   bsp_status st;
+  int ns = 0;
+  switch (dtype) {
+    case BSP_F16: ns = slab_choice<__half>(p, N, cols, B, ldb, engine, slab_cols); break;
+    case BSP_BF16: ns = slab_choice<__nv_bfloat16>(p, N, cols, B, ldb, engine, slab_cols); break;
+    case BSP_F32: ns = slab_choice<float>(p, N, cols, B, ldb, engine, slab_cols); break;
+    default: BSP_FAIL(BSP_ERR_UNSUPPORTED, "SpMM takes F16, BF16 or F32 values");
+  }
+  if (ns < 0 || (engine == BSP_SPMM_SLAB && ns == 0))
+    BSP_FAIL(BSP_ERR_UNSUPPORTED, "the slab engine needs 16-byte aligned B rows and a slab width that is a power "
+                                  "of two times 16 bytes dividing N");
+  if (ns > 0) {
+    if (nnz > 0 && !(colIdx && values && B)) BSP_FAIL(BSP_ERR_INVALID, "null pointer");
+    switch (dtype) {
+      case BSP_F16: return slab_typed<__half>(p, N, ns, rowPtr, colIdx, values, B, ldb, C, ldc, part, alpha, beta, s);
+      case BSP_BF16:
+        return slab_typed<__nv_bfloat16>(p, N, ns, rowPtr, colIdx, values, B, ldb, C, ldc, part, alpha, beta, s);
+      default: return slab_typed<float>(p, N, ns, rowPtr, colIdx, values, B, ldb, C, ldc, part, alpha, beta, s);
+    }
+  }
   switch (dtype) {
     case BSP_F16:
       st = chunked_typed<__half>(p, N, rowPtr, colIdx, values, B, ldb, C, ldc, part, alpha, beta, s);
@@ -1285,3 +1541,4 @@ extern "C" bsp_status bsp_spmm_csr_planned(const bsp_spmm_plan *p, int32_t cols,
   }
   return BSP_OK;
 }
+}  // namespace bsp

@@ -211,6 +211,49 @@ bsp_status bsp_bsr_spmv_host_pipelined(bsp_bsr_host_plan plan, const double *x_h
 bsp_status bsp_bsr_host_plan_destroy(bsp_bsr_host_plan plan);
 
 /* ---------------------------------------------------------------------- */
+/* BSR with FP16/BF16 values and one power-of-two scale per block.  No
+ * reference counterpart: the reference's BSR (bsrMAT, include/matrixFormat.hpp
+ * :59-83; SpMV bsr_spmv_tc_fp64, src/amgT.cu:210-274) stores FP64 values
+ * only, and its FP16 CSR path (src/spmv.cu:13-27) has no scales.  A block
+ * holds bs*bs 16-bit values q and one exponent e; its entries are q * 2^e.
+ * e makes the block's largest magnitude land in [2^14, 2^15) for FP16 (the
+ * whole normal range below it stays normal) and in [1, 2) for BF16, clamped
+ * to [-126, 127]; q = round-to-nearest-even of (float)(a * 2^-e).  Storage per
+ * 4x4 block: 32 bytes of values + 4 bytes of key, against 132 for FP64.
+ * blcVal is laid out in 4x4 tiles, row-major inside a tile; an 8x8 block is
+ * its tiles (0,0), (0,1), (1,0), (1,1) in that order, so every tile is one
+ * 32-byte load. */
+typedef struct {
+  int32_t row, col, bs;          /* bs = 4 or 8 */
+  int32_t blc_row, blc_col, blc_num;
+  int32_t dtype;                 /* BSP_F16 or BSP_BF16 */
+  int32_t *blcPtr;               /* [blc_row+1], as the source BSR */
+  uint32_t *blcKey;              /* [blc_num]: block column (bits 0-23) | (e + 128) << 24 */
+  uint16_t *blcVal;              /* [blc_num*bs*bs], 4x4 tiles */
+} bsp_bsr_scaled;
+
+/* Builds the scaled copy of a BSR matrix on the device (the source is left
+ * unchanged and may be freed afterwards).  Needs blc_col < 2^24; values whose
+ * block would overflow the target type return BSP_ERR_INVALID. */
+bsp_status bsp_bsr_scaled_create(const bsp_bsr *src, int32_t dtype, bsp_bsr_scaled *out,
+                                 bsp_stream_t stream);
+bsp_status bsp_bsr_scaled_free(bsp_bsr_scaled *m);
+
+/* y = alpha*A*x + beta*y with the scaled matrix: products and sums in FP32
+ * (x rounded to FP32 and multiplied by the block's 2^e, which is exact), then
+ * alpha*sum + beta*y in the type of y.  x_dtype, y_dtype: BSP_F64 or BSP_F32.
+ * Deterministic: every y element is written once, in a fixed order. */
+bsp_status bsp_bsr_scaled_spmv(const bsp_bsr_scaled *m, const void *x, int32_t x_dtype, void *y,
+                               int32_t y_dtype, double alpha, double beta, bsp_stream_t stream);
+
+/* The same with an explicit lane count per block row (4, 8, 16 or 32; for
+ * bs = 8 at least 4) and 1 or 2 blocks per lane per loop trip (tuning). */
+bsp_status bsp_bsr_scaled_spmv_variant(const bsp_bsr_scaled *m, const void *x, int32_t x_dtype,
+                                       void *y, int32_t y_dtype, double alpha, double beta,
+                                       int32_t lanes_per_blockrow, int32_t unroll,
+                                       bsp_stream_t stream);
+
+/* ---------------------------------------------------------------------- */
 /* Fixed-tile BCSR (BCSRFormat<double,int32_t>, reference
  * include/matrixFormat.hpp:16-30).  blockNum is 64-bit (rowRegions *
  * colRegions overflows int32 for n above ~46k with 1x1 tiles). */
@@ -369,7 +412,17 @@ bsp_status bsp_spmm_csr(int32_t rows, int32_t cols, int32_t nnz,
 /* Row-split CSR form for power-law rows: the plan cuts rows longer than
  * `chunk` nonzeros into chunks processed by separate warps; their partial
  * rows go to a workspace of bsp_spmm_plan_workspace(plan, N) bytes and are
- * summed in chunk order (deterministic). */
+ * summed in chunk order (deterministic).
+ *
+ * Two engines run a planned product.  "grouped": one warp per row or chunk
+ * over all N columns in one pass.  "slab": the columns are taken in slabs
+ * small enough that a slab of B stays in L2 (passes over A, one per slab),
+ * and rows of at most `chunk` nonzeros, sorted by length, are spread one per
+ * group of lanes (several rows per warp in flight), while long-row chunks
+ * keep a warp each.  The default picks the slab engine when all of B does
+ * not fit in 60% of L2.  Both give the same bits for a given slab width
+ * only if their sums run in the same order, which they do not: results
+ * differ in rounding, each within the FP32 accumulation bound. */
 typedef struct {
   int32_t rows, chunk;
   int64_t nchunks, nparts;
@@ -378,6 +431,9 @@ typedef struct {
   int32_t *part_ptr;   /* [rows+1] partial-row slots of split rows */
   int32_t *chunk_row;  /* [nchunks] */
   int32_t *split_rows; /* [nsplit] */
+  int32_t nshort;      /* rows of at most `chunk` nonzeros (empty rows included) */
+  int32_t *short_rows; /* [nshort] those rows, longest first (stable) */
+  int32_t *long_chunk; /* [nparts] chunk index of each partial-row slot */
 } bsp_spmm_plan;
 
 bsp_status bsp_spmm_plan_create(int32_t rows, int32_t nnz, const int32_t *rowPtr,
@@ -391,6 +447,19 @@ bsp_status bsp_spmm_csr_planned(const bsp_spmm_plan *plan, int32_t cols, int32_t
                                 int32_t N, int64_t ldb, float *C, int64_t ldc,
                                 float alpha, float beta, void *workspace,
                                 size_t workspace_bytes, bsp_stream_t stream);
+
+typedef enum { BSP_SPMM_AUTO = 0, BSP_SPMM_GROUPED = 1, BSP_SPMM_SLAB = 2 } bsp_spmm_engine;
+
+/* bsp_spmm_csr_planned with the engine and, for the slab engine, the slab
+ * width (columns per pass; 0 = from the L2 size; otherwise a power of two
+ * times 16 bytes of B row that divides N) chosen by the caller. */
+bsp_status bsp_spmm_csr_planned_variant(const bsp_spmm_plan *plan, int32_t cols, int32_t nnz,
+                                        const int32_t *rowPtr, const int32_t *colIdx,
+                                        const void *values, bsp_dtype dtype, const void *B,
+                                        int32_t N, int64_t ldb, float *C, int64_t ldc,
+                                        float alpha, float beta, void *workspace,
+                                        size_t workspace_bytes, int32_t engine,
+                                        int32_t slab_cols, bsp_stream_t stream);
 
 /* Block (SMaT) form: 16x16 tiles of the matrix (the reference's csrToBcsr
  * with TILE_M = TILE_K = 16, smat.cu:116-120) in F16 or BF16, staged with

@@ -107,6 +107,13 @@ void orc_dasp_free(orc_dasp *o);
 void orc_blockinfo(int32_t rows, const int32_t *rowPtr, const int32_t *colIdx, int64_t *blocks,
                    int64_t *blocks_recorder);
 
+/* Per-block power-of-two-scaled FP16 (dtype 2) / BF16 (dtype 3) BSR: the
+ * quantized arrays of the library's bsp_bsr_scaled, and their exact FP64
+ * values back in row-major blocks (oracle_formats.c). */
+int32_t orc_bsr_scale(int64_t nb, int32_t bs, int32_t dtype, const int32_t *blcIdx, const double *blcVal,
+                      uint32_t *key, uint16_t *val);
+void orc_bsr_unscale(int64_t nb, int32_t bs, int32_t dtype, const uint32_t *key, const uint16_t *val, double *out);
+
 /* Benchmark input generator (oracle_gen.c): the seeded 27-point stencil with
  * `dof` unknowns per node and the seeded uniform vector, bit-identical to the
  * library's generator.  orc_gen_stencil27 returns nnz (arrays may be NULL to

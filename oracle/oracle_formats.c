@@ -2,6 +2,7 @@
  * oracle_formats.c — CPU restatement of the reference's format converters
  * (BCSR, DBSR, block statistics).  TEST INFRASTRUCTURE ONLY (see oracle.h).
  */
+#include <math.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -424,4 +425,70 @@ void orc_blockinfo(int32_t rows, const int32_t *rowPtr, const int32_t *colIdx, i
   *blocks_recorder = distinct_u32(kr, nnz);
   free(kp);
   free(kr);
+}
+
+/* ------------------------------------------------------------------------
+ * Per-block power-of-two-scaled FP16/BF16 BSR (the format of the library's
+ * bsp_bsr_scaled; the reference has no scaled storage, its BSR values are
+ * FP64 only, src/amgT.cu:210-274).  Per block: m = max |a|, E = floor(log2 m)
+ * from the exponent bits, e = E - 14 (FP16: the largest magnitude lands in
+ * [2^14, 2^15)) or E (BF16: [1, 2)), clamped to [-126, 127], e = 0 for an
+ * all-zero block; q = round-to-nearest-even((float)(a * 2^-e)).  Values are
+ * stored in 4x4 tiles (row-major inside a tile; an 8x8 block's tiles in the
+ * order (0,0), (0,1), (1,0), (1,1)); key = block column | (e + 128) << 24.
+ * Returns 1 when a value is not finite or rounds to inf, else 0. */
+int32_t orc_bsr_scale(int64_t nb, int32_t bs, int32_t dtype, const int32_t *blcIdx, const double *blcVal,
+                      uint32_t *key, uint16_t *val) {
+  int32_t bad = 0;
+  const int bb = bs * bs, ts = bs / 4;
+  for (int64_t k = 0; k < nb; k++) {
+    const double *v = blcVal + k * bb;
+    double m = 0;
+    for (int i = 0; i < bb; i++) {
+      const double a = fabs(v[i]);
+      if (!(a <= 1.7976931348623157e308)) bad = 1;
+      if (a > m) m = a;
+    }
+    int e = 0;
+    if (m > 0) {
+      uint64_t bits;
+      memcpy(&bits, &m, 8);
+      const int E = (int)((bits >> 52) & 0x7ff) - 1023;
+      e = dtype == 2 ? E - 14 : E; /* 2 = FP16, 3 = BF16 */
+      if (e < -126) e = -126;
+      if (e > 127) e = 127;
+    }
+    const double down = ldexp(1.0, -e);
+    for (int r = 0; r < bs; r++)
+      for (int c = 0; c < bs; c++) {
+        const float f = (float)(v[r * bs + c] * down);
+        uint16_t q;
+        if (dtype == 2) {
+          q = orc_f32_to_f16(f);
+          if ((q & 0x7c00u) == 0x7c00u) bad = 1;
+        } else {
+          q = orc_f32_to_bf16(f);
+          if ((q & 0x7f80u) == 0x7f80u) bad = 1;
+        }
+        const int t = (r / 4) * ts + c / 4;
+        val[k * bb + t * 16 + (r % 4) * 4 + c % 4] = q;
+      }
+    key[k] = (uint32_t)blcIdx[k] | ((uint32_t)(e + 128) << 24);
+  }
+  return bad;
+}
+
+/* The scaled blocks back to FP64 in row-major block order (exact: q times a
+ * power of two). */
+void orc_bsr_unscale(int64_t nb, int32_t bs, int32_t dtype, const uint32_t *key, const uint16_t *val, double *out) {
+  const int bb = bs * bs, ts = bs / 4;
+  for (int64_t k = 0; k < nb; k++) {
+    const int e = (int)(key[k] >> 24) - 128;
+    for (int r = 0; r < bs; r++)
+      for (int c = 0; c < bs; c++) {
+        const uint16_t q = val[k * bb + ((r / 4) * ts + c / 4) * 16 + (r % 4) * 4 + c % 4];
+        const double f = dtype == 2 ? (double)orc_f16_to_f32(q) : (double)orc_bf16_to_f32(q);
+        out[k * bb + r * bs + c] = ldexp(f, e);
+      }
+  }
 }

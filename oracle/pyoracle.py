@@ -385,3 +385,57 @@ def gen_uniform(n: int, seed: int) -> np.ndarray:
     x = np.empty(n, np.float64)
     L.orc_gen_uniform(n, seed, _p(x))
     return x
+
+
+# ---------------------------------------------------------------------------
+# Per-block power-of-two-scaled FP16/BF16 BSR (oracle_formats.c)
+
+def bsr_scale(blcIdx, blcVal, bs: int, dtype: str) -> tuple:
+    """(key, val, bad) of the library's scaled BSR format from FP64 blocks."""
+    L = orc()
+    L.orc_bsr_scale.restype = _I32
+    L.orc_bsr_scale.argtypes = [_I64, _I32, _I32, _P, _P, _P, _P]
+    nb = blcIdx.size
+    key = np.empty(nb, np.uint32)
+    val = np.empty(nb * bs * bs, np.uint16)
+    dt = {"f16": 2, "bf16": 3}[dtype]
+    bad = L.orc_bsr_scale(nb, bs, dt, _p(np.ascontiguousarray(blcIdx, np.int32)),
+                          _p(np.ascontiguousarray(blcVal, np.float64)), _p(key), _p(val))
+    return key, val, int(bad)
+
+
+def bsr_unscale(key, val, bs: int, dtype: str) -> np.ndarray:
+    """Exact FP64 values of scaled blocks, row-major per block."""
+    L = orc()
+    L.orc_bsr_unscale.restype = None
+    L.orc_bsr_unscale.argtypes = [_I64, _I32, _I32, _P, _P, _P]
+    out = np.empty(val.size, np.float64)
+    L.orc_bsr_unscale(key.size, bs, {"f16": 2, "bf16": 3}[dtype], _p(key), _p(val), _p(out))
+    return out
+
+
+def bsr_spmv_f64(rows: int, blcPtr, blcIdx, blockvals, bs: int, x) -> tuple:
+    """FP64 y = A x of a BSR matrix given by row-major FP64 blocks, and
+    sum_j |a_ij x_j| per row (for the rounding bound); x is zero-padded to
+    whole block columns."""
+    nb = blcIdx.size
+    brow = blcPtr.size - 1
+    V = np.asarray(blockvals, np.float64).reshape(nb, bs, bs)
+    xp = np.zeros(((x.size + bs - 1) // bs + 1) * bs)
+    xp[:x.size] = x
+    Xb = xp[blcIdx.astype(np.int64)[:, None] * bs + np.arange(bs)[None, :]]          # [nb, bs]
+    part = np.einsum("krc,kc->kr", V, Xb)
+    apart = np.einsum("krc,kc->kr", np.abs(V), np.abs(Xb))
+    owner = np.repeat(np.arange(brow), np.diff(blcPtr))
+    y = np.zeros((brow, bs))
+    ay = np.zeros((brow, bs))
+    np.add.at(y, owner, part) if nb < 4096 else _segsum(y, blcPtr, part)
+    np.add.at(ay, owner, apart) if nb < 4096 else _segsum(ay, blcPtr, apart)
+    return y.reshape(-1)[:rows], ay.reshape(-1)[:rows]
+
+
+def _segsum(out, ptr, part) -> None:
+    """out[b] = sum of part[ptr[b]:ptr[b+1]] (rows of 2-D arrays)."""
+    nz = np.flatnonzero(np.diff(ptr) > 0)
+    if nz.size:
+        out[nz] = np.add.reduceat(part, ptr[nz].astype(np.int64), axis=0)

@@ -93,6 +93,40 @@ def test_c2_stencil64_bsr(cuda, stencil, bs, algo):
     torch.cuda.synchronize()
 
 
+@pytest.mark.parametrize("dtype", ["f16", "bf16"])
+def test_c2_stencil64_scaled_16bit(cuda, stencil, dtype):
+    """The headline matrix stored as FP16/BF16 with one power-of-two scale
+    per 4x4 block: the quantized arrays bit-exact with the oracle's
+    restatement of the format, the FP32-accumulated SpMV within
+    2*gamma_L(2^-24) * sum |a x| (L = row length + 3) of the FP64 product of
+    the dequantized matrix, and within that plus the 16-bit rounding (2^-11
+    FP16, 2^-8 BF16, of sum |a x|) of ref_spmv_fp64 on the FP64 matrix."""
+    A, x, ref, tol = stencil
+    rp, ci, va, xx = _dev(cuda, A.rowptr, A.colidx, A.values, x)
+    M = bsp.csr2bsr(rp, ci, va, rows=A.rows, cols=A.cols, bs=4)
+    del rp, ci, va
+    S = M.scaled(dtype)
+    src = M.arrays()
+    M.free()
+    got = S.arrays()
+    key, val, bad = pyoracle.bsr_scale(src["blcIdx"], src["blcVal"], 4, dtype)
+    assert bad == 0 and np.array_equal(got["blcKey"], key) and np.array_equal(got["blcVal"], val)
+    del got
+    y = S.spmv(xx).cpu().numpy()
+    S.free()
+    deq = pyoracle.bsr_unscale(key, val, 4, dtype)
+    del key, val
+    yq, ayq = pyoracle.bsr_spmv_f64(A.rows, src["blcPtr"], src["blcIdx"], deq, 4, x)
+    del deq
+    L = np.diff(A.rowptr).astype(np.float64) + 3.0
+    u = 2.0 ** -24
+    tq = 2.0 * (L * u / (1.0 - L * u)) * ayq + 1e-300
+    _assert_within(y, yq, tq, f"scaled {dtype} vs dequantized")
+    quant = {"f16": 2.0 ** -11, "bf16": 2.0 ** -8}[dtype]
+    absrow = pyoracle.abs_rowsum(A.rowptr, A.colidx, A.values, x)
+    _assert_within(y, ref, tq + tol + 1.01 * quant * absrow, f"scaled {dtype} vs ref_spmv_fp64")
+
+
 @pytest.mark.parametrize("bs", [4, 8])
 def test_c2c_random_block_fill(cuda, bs):
     """16 random block columns per block row, per-block fill U[30%, 100%]."""

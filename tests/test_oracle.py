@@ -215,3 +215,50 @@ def test_cpu_cg_oracle_converges():
     x, it = pyoracle.cg(A.rowptr, A.colidx, A.values, b, 1e-10)
     assert 0 < it < 500
     assert pyoracle.rel_residual(A.rowptr, A.colidx, A.values, b, x) <= 1e-10
+
+
+def test_scaled_bsr_oracle_known_answers_and_round_trip():
+    """orc_bsr_scale: a block whose largest magnitude is 1.0 gets e = -14
+    (FP16, 1.0 -> q = 2^14 = 0x7400) or e = 0 (BF16, q = 0x3F80); an all-zero
+    block e = 0; the dequantized values are within half an ulp of the 16-bit
+    type (relative 2^-11 / 2^-8 of the block's largest magnitude)."""
+    from oracle import pyoracle
+    blk = np.zeros(16)
+    blk[0] = 1.0
+    blk[5] = -0.5
+    vals = np.concatenate([blk, np.zeros(16)])
+    idx = np.array([3, 7], np.int32)
+    key, val, bad = pyoracle.bsr_scale(idx, vals, 4, "f16")
+    assert bad == 0 and list(key) == [3 | ((128 - 14) << 24), 7 | (128 << 24)]
+    assert val[0] == 0x7400 and val[5] == 0xF000 and not val[16:].any()
+    key, val, _ = pyoracle.bsr_scale(idx, vals, 4, "bf16")
+    assert list(key >> 24) == [128, 128] and val[0] == 0x3F80 and val[5] == 0xBF00
+    rng = np.random.default_rng(3)
+    for bs, dt, rel in ((4, "f16", 2.0 ** -11), (8, "f16", 2.0 ** -11), (4, "bf16", 2.0 ** -8), (8, "bf16", 2.0 ** -8)):
+        nb = 500
+        v = rng.standard_normal(nb * bs * bs) * np.repeat(10.0 ** rng.integers(-30, 30, nb), bs * bs)
+        key, val, bad = pyoracle.bsr_scale(np.arange(nb, dtype=np.int32), v, bs, dt)
+        assert bad == 0
+        back = pyoracle.bsr_unscale(key, val, bs, dt).reshape(nb, -1)
+        m = np.abs(v.reshape(nb, -1)).max(axis=1, keepdims=True)
+        assert np.all(np.abs(back - v.reshape(nb, -1)) <= rel * np.maximum(np.abs(v.reshape(nb, -1)), 2.0 ** -14 * m))
+    # tile layout of an 8x8 block: tile (r//4, c//4), entry (r%4, c%4)
+    v = np.arange(64, dtype=np.float64) + 1
+    key, val, _ = pyoracle.bsr_scale(np.zeros(1, np.int32), v, 8, "bf16")
+    back = pyoracle.bsr_unscale(key, val, 8, "bf16")
+    assert np.array_equal(back, v)    # small integers are exact in BF16 after a power-of-two scale
+    e = int(key[0] >> 24) - 128
+    q = np.array([np.ldexp(float(i + 1), -e) for i in range(64)], np.float32).view(np.uint32) >> 16
+    assert val[16 * 1 + 0] == q[4] and val[16 * 2 + 0] == q[32] and val[16 * 3 + 5] == q[36 + 9]
+
+
+def test_oracle_bsr_spmv_helper_matches_csr_spmv():
+    from oracle import pyoracle
+    import benchsp_b200 as bsp
+    A = bsp.gen_random_bsr(40, 4, 5, 0.3, 1.0, 2)
+    o = pyoracle.csr2bsr(A.rows, A.cols, A.rowptr, A.colidx, A.values, 4)
+    x = bsp.gen_uniform(A.cols, 5)
+    y, ay = pyoracle.bsr_spmv_f64(A.rows, o["blcPtr"], o["blcIdx"], o["blcVal"], 4, x)
+    ref = pyoracle.spmv_f64(A.rowptr, A.colidx, A.values, x)
+    assert np.allclose(y, ref, rtol=1e-13, atol=1e-13)
+    assert np.allclose(ay, pyoracle.abs_rowsum(A.rowptr, A.colidx, A.values, x), rtol=1e-13)

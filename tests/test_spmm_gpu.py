@@ -229,3 +229,53 @@ def test_smat_tcgen05_and_mma_sync_paths(cuda, name, N, kind):
     with pytest.raises(bsp.BspError):
         M.spmm(torch.zeros(A.cols, 96, dtype=Bd.dtype, device=cuda), path="tcgen05")   # N % 128 != 0
     M.free()
+
+
+@pytest.mark.parametrize("name", ["f16", "bf16", "f32"])
+@pytest.mark.parametrize("N,slab", [(32, 0), (64, 16), (128, 32), (128, 64), (256, 32), (40, 8), (256, 256)])
+def test_spmm_slab_engine_matches_fp64(cuda, name, N, slab):
+    """The slab engine (column slabs, length-sorted short rows one per lane
+    group, long-row chunks a warp each): every slab width against the FP64
+    oracle within the FP32 accumulation bound, with long rows (split into
+    chunks), empty rows, and alpha/beta; repeat calls give the same bits."""
+    import torch
+    if name == "f32" and slab > 128:
+        pytest.skip("F32 slabs are at most 32 lanes x 4 columns")
+    if name != "f32" and (N % 8 or (slab and slab % 8)):
+        pytest.skip("16-bit slabs are multiples of 8 columns")
+    rng = np.random.default_rng(N + slab)
+    n = 6000
+    lens = rng.integers(0, 40, n)
+    lens[rng.integers(0, n, 5)] = rng.integers(300, 3000, 5)   # split into 256-nonzero chunks
+    lens[::11] = 0
+    rp = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    ci = np.concatenate([np.sort(rng.choice(n, l, replace=False)) for l in lens]).astype(np.int32)
+    A = bsp.HostCSR(n, n, rp, ci, rng.uniform(-1, 1, rp[-1]))
+    vals_t, vals64, B_t, B64 = _case(A, N, name, 7)
+    Cin = rng.uniform(-1, 1, (n, N)).astype(np.float32)
+    rpd, cid = _dev(cuda, A.rowptr, A.colidx)
+    P = bsp.SpmmPlan(rpd, cid, vals_t.to(cuda), cols=A.cols, chunk=256)
+    assert P.nsplit == 5
+    Bd = B_t.to(cuda)
+    C1 = P.spmm(Bd, engine="slab", slab_cols=slab)
+    assert torch.equal(C1, P.spmm(Bd, engine="slab", slab_cols=slab))
+    Cref, absC = pyoracle.spmm_f64(A.rowptr, A.colidx, vals64, B64)
+    assert np.all(np.abs(C1.cpu().numpy().astype(np.float64) - Cref) <= _tol(A, absC))
+    Cd = torch.from_numpy(Cin.copy()).to(cuda)
+    P.spmm(Bd, Cd, alpha=0.5, beta=-1.5, engine="slab", slab_cols=slab)
+    want = 0.5 * Cref - 1.5 * Cin.astype(np.float64)
+    assert np.all(np.abs(Cd.cpu().numpy().astype(np.float64) - want) <= _tol(A, absC, 0.5, Cin, -1.5))
+    P.free()
+
+
+def test_spmm_slab_engine_rejects_bad_widths(cuda):
+    import torch
+    A = bsp.gen_powerlaw(500, 1.8, 100, 3)
+    rp, ci = _dev(cuda, A.rowptr, A.colidx)
+    v = torch.from_numpy(A.values).to(torch.float16).to(cuda)
+    B = torch.zeros(A.cols, 64, dtype=torch.float16, device=cuda)
+    P = bsp.SpmmPlan(rp, ci, v, cols=A.cols)
+    for bad in (24, 48, 512):   # not a power of two times 8, or wider than N
+        with pytest.raises(bsp.BspError):
+            P.spmm(B, engine="slab", slab_cols=bad)
+    P.free()
