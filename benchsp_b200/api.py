@@ -743,10 +743,11 @@ class SmatMatrix:
     def tiles(self) -> int:
         return self._d.tiles.nonzeroBlocks
 
-    _PATHS = {"auto": 0, "mma_sync": 1, "tcgen05": 2}
+    _PATHS = {"auto": 0, "mma_sync": 1, "tcgen05": 2, "tcgen05_w64": 3, "tcgen05_w128": 4}
 
     def spmm(self, B, C=None, *, alpha: float = 1.0, beta: float = 0.0, path: str = "auto", stream=None):
-        """path: "auto" (tcgen05 when N % 128 == 0), "mma_sync" or "tcgen05"."""
+        """path: "auto" / "tcgen05" (tensor cores, slab width from L2),
+        "tcgen05_w64" / "tcgen05_w128" (explicit slab width) or "mma_sync"."""
         torch = _torch()
         N = B.shape[1]
         if C is None:

@@ -514,8 +514,8 @@ extern "C" bsp_status bsp_spmm_choose_host(int32_t rows, int32_t cols, int32_t n
     if (colIdx[j] < 0 || colIdx[j] >= cols) return fail(BSP_ERR_INVALID, "bsp_spmm_choose: column out of range");
   bsp_spmm_choice c{};
   const bool smat_ok = N % 32 == 0;
-  c.smat_path = N % 128 == 0 ? BSP_SMAT_TCGEN05 : BSP_SMAT_MMA_SYNC;
-  const double per_tile = (N % 128 == 0 ? kTileColSecTc : kTileColSecMma) * N;
+  c.smat_path = BSP_SMAT_TCGEN05;
+  const double per_tile = kTileColSecTc * N;
   c.tiles_given = count_tiles(rows, rowPtr, colIdx, nullptr);
   c.tiles_reordered = -1;
   if (perm && rows > 0) {

@@ -514,9 +514,15 @@ __device__ __forceinline__ void umma_commit(uint64_t *bar) {
                : "memory");
 }
 
+// W (64 or 128) = C columns per CTA.  With W = 64 only the first 64-column
+// box of each stage is loaded and the MMA's rows 64..127 (whatever the stage
+// held) are never read back; this halves the B slab (B rows x W) that the
+// CTAs of one slab pass keep in L2.  Columns at or past N are zero-filled by
+// TMA and not stored.
 template <typename T>
 __global__ void __launch_bounds__(kTcThreads) spmm_tc_kernel(const __grid_constant__ CUtensorMap tmB, int32_t M,
-                                                             int32_t nbr, const int32_t *__restrict__ bptr,
+                                                             int32_t N, int32_t W, int32_t nbr,
+                                                             const int32_t *__restrict__ bptr,
                                                              const int32_t *__restrict__ bcol,
                                                              const T *__restrict__ tiles, float *__restrict__ C,
                                                              int64_t ldc, float alpha, float beta,
@@ -533,7 +539,8 @@ __global__ void __launch_bounds__(kTcThreads) spmm_tc_kernel(const __grid_consta
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int32_t br = blockIdx.x;
-  const int32_t n0 = blockIdx.y * kTcSlab;
+  const int32_t n0 = blockIdx.y * W;
+  const bool two_boxes = W > 64;
   const int32_t k0 = bptr[br], nk = bptr[br + 1] - k0;
 
   if (threadIdx.x == 0) {
@@ -567,9 +574,9 @@ __global__ void __launch_bounds__(kTcThreads) spmm_tc_kernel(const __grid_consta
     auto load = [&](int i) {
       const int st = i % kTcStages;
       const int32_t bc = bcol[k0 + i];
-      mbar_expect_tx(&full[st], kTcBBytes + kTcABytes);
+      mbar_expect_tx(&full[st], (two_boxes ? kTcBBytes : kTcBBytes / 2) + kTcABytes);
       tma_load_2d(bslab + st * kTcBBytes, &tmB, n0, bc * kTS, &full[st]);
-      tma_load_2d(bslab + st * kTcBBytes + kTcBBytes / 2, &tmB, n0 + 64, bc * kTS, &full[st]);
+      if (two_boxes) tma_load_2d(bslab + st * kTcBBytes + kTcBBytes / 2, &tmB, n0 + 64, bc * kTS, &full[st]);
       bulk_g2s(atile + st * kTcABytes, tiles + (int64_t)(k0 + i) * kTS * kTS, kTcABytes, &full[st]);
       ++issued;
     };
@@ -625,10 +632,11 @@ __global__ void __launch_bounds__(kTcThreads) spmm_tc_kernel(const __grid_consta
   }
   if (all_good) {
     const int64_t col = (int64_t)n0 + warp * 32 + lane;
+    const bool mine = warp * 32 < W && col < N;
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
       const int64_t row = (int64_t)br * kTS + j;
-      if (row < M) {
+      if (mine && row < M) {
         float *cp = C + row * ldc + col;
         float o = alpha * v[j];
         if (beta != 0.f) o += beta * *cp;
@@ -870,19 +878,30 @@ extern "C" bsp_status bsp_smat_free(bsp_smat *m) {
   return BSP_OK;
 }
 
+// Slab width of the tcgen05 path: 128 columns per CTA when N >= 128 and a
+// 128-column slab of B (cols x 128) fits in 60% of L2, else 64 (the CTAs of
+// a slab run together, blockIdx.x fastest, so a slab is what L2 must hold).
+static int tc_slab_width(int32_t N, int32_t cols) {
+  int dev = 0, l2 = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev) != cudaSuccess)
+    l2 = 126 << 20;
+  return (N >= 128 && (double)cols * 128 * 2 <= 0.6 * (double)l2) ? 128 : 64;
+}
+
 static bsp_status smat_spmm_tc(const bsp_smat *m, const void *B, int32_t N, int64_t ldb, float *C, int64_t ldc,
-                               float alpha, float beta, cudaStream_t s) {
+                               float alpha, float beta, int32_t W, cudaStream_t s) {
   CUtensorMap map;
   BSP_TRY(make_b_map(&map, B, m->cols, N, ldb, m->dtype == BSP_BF16));
-  const dim3 grid((unsigned)m->tiles.rowRegions, (unsigned)(N / kTcSlab));
+  if (W == 0) W = tc_slab_width(N, m->cols);
+  const dim3 grid((unsigned)m->tiles.rowRegions, (unsigned)ceil_div(N, W));
   if (m->dtype == BSP_F16)
-    spmm_tc_kernel<__half><<<grid, kTcThreads, kTcSmem, s>>>(map, m->rows, m->tiles.rowRegions,
+    spmm_tc_kernel<__half><<<grid, kTcThreads, kTcSmem, s>>>(map, m->rows, N, W, m->tiles.rowRegions,
                                                              m->tiles.bcsrRowPtr, m->tiles.bcsrcolIdx,
                                                              (const __half *)m->tile_val, C, ldc, alpha, beta,
                                                              m->err);
   else
     spmm_tc_kernel<__nv_bfloat16><<<grid, kTcThreads, kTcSmem, s>>>(
-        map, m->rows, m->tiles.rowRegions, m->tiles.bcsrRowPtr, m->tiles.bcsrcolIdx,
+        map, m->rows, N, W, m->tiles.rowRegions, m->tiles.bcsrRowPtr, m->tiles.bcsrcolIdx,
         (const __nv_bfloat16 *)m->tile_val, C, ldc, alpha, beta, m->err);
   BSP_LAUNCH_CHECK();
   return BSP_OK;
@@ -903,12 +922,12 @@ extern "C" bsp_status bsp_smat_spmm_path(const bsp_smat *m, const void *B, int32
   // cp.async.bulk needs 16-byte aligned sources and sizes
   BSP_CHECK_ARG((uintptr_t)B % 16 == 0 && (ldb * 2) % 16 == 0, "B must be 16-byte aligned with ldb % 8 == 0");
   BSP_CHECK_ARG((uintptr_t)m->tile_val % 16 == 0, "tile values must be 16-byte aligned");
-  BSP_CHECK_ARG(path >= BSP_SMAT_AUTO && path <= BSP_SMAT_TCGEN05, "unknown path");
-  BSP_CHECK_ARG(path != BSP_SMAT_TCGEN05 || N % kTcSlab == 0, "the tcgen05 path needs N % 128 == 0");
+  BSP_CHECK_ARG(path >= BSP_SMAT_AUTO && path <= BSP_SMAT_TCGEN05_W128, "unknown path");
   if (m->tiles.rowRegions == 0) return BSP_OK;
   cudaStream_t s = as_stream(stream);
-  if (path == BSP_SMAT_TCGEN05 || (path == BSP_SMAT_AUTO && N % kTcSlab == 0))
-    return smat_spmm_tc(m, B, N, ldb, C, ldc, alpha, beta, s);
+  if (path == BSP_SMAT_TCGEN05_W64) return smat_spmm_tc(m, B, N, ldb, C, ldc, alpha, beta, 64, s);
+  if (path == BSP_SMAT_TCGEN05_W128) return smat_spmm_tc(m, B, N, ldb, C, ldc, alpha, beta, 128, s);
+  if (path == BSP_SMAT_TCGEN05 || path == BSP_SMAT_AUTO) return smat_spmm_tc(m, B, N, ldb, C, ldc, alpha, beta, 0, s);
   const int nt = (N % 64 == 0) ? 8 : 4;
   const int64_t items = (int64_t)m->tiles.rowRegions * (N / (8 * nt));
   int64_t blocks = ceil_div(items, kWarpsPerCta);

@@ -482,15 +482,18 @@ bsp_status bsp_smat_create(int32_t rows, int32_t cols, int32_t nnz,
                            bsp_stream_t stream);
 bsp_status bsp_smat_free(bsp_smat *m);
 /* B: dtype of the matrix, 16-byte aligned, ldb % 8 == 0; N % 32 == 0.
- * N % 128 == 0 runs on the tcgen05 tensor cores (TMEM accumulator, TMA
- * staging of B), otherwise on mma.sync. */
+ * Runs on the tcgen05 tensor cores (TMEM accumulator, TMA staging of B) in
+ * slabs of 128 or 64 C columns per CTA (64 when a 128-column slab of B would
+ * not stay in L2, or N < 128); bsp_smat_spmm_path can ask for mma.sync. */
 bsp_status bsp_smat_spmm(const bsp_smat *m, const void *B, int32_t N,
                          int64_t ldb, float *C, int64_t ldc, float alpha,
                          float beta, bsp_stream_t stream);
 typedef enum {
   BSP_SMAT_AUTO = 0,
   BSP_SMAT_MMA_SYNC = 1, /* warp mma.sync.m16n8k16, FP32 accumulators in registers */
-  BSP_SMAT_TCGEN05 = 2   /* tcgen05.mma M=128 N=16 K=16 per tile; N % 128 == 0 */
+  BSP_SMAT_TCGEN05 = 2,  /* tcgen05.mma M=128 N=16 K=16 per tile, slab width chosen from L2 */
+  BSP_SMAT_TCGEN05_W64 = 3,  /* tcgen05, 64 C columns per CTA */
+  BSP_SMAT_TCGEN05_W128 = 4  /* tcgen05, 128 C columns per CTA */
 } bsp_smat_path;
 bsp_status bsp_smat_spmm_path(const bsp_smat *m, const void *B, int32_t N,
                               int64_t ldb, float *C, int64_t ldc, float alpha,
@@ -660,7 +663,7 @@ bsp_status bsp_reorder_similarity_host(int32_t rows, int32_t cols, int32_t nnz,
 enum { BSP_SPMM_ENGINE_CSR = 0, BSP_SPMM_ENGINE_SMAT = 1 };
 typedef struct bsp_spmm_choice {
   int32_t engine;
-  int32_t smat_path;   /* BSP_SMAT_TCGEN05 (N % 128 == 0) or BSP_SMAT_MMA_SYNC */
+  int32_t smat_path;   /* BSP_SMAT_TCGEN05 */
   int32_t reorder;     /* 1: the SMaT matrix is built from the rows in perm order */
   int32_t reserved;
   int64_t tiles_given, tiles_reordered;   /* tiles_reordered = -1 without perm */

@@ -201,11 +201,13 @@ def test_smat_alpha_beta_and_argument_errors(cuda):
 
 
 @pytest.mark.parametrize("name", ["f16", "bf16"])
-@pytest.mark.parametrize("N", [128, 256])
+@pytest.mark.parametrize("N", [32, 64, 96, 128, 256])
 @pytest.mark.parametrize("kind", ["dense_tiles", "ragged"])
 def test_smat_tcgen05_and_mma_sync_paths(cuda, name, N, kind):
-    """The tcgen05 path (TMEM accumulator, TMA-staged B) and the mma.sync path
-    against the FP64 oracle; both deterministic across calls."""
+    """The tcgen05 path (TMEM accumulator, TMA-staged B) at both slab widths
+    (64 and 128 C columns per CTA; columns past N zero-filled by TMA and not
+    stored) and the mma.sync path against the FP64 oracle; all deterministic
+    across calls."""
     import torch
     A = bsp.gen_random_bsr(96, 16, 6, 1.0, 1.0, 4) if kind == "dense_tiles" else bsp.gen_powerlaw(1003, 1.7, 400, 12)
     vals_t, vals64, B_t, B64 = _case(A, N, name, N + 7)
@@ -216,7 +218,7 @@ def test_smat_tcgen05_and_mma_sync_paths(cuda, name, N, kind):
     L = np.full((A.rows, 1), 16.0 * ((A.cols + 15) // 16) + 2.0)
     u = 2.0 ** -24
     tol = 2.0 * (L * u / (1 - L * u)) * absC + 1e-30
-    for path in ("tcgen05", "mma_sync"):
+    for path in ("tcgen05", "tcgen05_w64", "tcgen05_w128", "mma_sync"):
         C1 = M.spmm(Bd, path=path).cpu().numpy()
         C2 = M.spmm(Bd, path=path).cpu().numpy()
         M.check()
@@ -227,7 +229,7 @@ def test_smat_tcgen05_and_mma_sync_paths(cuda, name, N, kind):
     want = 0.5 * Cref + 2.0 * Cin.cpu().numpy().astype(np.float64)
     assert np.all(np.abs(Cb - want) <= tol + 4 * u * (0.5 * absC + 2.0 * np.abs(Cin.cpu().numpy())))
     with pytest.raises(bsp.BspError):
-        M.spmm(torch.zeros(A.cols, 96, dtype=Bd.dtype, device=cuda), path="tcgen05")   # N % 128 != 0
+        M.spmm(torch.zeros(A.cols, 48, dtype=Bd.dtype, device=cuda), path="tcgen05")   # N % 32 != 0
     M.free()
 
 
