@@ -345,11 +345,11 @@ int64_t count_tiles(int32_t n, const int32_t *rp, const int32_t *ci, const int32
 // SpMM engine cost model, seconds per unit per column of B, from the B200
 // measurements of the SMaT and grouped CSR SpMM at N = 128 (dense-tile and
 // row-shuffled 524,288-row matrices, power-law graph): tcgen05 tiles cost
-// 0.86-0.91 ns per tile (7.0e-12 s per tile-column), mma.sync tiles 1.6x
-// that, the grouped CSR kernel 1.93 ms for 67.1M nonzeros (2.3e-13 s per
+// 0.86-0.91 ns per tile (7.0e-12 s per tile-column; the tensor-core path
+// now takes every N, so mma.sync tiles, 1.6x that, are not modelled), the
+// grouped CSR kernel 1.93 ms for 67.1M nonzeros (2.3e-13 s per
 // nonzero-column).
 constexpr double kTileColSecTc = 7.0e-12;
-constexpr double kTileColSecMma = 1.12e-11;
 constexpr double kNnzColSecCsr = 2.3e-13;
 
 bool valid_csr(int32_t n, int32_t nnz, const int32_t *rp) {
@@ -515,7 +515,8 @@ extern "C" bsp_status bsp_spmm_choose_host(int32_t rows, int32_t cols, int32_t n
   bsp_spmm_choice c{};
   const bool smat_ok = N % 32 == 0;
   c.smat_path = BSP_SMAT_TCGEN05;
-  const double per_tile = kTileColSecTc * N;
+  // the tensor-core path works in slabs of 64 or 128 C columns
+  const double per_tile = kTileColSecTc * (double)(((int64_t)N + 63) / 64 * 64);
   c.tiles_given = count_tiles(rows, rowPtr, colIdx, nullptr);
   c.tiles_reordered = -1;
   if (perm && rows > 0) {

@@ -204,9 +204,9 @@ def test_spmm_choice_scattered_rows_and_n():
     d, _ = bsp.choose_spmm_host(G, 128)
     assert d["engine"] == "csr" and _argmin_engine(d) == "csr"
     S, _ = _grouped(64, 4, 256, 16)
-    d, perm = bsp.choose_spmm_host(S, 96, reorder=False)        # N % 128 != 0: the mma.sync tile cost
+    d, perm = bsp.choose_spmm_host(S, 96, reorder=False)        # N % 128 != 0: tcgen05 in 64-column slabs
     assert perm is None and d["tiles_reordered"] == -1 and d["est_seconds_smat_reordered"] == -1.0
-    assert d["smat_path"] == "mma_sync" and d["engine"] == {"csr": "csr", "smat_given": "smat"}[_argmin_engine(d)]
+    assert d["smat_path"] == "tcgen05" and d["engine"] == {"csr": "csr", "smat_given": "smat"}[_argmin_engine(d)]
     d, _ = bsp.choose_spmm_host(S, 100)                         # SMaT needs N % 32 == 0
     assert d["engine"] == "csr" and d["est_seconds_smat_given"] == -1.0
     with pytest.raises(bsp.BspError):
