@@ -219,7 +219,7 @@ class BspBatchMat(C.Structure):
 class BspBatchOptions(C.Structure):
     """Mirror of bsp_batch_options (include/bsp.h)."""
     _fields_ = [("tune", C.c_int32), ("seg_nnz", C.c_int32), ("long_row_nnz", C.c_int32), ("item_nnz", C.c_int32),
-                ("use_graph", C.c_int32)]
+                ("use_graph", C.c_int32), ("sell", C.c_int32)]
 
 
 _PROTOS.update({
@@ -230,6 +230,7 @@ _PROTOS.update({
     "bsp_batch_run_separate": (C.c_int, [C.c_void_p, _P]),
     "bsp_batch_set_vectors": (C.c_int, [C.c_void_p, _I32, _P, _P, _P]),
     "bsp_batch_lanes": (C.c_int, [C.c_void_p, _P]),
+    "bsp_batch_formats": (C.c_int, [C.c_void_p, _P]),
     "bsp_batch_stats": (C.c_int, [C.c_void_p, _PI64, _PI64, _PI64]),
     "bsp_batch_destroy": (C.c_int, [C.c_void_p]),
     "bsp_gen_banded": (C.c_int, [_I32, _I32, _U64, _PI32, _PI64, _P, _P, _P]),

@@ -792,11 +792,12 @@ class BatchPlan:
     """y_m = A_m x_m for many CSR matrices in one persistent, graph-captured
     launch.  `mats` is a list of (rowptr, colidx, values, x, y) device tensors;
     values/x/y F64 or F32; nrhs 1 or 8 (x: cols x 8, y: rows x 8 row-major).
-    tune=0 picks lanes per row from row statistics, tune=1 times the
-    candidates per matrix."""
+    tune=0 picks lanes per row (and SELL-32 storage for matrices with even
+    rows) from row statistics, tune=1 times the candidates per matrix;
+    sell=False keeps every matrix in CSR."""
 
     def __init__(self, mats, *, nrhs: int = 1, tune: int = 0, seg_nnz: int = 1024, long_row_nnz: int = 2048,
-                 item_nnz: int = 0, use_graph: bool = True, stream=None):
+                 item_nnz: int = 0, use_graph: bool = True, sell: bool = True, stream=None):
         torch = _torch()
         if not mats:
             raise ValueError("empty batch")
@@ -811,7 +812,7 @@ class BatchPlan:
             cols = x.shape[0] if nrhs > 1 else x.numel()
             arr[i] = _lib.BspBatchMat(rows, cols, ci.numel(), _dptr(rp, "rowptr"), _dptr(ci, "colidx"),
                                       _dptr(va, "values"), _dptr(x, "x"), _dptr(y, "y"))
-        opt = _lib.BspBatchOptions(tune, seg_nnz, long_row_nnz, item_nnz, 1 if use_graph else 0)
+        opt = _lib.BspBatchOptions(tune, seg_nnz, long_row_nnz, item_nnz, 1 if use_graph else 0, 1 if sell else 0)
         self._h = C.c_void_p()
         self.count = len(mats)
         self._keep = list(mats)
@@ -832,6 +833,12 @@ class BatchPlan:
     def lanes(self) -> np.ndarray:
         out = np.empty(self.count, np.int32)
         check(lib().bsp_batch_lanes(self._h, out.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def formats(self) -> np.ndarray:
+        """Per-matrix storage: 0 = CSR, 1 = SELL-32."""
+        out = np.empty(self.count, np.int32)
+        check(lib().bsp_batch_formats(self._h, out.ctypes.data_as(C.c_void_p)))
         return out
 
     def stats(self) -> dict:

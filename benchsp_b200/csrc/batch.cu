@@ -36,13 +36,21 @@ struct BatchMatDev {
   const void *x;
   void *y;
   int32_t rows, cols;
+  // SELL-32 copy (null when the matrix is stored only as CSR): slice s of 32
+  // rows spans entries [sell_ptr[s], sell_ptr[s + 1]); entry k of row l of
+  // the slice at sell_ptr[s] + 32k + l; column = row + sell_off[entry]
+  const int32_t *sell_ptr;
+  const void *sell_val;
+  const int16_t *sell_off;
 };
 
-// info >= 0: row item, rows [a, b), info = lanes per row.
+// info == kSellItem: SELL slices [a, b).
+// info >= 0 otherwise: row item, rows [a, b), info = lanes per row.
 // info < 0 : long-row segment, row a, segment b, long id = -(info + 1).
 struct BatchItem {
   int32_t mat, a, b, info;
 };
+constexpr int32_t kSellItem = 64;
 
 struct LongRow {
   int32_t part_base, nseg;
@@ -192,6 +200,76 @@ __device__ __forceinline__ void rows_item(const BatchMatDev &M, int32_t r0, int3
   }
 }
 
+// SELL-32 slices [s0, s1): lane l owns row 32*s + l and sums its entries
+// in stored order, U entries' loads issued before their gathers.  Value and
+// offset loads of a warp are 32 consecutive entries (coalesced), and for
+// banded matrices the gathered x rows are consecutive too.
+template <typename V, int NRHS>
+__device__ __forceinline__ void sell_item(const BatchMatDev &M, int32_t s0, int32_t s1, int lane) {
+  constexpr int U = NRHS == 1 ? 4 : 2;
+  const V *sv = static_cast<const V *>(M.sell_val);
+  const V *x = static_cast<const V *>(M.x);
+  V *y = static_cast<V *>(M.y);
+  for (int32_t sl = s0; sl < s1; ++sl) {
+    const int32_t row = sl * 32 + lane;
+    const bool live = row < M.rows;
+    const int32_t p0 = __ldg(M.sell_ptr + sl);
+    const int32_t w = live ? (__ldg(M.sell_ptr + sl + 1) - p0) >> 5 : 0;
+    const V *vp = sv + p0 + lane;
+    const int16_t *op = M.sell_off + p0 + lane;
+    V acc[NRHS];
+#pragma unroll
+    for (int k = 0; k < NRHS; ++k) acc[k] = V(0);
+    int32_t k = 0;
+    for (; k + U <= w; k += U) {
+      V a[U];
+      int32_t c[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        a[u] = __ldg(vp + 32 * (k + u));
+        c[u] = row + (int32_t)__ldg(op + 32 * (k + u));
+      }
+      V xr[U][NRHS];
+#pragma unroll
+      for (int u = 0; u < U; ++u) load_xrow<V, NRHS>(x, c[u], xr[u]);
+#pragma unroll
+      for (int u = 0; u < U; ++u) fma_row<V, NRHS>(acc, a[u], xr[u]);
+    }
+    for (; k < w; ++k) {
+      V xr[NRHS];
+      load_xrow<V, NRHS>(x, row + (int32_t)__ldg(op + 32 * k), xr);
+      fma_row<V, NRHS>(acc, __ldg(vp + 32 * k), xr);
+    }
+    if (live) {
+#pragma unroll
+      for (int j = 0; j < NRHS; ++j) y[(int64_t)row * NRHS + j] = acc[j];
+    }
+  }
+}
+
+// Fills the SELL-32 copy of one matrix: thread per row; padding entries get
+// value 0 and the column min(row, cols - 1).  *bad is set when a column
+// lies 32768 or more from its row.
+template <typename V>
+__global__ void batch_sell_fill_kernel(int32_t rows, int32_t cols, const int32_t *__restrict__ rp,
+                                       const int32_t *__restrict__ ci, const V *__restrict__ val,
+                                       const int32_t *__restrict__ sptr, V *__restrict__ sval,
+                                       int16_t *__restrict__ soff, int32_t *__restrict__ bad) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t sl = (int32_t)(r >> 5), l = (int32_t)(r & 31);
+    const int32_t p0 = sptr[sl], w = (sptr[sl + 1] - p0) >> 5;
+    const int32_t s = rp[r], len = rp[r + 1] - s;
+    const int32_t pc = (int32_t)(r < (int64_t)cols - 1 ? r : (int64_t)cols - 1);
+    for (int32_t k = 0; k < w; ++k) {
+      const bool real = k < len;
+      const int64_t d = (int64_t)(real ? ci[s + k] : pc) - r;
+      if (d < -32768 || d > 32767) atomicExch(bad, 1);
+      sval[p0 + 32 * k + l] = real ? val[s + k] : V(0);
+      soff[p0 + 32 * k + l] = (int16_t)(d < -32768 || d > 32767 ? 0 : d);
+    }
+  }
+}
+
 template <typename V, int NRHS>
 __device__ __forceinline__ void segment_item(const BatchMatDev &M, int32_t row, int32_t seg, int32_t lid,
                                              int32_t seg_nnz, const LongRow *__restrict__ longs,
@@ -244,6 +322,10 @@ __global__ void __launch_bounds__(kBatchThreads, (NRHS == 1 && sizeof(V) == 4) ?
     if (it >= nitems) return;
     const BatchItem I = items[it];
     const BatchMatDev M = mats[I.mat];
+    if (I.info == kSellItem) {
+      sell_item<V, NRHS>(M, I.a, I.b, lane);
+      continue;
+    }
     if (I.info < 0) {
       segment_item<V, NRHS>(M, I.a, I.b, -(I.info + 1), seg_nnz, longs, part, arrive, lane);
       continue;
@@ -270,6 +352,13 @@ struct bsp_batch_plan_s {
   std::vector<bsp_batch_mat> host_mats;
   std::vector<std::vector<int32_t>> lens;  // row lengths per matrix
   std::vector<int32_t> lanes;
+  std::vector<int32_t> fmt;                 // 0 CSR, 1 SELL-32
+  std::vector<uint8_t> sell_ok;             // the matrix has a SELL-32 copy
+  std::vector<std::vector<int32_t>> sell_slices;  // slice pointers (host copy)
+  std::vector<BatchMatDev> dm;              // host copy of the descriptors
+  void *d_sell_val = nullptr;
+  int16_t *d_sell_off = nullptr;
+  int32_t *d_sell_ptr = nullptr;
   BatchMatDev *d_mats = nullptr;
   // batched list (long segments first) and per-matrix lists
   BatchItem *d_items = nullptr, *d_items_sep = nullptr;
@@ -300,6 +389,40 @@ int model_lanes(const std::vector<int32_t> &len, int32_t long_thr, int nrhs) {
   int L = 1;
   while (L < 32 && (double)L * per_lane < mean) L <<= 1;
   return mean <= 2.0 * per_lane ? 1 : L;
+}
+
+// SELL-32 slice pointers of a matrix from its row lengths; empty when the
+// padding would add more than 1/8 to the entries, a row is longer than
+// long_thr, or the padded size passes 2^31.
+std::vector<int32_t> sell_slices(const std::vector<int32_t> &len, int32_t long_thr) {
+  const int64_t n = (int64_t)len.size();
+  const int64_t ns = (n + 31) / 32;
+  std::vector<int32_t> ptr((size_t)ns + 1, 0);
+  int64_t nnz = 0, acc = 0;
+  for (int64_t sl = 0; sl < ns; ++sl) {
+    int32_t w = 0;
+    for (int64_t r = sl * 32; r < std::min(n, sl * 32 + 32); ++r) {
+      if (len[r] > long_thr) return {};
+      w = std::max(w, len[r]);
+      nnz += len[r];
+    }
+    acc += 32 * (int64_t)w;
+    if (acc >= INT32_MAX) return {};
+    ptr[sl + 1] = (int32_t)acc;
+  }
+  if (n == 0 || 8 * acc > 9 * nnz) return {};
+  return ptr;
+}
+
+// Items of a SELL-32 matrix: runs of slices holding about item_nnz entries.
+void build_sell_items(int32_t m, const std::vector<int32_t> &sptr, int64_t item_nnz, std::vector<BatchItem> &out) {
+  const int32_t ns = (int32_t)sptr.size() - 1;
+  int32_t s0 = 0;
+  for (int32_t sl = 0; sl < ns; ++sl)
+    if ((int64_t)sptr[sl + 1] - sptr[s0] >= item_nnz || sl + 1 == ns) {
+      out.push_back({m, s0, sl + 1, kSellItem});
+      s0 = sl + 1;
+    }
 }
 
 // Items of matrix m for lanes L: long segments (appended to `lng`, with
@@ -343,6 +466,7 @@ extern "C" bsp_status bsp_batch_default_options(bsp_batch_options *o) {
   o->long_row_nnz = 2048;
   o->item_nnz = 0;
   o->use_graph = 1;
+  o->sell = 1;
   return BSP_OK;
 }
 
@@ -397,7 +521,10 @@ static bsp_status batch_build(bsp_batch_plan P, cudaStream_t s) {
   P->sep_off.assign(P->count + 1, 0);
   for (int32_t m = 0; m < P->count; ++m) {
     std::vector<BatchItem> l1, r1;
-    build_items(m, P->lens[m], P->lanes[m], o, l1, r1, longs, parts, item_nnz);
+    if (P->fmt[m] == 1)
+      build_sell_items(m, P->sell_slices[m], item_nnz, r1);
+    else
+      build_items(m, P->lens[m], P->lanes[m], o, l1, r1, longs, parts, item_nnz);
     lng.insert(lng.end(), l1.begin(), l1.end());
     rows.insert(rows.end(), r1.begin(), r1.end());
     sep.insert(sep.end(), l1.begin(), l1.end());
@@ -480,10 +607,89 @@ extern "C" bsp_status bsp_batch_destroy(bsp_batch_plan P) {
   dfree(P->d_arrive, s);
   dfree(P->d_next, s);
   if (P->d_part) cudaFreeAsync(P->d_part, s);
+  if (P->d_sell_val) cudaFreeAsync(P->d_sell_val, s);
+  dfree(P->d_sell_off, s);
+  dfree(P->d_sell_ptr, s);
   cudaStreamSynchronize(s);
   delete P;
   return BSP_OK;
 }
+
+namespace {
+// Builds the SELL-32 copies of every matrix that qualifies (one allocation
+// for all) and fills P->sell_ok; a matrix whose copy would need a column
+// offset outside int16 stays CSR-only.
+bsp_status build_sell(bsp_batch_plan P, cudaStream_t s) {
+  const int32_t count = P->count;
+  P->sell_ok.assign(count, 0);
+  P->sell_slices.assign(count, {});
+  if (!P->opt.sell) return BSP_OK;
+  int64_t total = 0, total_ptr = 0;
+  std::vector<int64_t> val_off(count, 0), ptr_off(count, 0);
+  for (int32_t m = 0; m < count; ++m) {
+    if (P->host_mats[m].cols <= 0) continue;
+    P->sell_slices[m] = sell_slices(P->lens[m], P->opt.long_row_nnz);
+    if (P->sell_slices[m].empty()) continue;
+    val_off[m] = total;
+    ptr_off[m] = total_ptr;
+    total += P->sell_slices[m].back();
+    total_ptr += (int64_t)P->sell_slices[m].size();
+    P->sell_ok[m] = 1;
+  }
+  if (total_ptr == 0) return BSP_OK;
+  const size_t es = P->dtype == BSP_F64 ? 8 : 4;
+  BSP_CUDA(cudaMallocAsync(&P->d_sell_val, (size_t)std::max<int64_t>(total, 1) * es, s));
+  BSP_TRY(dalloc(&P->d_sell_off, (size_t)std::max<int64_t>(total, 1), s));
+  BSP_TRY(dalloc(&P->d_sell_ptr, (size_t)total_ptr, s));
+  int32_t *bad = nullptr;
+  BSP_TRY(dalloc(&bad, (size_t)count, s));
+  BSP_CUDA(cudaMemsetAsync(bad, 0, sizeof(int32_t) * count, s));
+  BSP_CUDA(cudaMemsetAsync(P->d_sell_val, 0, (size_t)std::max<int64_t>(total, 1) * es, s));
+  BSP_CUDA(cudaMemsetAsync(P->d_sell_off, 0, sizeof(int16_t) * (size_t)std::max<int64_t>(total, 1), s));
+  for (int32_t m = 0; m < count; ++m) {
+    if (!P->sell_ok[m]) continue;
+    const std::vector<int32_t> &sp = P->sell_slices[m];
+    int32_t *dptr = P->d_sell_ptr + ptr_off[m];
+    BSP_CUDA(cudaMemcpyAsync(dptr, sp.data(), sp.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    const bsp_batch_mat &A = P->host_mats[m];
+    const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div(A.rows, 256), 4096));
+    int16_t *off = P->d_sell_off + val_off[m];
+    if (P->dtype == BSP_F64) {
+      double *v = static_cast<double *>(P->d_sell_val) + val_off[m];
+      batch_sell_fill_kernel<double><<<grid, 256, 0, s>>>(A.rows, A.cols, A.rowPtr, A.colIdx,
+                                                          static_cast<const double *>(A.values), dptr, v, off,
+                                                          bad + m);
+      P->dm[m].sell_val = v;
+    } else {
+      float *v = static_cast<float *>(P->d_sell_val) + val_off[m];
+      batch_sell_fill_kernel<float><<<grid, 256, 0, s>>>(A.rows, A.cols, A.rowPtr, A.colIdx,
+                                                         static_cast<const float *>(A.values), dptr, v, off, bad + m);
+      P->dm[m].sell_val = v;
+    }
+    BSP_LAUNCH_CHECK();
+    P->dm[m].sell_ptr = dptr;
+    P->dm[m].sell_off = off;
+    // the copy sees the sync below: host vectors stay alive until then
+  }
+  std::vector<int32_t> hbad(count, 0);
+  BSP_CUDA(cudaMemcpyAsync(hbad.data(), bad, sizeof(int32_t) * count, cudaMemcpyDeviceToHost, s));
+  BSP_CUDA(cudaStreamSynchronize(s));
+  dfree(bad, s);
+  for (int32_t m = 0; m < count; ++m)
+    if (hbad[m]) {
+      P->sell_ok[m] = 0;
+      P->dm[m].sell_ptr = nullptr;
+      P->dm[m].sell_val = nullptr;
+      P->dm[m].sell_off = nullptr;
+    }
+  return BSP_OK;
+}
+
+// The row-statistics choice: SELL-32 for every qualifying matrix (rows even
+// enough that padding adds at most 1/8: every access coalesced and no
+// row-pointer round trip, against CSR's per-row dependent loads).
+int32_t model_format(const bsp_batch_plan P, int32_t m) { return P->sell_ok[m] ? 1 : 0; }
+}  // namespace
 
 extern "C" bsp_status bsp_batch_create(int32_t count, const bsp_batch_mat *mats, bsp_dtype dtype, int32_t nrhs,
                                        const bsp_batch_options *opt, bsp_batch_plan *out, bsp_stream_t stream) {
@@ -541,32 +747,45 @@ extern "C" bsp_status bsp_batch_create(int32_t count, const bsp_batch_mat *mats,
     P->total_nnz += A.nnz;
     P->lanes[m] = model_lanes(L, o.long_row_nnz, nrhs);
   }
-  std::vector<BatchMatDev> dm(count);
+  P->dm.resize(count);
   for (int32_t m = 0; m < count; ++m)
-    dm[m] = {mats[m].rowPtr, mats[m].colIdx, mats[m].values, mats[m].x, mats[m].y, mats[m].rows, mats[m].cols};
+    P->dm[m] = {mats[m].rowPtr, mats[m].colIdx, mats[m].values, mats[m].x, mats[m].y, mats[m].rows, mats[m].cols,
+                nullptr, nullptr, nullptr};
+  bsp_status st = build_sell(P, s);
+  if (st != BSP_OK) return fail(st);
+  P->fmt.assign(count, 0);
+  for (int32_t m = 0; m < count; ++m) P->fmt[m] = model_format(P, m);
   if (dalloc(&P->d_mats, (size_t)count, s) != BSP_OK || dalloc(&P->d_next, (size_t)count + 1, s) != BSP_OK)
     return fail(BSP_ERR_ALLOC);
   if (count > 0 &&
-      cudaMemcpyAsync(P->d_mats, dm.data(), dm.size() * sizeof(BatchMatDev), cudaMemcpyHostToDevice, s) !=
+      cudaMemcpyAsync(P->d_mats, P->dm.data(), P->dm.size() * sizeof(BatchMatDev), cudaMemcpyHostToDevice, s) !=
           cudaSuccess) {
     set_error("bsp_batch_create: copying descriptors failed");
     return fail(BSP_ERR_CUDA);
   }
-  bsp_status st = batch_build(P, s);
+  st = batch_build(P, s);
   if (st != BSP_OK) return fail(st);
   if (o.tune == 1) {
-    // time every candidate lanes value with one launch per matrix; keep the
-    // fastest (outputs are overwritten, inputs untouched)
+    // time every candidate (lanes 1..32 on CSR, then SELL-32 where the
+    // matrix has a copy) with one launch per matrix; keep the fastest
+    // (outputs are overwritten, inputs untouched)
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    const int cand[6] = {1, 2, 4, 8, 16, 32};
+    const int cand[7] = {1, 2, 4, 8, 16, 32, 0};   // 0: SELL-32
     std::vector<float> best(count, 1e30f);
     std::vector<int> best_l(P->lanes);
-    for (int ci = 0; ci < 6 && st == BSP_OK; ++ci) {
-      std::fill(P->lanes.begin(), P->lanes.end(), cand[ci]);
+    std::vector<int32_t> best_f(count, 0);
+    for (int ci = 0; ci < 7 && st == BSP_OK; ++ci) {
+      const bool sell = cand[ci] == 0;
+      if (sell && std::none_of(P->sell_ok.begin(), P->sell_ok.end(), [](uint8_t v) { return v != 0; })) break;
+      for (int32_t m = 0; m < count; ++m) {
+        P->fmt[m] = sell && P->sell_ok[m] ? 1 : 0;
+        if (!sell) P->lanes[m] = cand[ci];
+      }
       st = batch_build(P, s);
       for (int32_t m = 0; m < count && st == BSP_OK; ++m) {
+        if (sell && !P->sell_ok[m]) continue;
         float tmin = 1e30f;
         for (int rep = 0; rep < 3 && st == BSP_OK; ++rep) {
           cudaEventRecord(e0, s);
@@ -579,7 +798,10 @@ extern "C" bsp_status bsp_batch_create(int32_t count, const bsp_batch_mat *mats,
         }
         if (tmin < best[m]) {
           best[m] = tmin;
-          best_l[m] = cand[ci];
+          if (sell)
+            best_f[m] = 1;
+          else
+            best_l[m] = cand[ci], best_f[m] = 0;
         }
       }
     }
@@ -587,6 +809,7 @@ extern "C" bsp_status bsp_batch_create(int32_t count, const bsp_batch_mat *mats,
     cudaEventDestroy(e1);
     if (st != BSP_OK) return fail(st);
     P->lanes = best_l;
+    P->fmt = best_f;
     st = batch_build(P, s);
     if (st != BSP_OK) return fail(st);
   }
@@ -626,7 +849,9 @@ extern "C" bsp_status bsp_batch_set_vectors(bsp_batch_plan P, int32_t m, const v
   cudaStream_t s = as_stream(stream);
   P->host_mats[m].x = x;
   P->host_mats[m].y = y;
-  const BatchMatDev d{A.rowPtr, A.colIdx, A.values, x, y, A.rows, A.cols};
+  P->dm[m].x = x;
+  P->dm[m].y = y;
+  const BatchMatDev d = P->dm[m];
   // the descriptor is read by the kernel: update it in stream order
   BSP_CUDA(cudaMemcpyAsync(P->d_mats + m, &d, sizeof(d), cudaMemcpyHostToDevice, s));
   BSP_CUDA(cudaStreamSynchronize(s));
@@ -636,7 +861,14 @@ extern "C" bsp_status bsp_batch_set_vectors(bsp_batch_plan P, int32_t m, const v
 extern "C" bsp_status bsp_batch_lanes(bsp_batch_plan P, int32_t *lanes) {
   clear_error();
   BSP_CHECK_ARG(P && lanes, "null pointer");
-  for (int32_t m = 0; m < P->count; ++m) lanes[m] = P->lanes[m];
+  for (int32_t m = 0; m < P->count; ++m) lanes[m] = P->fmt[m] == 1 ? 0 : P->lanes[m];
+  return BSP_OK;
+}
+
+extern "C" bsp_status bsp_batch_formats(bsp_batch_plan P, int32_t *formats) {
+  clear_error();
+  BSP_CHECK_ARG(P && formats, "null pointer");
+  for (int32_t m = 0; m < P->count; ++m) formats[m] = P->fmt[m];
   return BSP_OK;
 }
 

@@ -744,7 +744,17 @@ bsp_status bsp_spmv_plan_destroy(bsp_spmv_plan plan);
  * deterministic.  Warps take items from a counter, long segments first.
  * The launch (counter reset + kernel) is captured once in a CUDA graph.
  * y_m = A_m x_m for every matrix m; with nrhs = 8, x_m and y_m are
- * row-major rows x 8 / cols x 8 blocks. */
+ * row-major rows x 8 / cols x 8 blocks.
+ *
+ * Per matrix the tuner also picks the storage: CSR as given, or a SELL-32
+ * copy the plan builds (slices of 32 consecutive rows padded to the slice's
+ * longest row, entry k of row l at slice_start + 32k + l, values in the
+ * batch's type and 16-bit column offsets from the row), which a warp reads
+ * one slice at a time with every access coalesced.  A matrix qualifies for
+ * SELL when padding adds at most 1/8 to its entries, it has no row longer
+ * than long_row_nnz and every |column - row| < 32768; with tune = 0 every
+ * qualifying matrix takes SELL, with tune = 1 SELL is timed like the lane
+ * counts. */
 typedef struct {
   int32_t rows, cols, nnz;
   const int32_t *rowPtr; /* device */
@@ -760,6 +770,7 @@ typedef struct {
   int32_t long_row_nnz; /* rows above this are split (default 2048) */
   int32_t item_nnz;     /* target nonzeros per row item, 0 = automatic */
   int32_t use_graph;    /* capture the launch in a CUDA graph (default 1) */
+  int32_t sell;         /* 1: the tuner may store matrices as SELL-32 (default 1) */
 } bsp_batch_options;
 
 typedef struct bsp_batch_plan_s *bsp_batch_plan;
@@ -777,8 +788,11 @@ bsp_status bsp_batch_run_separate(bsp_batch_plan plan, bsp_stream_t stream);
 /* Replaces the x / y pointers of matrix m (no re-capture needed). */
 bsp_status bsp_batch_set_vectors(bsp_batch_plan plan, int32_t m, const void *x,
                                  void *y, bsp_stream_t stream);
-/* Per-matrix choice of the tuner: lanes per row (1..32). */
+/* Per-matrix choice of the tuner: lanes per row (1..32) for CSR matrices,
+ * 0 for matrices stored as SELL-32. */
 bsp_status bsp_batch_lanes(bsp_batch_plan plan, int32_t *lanes /* count */);
+/* Per-matrix storage: 0 = CSR, 1 = SELL-32. */
+bsp_status bsp_batch_formats(bsp_batch_plan plan, int32_t *formats /* count */);
 bsp_status bsp_batch_stats(bsp_batch_plan plan, int64_t *items,
                            int64_t *long_segments, int64_t *total_nnz);
 bsp_status bsp_batch_destroy(bsp_batch_plan plan);

@@ -108,7 +108,8 @@ def test_batch_tuner_choices_and_results(cuda):
     dev, host = _upload(cuda, mats, "f64", 1, 9)
     P = bsp.BatchPlan(dev, tune=1)
     lanes = P.lanes()
-    assert set(lanes.tolist()) <= {1, 2, 4, 8, 16, 32}
+    assert set(lanes.tolist()) <= {0, 1, 2, 4, 8, 16, 32}
+    assert np.array_equal(lanes == 0, P.formats() == 1)     # lanes 0 = stored as SELL-32
     P.run()
     _check(mats, dev, host, "f64", 1)
     P.close()
@@ -146,3 +147,61 @@ def test_batch_rejects_bad_arguments(cuda):
     with pytest.raises(ValueError):
         bsp.BatchPlan([(dev[0][0], dev[0][1], dev[0][2].half(), dev[0][3].half(), dev[0][4].half())])
     _ = torch
+
+
+def _sell_batch(seed):
+    """Banded matrices (even rows: SELL-32 candidates), a rectangular banded
+    block, a matrix whose columns reach 40,000 from their rows (int16 offsets
+    do not fit: stays CSR), power-law rows (uneven: CSR), and a banded matrix
+    with every 5th row empty (padding over 1/8: CSR)."""
+    rng = np.random.default_rng(seed)
+    mats = [bsp.gen_banded(int(rng.integers(100, 5000)), int(w), seed + i) for i, w in enumerate((3, 9, 15, 27))]
+    B = bsp.gen_banded(3000, 11, seed + 7)
+    keep = B.rowptr[2000]
+    mats.append(bsp.HostCSR(2000, 3000, B.rowptr[:2001].copy(), B.colidx[:keep].copy(), B.values[:keep].copy()))
+    n = 50000
+    rp = np.arange(0, 2 * n + 1, 2, dtype=np.int32)
+    ci = np.stack([np.arange(n), (np.arange(n) + 40000) % n], 1)
+    ci.sort(axis=1)
+    mats.append(bsp.HostCSR(n, n, rp, ci.reshape(-1).astype(np.int32), rng.standard_normal(2 * n)))
+    mats.append(bsp.gen_powerlaw(4000, 2.2, 4000, seed + 9))
+    E = bsp.gen_banded(1000, 9, seed + 11)
+    lens = np.diff(E.rowptr)
+    lens[::5] = 0
+    keepmask = np.repeat(lens > 0, np.diff(E.rowptr))
+    erp = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    mats.append(bsp.HostCSR(1000, 1000, erp, E.colidx[keepmask].copy(), E.values[keepmask].copy()))
+    return mats
+
+
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+@pytest.mark.parametrize("nrhs", [1, 8])
+def test_batch_sell_format_choice_and_results(cuda, dtype, nrhs):
+    import torch
+    mats = _sell_batch(70 + nrhs)
+    dev, host = _upload(cuda, mats, dtype, nrhs, 12)
+    P = bsp.BatchPlan(dev, nrhs=nrhs)
+    fm = P.formats()
+    assert fm.tolist() == [1, 1, 1, 1, 1, 0, 0, 0]
+    assert P.lanes()[:5].tolist() == [0] * 5
+    P.run()
+    torch.cuda.synchronize()
+    _check(mats, dev, host, dtype, nrhs)
+    first = [d[4].clone() for d in dev]
+    for d in dev:
+        d[4].fill_(float("nan"))
+    P.run_separate()
+    for a, d in zip(first, dev):
+        assert torch.equal(a, d[4])
+    Q = bsp.BatchPlan(dev, nrhs=nrhs, sell=False)
+    assert not Q.formats().any()
+    Q.run()
+    torch.cuda.synchronize()
+    _check(mats, dev, host, dtype, nrhs)
+    T = bsp.BatchPlan(dev, nrhs=nrhs, tune=1)
+    assert not T.formats()[5:].any()            # not SELL-eligible
+    T.run()
+    torch.cuda.synchronize()
+    _check(mats, dev, host, dtype, nrhs)
+    for X in (P, Q, T):
+        X.close()
