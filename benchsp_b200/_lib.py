@@ -113,6 +113,7 @@ _PROTOS = {
     "bsp_device_sync": (C.c_int, []),
     "bsp_device_alloc": (C.c_int, [C.POINTER(C.c_void_p), C.c_size_t]),
     "bsp_device_free": (C.c_int, [_P]),
+    "bsp_gather_probe": (C.c_int, [_P, C.c_size_t, _I32, _I64, _U64, _P, _P]),
     "bsp_csr_spmv": (C.c_int, [_I32, _I32, _I32, _P, _P, _P, C.c_int, _P, _P, _D, _D, _I32, _I32, _P]),
     "bsp_csr_merge_workspace": (C.c_size_t, [_I32, _I32]),
     "bsp_csr_spmv_merge_f64": (C.c_int, [_I32, _I32, _I32, _P, _P, _P, _P, _P, _D, _D, _P, C.c_size_t, _P]),

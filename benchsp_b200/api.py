@@ -691,8 +691,9 @@ class SpmmPlan:
     def spmm(self, B, C_out=None, *, alpha: float = 1.0, beta: float = 0.0, engine: str = "auto",
              slab_cols: int = 0, stream=None):
         """C = alpha*A*B + beta*C.  engine "grouped" (one pass over all
-        columns), "slab" (passes over column slabs that fit in L2; slab_cols
-        0 = from the L2 size) or "auto"."""
+        columns), "slab" (passes over column slabs with length-sorted rows
+        spread over lane groups; slab_cols 0 = the default width) or
+        "auto"."""
         torch = _torch()
         N = B.shape[1]
         if self.values.dtype != B.dtype:
@@ -1138,3 +1139,12 @@ def write_mtx(path, A: HostCSR, *, pattern: bool = False, threads: int = 0) -> N
     va = None if pattern else np.ascontiguousarray(A.values, np.float64)
     check(lib().bsp_mtx_write_csr_host(os.fsencode(os.fspath(path)), A.rows, A.cols, ci.size, _np_ptr(rp),
                                        _np_ptr(ci), None if va is None else _np_ptr(va), int(threads)))
+
+
+def gather_probe(buf, width: int, count: int, seed: int = 1, stream=None) -> None:
+    """Launches the random-gather rate probe over the device tensor `buf`
+    (`count` gathers of `width` bytes); time it with CUDA events."""
+    torch = _torch()
+    sink = torch.zeros(1, dtype=torch.int64, device=buf.device)
+    check(lib().bsp_gather_probe(_dptr(buf, "buf"), buf.numel() * buf.element_size(), width, count, seed,
+                                 _dptr(sink, "sink"), _stream(stream)))

@@ -190,3 +190,80 @@ extern "C" bsp_status bsp_device_free(void *ptr) {
   if (ptr) BSP_CUDA(cudaFree(ptr));
   return BSP_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Random-gather rate probe (measurement only).  `count` gathers of `width`
+// bytes at pseudo-random width-aligned offsets of buf: width 8 is one 8-byte
+// load per thread (a DASP / CSR x gather), width 16..256 is width/16 lanes
+// each loading 16 bytes of one row (the SpMM B-row gathers).  Eight gathers
+// per thread are issued before any is consumed; the loaded words are folded
+// into an integer that is stored only if it hits an impossible value, so the
+// loads stay.  Read-only path, default caching, as the SpMV/SpMM kernels.
+namespace bsp {
+__device__ __forceinline__ uint64_t probe_hash(uint64_t z) {
+  z ^= z >> 33;
+  z *= 0xff51afd7ed558ccdull;
+  z ^= z >> 33;
+  return z;
+}
+
+template <int W>
+__global__ void __launch_bounds__(256) gather_probe_kernel(const unsigned char *__restrict__ buf, int64_t nslots,
+                                                           int64_t count, uint64_t seed,
+                                                           unsigned long long *__restrict__ sink) {
+  constexpr int L = W >= 16 ? W / 16 : 1;       // lanes per gather
+  constexpr int U = 8;                          // gathers in flight per thread
+  const int64_t lane_grp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / L;
+  const int sub = threadIdx.x % L;
+  const int64_t groups = (int64_t)gridDim.x * blockDim.x / L;
+  uint64_t acc = 0;
+  for (int64_t g0 = lane_grp * U; g0 < count; g0 += groups * U) {
+    uint64_t v[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int64_t g = g0 + u;
+      const int64_t slot = (int64_t)__umul64hi(probe_hash(seed ^ (uint64_t)g), (uint64_t)nslots);  // < nslots
+      if (g < count) {
+        if constexpr (W == 8) {
+          v[u] = __ldg(reinterpret_cast<const unsigned long long *>(buf) + slot);
+        } else {
+          const uint4 q = __ldg(reinterpret_cast<const uint4 *>(buf + slot * W) + sub);
+          v[u] = (uint64_t)q.x ^ ((uint64_t)q.y << 7) ^ ((uint64_t)q.z << 13) ^ ((uint64_t)q.w << 29);
+        }
+      } else {
+        v[u] = 0;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) acc += v[u];
+  }
+  if (acc == 0x9E3779B97F4A7C15ull) *sink = acc;
+}
+}  // namespace bsp
+
+extern "C" bsp_status bsp_gather_probe(const void *buf, size_t bytes, int32_t width, int64_t count, uint64_t seed,
+                                       void *sink, bsp_stream_t stream) {
+  using namespace bsp;
+  clear_error();
+  BSP_CHECK_ARG(buf && sink && count >= 0, "bad argument");
+  BSP_CHECK_ARG(width == 8 || width == 16 || width == 32 || width == 64 || width == 128 || width == 256,
+                "width must be 8, 16, 32, 64, 128 or 256 bytes");
+  BSP_CHECK_ARG((uintptr_t)buf % 16 == 0 && bytes >= (size_t)width, "buffer must be 16-byte aligned and hold a row");
+  const int64_t nslots = (int64_t)(bytes / (size_t)width);
+  cudaStream_t s = as_stream(stream);
+  int blocks = 0;
+  const unsigned grid = (unsigned)sm_count() * 8;
+  auto *k = reinterpret_cast<unsigned long long *>(sink);
+  const auto *b = static_cast<const unsigned char *>(buf);
+  switch (width) {
+    case 8: gather_probe_kernel<8><<<grid, 256, 0, s>>>(b, nslots, count, seed, k); break;
+    case 16: gather_probe_kernel<16><<<grid, 256, 0, s>>>(b, nslots, count, seed, k); break;
+    case 32: gather_probe_kernel<32><<<grid, 256, 0, s>>>(b, nslots, count, seed, k); break;
+    case 64: gather_probe_kernel<64><<<grid, 256, 0, s>>>(b, nslots, count, seed, k); break;
+    case 128: gather_probe_kernel<128><<<grid, 256, 0, s>>>(b, nslots, count, seed, k); break;
+    default: gather_probe_kernel<256><<<grid, 256, 0, s>>>(b, nslots, count, seed, k); break;
+  }
+  (void)blocks;
+  BSP_LAUNCH_CHECK();
+  return BSP_OK;
+}

@@ -62,6 +62,15 @@ bsp_status bsp_device_sync(void);
  * cudaFree on the current device). */
 bsp_status bsp_device_alloc(void **ptr, size_t bytes);
 bsp_status bsp_device_free(void *ptr);
+/* Measurement utility (no reference counterpart): `count` gathers of `width`
+ * bytes (8, or 16..256 read as width/16 lanes x 16 bytes) at pseudo-random
+ * width-aligned offsets of the device buffer `buf` (`bytes` long), eight in
+ * flight per thread, one full wave of CTAs.  Time it to get the random-gather
+ * rate of the memory level the buffer's size selects (L2 when it fits): the
+ * ceiling for kernels whose time goes to scattered x or B-row gathers.
+ * `sink` is a device word the kernel writes only on an impossible value. */
+bsp_status bsp_gather_probe(const void *buf, size_t bytes, int32_t width, int64_t count, uint64_t seed,
+                            void *sink, bsp_stream_t stream);
 
 /* ---------------------------------------------------------------------- */
 /* CSR SpMV  y = alpha*A*x + beta*y
@@ -415,14 +424,14 @@ bsp_status bsp_spmm_csr(int32_t rows, int32_t cols, int32_t nnz,
  * summed in chunk order (deterministic).
  *
  * Two engines run a planned product.  "grouped": one warp per row or chunk
- * over all N columns in one pass.  "slab": the columns are taken in slabs
- * small enough that a slab of B stays in L2 (passes over A, one per slab),
- * and rows of at most `chunk` nonzeros, sorted by length, are spread one per
- * group of lanes (several rows per warp in flight), while long-row chunks
- * keep a warp each.  The default picks the slab engine when all of B does
- * not fit in 60% of L2.  Both give the same bits for a given slab width
- * only if their sums run in the same order, which they do not: results
- * differ in rounding, each within the FP32 accumulation bound. */
+ * over all N columns in one pass.  "slab": the columns are taken in slabs of
+ * up to 16 lanes x 16 bytes of B row (128 FP16 columns; one pass over A per
+ * slab), rows of at most `chunk` nonzeros, sorted by length, are spread one
+ * per group of lanes (several rows per warp in flight), and long-row chunks
+ * keep a warp each.  The default is the slab engine whenever B's rows are
+ * 16-byte aligned and N is a multiple of 16 bytes of elements.  The engines
+ * sum in different orders: results differ in rounding, each within the FP32
+ * accumulation bound. */
 typedef struct {
   int32_t rows, chunk;
   int64_t nchunks, nparts;
@@ -451,8 +460,8 @@ bsp_status bsp_spmm_csr_planned(const bsp_spmm_plan *plan, int32_t cols, int32_t
 typedef enum { BSP_SPMM_AUTO = 0, BSP_SPMM_GROUPED = 1, BSP_SPMM_SLAB = 2 } bsp_spmm_engine;
 
 /* bsp_spmm_csr_planned with the engine and, for the slab engine, the slab
- * width (columns per pass; 0 = from the L2 size; otherwise a power of two
- * times 16 bytes of B row that divides N) chosen by the caller. */
+ * width (columns per pass; 0 = the default; otherwise 1..32 lanes, a power
+ * of two, times 16 bytes of B row, dividing N) chosen by the caller. */
 bsp_status bsp_spmm_csr_planned_variant(const bsp_spmm_plan *plan, int32_t cols, int32_t nnz,
                                         const int32_t *rowPtr, const int32_t *colIdx,
                                         const void *values, bsp_dtype dtype, const void *B,

@@ -257,7 +257,7 @@ def test_spmm_slab_engine_matches_fp64(cuda, name, N, slab):
     Cin = rng.uniform(-1, 1, (n, N)).astype(np.float32)
     rpd, cid = _dev(cuda, A.rowptr, A.colidx)
     P = bsp.SpmmPlan(rpd, cid, vals_t.to(cuda), cols=A.cols, chunk=256)
-    assert P.nsplit == 5
+    assert P.nsplit == int(np.sum(lens > 256))
     Bd = B_t.to(cuda)
     C1 = P.spmm(Bd, engine="slab", slab_cols=slab)
     assert torch.equal(C1, P.spmm(Bd, engine="slab", slab_cols=slab))
