@@ -126,6 +126,7 @@ _PROTOS = {
     "bsp_bsr_host_plan_create": (C.c_int, [C.POINTER(BspBsr), _I32, C.POINTER(C.c_void_p), _P]),
     "bsp_bsr_spmv_host_pipelined": (C.c_int, [C.c_void_p, _P, _P, _D, _D, _P]),
     "bsp_bsr_host_plan_destroy": (C.c_int, [C.c_void_p]),
+    "bsp_bsr_host_plan_set_graph": (C.c_int, [C.c_void_p, _I32]),
     "bsp_csr2bcsr": (C.c_int, [_I32, _I32, _I32, _P, _P, _P, _I32, _I32, _I32, C.POINTER(BspBcsr), _P]),
     "bsp_bcsr_free": (C.c_int, [C.POINTER(BspBcsr)]),
     "bsp_bcsr_spmv": (C.c_int, [C.POINTER(BspBcsr), _P, _P, _D, _D, _P]),

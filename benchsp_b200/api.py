@@ -180,9 +180,9 @@ class BsrMatrix:
         """FP16/BF16 copy with one power-of-two scale per block."""
         return BsrScaledMatrix(self, dtype, stream)
 
-    def host_plan(self, chunks: int = 8, stream=None) -> "BsrHostPlan":
+    def host_plan(self, chunks: int = 8, stream=None, use_graph: bool = True) -> "BsrHostPlan":
         """Overlapped host-buffer SpMV plan (see BsrHostPlan)."""
-        return BsrHostPlan(self, chunks, stream)
+        return BsrHostPlan(self, chunks, stream, use_graph)
 
     def free(self) -> None:
         if self._live:
@@ -200,10 +200,12 @@ class BsrHostPlan:
     """Host-buffer BSR SpMV with the x upload, the SpMV and the y download
     overlapped in block-row chunks (keeps the matrix alive)."""
 
-    def __init__(self, M: "BsrMatrix", chunks: int = 8, stream=None):
+    def __init__(self, M: "BsrMatrix", chunks: int = 8, stream=None, use_graph: bool = True):
         self._m = M
         self._h = C.c_void_p()
         check(lib().bsp_bsr_host_plan_create(C.byref(M._d), chunks, C.byref(self._h), _stream(stream)))
+        if not use_graph:
+            check(lib().bsp_bsr_host_plan_set_graph(self._h, 0))
 
     def spmv(self, x_host: np.ndarray, y_host: np.ndarray, *, alpha: float = 1.0, beta: float = 0.0,
              stream=None) -> np.ndarray:

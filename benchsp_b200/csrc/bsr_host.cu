@@ -57,6 +57,7 @@ struct bsp_bsr_host_plan_s {
   const double *g_x = nullptr;
   double *g_y = nullptr;
   double g_alpha = 0.0, g_beta = 0.0;
+  int32_t use_graph = 1;
 };
 
 static void plan_release(bsp_bsr_host_plan_s *P) {
@@ -176,6 +177,11 @@ extern "C" bsp_status bsp_bsr_spmv_host_pipelined(bsp_bsr_host_plan P, const dou
   clear_error();
   BSP_CHECK_ARG(P && x_host && y_host, "null pointer");
   cudaStream_t s = as_stream(stream);
+  if (!P->use_graph) {
+    BSP_TRY(enqueue(P, x_host, y_host, alpha, beta, s));
+    BSP_CUDA(cudaStreamSynchronize(s));
+    return BSP_OK;
+  }
   const bool same = P->graph && P->g_x == x_host && P->g_y == y_host && P->g_alpha == alpha && P->g_beta == beta;
   if (!same) {
     if (P->graph) {
@@ -201,6 +207,13 @@ extern "C" bsp_status bsp_bsr_spmv_host_pipelined(bsp_bsr_host_plan P, const dou
   }
   BSP_CUDA(cudaGraphLaunch(P->graph, s));
   BSP_CUDA(cudaStreamSynchronize(s));
+  return BSP_OK;
+}
+
+extern "C" bsp_status bsp_bsr_host_plan_set_graph(bsp_bsr_host_plan P, int32_t use_graph) {
+  clear_error();
+  BSP_CHECK_ARG(P, "null plan");
+  P->use_graph = use_graph ? 1 : 0;
   return BSP_OK;
 }
 

@@ -1408,7 +1408,8 @@ static bsp_status launch_slab(const bsp_spmm_plan *p, const int32_t *rp, const i
 
 // Slab width (columns per pass) for the slab engine; 0 when it cannot run
 // (B rows not 16-byte aligned, N not a multiple of VEC).  With `want` == 0:
-// the widest slab of at most 16 lanes of 16 bytes that divides N.  Slabs
+// the widest slab of at most 32 lanes of 16 bytes that divides N (graph
+// 2^20, FP16, N = 256: 32 lanes 3.49 ms, 16 lanes in two passes 3.62).  Slabs
 // sized so that B's slab stays in L2 measured slower (power-law graph 2^20,
 // FP16, N = 128: four 32-column passes 2.42 ms against one 128-column pass
 // 1.81 ms): the gathers run at the same rate from L2 as from DRAM, and every
@@ -1424,7 +1425,7 @@ static int slab_width(int32_t N, int32_t cols, const void *B, int64_t ldb, int32
     return want;
   }
   (void)cols;
-  int l = 16;
+  int l = 32;
   while (l > 1 && N % (l * VEC) != 0) l >>= 1;
   return l * VEC;
 }

@@ -217,6 +217,9 @@ bsp_status bsp_bsr_host_plan_create(const bsp_bsr *m, int32_t chunks,
 bsp_status bsp_bsr_spmv_host_pipelined(bsp_bsr_host_plan plan, const double *x_host,
                                        double *y_host, double alpha, double beta,
                                        bsp_stream_t stream);
+/* 1 (default): record the sequence once as a CUDA graph and replay it;
+ * 0: issue the copies and launches on the streams at every call. */
+bsp_status bsp_bsr_host_plan_set_graph(bsp_bsr_host_plan plan, int32_t use_graph);
 bsp_status bsp_bsr_host_plan_destroy(bsp_bsr_host_plan plan);
 
 /* ---------------------------------------------------------------------- */
@@ -425,7 +428,7 @@ bsp_status bsp_spmm_csr(int32_t rows, int32_t cols, int32_t nnz,
  *
  * Two engines run a planned product.  "grouped": one warp per row or chunk
  * over all N columns in one pass.  "slab": the columns are taken in slabs of
- * up to 16 lanes x 16 bytes of B row (128 FP16 columns; one pass over A per
+ * up to 32 lanes x 16 bytes of B row (256 FP16 columns; one pass over A per
  * slab), rows of at most `chunk` nonzeros, sorted by length, are spread one
  * per group of lanes (several rows per warp in flight), and long-row chunks
  * keep a warp each.  The default is the slab engine whenever B's rows are
