@@ -631,6 +631,9 @@ def run_suite(args) -> None:
     # --- CG with 8 right-hand sides at once vs 8 single solves
     run_cg_multi(bsp, up, dev)
 
+    # --- random-gather rate of this GPU (the ceiling of the gather-bound kernels)
+    gpk = run_gather_peaks(bsp, dev)
+
     # --- SpMM on a power-law graph (n = 2^20, Zipf 1.8, mean degree 32)
     A = bsp.gen_graph(1 << 20, 1.8, 32, SEED + 4)
     rp, ci, v64 = up(A.rowptr, A.colidx, A.values)
@@ -646,15 +649,24 @@ def run_suite(args) -> None:
             Cref = A64 @ B.double()
             err = float(torch.linalg.norm(Cm.double() - Cref) / torch.linalg.norm(Cref))
             t = _timed(lambda: P.spmm(B, Cm), 10)
+            tg = _timed(lambda: P.spmm(B, Cm, engine="grouped"), 10)
             Af = torch.sparse_csr_tensor(rp.long(), ci.long(), v.float(), size=(A.rows, A.cols))
             Bf = B.float()
             tcs = _timed(lambda: Af @ Bf, 5)
             nb = A.nnz * 6 + (A.rows + 1) * 4 + A.cols * N * 2 + A.rows * N * 4
-            res[f"{name}_N{N}"] = {"ms": round(t * 1e3, 3), "gflops": round(2 * A.nnz * N / t / 1e9, 1),
+            gb = A.nnz * N * 2    # B-row bytes gathered (one B row per nonzero)
+            w = min(256, 2 * N)
+            res[f"{name}_N{N}"] = {"ms": round(t * 1e3, 3), "engine": "slab", "grouped_engine_ms": round(tg * 1e3, 3),
+                                   "gflops": round(2 * A.nnz * N / t / 1e9, 1),
                                    "rel_err_vs_fp64": err, "cusparse_f32_ms": round(tcs * 1e3, 3),
-                                   "min_bytes_gbs": round(nb / t / 1e9, 1)}
+                                   "min_bytes_gbs": round(nb / t / 1e9, 1),
+                                   "gather_roofline": {"bound": "random gathers", "achieved": round(gb / t / 1e9, 1),
+                                                       "peak": gpk[f"w{w}_dram"]["gbs"], "unit": "GB/s",
+                                                       "frac": round(gb / t / 1e9 / gpk[f"w{w}_dram"]["gbs"], 3),
+                                                       "peak_src": f"bsp_gather_probe width {w} B, buffer > L2"}}
         P.free()
     _emit("spmm_graph_1M_zipf1.8_deg32", n=A.rows, nnz=A.nnz, max_row=int(np.diff(A.rowptr).max()), variants=res)
+    run_smat_graph(bsp, dev, up, A)
     del rp, ci, v64, A64
 
     # --- block SpMM on dense 16x16 tiles: tcgen05 vs mma.sync vs CSR
@@ -664,11 +676,11 @@ def run_suite(args) -> None:
     for name, tdt in (("f16", torch.float16), ("bf16", torch.bfloat16)):
         M = bsp.SmatMatrix(rp, ci, v64, rows=A.rows, cols=A.cols, dtype=name)
         v = v64.to(tdt)
-        for N in (128, 256):
+        for N in (32, 64, 128, 256):
             B = (torch.rand(A.cols, N, generator=torch.Generator().manual_seed(N)) * 2 - 1).to(tdt).to(dev)
             Cref = torch.sparse_csr_tensor(rp.long(), ci.long(), v64, size=(A.rows, A.cols)) @ B.double()
             row = {}
-            for path in ("tcgen05", "mma_sync"):
+            for path in ("tcgen05", "tcgen05_w64", "tcgen05_w128", "mma_sync"):
                 Cm = M.spmm(B, path=path)
                 err = float(torch.linalg.norm(Cm.double() - Cref) / torch.linalg.norm(Cref))
                 t = _timed(lambda: M.spmm(B, Cm, path=path), 10)
@@ -682,6 +694,9 @@ def run_suite(args) -> None:
     _emit("smat_dense16_tiles_524k_rows_8_per_row", rows=A.rows, nnz=A.nnz, tiles=A.nnz // 256, variants=res)
     del rp, ci, v64
 
+    # --- per-block scaled FP16/BF16 BSR on the headline matrix
+    run_scaled_bsr(bsp, dev, pk, up)
+
     # --- 512 independent SpMVs (and 8-RHS SpMMs) in one persistent launch
     run_batch(bsp, dev, pk, up)
 
@@ -690,6 +705,84 @@ def run_suite(args) -> None:
 
     # --- row-similarity reordering of a row-shuffled tile matrix
     run_reorder_similarity(bsp, dev, up)
+
+
+def run_gather_peaks(bsp, dev) -> dict:
+    """bsp_gather_probe: random gathers of 8 B (a CSR/DASP x gather), 64 B
+    and 256 B (B-row slices of the SpMM) from a buffer that fits L2 (16 or 64
+    MB) and from one that does not (2 GB); 10 timed launches after 3."""
+    import torch
+    out = {}
+    for width, count in ((8, 50_000_000), (64, 33_554_432), (256, 33_554_432)):
+        for where, mb in (("l2", 16 if width == 8 else 64), ("dram", 2048)):
+            buf = torch.zeros((mb << 20) // 4, dtype=torch.int32, device=dev)
+            t = _timed(lambda: bsp.gather_probe(buf, width, count), 10)
+            out[f"w{width}_{where}"] = {"buffer_mb": mb, "ggathers_s": round(count / t / 1e9, 2),
+                                        "gbs": round(count * width / t / 1e9, 1)}
+            del buf
+    _emit("gather_probe", variants=out)
+    return out
+
+
+def run_smat_graph(bsp, dev, up, A) -> None:
+    """The SMaT tensor-core path on the power-law graph itself: rows
+    regrouped by row similarity (host, one-time), 16x16 tiles of the
+    reordered rows, tcgen05 SpMM at N = 32 / 128 / 256 (FP16), beside the
+    slab CSR engine on the same rows; the engine choice's estimates."""
+    import time
+
+    import torch
+    t0 = time.perf_counter()
+    perm = bsp.reorder_similarity_host(A.rowptr, A.colidx, A.cols)
+    reorder_s = time.perf_counter() - t0
+    R = bsp.permute_rows_csr_host(A, perm)
+    rp, ci, va = up(R.rowptr, R.colidx, R.values)
+    Sm = bsp.SmatMatrix(rp, ci, va, rows=R.rows, cols=R.cols, dtype="f16")
+    P = bsp.SpmmPlan(rp, ci, va.half(), cols=R.cols, chunk=256)
+    res = {}
+    for N in (32, 128, 256):
+        B = (torch.rand(R.cols, N, generator=torch.Generator().manual_seed(N)) * 2 - 1).half().to(dev)
+        Ct = Sm.spmm(B, path="tcgen05")
+        Cs = P.spmm(B)
+        t = _timed(lambda: Sm.spmm(B, Ct, path="tcgen05"), 5)
+        ts = _timed(lambda: P.spmm(B, Cs), 5)
+        rel = float(torch.linalg.norm(Ct.double() - Cs.double()) / torch.linalg.norm(Cs.double()))
+        choice, _ = bsp.choose_spmm_host(R, N, reorder=False)
+        res[f"N{N}"] = {"smat_tcgen05_ms": round(t * 1e3, 3), "slab_csr_ms": round(ts * 1e3, 3),
+                        "tflops_tcgen05": round(2 * R.nnz * N / t / 1e12, 3), "rel_diff_tc_vs_csr": rel,
+                        "chooser": choice["engine"]}
+    Sm.check()
+    _emit("smat_tcgen05_graph_1M_reordered", rows=R.rows, nnz=R.nnz, reorder_host_s=round(reorder_s, 2),
+          tiles=Sm.tiles, tile_fill=round(Sm.fill, 4), variants=res)
+    Sm.free()
+    P.free()
+
+
+def run_scaled_bsr(bsp, dev, pk, up) -> None:
+    """FP64 BSR against the FP16/BF16 per-block-scaled copy on the stencil
+    64^3 x 4 dof, 4x4 and 8x8 blocks, FP64 and FP32 x/y; roofline on the
+    stored bytes."""
+    import torch
+    A, xh = make_matrix(GRID)
+    rp, ci, va, x = up(A.rowptr, A.colidx, A.values, xh)
+    y = torch.empty(A.rows, dtype=torch.float64, device=dev)
+    x32, y32 = x.float(), torch.empty(A.rows, dtype=torch.float32, device=dev)
+    res = {}
+    for bs in (4, 8):
+        M = bsp.csr2bsr(rp, ci, va, rows=A.rows, cols=A.cols, bs=bs)
+        t64 = _timed(lambda: M.spmv(x, y), 20)
+        row = {"fp64_us": round(t64 * 1e6, 2)}
+        for dt in ("f16", "bf16"):
+            S = M.scaled(dt)
+            for xy, xx, yy, vb in (("f64xy", x, y, 8), ("f32xy", x32, y32, 4)):
+                t = _timed(lambda: S.spmv(xx, yy), 20)
+                nb = S.stored_bytes() + vb * (A.rows + A.cols)
+                row[f"{dt}_{xy}"] = {"us": round(t * 1e6, 2), "gflops": round(2 * A.nnz / t / 1e9, 1),
+                                     "speedup_vs_fp64": round(t64 / t, 2), "roofline": _roof(nb, t, pk)}
+            S.free()
+        res[f"bs{bs}"] = row
+        M.free()
+    _emit("bsr_scaled16_stencil27_64cubed_4dof", n=A.rows, nnz=A.nnz, variants=res)
 
 
 def run_batch(bsp, dev, pk, up) -> None:
@@ -715,6 +808,7 @@ def run_batch(bsp, dev, pk, up) -> None:
             tb = _timed(P.run, 50)
             ts = _timed(P.run_separate, 5)
             choice = {int(k): int(v) for k, v in zip(*np.unique(P.lanes(), return_counts=True))}
+            n_sell = int((P.formats() == 1).sum())
             Pm = bsp.BatchPlan(d, nrhs=nrhs, tune=0)
             tm = _timed(Pm.run, 50)
             Pm.close()
@@ -724,7 +818,7 @@ def run_batch(bsp, dev, pk, up) -> None:
                                          "frac": round(nb / tb / 1e9 / pk, 4),
                                          "gflops": round(2 * nnz * nrhs / tb / 1e9, 1), "launches_batched": 1,
                                          "launches_separate": len(mats), "model_plan_us": round(tm * 1e6, 1),
-                                         "lanes_chosen": choice}
+                                         "lanes_chosen": choice, "sell32_matrices": n_sell}
             if nrhs == 1:
                 fns = [_cusparse_spmv(rp, ci, va, xx, m.rows, m.cols) for m, (rp, ci, va, xx, _) in zip(mats, d)]
                 res[f"{dname}_rhs1"]["cusparse_separate_us"] = round(_timed(lambda: [f() for f in fns], 5) * 1e6, 1)

@@ -115,24 +115,10 @@ __device__ __forceinline__ void strided_dot(const int32_t *__restrict__ ci, cons
 #pragma unroll
     for (int u = 0; u < 4; ++u) fma_row<V, NRHS>(acc, a[u], xr[u]);
   }
-  // the last 1..3 entries: loads issued together, summed in the same order
-  // (a short row would otherwise pay one column -> x round trip per entry)
-  if (j < e) {
-    int32_t c[3];
-    V a[3];
-#pragma unroll
-    for (int u = 0; u < 3; ++u) {
-      const bool ok = j + u * stride < e;
-      c[u] = ok ? __ldg(ci + j + u * stride) : -1;
-      a[u] = ok ? __ldg(val + j + u * stride) : V(0);
-    }
-    V xr[3][NRHS];
-#pragma unroll
-    for (int u = 0; u < 3; ++u)
-      if (c[u] >= 0) load_xrow<V, NRHS>(x, c[u], xr[u]);
-#pragma unroll
-    for (int u = 0; u < 3; ++u)
-      if (c[u] >= 0) fma_row<V, NRHS>(acc, a[u], xr[u]);
+  for (; j < e; j += stride) {
+    V xr[NRHS];
+    load_xrow<V, NRHS>(x, __ldg(ci + j), xr);
+    fma_row<V, NRHS>(acc, __ldg(val + j), xr);
   }
 }
 
@@ -224,17 +210,11 @@ __device__ __forceinline__ void sell_item(const BatchMatDev &M, int32_t s0, int3
   const V *sv = static_cast<const V *>(M.sell_val);
   const V *x = static_cast<const V *>(M.x);
   V *y = static_cast<V *>(M.y);
-  // the next slice's bounds are loaded while this slice is summed
-  int32_t q0 = s0 < s1 ? __ldg(M.sell_ptr + s0) : 0, q1 = s0 < s1 ? __ldg(M.sell_ptr + s0 + 1) : 0;
   for (int32_t sl = s0; sl < s1; ++sl) {
     const int32_t row = sl * 32 + lane;
     const bool live = row < M.rows;
-    const int32_t p0 = q0;
-    const int32_t w = live ? (q1 - p0) >> 5 : 0;
-    if (sl + 1 < s1) {
-      q0 = q1;
-      q1 = __ldg(M.sell_ptr + sl + 2);
-    }
+    const int32_t p0 = __ldg(M.sell_ptr + sl);
+    const int32_t w = live ? (__ldg(M.sell_ptr + sl + 1) - p0) >> 5 : 0;
     const V *vp = sv + p0 + lane;
     const int16_t *op = M.sell_off + p0 + lane;
     V acc[NRHS];
