@@ -1044,7 +1044,7 @@ def run_profile(args) -> None:
         rp, ci, va, b = up(A.rowptr, A.colidx, A.values, bsp.gen_uniform(A.rows, SEED + 3))
         S = bsp.CgSolver(rp, ci, va, mode=w[3:], max_iters=32, check_every=16, use_graphs=False)
         S.solve(b, raise_on_stall=False)
-    elif w == "spmm":   # power-law graph 2^20, FP16, N = 128, row-split CSR
+    elif w == "spmm":   # power-law graph 2^20, FP16, N = 128, planned (slab engine)
         A = bsp.gen_graph(1 << 20, 1.8, 32, SEED + 4)
         rp, ci, v64 = up(A.rowptr, A.colidx, A.values)
         v = v64.half()
@@ -1052,14 +1052,26 @@ def run_profile(args) -> None:
         B = (torch.rand(A.cols, 128, generator=torch.Generator().manual_seed(1)) * 2 - 1).half().to(dev)
         for _ in range(reps):
             P.spmm(B)
-    elif w in ("smat_tc", "smat_mma"):   # dense 16x16 tiles, 8 per block-row, 524,288 rows, N = 256, FP16
+    elif w in ("smat_tc", "smat_mma", "smat_tc_w64", "smat_tc_w128"):
+        # dense 16x16 tiles, 8 per block-row, 524,288 rows, N = 256, FP16
         A = bsp.gen_random_bsr(32768, 16, 8, 1.0, 1.0, SEED + 5)
         rp, ci, va = up(A.rowptr, A.colidx, A.values)
         M = bsp.SmatMatrix(rp, ci, va, rows=A.rows, cols=A.cols, dtype="f16")
         B = (torch.rand(A.cols, 256, generator=torch.Generator().manual_seed(1)) * 2 - 1).half().to(dev)
+        path = {"smat_tc": "tcgen05", "smat_mma": "mma_sync", "smat_tc_w64": "tcgen05_w64",
+                "smat_tc_w128": "tcgen05_w128"}[w]
         for _ in range(reps):
-            M.spmm(B, path="tcgen05" if w == "smat_tc" else "mma_sync")
+            M.spmm(B, path=path)
         M.check()
+    elif w == "bsr_scaled":   # FP16 per-block-scaled 4x4 BSR, stencil 40^3 x 4 dof (> L2)
+        A, xh = make_matrix(40)
+        rp, ci, va, x = up(A.rowptr, A.colidx, A.values, xh)
+        M = bsp.csr2bsr(rp, ci, va, rows=A.rows, cols=A.cols, bs=4)
+        S = M.scaled("f16")
+        M.free()
+        y = torch.empty(A.rows, dtype=torch.float64, device=dev)
+        for _ in range(reps):
+            S.spmv(x, y)
     elif w == "csr":   # CSR FP64 vector kernel, 2-D Laplacian 512x512 (21 MB; ncu replays cold-cache)
         A = bsp.gen_laplace2d(512, 512)
         rp, ci, va, x = up(A.rowptr, A.colidx, A.values, bsp.gen_uniform(A.cols, SEED + 10))
@@ -1114,7 +1126,8 @@ def main():
     ap.add_argument("--grid", type=int, default=GRID, help="stencil grid edge (64 = the benchmark config; "
                     "smaller values only for profiling captures)")
     ap.add_argument("--profile", choices=["dasp", "cg_fp64", "cg_f16", "spmm", "batch", "smat_tc", "smat_mma", "csr",
-                                          "pcg_bj", "spmm_grouped", "cg_multi"],
+                                          "pcg_bj", "spmm_grouped", "cg_multi", "smat_tc_w64", "smat_tc_w128",
+                                          "bsr_scaled"],
                     help="a few calls of one workload's kernels (for ncu captures)")
     args = ap.parse_args()
     if args.profile:
