@@ -683,7 +683,7 @@ def run_suite(args) -> None:
             B = (torch.rand(A.cols, N, generator=torch.Generator().manual_seed(N)) * 2 - 1).to(tdt).to(dev)
             Cref = torch.sparse_csr_tensor(rp.long(), ci.long(), v64, size=(A.rows, A.cols)) @ B.double()
             row = {}
-            for path in ("tcgen05", "tcgen05_w64", "tcgen05_w128", "mma_sync"):
+            for path in ("tcgen05", "tcgen05_w64", "tcgen05_w128", "tcgen05_persistent", "tcgen05_persistent_w64", "mma_sync"):
                 Cm = M.spmm(B, path=path)
                 err = float(torch.linalg.norm(Cm.double() - Cref) / torch.linalg.norm(Cref))
                 t = _timed(lambda: M.spmm(B, Cm, path=path), 10)
@@ -1052,14 +1052,15 @@ def run_profile(args) -> None:
         B = (torch.rand(A.cols, 128, generator=torch.Generator().manual_seed(1)) * 2 - 1).half().to(dev)
         for _ in range(reps):
             P.spmm(B)
-    elif w in ("smat_tc", "smat_mma", "smat_tc_w64", "smat_tc_w128"):
+    elif w in ("smat_tc", "smat_mma", "smat_tc_w64", "smat_tc_w128", "smat_tcp", "smat_tcp_w64"):
         # dense 16x16 tiles, 8 per block-row, 524,288 rows, N = 256, FP16
         A = bsp.gen_random_bsr(32768, 16, 8, 1.0, 1.0, SEED + 5)
         rp, ci, va = up(A.rowptr, A.colidx, A.values)
         M = bsp.SmatMatrix(rp, ci, va, rows=A.rows, cols=A.cols, dtype="f16")
         B = (torch.rand(A.cols, 256, generator=torch.Generator().manual_seed(1)) * 2 - 1).half().to(dev)
         path = {"smat_tc": "tcgen05", "smat_mma": "mma_sync", "smat_tc_w64": "tcgen05_w64",
-                "smat_tc_w128": "tcgen05_w128"}[w]
+                "smat_tc_w128": "tcgen05_w128", "smat_tcp": "tcgen05_persistent",
+                "smat_tcp_w64": "tcgen05_persistent_w64"}[w]
         for _ in range(reps):
             M.spmm(B, path=path)
         M.check()
@@ -1127,7 +1128,7 @@ def main():
                     "smaller values only for profiling captures)")
     ap.add_argument("--profile", choices=["dasp", "cg_fp64", "cg_f16", "spmm", "batch", "smat_tc", "smat_mma", "csr",
                                           "pcg_bj", "spmm_grouped", "cg_multi", "smat_tc_w64", "smat_tc_w128",
-                                          "bsr_scaled"],
+                                          "bsr_scaled", "smat_tcp", "smat_tcp_w64"],
                     help="a few calls of one workload's kernels (for ncu captures)")
     args = ap.parse_args()
     if args.profile:

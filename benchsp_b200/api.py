@@ -746,7 +746,8 @@ class SmatMatrix:
     def tiles(self) -> int:
         return self._d.tiles.nonzeroBlocks
 
-    _PATHS = {"auto": 0, "mma_sync": 1, "tcgen05": 2, "tcgen05_w64": 3, "tcgen05_w128": 4}
+    _PATHS = {"auto": 0, "mma_sync": 1, "tcgen05": 2, "tcgen05_w64": 3, "tcgen05_w128": 4, "tcgen05_persistent": 5,
+              "tcgen05_persistent_w64": 6}
 
     def spmm(self, B, C=None, *, alpha: float = 1.0, beta: float = 0.0, path: str = "auto", stream=None):
         """path: "auto" / "tcgen05" (tensor cores, slab width from L2),
@@ -839,7 +840,8 @@ class BatchPlan:
         return out
 
     def formats(self) -> np.ndarray:
-        """Per-matrix storage: 0 = CSR, 1 = SELL-32."""
+        """Per-matrix storage: 0 = CSR, 1 = SELL-32 (rows in order, 16-bit
+        column offsets), 2 = SELL-32 of length-sorted rows (32-bit columns)."""
         out = np.empty(self.count, np.int32)
         check(lib().bsp_batch_formats(self._h, out.ctypes.data_as(C.c_void_p)))
         return out

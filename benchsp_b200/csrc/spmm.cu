@@ -653,6 +653,204 @@ __global__ void __launch_bounds__(kTcThreads) spmm_tc_kernel(const __grid_consta
                  : "memory");
 }
 
+// ---------------------------------------------------------------------------
+// Persistent, warp-specialised form of the tcgen05 block SpMM.  The CTAs of
+// one launch stay resident and walk the work items w = blockIdx.x +
+// j * gridDim.x (item = (16-row block br, slab of W C columns), slab-major),
+// so the set-up (barriers, TMEM allocation) is paid once per CTA instead of
+// once per block row, and the tile stream runs on across block rows:
+//   warp 0 (one lane): producer -- per tile, waits for its stage to be free,
+//     then TMA-loads the B slab box(es) and bulk-copies the stored tile;
+//   warp 1 (one lane): MMA issuer -- per tile one tcgen05.mma into the item's
+//     accumulator (TMEM columns 16 * (j & 1): two accumulators, so block row
+//     j + 1 accumulates while block row j is read out), commit frees the
+//     stage; after an item's last tile a commit signals the epilogue;
+//   warps 2-5: epilogue -- each reads its quarter of the TMEM lanes
+//     (tcgen05.ld 32x32b.x16: 32 C columns x 16 C rows), hands the
+//     accumulator back, and writes C.
+// Every wait is bounded; a timeout sets the shared abort flag, which the
+// other roles see at their next wait, and the error flag; the producer then
+// waits (bounded) for the copies it issued before leaving.
+constexpr int kTcpThreads = 192;
+constexpr int kTcpSmem = 1024 + kTcStages * (kTcBBytes + kTcABytes) + 256;
+
+__device__ __forceinline__ bool tcp_wait(uint64_t *bar, unsigned parity, volatile int *abort_flag) {
+  for (long long i = 0; i < kSpinLimit; ++i) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((i & 1023) == 1023 && *abort_flag) return false;
+  }
+  *abort_flag = 1;
+  return false;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kTcpThreads) spmm_tcp_kernel(const __grid_constant__ CUtensorMap tmB, int32_t M,
+                                                               int32_t N, int32_t W, int32_t nbr,
+                                                               const int32_t *__restrict__ bptr,
+                                                               const int32_t *__restrict__ bcol,
+                                                               const T *__restrict__ tiles, float *__restrict__ C,
+                                                               int64_t ldc, float alpha, float beta,
+                                                               int32_t *__restrict__ err) {
+  extern __shared__ unsigned char smem_raw[];
+  const uint32_t raw = smem_u32(smem_raw);
+  unsigned char *sm = smem_raw + ((1024u - (raw & 1023u)) & 1023u);
+  unsigned char *bslab = sm;
+  unsigned char *atile = sm + kTcStages * kTcBBytes;
+  uint64_t *full = reinterpret_cast<uint64_t *>(atile + kTcStages * kTcABytes);
+  uint64_t *empty = full + kTcStages;
+  uint64_t *done = empty + kTcStages;   // [2]
+  uint64_t *accfree = done + 2;         // [2]
+  uint64_t *drain = accfree + 2;        // the MMA issuer's last commit
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nslab = (N + W - 1) / W;
+  const int64_t total = (int64_t)nbr * nslab;
+  const bool two_boxes = W > 64;
+
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < kTcStages; ++i) {
+      mbar_init(&full[i], 1);
+      mbar_init(&empty[i], 1);
+    }
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(&done[i], 1);
+      mbar_init(&accfree[i], 4);
+    }
+    mbar_init(drain, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"((uint32_t)kTcTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0 && lane == 0) {
+    // ---- producer
+    int64_t it = 0;
+    bool ok = true;
+    for (int64_t w = blockIdx.x; w < total && ok; w += gridDim.x) {
+      const int32_t br = (int32_t)(w % nbr);
+      const int32_t n0 = (int32_t)(w / nbr) * W;
+      const int32_t k0 = bptr[br], nk = bptr[br + 1] - k0;
+      for (int32_t i = 0; i < nk; ++i, ++it) {
+        const int st = (int)(it % kTcStages);
+        if (it >= kTcStages && !tcp_wait(&empty[st], (unsigned)((it / kTcStages - 1) & 1), abort_flag)) {
+          ok = false;
+          break;
+        }
+        const int32_t bc = bcol[k0 + i];
+        mbar_expect_tx(&full[st], (two_boxes ? kTcBBytes : kTcBBytes / 2) + kTcABytes);
+        tma_load_2d(bslab + st * kTcBBytes, &tmB, n0, bc * kTS, &full[st]);
+        if (two_boxes) tma_load_2d(bslab + st * kTcBBytes + kTcBBytes / 2, &tmB, n0 + 64, bc * kTS, &full[st]);
+        bulk_g2s(atile + st * kTcABytes, tiles + (int64_t)(k0 + i) * kTS * kTS, kTcABytes, &full[st]);
+      }
+    }
+    if (!ok) {
+      // the copies issued into the last kTcStages stages land before the CTA goes away
+      for (int64_t j = it > kTcStages ? it - kTcStages : 0; j < it; ++j)
+        (void)mbar_wait(&full[j % kTcStages], (unsigned)((j / kTcStages) & 1));
+      atomicExch(err, 1);
+    }
+  } else if (warp == 1 && lane == 0) {
+    // ---- MMA issuer
+    constexpr uint32_t fmt = std::is_same<T, __nv_bfloat16>::value ? 1u : 0u;
+    constexpr uint32_t idesc = (1u << 4) | (fmt << 7) | (fmt << 10) | (1u << 15) | ((16u >> 3) << 17) |
+                               ((uint32_t)(kTcSlab >> 4) << 24);
+    int64_t it = 0, j = 0;
+    bool ok = true;
+    for (int64_t w = blockIdx.x; w < total && ok; w += gridDim.x, ++j) {
+      const int32_t br = (int32_t)(w % nbr);
+      const int32_t nk = bptr[br + 1] - bptr[br];
+      const int buf = (int)(j & 1);
+      if (j >= 2 && !tcp_wait(&accfree[buf], (unsigned)((j / 2 - 1) & 1), abort_flag)) {
+        ok = false;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      for (int32_t i = 0; i < nk; ++i, ++it) {
+        const int st = (int)(it % kTcStages);
+        if (!tcp_wait(&full[st], (unsigned)((it / kTcStages) & 1), abort_flag)) {
+          ok = false;
+          break;
+        }
+        const uint64_t adesc = umma_smem_desc(smem_u32(bslab + st * kTcBBytes), 2048u, 1024u, 2u);
+        const uint64_t bdesc = umma_smem_desc(smem_u32(atile + st * kTcABytes), 128u, 256u, 0u);
+        umma_f16(tmem + 16u * (uint32_t)buf, adesc, bdesc, idesc, i > 0 ? 1u : 0u);
+        umma_commit(&empty[st]);
+      }
+      umma_commit(&done[buf]);   // arrives when every MMA issued so far has completed
+    }
+    // no MMA may still be writing TMEM when the CTA frees it
+    umma_commit(drain);
+    if (!mbar_wait(drain, 0u)) ok = false;
+    if (!ok) atomicExch(err, 1);
+  } else if (warp >= 2) {
+    // ---- epilogue: warp w reads TMEM lanes 32 * (w % 4) .. + 31
+    const int q = warp & 3;
+    int64_t j = 0;
+    for (int64_t w = blockIdx.x; w < total; w += gridDim.x, ++j) {
+      const int32_t br = (int32_t)(w % nbr);
+      const int32_t n0 = (int32_t)(w / nbr) * W;
+      const int32_t nk = bptr[br + 1] - bptr[br];
+      const int buf = (int)(j & 1);
+      if (!tcp_wait(&done[buf], (unsigned)((j / 2) & 1), abort_flag)) {
+        atomicExch(err, 1);
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      float v[16];
+#pragma unroll
+      for (int r = 0; r < 16; ++r) v[r] = 0.f;
+      if (nk > 0) {
+        uint32_t r[16];
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+            "%14, %15}, [%16];"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+              "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+            : "r"(tmem + ((uint32_t)(q * 32) << 16) + 16u * (uint32_t)buf));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+        for (int c = 0; c < 16; ++c) v[c] = __uint_as_float(r[c]);
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&accfree[buf]);
+      const int64_t col = (int64_t)n0 + q * 32 + lane;
+      if (q * 32 < W && col < N) {
+#pragma unroll
+        for (int r = 0; r < 16; ++r) {
+          const int64_t row = (int64_t)br * kTS + r;
+          if (row < M) {
+            float *cp = C + row * ldc + col;
+            float o = alpha * v[r];
+            if (beta != 0.f) o += beta * *cp;
+            *cp = o;
+          }
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 1)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)kTcTmemCols)
+                 : "memory");
+}
+
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link
 // against libcuda).
 static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
@@ -888,6 +1086,42 @@ static int tc_slab_width(int32_t N, int32_t cols) {
   return (N >= 128 && (double)cols * 128 * 2 <= 0.6 * (double)l2) ? 128 : 64;
 }
 
+template <typename T>
+static int tcp_blocks_per_sm() {
+  static int b = 0;
+  if (b == 0) {
+    int v = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, spmm_tcp_kernel<T>, kTcpThreads, kTcpSmem) != cudaSuccess ||
+        v < 1)
+      v = 1;
+    b = v;
+  }
+  return b;
+}
+
+// Persistent form: one wave of resident CTAs walking all (block row, slab)
+// items, slab-major.
+static bsp_status smat_spmm_tcp(const bsp_smat *m, const void *B, int32_t N, int64_t ldb, float *C, int64_t ldc,
+                                float alpha, float beta, int32_t W, cudaStream_t s) {
+  CUtensorMap map;
+  BSP_TRY(make_b_map(&map, B, m->cols, N, ldb, m->dtype == BSP_BF16));
+  const int64_t total = (int64_t)m->tiles.rowRegions * ceil_div(N, W);
+  const bool bf = m->dtype == BSP_BF16;
+  const int per_sm = bf ? tcp_blocks_per_sm<__nv_bfloat16>() : tcp_blocks_per_sm<__half>();
+  const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(total, (int64_t)sm_count() * per_sm));
+  if (!bf)
+    spmm_tcp_kernel<__half><<<grid, kTcpThreads, kTcpSmem, s>>>(map, m->rows, N, W, m->tiles.rowRegions,
+                                                                m->tiles.bcsrRowPtr, m->tiles.bcsrcolIdx,
+                                                                (const __half *)m->tile_val, C, ldc, alpha, beta,
+                                                                m->err);
+  else
+    spmm_tcp_kernel<__nv_bfloat16><<<grid, kTcpThreads, kTcpSmem, s>>>(
+        map, m->rows, N, W, m->tiles.rowRegions, m->tiles.bcsrRowPtr, m->tiles.bcsrcolIdx,
+        (const __nv_bfloat16 *)m->tile_val, C, ldc, alpha, beta, m->err);
+  BSP_LAUNCH_CHECK();
+  return BSP_OK;
+}
+
 static bsp_status smat_spmm_tc(const bsp_smat *m, const void *B, int32_t N, int64_t ldb, float *C, int64_t ldc,
                                float alpha, float beta, int32_t W, cudaStream_t s) {
   CUtensorMap map;
@@ -922,9 +1156,12 @@ extern "C" bsp_status bsp_smat_spmm_path(const bsp_smat *m, const void *B, int32
   // cp.async.bulk needs 16-byte aligned sources and sizes
   BSP_CHECK_ARG((uintptr_t)B % 16 == 0 && (ldb * 2) % 16 == 0, "B must be 16-byte aligned with ldb % 8 == 0");
   BSP_CHECK_ARG((uintptr_t)m->tile_val % 16 == 0, "tile values must be 16-byte aligned");
-  BSP_CHECK_ARG(path >= BSP_SMAT_AUTO && path <= BSP_SMAT_TCGEN05_W128, "unknown path");
+  BSP_CHECK_ARG(path >= BSP_SMAT_AUTO && path <= BSP_SMAT_TCGEN05_PERSISTENT_W64, "unknown path");
   if (m->tiles.rowRegions == 0) return BSP_OK;
   cudaStream_t s = as_stream(stream);
+  if (path == BSP_SMAT_TCGEN05_PERSISTENT)
+    return smat_spmm_tcp(m, B, N, ldb, C, ldc, alpha, beta, N >= 128 ? 128 : 64, s);
+  if (path == BSP_SMAT_TCGEN05_PERSISTENT_W64) return smat_spmm_tcp(m, B, N, ldb, C, ldc, alpha, beta, 64, s);
   if (path == BSP_SMAT_TCGEN05_W64) return smat_spmm_tc(m, B, N, ldb, C, ldc, alpha, beta, 64, s);
   if (path == BSP_SMAT_TCGEN05_W128) return smat_spmm_tc(m, B, N, ldb, C, ldc, alpha, beta, 128, s);
   if (path == BSP_SMAT_TCGEN05 || path == BSP_SMAT_AUTO) return smat_spmm_tc(m, B, N, ldb, C, ldc, alpha, beta, 0, s);

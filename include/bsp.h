@@ -505,7 +505,12 @@ typedef enum {
   BSP_SMAT_MMA_SYNC = 1, /* warp mma.sync.m16n8k16, FP32 accumulators in registers */
   BSP_SMAT_TCGEN05 = 2,  /* tcgen05.mma M=128 N=16 K=16 per tile, slab width chosen from L2 */
   BSP_SMAT_TCGEN05_W64 = 3,  /* tcgen05, 64 C columns per CTA */
-  BSP_SMAT_TCGEN05_W128 = 4  /* tcgen05, 128 C columns per CTA */
+  BSP_SMAT_TCGEN05_W128 = 4, /* tcgen05, 128 C columns per CTA */
+  BSP_SMAT_TCGEN05_PERSISTENT = 5, /* tcgen05, resident CTAs walking every block row: a producer
+                                     warp, an MMA warp and four epilogue warps, two TMEM
+                                     accumulators so one block row's read-out overlaps the
+                                     next one's MMAs */
+  BSP_SMAT_TCGEN05_PERSISTENT_W64 = 6 /* the persistent form in 64-column slabs */
 } bsp_smat_path;
 bsp_status bsp_smat_spmm_path(const bsp_smat *m, const void *B, int32_t N,
                               int64_t ldb, float *C, int64_t ldc, float alpha,
@@ -759,14 +764,17 @@ bsp_status bsp_spmv_plan_destroy(bsp_spmv_plan plan);
  * row-major rows x 8 / cols x 8 blocks.
  *
  * Per matrix the tuner also picks the storage: CSR as given, or a SELL-32
- * copy the plan builds (slices of 32 consecutive rows padded to the slice's
- * longest row, entry k of row l at slice_start + 32k + l, values in the
- * batch's type and 16-bit column offsets from the row), which a warp reads
- * one slice at a time with every access coalesced.  A matrix qualifies for
- * SELL when padding adds at most 1/8 to its entries, it has no row longer
- * than long_row_nnz and every |column - row| < 32768; with tune = 0 every
- * qualifying matrix takes SELL, with tune = 1 SELL is timed like the lane
- * counts. */
+ * copy the plan builds (slices of 32 rows padded to the slice's longest row,
+ * entry k of slice row l at slice_start + 32k + l, values in the batch's
+ * type), which a warp reads one slice at a time with every access coalesced.
+ * Narrow form: the rows in order with 16-bit column offsets from the row,
+ * for matrices whose padding in row order adds at most 1/8, with no row
+ * longer than long_row_nnz and every |column - row| < 32768.  Wide form,
+ * for the others: the rows of at most T entries sorted by length with
+ * 32-bit columns and a row permutation, T the largest power of two
+ * (<= long_row_nnz) at which padding adds at most 1/8; rows above T go to
+ * whole-warp segments.  With tune = 0 every qualifying matrix takes SELL,
+ * with tune = 1 SELL is timed like the lane counts. */
 typedef struct {
   int32_t rows, cols, nnz;
   const int32_t *rowPtr; /* device */
@@ -803,7 +811,7 @@ bsp_status bsp_batch_set_vectors(bsp_batch_plan plan, int32_t m, const void *x,
 /* Per-matrix choice of the tuner: lanes per row (1..32) for CSR matrices,
  * 0 for matrices stored as SELL-32. */
 bsp_status bsp_batch_lanes(bsp_batch_plan plan, int32_t *lanes /* count */);
-/* Per-matrix storage: 0 = CSR, 1 = SELL-32. */
+/* Per-matrix storage: 0 = CSR, 1 = SELL-32 narrow form, 2 = SELL-32 wide form. */
 bsp_status bsp_batch_formats(bsp_batch_plan plan, int32_t *formats /* count */);
 bsp_status bsp_batch_stats(bsp_batch_plan plan, int64_t *items,
                            int64_t *long_segments, int64_t *total_nnz);

@@ -150,10 +150,11 @@ def test_batch_rejects_bad_arguments(cuda):
 
 
 def _sell_batch(seed):
-    """Banded matrices (even rows: SELL-32 candidates), a rectangular banded
+    """Banded matrices (even rows: narrow SELL-32), a rectangular banded
     block, a matrix whose columns reach 40,000 from their rows (int16 offsets
-    do not fit: stays CSR), power-law rows (uneven: CSR), and a banded matrix
-    with every 5th row empty (padding over 1/8: CSR)."""
+    do not fit: stays CSR), power-law rows (uneven: wide SELL-32, rows sorted
+    by length in windows, its long rows left to segments), and a banded
+    matrix with every 5th row empty (padding in row order over 1/8: wide)."""
     rng = np.random.default_rng(seed)
     mats = [bsp.gen_banded(int(rng.integers(100, 5000)), int(w), seed + i) for i, w in enumerate((3, 9, 15, 27))]
     B = bsp.gen_banded(3000, 11, seed + 7)
@@ -164,7 +165,7 @@ def _sell_batch(seed):
     ci = np.stack([np.arange(n), (np.arange(n) + 40000) % n], 1)
     ci.sort(axis=1)
     mats.append(bsp.HostCSR(n, n, rp, ci.reshape(-1).astype(np.int32), rng.standard_normal(2 * n)))
-    mats.append(bsp.gen_powerlaw(4000, 2.2, 4000, seed + 9))
+    mats.append(bsp.gen_powerlaw(8000, 2.2, 8000, seed + 9))
     E = bsp.gen_banded(1000, 9, seed + 11)
     lens = np.diff(E.rowptr)
     lens[::5] = 0
@@ -180,10 +181,11 @@ def test_batch_sell_format_choice_and_results(cuda, dtype, nrhs):
     import torch
     mats = _sell_batch(70 + nrhs)
     dev, host = _upload(cuda, mats, dtype, nrhs, 12)
-    P = bsp.BatchPlan(dev, nrhs=nrhs)
+    P = bsp.BatchPlan(dev, nrhs=nrhs, long_row_nnz=1024, seg_nnz=256)
     fm = P.formats()
-    assert fm.tolist() == [1, 1, 1, 1, 1, 0, 0, 0]
-    assert P.lanes()[:5].tolist() == [0] * 5
+    assert fm.tolist() == [1, 1, 1, 1, 1, 0, 2, 2]
+    assert mats[6].rowptr[1:].__sub__(mats[6].rowptr[:-1]).max() > 1024   # the wide matrix has long rows
+    assert P.lanes().tolist() == [0] * 5 + [P.lanes()[5], 0, 0]
     P.run()
     torch.cuda.synchronize()
     _check(mats, dev, host, dtype, nrhs)
@@ -198,8 +200,8 @@ def test_batch_sell_format_choice_and_results(cuda, dtype, nrhs):
     Q.run()
     torch.cuda.synchronize()
     _check(mats, dev, host, dtype, nrhs)
-    T = bsp.BatchPlan(dev, nrhs=nrhs, tune=1)
-    assert not T.formats()[5:].any()            # not SELL-eligible
+    T = bsp.BatchPlan(dev, nrhs=nrhs, tune=1, long_row_nnz=1024, seg_nnz=256)
+    assert T.formats()[5] == 0                  # not SELL-eligible
     T.run()
     torch.cuda.synchronize()
     _check(mats, dev, host, dtype, nrhs)

@@ -206,8 +206,9 @@ def test_smat_alpha_beta_and_argument_errors(cuda):
 def test_smat_tcgen05_and_mma_sync_paths(cuda, name, N, kind):
     """The tcgen05 path (TMEM accumulator, TMA-staged B) at both slab widths
     (64 and 128 C columns per CTA; columns past N zero-filled by TMA and not
-    stored) and the mma.sync path against the FP64 oracle; all deterministic
-    across calls."""
+    stored), its persistent warp-specialised form (empty block rows and
+    more block rows than resident CTAs included) and the mma.sync path
+    against the FP64 oracle; all deterministic across calls."""
     import torch
     A = bsp.gen_random_bsr(96, 16, 6, 1.0, 1.0, 4) if kind == "dense_tiles" else bsp.gen_powerlaw(1003, 1.7, 400, 12)
     vals_t, vals64, B_t, B64 = _case(A, N, name, N + 7)
@@ -218,7 +219,7 @@ def test_smat_tcgen05_and_mma_sync_paths(cuda, name, N, kind):
     L = np.full((A.rows, 1), 16.0 * ((A.cols + 15) // 16) + 2.0)
     u = 2.0 ** -24
     tol = 2.0 * (L * u / (1 - L * u)) * absC + 1e-30
-    for path in ("tcgen05", "tcgen05_w64", "tcgen05_w128", "mma_sync"):
+    for path in ("tcgen05", "tcgen05_w64", "tcgen05_w128", "tcgen05_persistent", "tcgen05_persistent_w64", "mma_sync"):
         C1 = M.spmm(Bd, path=path).cpu().numpy()
         C2 = M.spmm(Bd, path=path).cpu().numpy()
         M.check()
@@ -281,3 +282,36 @@ def test_spmm_slab_engine_rejects_bad_widths(cuda):
         with pytest.raises(bsp.BspError):
             P.spmm(B, engine="slab", slab_cols=bad)
     P.free()
+
+
+@pytest.mark.parametrize("N", [64, 128, 256])
+def test_smat_tcgen05_persistent_many_block_rows(cuda, N):
+    """Persistent tcgen05 kernel on far more block rows than resident CTAs
+    (each CTA walks many block rows, alternating its two TMEM accumulators),
+    with every 7th block row empty: the same bits as the one-CTA-per-block-row
+    kernel (same MMAs in the same order) and within the FP32 bound."""
+    import torch
+    A = bsp.gen_random_bsr(3000, 16, 4, 0.5, 1.0, 21)
+    keep = (np.arange(A.rows) // 16) % 7 != 0
+    lens = np.where(keep, np.diff(A.rowptr), 0)
+    mask = np.repeat(keep, np.diff(A.rowptr))
+    rp = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    A = bsp.HostCSR(A.rows, A.cols, rp, A.colidx[mask].copy(), A.values[mask].copy())
+    vals_t, vals64, B_t, B64 = _case(A, N, "f16", 31)
+    rpd, cid, v64 = _dev(cuda, A.rowptr, A.colidx, vals64)
+    M = bsp.SmatMatrix(rpd, cid, v64, rows=A.rows, cols=A.cols, dtype="f16")
+    Bd = B_t.to(cuda)
+    Cin = torch.from_numpy(np.random.default_rng(2).uniform(-1, 1, (A.rows, N)).astype(np.float32)).to(cuda)
+    ref_path = "tcgen05_w128" if N >= 128 else "tcgen05_w64"
+    C0 = M.spmm(Bd, Cin.clone(), alpha=1.5, beta=-0.5, path=ref_path)
+    for _ in range(2):
+        C1 = M.spmm(Bd, Cin.clone(), alpha=1.5, beta=-0.5, path="tcgen05_persistent")
+        M.check()
+        assert torch.equal(C0, C1)
+    Cref, absC = pyoracle.spmm_f64(A.rowptr, A.colidx, vals64, B64)
+    want = 1.5 * Cref - 0.5 * Cin.cpu().numpy().astype(np.float64)
+    L = np.full((A.rows, 1), 16.0 * ((A.cols + 15) // 16) + 2.0)
+    u = 2.0 ** -24
+    tol = 2.0 * (L * u / (1 - L * u)) * 1.5 * absC + 4 * u * (1.5 * absC + 0.5 * np.abs(Cin.cpu().numpy())) + 1e-30
+    assert np.all(np.abs(C1.cpu().numpy().astype(np.float64) - want) <= tol)
+    M.free()
