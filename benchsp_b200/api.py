@@ -796,9 +796,9 @@ class BatchPlan:
     """y_m = A_m x_m for many CSR matrices in one persistent, graph-captured
     launch.  `mats` is a list of (rowptr, colidx, values, x, y) device tensors;
     values/x/y F64 or F32; nrhs 1 or 8 (x: cols x 8, y: rows x 8 row-major).
-    tune=0 picks lanes per row (and SELL-32 storage for matrices with even
-    rows) from row statistics, tune=1 times the candidates per matrix;
-    sell=False keeps every matrix in CSR."""
+    Matrices with even rows are stored as SELL-32 (sell=False keeps every
+    matrix in CSR); for the others tune=0 picks lanes per row from row
+    statistics, tune=1 times the lane counts per matrix."""
 
     def __init__(self, mats, *, nrhs: int = 1, tune: int = 0, seg_nnz: int = 1024, long_row_nnz: int = 2048,
                  item_nnz: int = 0, use_graph: bool = True, sell: bool = True, stream=None):
@@ -840,8 +840,7 @@ class BatchPlan:
         return out
 
     def formats(self) -> np.ndarray:
-        """Per-matrix storage: 0 = CSR, 1 = SELL-32 (rows in order, 16-bit
-        column offsets), 2 = SELL-32 of length-sorted rows (32-bit columns)."""
+        """Per-matrix storage: 0 = CSR, 1 = SELL-32."""
         out = np.empty(self.count, np.int32)
         check(lib().bsp_batch_formats(self._h, out.ctypes.data_as(C.c_void_p)))
         return out

@@ -763,18 +763,14 @@ bsp_status bsp_spmv_plan_destroy(bsp_spmv_plan plan);
  * y_m = A_m x_m for every matrix m; with nrhs = 8, x_m and y_m are
  * row-major rows x 8 / cols x 8 blocks.
  *
- * Per matrix the tuner also picks the storage: CSR as given, or a SELL-32
- * copy the plan builds (slices of 32 rows padded to the slice's longest row,
- * entry k of slice row l at slice_start + 32k + l, values in the batch's
- * type), which a warp reads one slice at a time with every access coalesced.
- * Narrow form: the rows in order with 16-bit column offsets from the row,
- * for matrices whose padding in row order adds at most 1/8, with no row
- * longer than long_row_nnz and every |column - row| < 32768.  Wide form,
- * for the others: the rows of at most T entries sorted by length with
- * 32-bit columns and a row permutation, T the largest power of two
- * (<= long_row_nnz) at which padding adds at most 1/8; rows above T go to
- * whole-warp segments.  With tune = 0 every qualifying matrix takes SELL,
- * with tune = 1 SELL is timed like the lane counts. */
+ * Per matrix the plan also picks the storage: CSR as given, or a SELL-32
+ * copy it builds (slices of 32 consecutive rows padded to the slice's
+ * longest row, entry k of row l at slice_start + 32k + l, values in the
+ * batch's type and 16-bit column offsets from the row), which a warp reads
+ * one slice at a time with every access coalesced.  A matrix takes SELL when
+ * padding adds at most 1/8 to its entries, it has no row longer than
+ * long_row_nnz and every |column - row| < 32768; the others stay CSR, where
+ * tune = 1 times the lane counts per matrix. */
 typedef struct {
   int32_t rows, cols, nnz;
   const int32_t *rowPtr; /* device */
@@ -811,7 +807,7 @@ bsp_status bsp_batch_set_vectors(bsp_batch_plan plan, int32_t m, const void *x,
 /* Per-matrix choice of the tuner: lanes per row (1..32) for CSR matrices,
  * 0 for matrices stored as SELL-32. */
 bsp_status bsp_batch_lanes(bsp_batch_plan plan, int32_t *lanes /* count */);
-/* Per-matrix storage: 0 = CSR, 1 = SELL-32 narrow form, 2 = SELL-32 wide form. */
+/* Per-matrix storage: 0 = CSR, 1 = SELL-32. */
 bsp_status bsp_batch_formats(bsp_batch_plan plan, int32_t *formats /* count */);
 bsp_status bsp_batch_stats(bsp_batch_plan plan, int64_t *items,
                            int64_t *long_segments, int64_t *total_nnz);
