@@ -221,7 +221,7 @@ class BspBatchMat(C.Structure):
 class BspBatchOptions(C.Structure):
     """Mirror of bsp_batch_options (include/bsp.h)."""
     _fields_ = [("tune", C.c_int32), ("seg_nnz", C.c_int32), ("long_row_nnz", C.c_int32), ("item_nnz", C.c_int32),
-                ("use_graph", C.c_int32), ("sell", C.c_int32)]
+                ("use_graph", C.c_int32), ("sell", C.c_int32), ("sell_wide", C.c_int32)]
 
 
 _PROTOS.update({

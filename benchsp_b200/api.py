@@ -797,11 +797,13 @@ class BatchPlan:
     launch.  `mats` is a list of (rowptr, colidx, values, x, y) device tensors;
     values/x/y F64 or F32; nrhs 1 or 8 (x: cols x 8, y: rows x 8 row-major).
     Matrices with even rows are stored as SELL-32 (sell=False keeps every
-    matrix in CSR); for the others tune=0 picks lanes per row from row
-    statistics, tune=1 times the lane counts per matrix."""
+    matrix in CSR; sell_wide=True also stores uneven ones as length-sorted
+    SELL-32); for the others tune=0 picks lanes per row from row statistics,
+    tune=1 times the lane counts per matrix."""
 
     def __init__(self, mats, *, nrhs: int = 1, tune: int = 0, seg_nnz: int = 1024, long_row_nnz: int = 2048,
-                 item_nnz: int = 0, use_graph: bool = True, sell: bool = True, stream=None):
+                 item_nnz: int = 0, use_graph: bool = True, sell: bool = True, sell_wide: bool = False,
+                 stream=None):
         torch = _torch()
         if not mats:
             raise ValueError("empty batch")
@@ -816,7 +818,8 @@ class BatchPlan:
             cols = x.shape[0] if nrhs > 1 else x.numel()
             arr[i] = _lib.BspBatchMat(rows, cols, ci.numel(), _dptr(rp, "rowptr"), _dptr(ci, "colidx"),
                                       _dptr(va, "values"), _dptr(x, "x"), _dptr(y, "y"))
-        opt = _lib.BspBatchOptions(tune, seg_nnz, long_row_nnz, item_nnz, 1 if use_graph else 0, 1 if sell else 0)
+        opt = _lib.BspBatchOptions(tune, seg_nnz, long_row_nnz, item_nnz, 1 if use_graph else 0, 1 if sell else 0,
+                                   1 if sell_wide else 0)
         self._h = C.c_void_p()
         self.count = len(mats)
         self._keep = list(mats)
@@ -840,7 +843,8 @@ class BatchPlan:
         return out
 
     def formats(self) -> np.ndarray:
-        """Per-matrix storage: 0 = CSR, 1 = SELL-32."""
+        """Per-matrix storage: 0 = CSR, 1 = SELL-32 (rows in order, 16-bit
+        column offsets), 2 = SELL-32 of length-sorted rows (sell_wide=True)."""
         out = np.empty(self.count, np.int32)
         check(lib().bsp_batch_formats(self._h, out.ctypes.data_as(C.c_void_p)))
         return out

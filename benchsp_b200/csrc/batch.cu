@@ -38,19 +38,26 @@ struct BatchMatDev {
   int32_t rows, cols;
   // SELL-32 copy (null when the matrix is stored only as CSR): slice s of 32
   // rows spans entries [sell_ptr[s], sell_ptr[s + 1]); entry k of row l of
-  // the slice at sell_ptr[s] + 32k + l; column = row + sell_off[entry]
+  // the slice at sell_ptr[s] + 32k + l.  Narrow form: slice rows are the
+  // matrix rows in order, column = row + sell_off[entry].  Wide form: slice
+  // row l of slice s is matrix row sell_perm[32s + l] (rows sorted by length
+  // inside windows, rows of long segments left out), column = sell_col[entry].
   const int32_t *sell_ptr;
   const void *sell_val;
   const int16_t *sell_off;
+  const int32_t *sell_perm;
+  const int32_t *sell_col;
+  int32_t sell_rows;
 };
 
-// info == kSellItem: SELL slices [a, b).
+// info == kSellItem / kSellWideItem: SELL slices [a, b) (narrow / wide form).
 // info >= 0 otherwise: row item, rows [a, b), info = lanes per row.
 // info < 0 : long-row segment, row a, segment b, long id = -(info + 1).
 struct BatchItem {
   int32_t mat, a, b, info;
 };
 constexpr int32_t kSellItem = 64;
+constexpr int32_t kSellWideItem = 65;
 
 struct LongRow {
   int32_t part_base, nseg;
@@ -220,23 +227,25 @@ __device__ __forceinline__ void rows_item(const BatchMatDev &M, int32_t r0, int3
   }
 }
 
-// SELL-32 slices [s0, s1): lane l owns row 32*s + l and sums its entries
+// SELL-32 slices [s0, s1): lane l owns slice row l and sums its entries
 // in stored order, U entries' loads issued before their gathers.  Value and
-// offset loads of a warp are 32 consecutive entries (coalesced), and for
-// banded matrices the gathered x rows are consecutive too.
-template <typename V, int NRHS>
+// column loads of a warp are 32 consecutive entries (coalesced); for banded
+// matrices (narrow form) the gathered x rows are consecutive too.
+template <typename V, int NRHS, bool WIDE>
 __device__ __forceinline__ void sell_item(const BatchMatDev &M, int32_t s0, int32_t s1, int lane) {
   constexpr int U = NRHS == 1 ? 4 : 2;
   const V *sv = static_cast<const V *>(M.sell_val);
   const V *x = static_cast<const V *>(M.x);
   V *y = static_cast<V *>(M.y);
   for (int32_t sl = s0; sl < s1; ++sl) {
-    const int32_t row = sl * 32 + lane;
-    const bool live = row < M.rows;
+    const int32_t pos = sl * 32 + lane;
+    const bool live = pos < (WIDE ? M.sell_rows : M.rows);
+    const int32_t row = WIDE ? (live ? __ldg(M.sell_perm + pos) : 0) : pos;
     const int32_t p0 = __ldg(M.sell_ptr + sl);
     const int32_t w = live ? (__ldg(M.sell_ptr + sl + 1) - p0) >> 5 : 0;
     const V *vp = sv + p0 + lane;
     const int16_t *op = M.sell_off + p0 + lane;
+    const int32_t *cp = M.sell_col + p0 + lane;
     V acc[NRHS];
 #pragma unroll
     for (int k = 0; k < NRHS; ++k) acc[k] = V(0);
@@ -247,7 +256,7 @@ __device__ __forceinline__ void sell_item(const BatchMatDev &M, int32_t s0, int3
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         a[u] = __ldg(vp + 32 * (k + u));
-        c[u] = row + (int32_t)__ldg(op + 32 * (k + u));
+        c[u] = WIDE ? __ldg(cp + 32 * (k + u)) : row + (int32_t)__ldg(op + 32 * (k + u));
       }
       V xr[U][NRHS];
 #pragma unroll
@@ -257,7 +266,7 @@ __device__ __forceinline__ void sell_item(const BatchMatDev &M, int32_t s0, int3
     }
     for (; k < w; ++k) {
       V xr[NRHS];
-      load_xrow<V, NRHS>(x, row + (int32_t)__ldg(op + 32 * k), xr);
+      load_xrow<V, NRHS>(x, WIDE ? __ldg(cp + 32 * k) : row + (int32_t)__ldg(op + 32 * k), xr);
       fma_row<V, NRHS>(acc, __ldg(vp + 32 * k), xr);
     }
     if (live) {
@@ -286,6 +295,26 @@ __global__ void batch_sell_fill_kernel(int32_t rows, int32_t cols, const int32_t
       if (d < -32768 || d > 32767) atomicExch(bad, 1);
       sval[p0 + 32 * k + l] = real ? val[s + k] : V(0);
       soff[p0 + 32 * k + l] = (int16_t)(d < -32768 || d > 32767 ? 0 : d);
+    }
+  }
+}
+
+// Fills the wide SELL-32 copy: thread per slice row; slice row p is matrix
+// row perm[p]; padding entries get value 0 and column 0.
+template <typename V>
+__global__ void batch_sell_fill_wide_kernel(int32_t nrows, const int32_t *__restrict__ perm,
+                                            const int32_t *__restrict__ rp, const int32_t *__restrict__ ci,
+                                            const V *__restrict__ val, const int32_t *__restrict__ sptr,
+                                            V *__restrict__ sval, int32_t *__restrict__ scol) {
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < nrows; p += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t sl = (int32_t)(p >> 5), l = (int32_t)(p & 31);
+    const int32_t p0 = sptr[sl], w = (sptr[sl + 1] - p0) >> 5;
+    const int32_t r = perm[p];
+    const int32_t s = rp[r], len = rp[r + 1] - s;
+    for (int32_t k = 0; k < w; ++k) {
+      const bool real = k < len;
+      sval[p0 + 32 * k + l] = real ? val[s + k] : V(0);
+      scol[p0 + 32 * k + l] = real ? ci[s + k] : 0;
     }
   }
 }
@@ -325,10 +354,10 @@ __device__ __forceinline__ void segment_item(const BatchMatDev &M, int32_t row, 
 }
 
 // One FP32 vector: capped at 40 registers (6 resident CTAs per SM).  At 32
-// registers (8 CTAs) it measured faster before the SELL items and the
-// grouped short-row loads joined the kernel (222.5 -> 204.5 us); with them
-// 6 CTAs measured faster (512-matrix batch, tuned lanes: 190.7 -> 174.1 us).
-// FP64 and the 8-vector forms keep the compiler's choice.
+// registers (8 CTAs) it was faster before the SELL items joined the kernel
+// (222.5 -> 204.5 us) but now spills there, and 6 CTAs measured faster
+// (512-matrix batch, tuned: 190.7 -> 174.1 us).  FP64 and the 8-vector forms
+// keep the compiler's choice.
 template <typename V, int NRHS>
 __global__ void __launch_bounds__(kBatchThreads, (NRHS == 1 && sizeof(V) == 4) ? 6 : 0) batch_kernel(const BatchMatDev *__restrict__ mats,
                                                               const BatchItem *__restrict__ items, int32_t nitems,
@@ -345,7 +374,11 @@ __global__ void __launch_bounds__(kBatchThreads, (NRHS == 1 && sizeof(V) == 4) ?
     const BatchItem I = items[it];
     const BatchMatDev M = mats[I.mat];
     if (I.info == kSellItem) {
-      sell_item<V, NRHS>(M, I.a, I.b, lane);
+      sell_item<V, NRHS, false>(M, I.a, I.b, lane);
+      continue;
+    }
+    if (I.info == kSellWideItem) {
+      sell_item<V, NRHS, true>(M, I.a, I.b, lane);
       continue;
     }
     if (I.info < 0) {
@@ -374,13 +407,16 @@ struct bsp_batch_plan_s {
   std::vector<bsp_batch_mat> host_mats;
   std::vector<std::vector<int32_t>> lens;  // row lengths per matrix
   std::vector<int32_t> lanes;
-  std::vector<int32_t> fmt;                 // 0 CSR, 1 SELL-32
-  std::vector<uint8_t> sell_ok;             // the matrix has a SELL-32 copy
+  std::vector<int32_t> fmt;                 // 0 CSR, 1 SELL-32 narrow, 2 SELL-32 wide
+  std::vector<uint8_t> sell_ok;             // 0 none, 1 narrow, 2 wide copy built
   std::vector<std::vector<int32_t>> sell_slices;  // slice pointers (host copy)
+  std::vector<int32_t> sell_T;              // wide form: rows above this go to segments
   std::vector<BatchMatDev> dm;              // host copy of the descriptors
   void *d_sell_val = nullptr;
   int16_t *d_sell_off = nullptr;
   int32_t *d_sell_ptr = nullptr;
+  int32_t *d_sell_col = nullptr;
+  int32_t *d_sell_perm = nullptr;
   BatchMatDev *d_mats = nullptr;
   // batched list (long segments first) and per-matrix lists
   BatchItem *d_items = nullptr, *d_items_sep = nullptr;
@@ -436,18 +472,60 @@ std::vector<int32_t> sell_slices(const std::vector<int32_t> &len, int32_t long_t
   return ptr;
 }
 
+// Wide SELL-32 layout: the rows of at most T entries sorted by length
+// (longest first, stable) and cut into slices of 32; `perm` gets the slice
+// rows' matrix rows, *T_out the cut.  T is the largest power of two <=
+// long_thr (down to 8) whose padding adds at most 1/8 to those rows'
+// entries; the rows above T are taken by whole warps as segments.  On the
+// batch's Zipf(2.2) matrices a full sort pads by a median 3% at T = 32,
+// where sorting inside windows of 1024 rows padded by 29%.  Empty when no T
+// qualifies or the padded size passes 2^31.
+std::vector<int32_t> sell_slices_wide(const std::vector<int32_t> &len, int32_t long_thr, std::vector<int32_t> &perm,
+                                      int32_t *T_out) {
+  std::vector<int32_t> order(len.size());
+  for (size_t r = 0; r < len.size(); ++r) order[r] = (int32_t)r;
+  std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return len[a] > len[b]; });
+  int32_t T = 8;
+  while (T * 2 <= long_thr) T *= 2;
+  for (; T >= 8; T /= 2) {
+    // rows of at most T entries: a suffix of the sorted order
+    size_t first = 0;
+    while (first < order.size() && len[order[first]] > T) ++first;
+    const int64_t n = (int64_t)(order.size() - first);
+    if (n == 0) continue;
+    const int64_t ns = (n + 31) / 32;
+    std::vector<int32_t> ptr((size_t)ns + 1, 0);
+    int64_t nnz = 0, acc = 0;
+    bool fits = true;
+    for (int64_t sl = 0; sl < ns && fits; ++sl) {
+      const int32_t w = len[order[first + sl * 32]];   // longest of the slice
+      for (int64_t p = sl * 32; p < std::min(n, sl * 32 + 32); ++p) nnz += len[order[first + p]];
+      acc += 32 * (int64_t)w;
+      if (acc >= INT32_MAX) fits = false;
+      else ptr[sl + 1] = (int32_t)acc;
+    }
+    if (!fits || 8 * acc > 9 * nnz) continue;
+    perm.assign(order.begin() + first, order.end());
+    *T_out = T;
+    return ptr;
+  }
+  perm.clear();
+  return {};
+}
+
 // Items of a SELL-32 matrix: runs of slices costing about item_nnz, a
 // slice costing its entries plus 64 (its rows' overhead, as the CSR row
-// items count 2 per row): banded half of the 512-matrix batch, FP64, 136.6
-// -> 129.3 us against counting entries alone.
-void build_sell_items(int32_t m, const std::vector<int32_t> &sptr, int64_t item_nnz, std::vector<BatchItem> &out) {
+// items count 2 per row): slices of one-entry rows would otherwise pile
+// dozens of dependent slice walks on one warp.
+void build_sell_items(int32_t m, const std::vector<int32_t> &sptr, int64_t item_nnz, int32_t info,
+                      std::vector<BatchItem> &out) {
   const int32_t ns = (int32_t)sptr.size() - 1;
   int32_t s0 = 0;
   int64_t acc = 0;
   for (int32_t sl = 0; sl < ns; ++sl) {
     acc += (int64_t)sptr[sl + 1] - sptr[sl] + 64;
     if (acc >= item_nnz || sl + 1 == ns) {
-      out.push_back({m, s0, sl + 1, kSellItem});
+      out.push_back({m, s0, sl + 1, info});
       s0 = sl + 1;
       acc = 0;
     }
@@ -458,16 +536,18 @@ void build_sell_items(int32_t m, const std::vector<int32_t> &sptr, int64_t item_
 // their long-row entries), then row items (to `rows`).
 void build_items(int32_t m, const std::vector<int32_t> &len, int L, const bsp_batch_options &o,
                  std::vector<BatchItem> &lng, std::vector<BatchItem> &rows, std::vector<LongRow> &longs,
-                 int64_t &parts, int64_t item_nnz) {
+                 int64_t &parts, int64_t item_nnz, int32_t long_only_thr = -1) {
   const int32_t n = (int32_t)len.size();
+  const int32_t thr = long_only_thr >= 0 ? long_only_thr : o.long_row_nnz;
   for (int32_t r = 0; r < n; ++r)
-    if (len[r] > o.long_row_nnz) {
+    if (len[r] > thr) {
       const int32_t ns = (len[r] + o.seg_nnz - 1) / o.seg_nnz;
       const int32_t lid = (int32_t)longs.size();
       longs.push_back({(int32_t)parts, ns});
       parts += ns;
       for (int32_t s = 0; s < ns; ++s) lng.push_back({m, r, s, -(lid + 1)});
     }
+  if (long_only_thr >= 0) return;
   const int64_t max_rows = (int64_t)(32 / L) * 256;
   int32_t r0 = 0;
   int64_t acc = 0;
@@ -496,6 +576,7 @@ extern "C" bsp_status bsp_batch_default_options(bsp_batch_options *o) {
   o->item_nnz = 0;
   o->use_graph = 1;
   o->sell = 1;
+  o->sell_wide = 0;
   return BSP_OK;
 }
 
@@ -550,10 +631,14 @@ static bsp_status batch_build(bsp_batch_plan P, cudaStream_t s) {
   P->sep_off.assign(P->count + 1, 0);
   for (int32_t m = 0; m < P->count; ++m) {
     std::vector<BatchItem> l1, r1;
-    if (P->fmt[m] == 1)
-      build_sell_items(m, P->sell_slices[m], item_nnz, r1);
-    else
+    if (P->fmt[m] == 1) {
+      build_sell_items(m, P->sell_slices[m], item_nnz, kSellItem, r1);
+    } else if (P->fmt[m] == 2) {   // long rows as segments, the rest from the wide copy
+      build_items(m, P->lens[m], P->lanes[m], o, l1, r1, longs, parts, item_nnz, P->sell_T[m]);
+      build_sell_items(m, P->sell_slices[m], item_nnz, kSellWideItem, r1);
+    } else {
       build_items(m, P->lens[m], P->lanes[m], o, l1, r1, longs, parts, item_nnz);
+    }
     lng.insert(lng.end(), l1.begin(), l1.end());
     rows.insert(rows.end(), r1.begin(), r1.end());
     sep.insert(sep.end(), l1.begin(), l1.end());
@@ -639,67 +724,111 @@ extern "C" bsp_status bsp_batch_destroy(bsp_batch_plan P) {
   if (P->d_sell_val) cudaFreeAsync(P->d_sell_val, s);
   dfree(P->d_sell_off, s);
   dfree(P->d_sell_ptr, s);
+  dfree(P->d_sell_col, s);
+  dfree(P->d_sell_perm, s);
   cudaStreamSynchronize(s);
   delete P;
   return BSP_OK;
 }
 
 namespace {
-// Builds the SELL-32 copies of every matrix that qualifies (one allocation
-// for all) and fills P->sell_ok; a matrix whose copy would need a column
-// offset outside int16 stays CSR-only.
+// Builds the SELL-32 copies (one allocation per array kind for all
+// matrices) and fills P->sell_ok: the narrow form (rows in order, 16-bit
+// offsets) where it qualifies, else the wide form (rows sorted by length in
+// windows, 32-bit columns, long rows left to segments) where its padding
+// qualifies.  A narrow copy whose offsets turn out not to fit int16 is
+// dropped and the matrix stays CSR.
 bsp_status build_sell(bsp_batch_plan P, cudaStream_t s) {
   const int32_t count = P->count;
   P->sell_ok.assign(count, 0);
   P->sell_slices.assign(count, {});
+  P->sell_T.assign(count, 0);
   if (!P->opt.sell) return BSP_OK;
-  int64_t total = 0, total_ptr = 0;
-  std::vector<int64_t> val_off(count, 0), ptr_off(count, 0);
+  std::vector<std::vector<int32_t>> perms(count);
+  int64_t tot_val = 0, tot_narrow = 0, tot_wide = 0, tot_ptr = 0, tot_perm = 0;
+  std::vector<int64_t> val_off(count, 0), off_off(count, 0), col_off(count, 0), ptr_off(count, 0), perm_off(count, 0);
   for (int32_t m = 0; m < count; ++m) {
     if (P->host_mats[m].cols <= 0) continue;
-    P->sell_slices[m] = sell_slices(P->lens[m], P->opt.long_row_nnz);
-    if (P->sell_slices[m].empty()) continue;
-    val_off[m] = total;
-    ptr_off[m] = total_ptr;
-    total += P->sell_slices[m].back();
-    total_ptr += (int64_t)P->sell_slices[m].size();
-    P->sell_ok[m] = 1;
+    std::vector<int32_t> sp = sell_slices(P->lens[m], P->opt.long_row_nnz);
+    uint8_t kind = 1;
+    if (sp.empty() && P->opt.sell_wide) {
+      sp = sell_slices_wide(P->lens[m], P->opt.long_row_nnz, perms[m], &P->sell_T[m]);
+      kind = 2;
+    }
+    if (sp.empty()) continue;
+    const int64_t ent = sp.back();
+    val_off[m] = tot_val;
+    tot_val += ent;
+    if (kind == 1) {
+      off_off[m] = tot_narrow;
+      tot_narrow += ent;
+    } else {
+      col_off[m] = tot_wide;
+      tot_wide += ent;
+      perm_off[m] = tot_perm;
+      tot_perm += (int64_t)perms[m].size();
+    }
+    ptr_off[m] = tot_ptr;
+    tot_ptr += (int64_t)sp.size();
+    P->sell_slices[m] = std::move(sp);
+    P->sell_ok[m] = kind;
   }
-  if (total_ptr == 0) return BSP_OK;
+  if (tot_ptr == 0) return BSP_OK;
   const size_t es = P->dtype == BSP_F64 ? 8 : 4;
-  BSP_CUDA(cudaMallocAsync(&P->d_sell_val, (size_t)std::max<int64_t>(total, 1) * es, s));
-  BSP_TRY(dalloc(&P->d_sell_off, (size_t)std::max<int64_t>(total, 1), s));
-  BSP_TRY(dalloc(&P->d_sell_ptr, (size_t)total_ptr, s));
+  BSP_CUDA(cudaMallocAsync(&P->d_sell_val, (size_t)std::max<int64_t>(tot_val, 1) * es, s));
+  BSP_TRY(dalloc(&P->d_sell_off, (size_t)std::max<int64_t>(tot_narrow, 1), s));
+  BSP_TRY(dalloc(&P->d_sell_col, (size_t)std::max<int64_t>(tot_wide, 1), s));
+  BSP_TRY(dalloc(&P->d_sell_perm, (size_t)std::max<int64_t>(tot_perm, 1), s));
+  BSP_TRY(dalloc(&P->d_sell_ptr, (size_t)tot_ptr, s));
   int32_t *bad = nullptr;
   BSP_TRY(dalloc(&bad, (size_t)count, s));
   BSP_CUDA(cudaMemsetAsync(bad, 0, sizeof(int32_t) * count, s));
-  BSP_CUDA(cudaMemsetAsync(P->d_sell_val, 0, (size_t)std::max<int64_t>(total, 1) * es, s));
-  BSP_CUDA(cudaMemsetAsync(P->d_sell_off, 0, sizeof(int16_t) * (size_t)std::max<int64_t>(total, 1), s));
+  BSP_CUDA(cudaMemsetAsync(P->d_sell_val, 0, (size_t)std::max<int64_t>(tot_val, 1) * es, s));
+  BSP_CUDA(cudaMemsetAsync(P->d_sell_off, 0, sizeof(int16_t) * (size_t)std::max<int64_t>(tot_narrow, 1), s));
+  BSP_CUDA(cudaMemsetAsync(P->d_sell_col, 0, sizeof(int32_t) * (size_t)std::max<int64_t>(tot_wide, 1), s));
   for (int32_t m = 0; m < count; ++m) {
     if (!P->sell_ok[m]) continue;
     const std::vector<int32_t> &sp = P->sell_slices[m];
     int32_t *dptr = P->d_sell_ptr + ptr_off[m];
     BSP_CUDA(cudaMemcpyAsync(dptr, sp.data(), sp.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
     const bsp_batch_mat &A = P->host_mats[m];
-    const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div(A.rows, 256), 4096));
-    int16_t *off = P->d_sell_off + val_off[m];
-    if (P->dtype == BSP_F64) {
-      double *v = static_cast<double *>(P->d_sell_val) + val_off[m];
-      batch_sell_fill_kernel<double><<<grid, 256, 0, s>>>(A.rows, A.cols, A.rowPtr, A.colIdx,
-                                                          static_cast<const double *>(A.values), dptr, v, off,
-                                                          bad + m);
-      P->dm[m].sell_val = v;
+    void *v = static_cast<char *>(P->d_sell_val) + val_off[m] * (int64_t)es;
+    if (P->sell_ok[m] == 1) {
+      const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div(A.rows, 256), 4096));
+      int16_t *off = P->d_sell_off + off_off[m];
+      if (P->dtype == BSP_F64)
+        batch_sell_fill_kernel<double><<<grid, 256, 0, s>>>(A.rows, A.cols, A.rowPtr, A.colIdx,
+                                                            static_cast<const double *>(A.values), dptr,
+                                                            static_cast<double *>(v), off, bad + m);
+      else
+        batch_sell_fill_kernel<float><<<grid, 256, 0, s>>>(A.rows, A.cols, A.rowPtr, A.colIdx,
+                                                           static_cast<const float *>(A.values), dptr,
+                                                           static_cast<float *>(v), off, bad + m);
+      P->dm[m].sell_off = off;
+      P->dm[m].sell_rows = A.rows;
     } else {
-      float *v = static_cast<float *>(P->d_sell_val) + val_off[m];
-      batch_sell_fill_kernel<float><<<grid, 256, 0, s>>>(A.rows, A.cols, A.rowPtr, A.colIdx,
-                                                         static_cast<const float *>(A.values), dptr, v, off, bad + m);
-      P->dm[m].sell_val = v;
+      const int32_t nr = (int32_t)perms[m].size();
+      int32_t *perm = P->d_sell_perm + perm_off[m];
+      int32_t *col = P->d_sell_col + col_off[m];
+      BSP_CUDA(cudaMemcpyAsync(perm, perms[m].data(), sizeof(int32_t) * nr, cudaMemcpyHostToDevice, s));
+      const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div(nr, 256), 4096));
+      if (P->dtype == BSP_F64)
+        batch_sell_fill_wide_kernel<double><<<grid, 256, 0, s>>>(nr, perm, A.rowPtr, A.colIdx,
+                                                                 static_cast<const double *>(A.values), dptr,
+                                                                 static_cast<double *>(v), col);
+      else
+        batch_sell_fill_wide_kernel<float><<<grid, 256, 0, s>>>(nr, perm, A.rowPtr, A.colIdx,
+                                                                static_cast<const float *>(A.values), dptr,
+                                                                static_cast<float *>(v), col);
+      P->dm[m].sell_perm = perm;
+      P->dm[m].sell_col = col;
+      P->dm[m].sell_rows = nr;
     }
     BSP_LAUNCH_CHECK();
     P->dm[m].sell_ptr = dptr;
-    P->dm[m].sell_off = off;
-    // the copy sees the sync below: host vectors stay alive until then
+    P->dm[m].sell_val = v;
   }
+  // host vectors (slice pointers, permutations) stay alive until this sync
   std::vector<int32_t> hbad(count, 0);
   BSP_CUDA(cudaMemcpyAsync(hbad.data(), bad, sizeof(int32_t) * count, cudaMemcpyDeviceToHost, s));
   BSP_CUDA(cudaStreamSynchronize(s));
@@ -717,7 +846,7 @@ bsp_status build_sell(bsp_batch_plan P, cudaStream_t s) {
 // The row-statistics choice: SELL-32 for every qualifying matrix (rows even
 // enough that padding adds at most 1/8: every access coalesced and no
 // row-pointer round trip, against CSR's per-row dependent loads).
-int32_t model_format(const bsp_batch_plan P, int32_t m) { return P->sell_ok[m] ? 1 : 0; }
+int32_t model_format(const bsp_batch_plan P, int32_t m) { return P->sell_ok[m]; }
 }  // namespace
 
 extern "C" bsp_status bsp_batch_create(int32_t count, const bsp_batch_mat *mats, bsp_dtype dtype, int32_t nrhs,
@@ -779,7 +908,7 @@ extern "C" bsp_status bsp_batch_create(int32_t count, const bsp_batch_mat *mats,
   P->dm.resize(count);
   for (int32_t m = 0; m < count; ++m)
     P->dm[m] = {mats[m].rowPtr, mats[m].colIdx, mats[m].values, mats[m].x, mats[m].y, mats[m].rows, mats[m].cols,
-                nullptr, nullptr, nullptr};
+                nullptr, nullptr, nullptr, nullptr, nullptr, 0};
   bsp_status st = build_sell(P, s);
   if (st != BSP_OK) return fail(st);
   P->fmt.assign(count, 0);
@@ -801,7 +930,7 @@ extern "C" bsp_status bsp_batch_create(int32_t count, const bsp_batch_mat *mats,
     // matrix per launch, SELL lost to CSR on most banded matrices, yet the
     // batched launch with every qualifying matrix in SELL was the fastest
     // (512-matrix batch, FP64: 201.3 us against 213.9 with the per-matrix
-    // choice and 228.1 all CSR).
+    // choice and 227.7 all CSR).
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
@@ -884,7 +1013,7 @@ extern "C" bsp_status bsp_batch_set_vectors(bsp_batch_plan P, int32_t m, const v
 extern "C" bsp_status bsp_batch_lanes(bsp_batch_plan P, int32_t *lanes) {
   clear_error();
   BSP_CHECK_ARG(P && lanes, "null pointer");
-  for (int32_t m = 0; m < P->count; ++m) lanes[m] = P->fmt[m] == 1 ? 0 : P->lanes[m];
+  for (int32_t m = 0; m < P->count; ++m) lanes[m] = P->fmt[m] != 0 ? 0 : P->lanes[m];
   return BSP_OK;
 }
 

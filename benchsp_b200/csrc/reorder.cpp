@@ -343,13 +343,12 @@ int64_t count_tiles(int32_t n, const int32_t *rp, const int32_t *ci, const int32
 }
 
 // SpMM engine cost model, seconds per unit per column of B, from the B200
-// measurements of the SMaT and grouped CSR SpMM at N = 128 (dense-tile and
-// row-shuffled 524,288-row matrices, power-law graph): tcgen05 tiles cost
-// 0.86-0.91 ns per tile (7.0e-12 s per tile-column; the tensor-core path
-// now takes every N, so mma.sync tiles, 1.6x that, are not modelled), the
-// grouped CSR kernel 1.93 ms for 67.1M nonzeros (2.3e-13 s per
-// nonzero-column).
-constexpr double kTileColSecTc = 7.0e-12;
+// measurements of the SMaT and CSR SpMM at N = 128 (dense-tile and
+// row-shuffled 524,288-row matrices, power-law graph): the persistent
+// tcgen05 kernel 163 us for 262,144 tiles at N = 128 (4.9e-12 s per
+// tile-column, 64-column slabs below N = 128), the grouped CSR kernel
+// 1.93 ms for 67.1M nonzeros (2.3e-13 s per nonzero-column).
+constexpr double kTileColSecTc = 4.9e-12;
 constexpr double kNnzColSecCsr = 2.3e-13;
 
 bool valid_csr(int32_t n, int32_t nnz, const int32_t *rp) {

@@ -1076,14 +1076,13 @@ extern "C" bsp_status bsp_smat_free(bsp_smat *m) {
   return BSP_OK;
 }
 
-// Slab width of the tcgen05 path: 128 columns per CTA when N >= 128 and a
-// 128-column slab of B (cols x 128) fits in 60% of L2, else 64 (the CTAs of
-// a slab run together, blockIdx.x fastest, so a slab is what L2 must hold).
+// Slab width of the one-CTA-per-block-row tcgen05 kernel when none is given:
+// 128 columns per CTA for N >= 128, else 64.  Keeping a slab of B within L2
+// by taking 64 columns at N >= 128 measured slower (N = 128: 431 vs 233 us):
+// twice the CTAs, each paying its set-up.
 static int tc_slab_width(int32_t N, int32_t cols) {
-  int dev = 0, l2 = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev) != cudaSuccess)
-    l2 = 126 << 20;
-  return (N >= 128 && (double)cols * 128 * 2 <= 0.6 * (double)l2) ? 128 : 64;
+  (void)cols;
+  return N >= 128 ? 128 : 64;
 }
 
 // Resident CTAs per SM for the persistent kernel: 8 (the register and
@@ -1160,7 +1159,12 @@ extern "C" bsp_status bsp_smat_spmm_path(const bsp_smat *m, const void *B, int32
   if (path == BSP_SMAT_TCGEN05_PERSISTENT_W64) return smat_spmm_tcp(m, B, N, ldb, C, ldc, alpha, beta, 64, s);
   if (path == BSP_SMAT_TCGEN05_W64) return smat_spmm_tc(m, B, N, ldb, C, ldc, alpha, beta, 64, s);
   if (path == BSP_SMAT_TCGEN05_W128) return smat_spmm_tc(m, B, N, ldb, C, ldc, alpha, beta, 128, s);
-  if (path == BSP_SMAT_TCGEN05 || path == BSP_SMAT_AUTO) return smat_spmm_tc(m, B, N, ldb, C, ldc, alpha, beta, 0, s);
+  // default tensor-core path: the persistent kernel (dense 16x16 tiles, 8 per
+  // block row, 524,288 rows: N = 32 / 64 / 128 / 256 in 114 / 116 / 163 / 328
+  // us, against 215 / 220 / 233 / 461 us with a CTA per block row and
+  // 156 / 195 / 370 / 739 us on mma.sync)
+  if (path == BSP_SMAT_TCGEN05 || path == BSP_SMAT_AUTO)
+    return smat_spmm_tcp(m, B, N, ldb, C, ldc, alpha, beta, N >= 128 ? 128 : 64, s);
   const int nt = (N % 64 == 0) ? 8 : 4;
   const int64_t items = (int64_t)m->tiles.rowRegions * (N / (8 * nt));
   int64_t blocks = ceil_div(items, kWarpsPerCta);

@@ -494,18 +494,18 @@ bsp_status bsp_smat_create(int32_t rows, int32_t cols, int32_t nnz,
                            bsp_stream_t stream);
 bsp_status bsp_smat_free(bsp_smat *m);
 /* B: dtype of the matrix, 16-byte aligned, ldb % 8 == 0; N % 32 == 0.
- * Runs on the tcgen05 tensor cores (TMEM accumulator, TMA staging of B) in
- * slabs of 128 or 64 C columns per CTA (64 when a 128-column slab of B would
- * not stay in L2, or N < 128); bsp_smat_spmm_path can ask for mma.sync. */
+ * Runs on the tcgen05 tensor cores (TMEM accumulators, TMA staging of B):
+ * resident CTAs walk every (block row, slab of 128 C columns, or 64 when
+ * N < 128); bsp_smat_spmm_path can ask for the other kernels. */
 bsp_status bsp_smat_spmm(const bsp_smat *m, const void *B, int32_t N,
                          int64_t ldb, float *C, int64_t ldc, float alpha,
                          float beta, bsp_stream_t stream);
 typedef enum {
   BSP_SMAT_AUTO = 0,
   BSP_SMAT_MMA_SYNC = 1, /* warp mma.sync.m16n8k16, FP32 accumulators in registers */
-  BSP_SMAT_TCGEN05 = 2,  /* tcgen05.mma M=128 N=16 K=16 per tile, slab width chosen from L2 */
-  BSP_SMAT_TCGEN05_W64 = 3,  /* tcgen05, 64 C columns per CTA */
-  BSP_SMAT_TCGEN05_W128 = 4, /* tcgen05, 128 C columns per CTA */
+  BSP_SMAT_TCGEN05 = 2,  /* tcgen05.mma M=128 N=16 K=16 per tile: the persistent kernel (5) */
+  BSP_SMAT_TCGEN05_W64 = 3,  /* tcgen05, one CTA per block row, 64 C columns per CTA */
+  BSP_SMAT_TCGEN05_W128 = 4, /* tcgen05, one CTA per block row, 128 C columns per CTA */
   BSP_SMAT_TCGEN05_PERSISTENT = 5, /* tcgen05, resident CTAs walking every block row: a producer
                                      warp, an MMA warp and four epilogue warps, two TMEM
                                      accumulators so one block row's read-out overlaps the
@@ -764,13 +764,18 @@ bsp_status bsp_spmv_plan_destroy(bsp_spmv_plan plan);
  * row-major rows x 8 / cols x 8 blocks.
  *
  * Per matrix the plan also picks the storage: CSR as given, or a SELL-32
- * copy it builds (slices of 32 consecutive rows padded to the slice's
- * longest row, entry k of row l at slice_start + 32k + l, values in the
- * batch's type and 16-bit column offsets from the row), which a warp reads
- * one slice at a time with every access coalesced.  A matrix takes SELL when
- * padding adds at most 1/8 to its entries, it has no row longer than
- * long_row_nnz and every |column - row| < 32768; the others stay CSR, where
- * tune = 1 times the lane counts per matrix. */
+ * copy it builds (slices of 32 rows padded to the slice's longest row, entry
+ * k of slice row l at slice_start + 32k + l, values in the batch's type),
+ * which a warp reads one slice at a time with every access coalesced.
+ * Narrow form (the default): the rows in order with 16-bit column offsets
+ * from the row, for matrices whose padding adds at most 1/8, with no row
+ * longer than long_row_nnz and every |column - row| < 32768.  Wide form
+ * (opt-in, sell_wide = 1): the rows of at most T entries sorted by length,
+ * 32-bit columns and a row permutation, T the largest power of two at which
+ * padding adds at most 1/8, rows above T as whole-warp segments; it measured
+ * slower than CSR on power-law rows (512-matrix batch, Zipf half: 534 vs 107
+ * us), so it is off by default.  SELL matrices are chosen by these rules;
+ * for the CSR ones tune = 1 times the lane counts per matrix. */
 typedef struct {
   int32_t rows, cols, nnz;
   const int32_t *rowPtr; /* device */
@@ -786,7 +791,8 @@ typedef struct {
   int32_t long_row_nnz; /* rows above this are split (default 2048) */
   int32_t item_nnz;     /* target nonzeros per row item, 0 = automatic */
   int32_t use_graph;    /* capture the launch in a CUDA graph (default 1) */
-  int32_t sell;         /* 1: the tuner may store matrices as SELL-32 (default 1) */
+  int32_t sell;         /* 1: store qualifying matrices as SELL-32 (default 1) */
+  int32_t sell_wide;    /* 1: also the wide (length-sorted) SELL-32 form (default 0) */
 } bsp_batch_options;
 
 typedef struct bsp_batch_plan_s *bsp_batch_plan;
@@ -807,7 +813,7 @@ bsp_status bsp_batch_set_vectors(bsp_batch_plan plan, int32_t m, const void *x,
 /* Per-matrix choice of the tuner: lanes per row (1..32) for CSR matrices,
  * 0 for matrices stored as SELL-32. */
 bsp_status bsp_batch_lanes(bsp_batch_plan plan, int32_t *lanes /* count */);
-/* Per-matrix storage: 0 = CSR, 1 = SELL-32. */
+/* Per-matrix storage: 0 = CSR, 1 = SELL-32 narrow form, 2 = SELL-32 wide form. */
 bsp_status bsp_batch_formats(bsp_batch_plan plan, int32_t *formats /* count */);
 bsp_status bsp_batch_stats(bsp_batch_plan plan, int64_t *items,
                            int64_t *long_segments, int64_t *total_nnz);

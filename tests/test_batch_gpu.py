@@ -205,3 +205,24 @@ def test_batch_sell_format_choice_and_results(cuda, dtype, nrhs):
     _check(mats, dev, host, dtype, nrhs)
     for X in (P, Q, T):
         X.close()
+
+
+@pytest.mark.parametrize("nrhs", [1, 8])
+def test_batch_wide_sell_form(cuda, nrhs):
+    """The opt-in wide SELL-32 form: the power-law matrix and the banded one
+    with empty rows (both uneven in row order) are stored as length-sorted
+    SELL-32 with their longest rows as whole-warp segments; results within
+    the bound and identical between the batched and the separate launches."""
+    import torch
+    mats = _sell_batch(90 + nrhs)
+    dev, host = _upload(cuda, mats, "f64", nrhs, 13)
+    P = bsp.BatchPlan(dev, nrhs=nrhs, long_row_nnz=1024, seg_nnz=256, sell_wide=True)
+    assert P.formats().tolist() == [1, 1, 1, 1, 1, 0, 2, 2]
+    P.run()
+    torch.cuda.synchronize()
+    _check(mats, dev, host, "f64", nrhs)
+    first = [d[4].clone() for d in dev]
+    P.run_separate()
+    for a, d in zip(first, dev):
+        assert torch.equal(a, d[4])
+    P.close()
