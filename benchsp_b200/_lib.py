@@ -344,3 +344,22 @@ _PROTOS.update({
     "bsp_bsr_scaled_spmv_variant": (C.c_int, [C.POINTER(BspBsrScaled), _P, _I32, _P, _I32, _D, _D, _I32, _I32,
                                               _P]),
 })
+
+
+class BspGtile(C.Structure):
+    """Mirror of bsp_gtile (include/bsp.h): gathered-tile SpMM matrix."""
+    _fields_ = [("rows", C.c_int32), ("cols", C.c_int32), ("nnz", C.c_int32), ("dtype", C.c_int32),
+                ("nchunks", C.c_int64), ("ngroups", C.c_int32), ("npieces", C.c_int32), ("nsplit", C.c_int32),
+                ("nslots", C.c_int32), ("piece_ptr", C.c_void_p), ("piece_group", C.c_void_p),
+                ("piece_slot", C.c_void_p), ("group_piece", C.c_void_p), ("split_groups", C.c_void_p),
+                ("chunk_cols", C.c_void_p), ("chunk_tiles", C.c_void_p), ("err", C.c_void_p)]
+
+
+_PROTOS.update({
+    "bsp_gtile_create_host": (C.c_int, [_I32, _I32, _I32, _P, _P, _P, C.c_int, C.POINTER(BspGtile)]),
+    "bsp_gtile_workspace": (C.c_size_t, [C.POINTER(BspGtile), _I32]),
+    "bsp_gtile_spmm": (C.c_int, [C.POINTER(BspGtile), _P, _I32, _I64, _P, _I64, C.c_float, C.c_float, _P,
+                                 C.c_size_t, _P]),
+    "bsp_gtile_check": (C.c_int, [C.POINTER(BspGtile), _P]),
+    "bsp_gtile_free": (C.c_int, [C.POINTER(BspGtile)]),
+})

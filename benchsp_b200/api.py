@@ -776,6 +776,65 @@ class SmatMatrix:
             pass
 
 
+class GatherTileMatrix:
+    """Gathered-tile tensor-core SpMM matrix (bsp_gtile) built from host CSR
+    arrays: each 16-row group's distinct columns in chunks of 16 with their
+    16x16 tiles; C = alpha*A*B + beta*C on tcgen05 with the chunk's B rows
+    gathered into shared memory."""
+
+    def __init__(self, A: "HostCSR", dtype: str = "f16"):
+        self._d = _lib.BspGtile()
+        dt = {"f16": _lib.F16, "bf16": _lib.BF16}[dtype]
+        rp = np.ascontiguousarray(A.rowptr, np.int32)
+        ci = np.ascontiguousarray(A.colidx, np.int32)
+        va = np.ascontiguousarray(A.values, np.float64)
+        check(lib().bsp_gtile_create_host(A.rows, A.cols, ci.size, _np_ptr(rp), _np_ptr(ci), _np_ptr(va), dt,
+                                          C.byref(self._d)))
+        self._live = True
+        self._ws = None
+
+    def __getattr__(self, name):
+        d = self.__dict__.get("_d")
+        if d is not None and name in dict(_lib.BspGtile._fields_):
+            return getattr(d, name)
+        raise AttributeError(name)
+
+    def chunks_per_group(self) -> np.ndarray:
+        d = self._d
+        pp = _d2h(d.piece_ptr, d.npieces + 1, np.int32)
+        gp = _d2h(d.group_piece, d.ngroups + 1, np.int32)
+        return (pp[gp[1:]] - pp[gp[:-1]]).astype(np.int64)
+
+    def spmm(self, B, C_out=None, *, alpha: float = 1.0, beta: float = 0.0, stream=None):
+        torch = _torch()
+        N = B.shape[1]
+        if C_out is None:
+            C_out = torch.empty(self._d.rows, N, dtype=torch.float32, device=B.device)
+            beta = 0.0
+        need = lib().bsp_gtile_workspace(C.byref(self._d), N)
+        if need and (self._ws is None or self._ws.numel() < need):
+            self._ws = torch.empty(need, dtype=torch.uint8, device=B.device)
+        ws = self._ws if need else None
+        check(lib().bsp_gtile_spmm(C.byref(self._d), _dptr(B, "B"), N, B.stride(0), _dptr(C_out, "C"),
+                                   C_out.stride(0), float(alpha), float(beta),
+                                   ws.data_ptr() if ws is not None else None, need, _stream(stream)))
+        return C_out
+
+    def check(self, stream=None) -> None:
+        check(lib().bsp_gtile_check(C.byref(self._d), _stream(stream)))
+
+    def free(self) -> None:
+        if self._live:
+            self._live = False
+            check(lib().bsp_gtile_free(C.byref(self._d)))
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
 def C_byref(obj):
     return C.byref(obj)
 

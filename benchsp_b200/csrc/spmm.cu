@@ -22,7 +22,11 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include <algorithm>
 #include <mutex>
+#include <type_traits>
+#include <utility>
+#include <vector>
 
 #include "bsp_internal.cuh"
 #include "util.cuh"
@@ -849,6 +853,239 @@ __global__ void __launch_bounds__(kTcpThreads) spmm_tcp_kernel(const __grid_cons
   if (warp == 1)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)kTcTmemCols)
                  : "memory");
+}
+
+// ---------------------------------------------------------------------------
+// Gathered-tile tensor-core SpMM (bsp_gtile): for matrices whose nonzeros
+// scatter over all columns (graph adjacency), 16x16 tiles of the matrix as
+// given are almost empty.  Here every 16-row group's distinct columns are
+// compacted: chunk c of a group holds 16 of them (chunk_cols) and the 16x16
+// tile of the group's values in those columns (chunk_tiles, the K-major core
+// layout of tile_pos).  The product of a chunk is D (C columns x 16 rows) +=
+// Bg^T x tile^T, Bg = the 16 gathered B rows: the same tcgen05.mma as the
+// block kernel, with the B rows gathered by the producer warp (cp.async, 16
+// bytes per lane and copy, written in the 128-byte swizzled layout the TMA
+// would produce) instead of one TMA box.  Structure as spmm_tcp_kernel:
+// resident CTAs walk (piece, slab) items, a piece being a run of up to
+// kGtPieceChunks chunks of one group; groups with several pieces write
+// partial rows, summed in piece order by gtile_reduce_kernel.
+constexpr int kGtPieceChunks = 64;
+
+__device__ __forceinline__ void cp_async16(void *dst, const void *src, bool valid) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src),
+               "r"(valid ? 16 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_arrive_noinc(uint64_t *bar) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kTcpThreads) spmm_gtc_kernel(
+    int32_t M, int32_t N, int32_t W, int32_t npieces, const int32_t *__restrict__ piece_ptr,
+    const int32_t *__restrict__ piece_group, const int32_t *__restrict__ piece_slot,
+    const int32_t *__restrict__ chunk_cols, const T *__restrict__ tiles, const T *__restrict__ B, int64_t ldb,
+    float *__restrict__ C, int64_t ldc, float *__restrict__ part, float alpha, float beta,
+    int32_t *__restrict__ err) {
+  extern __shared__ unsigned char smem_raw[];
+  const uint32_t raw = smem_u32(smem_raw);
+  unsigned char *sm = smem_raw + ((1024u - (raw & 1023u)) & 1023u);
+  unsigned char *bslab = sm;
+  unsigned char *atile = sm + kTcStages * kTcBBytes;
+  uint64_t *full = reinterpret_cast<uint64_t *>(atile + kTcStages * kTcABytes);
+  uint64_t *empty = full + kTcStages;
+  uint64_t *done = empty + kTcStages;   // [2]
+  uint64_t *accfree = done + 2;         // [2]
+  uint64_t *drain = accfree + 2;
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nslab = (N + W - 1) / W;
+  const int64_t total = (int64_t)npieces * nslab;
+
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < kTcStages; ++i) {
+      mbar_init(&full[i], 33);   // 32 cp.async arrivals + the tile copy's expect_tx
+      mbar_init(&empty[i], 1);
+    }
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(&done[i], 1);
+      mbar_init(&accfree[i], 4);
+    }
+    mbar_init(drain, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"((uint32_t)kTcTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0) {
+    // ---- producer warp: gathers 16 B rows per chunk, lane 0 copies the tile
+    const int cpr = W / 8;   // 16-byte pieces per gathered row
+    int64_t it = 0;
+    bool ok = true;
+    for (int64_t w = blockIdx.x; w < total && ok; w += gridDim.x) {
+      const int32_t p = (int32_t)(w % npieces);
+      const int32_t n0 = (int32_t)(w / npieces) * W;
+      const int32_t c0 = piece_ptr[p], c1 = piece_ptr[p + 1];
+      for (int32_t c = c0; c < c1; ++c, ++it) {
+        const int st = (int)(it % kTcStages);
+        int good = 1;
+        if (lane == 0 && it >= kTcStages)
+          good = tcp_wait(&empty[st], (unsigned)((it / kTcStages - 1) & 1), abort_flag) ? 1 : 0;
+        good = __shfl_sync(0xffffffffu, good, 0);
+        if (!good) {
+          ok = false;
+          break;
+        }
+        const int32_t col_l = lane < 16 ? chunk_cols[(int64_t)c * 16 + lane] : 0;
+        unsigned char *dst0 = bslab + st * kTcBBytes;
+        for (int q = lane; q < 16 * cpr; q += 32) {   // same trip count on every lane
+          const int k = q / cpr, j = q % cpr;
+          const int32_t brow = __shfl_sync(0xffffffffu, col_l, k);
+          const int32_t cc = n0 + j * 8;
+          const bool valid = cc < N;
+          const T *src = valid ? B + (int64_t)brow * ldb + cc : B;
+          unsigned char *dst = dst0 + (j >> 3) * 2048 + k * 128 + (((j & 7) ^ (k & 7)) << 4);
+          cp_async16(dst, src, valid);
+        }
+        if (lane == 0) {
+          mbar_expect_tx(&full[st], kTcABytes);
+          bulk_g2s(atile + st * kTcABytes, tiles + (int64_t)c * kTS * kTS, kTcABytes, &full[st]);
+        }
+        cp_async_arrive_noinc(&full[st]);
+      }
+    }
+    if (!ok) {
+      if (lane == 0) {
+        for (int64_t j = it > kTcStages ? it - kTcStages : 0; j < it; ++j)
+          (void)mbar_wait(&full[j % kTcStages], (unsigned)((j / kTcStages) & 1));
+        atomicExch(err, 1);
+      }
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+  } else if (warp == 1 && lane == 0) {
+    // ---- MMA issuer
+    constexpr uint32_t fmt = std::is_same<T, __nv_bfloat16>::value ? 1u : 0u;
+    constexpr uint32_t idesc = (1u << 4) | (fmt << 7) | (fmt << 10) | (1u << 15) | ((16u >> 3) << 17) |
+                               ((uint32_t)(kTcSlab >> 4) << 24);
+    int64_t it = 0, j = 0;
+    bool ok = true;
+    for (int64_t w = blockIdx.x; w < total && ok; w += gridDim.x, ++j) {
+      const int32_t p = (int32_t)(w % npieces);
+      const int32_t nk = piece_ptr[p + 1] - piece_ptr[p];
+      const int buf = (int)(j & 1);
+      if (j >= 2 && !tcp_wait(&accfree[buf], (unsigned)((j / 2 - 1) & 1), abort_flag)) {
+        ok = false;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      for (int32_t i = 0; i < nk; ++i, ++it) {
+        const int st = (int)(it % kTcStages);
+        if (!tcp_wait(&full[st], (unsigned)((it / kTcStages) & 1), abort_flag)) {
+          ok = false;
+          break;
+        }
+        // the gathered rows were written through the generic proxy (cp.async)
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        const uint64_t adesc = umma_smem_desc(smem_u32(bslab + st * kTcBBytes), 2048u, 1024u, 2u);
+        const uint64_t bdesc = umma_smem_desc(smem_u32(atile + st * kTcABytes), 128u, 256u, 0u);
+        umma_f16(tmem + 16u * (uint32_t)buf, adesc, bdesc, idesc, i > 0 ? 1u : 0u);
+        umma_commit(&empty[st]);
+      }
+      umma_commit(&done[buf]);
+    }
+    umma_commit(drain);
+    if (!mbar_wait(drain, 0u)) ok = false;
+    if (!ok) atomicExch(err, 1);
+  } else if (warp >= 2) {
+    // ---- epilogue
+    const int q = warp & 3;
+    int64_t j = 0;
+    for (int64_t w = blockIdx.x; w < total; w += gridDim.x, ++j) {
+      const int32_t p = (int32_t)(w % npieces);
+      const int32_t n0 = (int32_t)(w / npieces) * W;
+      const int32_t nk = piece_ptr[p + 1] - piece_ptr[p];
+      const int32_t g = piece_group[p], slot = piece_slot[p];
+      const int buf = (int)(j & 1);
+      if (!tcp_wait(&done[buf], (unsigned)((j / 2) & 1), abort_flag)) {
+        atomicExch(err, 1);
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      float v[16];
+#pragma unroll
+      for (int r = 0; r < 16; ++r) v[r] = 0.f;
+      if (nk > 0) {
+        uint32_t r[16];
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+            "%14, %15}, [%16];"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+              "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+            : "r"(tmem + ((uint32_t)(q * 32) << 16) + 16u * (uint32_t)buf));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+        for (int c = 0; c < 16; ++c) v[c] = __uint_as_float(r[c]);
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&accfree[buf]);
+      const int64_t col = (int64_t)n0 + q * 32 + lane;
+      if (q * 32 < W && col < N) {
+#pragma unroll
+        for (int r = 0; r < 16; ++r) {
+          const int64_t row = (int64_t)g * kTS + r;
+          if (row >= M) continue;
+          if (slot >= 0) {
+            part[((int64_t)slot * kTS + r) * N + col] = v[r];
+          } else {
+            float *cp = C + row * ldc + col;
+            float o = alpha * v[r];
+            if (beta != 0.f) o += beta * *cp;
+            *cp = o;
+          }
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 1)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)kTcTmemCols)
+                 : "memory");
+}
+
+// C rows of the groups split into several pieces: alpha * (sum of the
+// pieces' partial rows, in piece order) + beta * C.  Thread per (row, column).
+__global__ void gtile_reduce_kernel(int32_t nsplit, const int32_t *__restrict__ split_groups,
+                                    const int32_t *__restrict__ group_piece, const int32_t *__restrict__ piece_slot,
+                                    int32_t M, int32_t N, const float *__restrict__ part, float *__restrict__ C,
+                                    int64_t ldc, float alpha, float beta) {
+  const int64_t total = (int64_t)nsplit * kTS * N;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t col = (int32_t)(i % N);
+    const int32_t r = (int32_t)((i / N) % kTS);
+    const int32_t g = split_groups[i / ((int64_t)N * kTS)];
+    const int64_t row = (int64_t)g * kTS + r;
+    if (row >= M) continue;
+    float acc = 0.f;
+    for (int32_t p = group_piece[g]; p < group_piece[g + 1]; ++p)
+      acc += part[((int64_t)piece_slot[p] * kTS + r) * N + col];
+    float *cp = C + row * ldc + col;
+    float o = alpha * acc;
+    if (beta != 0.f) o += beta * *cp;
+    *cp = o;
+  }
 }
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link
@@ -1796,3 +2033,187 @@ static bsp_status spmm_planned_impl(const bsp_spmm_plan *p, int32_t cols, int32_
   return BSP_OK;
 }
 }  // namespace bsp
+
+// ---------------------------------------------------------------------------
+// Gathered-tile matrix (bsp_gtile): built on the host from host CSR arrays.
+namespace bsp {
+template <typename T>
+static T host_cvt(double v);
+template <> __half host_cvt<__half>(double v) { return __double2half(v); }
+template <> __nv_bfloat16 host_cvt<__nv_bfloat16>(double v) { return __float2bfloat16_rn((float)v); }
+
+template <typename T>
+static bsp_status gtile_build(int32_t rows, int32_t cols, int32_t nnz, const int32_t *rp, const int32_t *ci,
+                              const double *val, bsp_gtile *g) {
+  const int32_t ng = (rows + kTS - 1) / kTS;
+  std::vector<int64_t> nch(ng + 1, 0);
+  std::vector<std::vector<std::pair<int32_t, int32_t>>> ent(ng);   // (column, entry index) per group
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int32_t gi = 0; gi < ng; ++gi) {
+    auto &e = ent[gi];
+    const int32_t r0 = gi * kTS, r1 = std::min(rows, r0 + kTS);
+    e.reserve(rp[r1] - rp[r0]);
+    for (int32_t k = rp[r0]; k < rp[r1]; ++k) e.push_back({ci[k], k});
+    std::stable_sort(e.begin(), e.end(), [](const std::pair<int32_t, int32_t> &a, const std::pair<int32_t, int32_t> &b) {
+      return a.first < b.first;
+    });
+    int64_t d = 0;
+    for (size_t i = 0; i < e.size(); ++i)
+      if (i == 0 || e[i].first != e[i - 1].first) ++d;
+    nch[gi + 1] = (d + kTS - 1) / kTS;
+  }
+  for (int32_t gi = 0; gi < ng; ++gi) nch[gi + 1] += nch[gi];
+  const int64_t nchunks = nch[ng];
+  if (nchunks > INT32_MAX / 256) BSP_FAIL(BSP_ERR_UNSUPPORTED, "gathered tiles: too many chunks for int32 indexing");
+  std::vector<int32_t> hcols((size_t)nchunks * kTS, 0);
+  std::vector<T> htiles((size_t)nchunks * kTS * kTS, host_cvt<T>(0.0));
+  // row of each entry: walk the group's rows
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int32_t gi = 0; gi < ng; ++gi) {
+    const auto &e = ent[gi];
+    const int32_t r0 = gi * kTS;
+    int64_t s = -1;
+    for (size_t i = 0; i < e.size(); ++i) {
+      if (i == 0 || e[i].first != e[i - 1].first) {
+        ++s;
+        hcols[(size_t)((nch[gi] + s / kTS) * kTS + s % kTS)] = e[i].first;
+      }
+      const int32_t k = e[i].second;
+      // the entry's row: the last row of the group whose start is <= k
+      int32_t r = r0;
+      while (r + 1 < std::min(rows, r0 + kTS) && rp[r + 1] <= k) ++r;
+      const int64_t chunk = nch[gi] + s / kTS;
+      htiles[(size_t)chunk * kTS * kTS + tile_pos(r - r0, (int)(s % kTS))] = host_cvt<T>(val[k]);
+    }
+  }
+  // pieces of up to kGtPieceChunks chunks; groups with several get partial slots
+  std::vector<int32_t> pptr{0}, pgroup, pslot, gpiece(ng + 1, 0), split;
+  int32_t slots = 0;
+  for (int32_t gi = 0; gi < ng; ++gi) {
+    const int64_t c0 = nch[gi], c1 = nch[gi + 1];
+    const int64_t np = std::max<int64_t>(1, (c1 - c0 + kGtPieceChunks - 1) / kGtPieceChunks);
+    if (np > 1) split.push_back(gi);
+    for (int64_t p = 0; p < np; ++p) {
+      pptr.push_back((int32_t)std::min(c1, c0 + (p + 1) * kGtPieceChunks));
+      pgroup.push_back(gi);
+      pslot.push_back(np > 1 ? slots++ : -1);
+    }
+    gpiece[gi + 1] = (int32_t)pgroup.size();
+  }
+  bsp_gtile o{};
+  o.rows = rows;
+  o.cols = cols;
+  o.nnz = nnz;
+  o.dtype = std::is_same<T, __half>::value ? BSP_F16 : BSP_BF16;
+  o.nchunks = nchunks;
+  o.ngroups = ng;
+  o.npieces = (int32_t)pgroup.size();
+  o.nsplit = (int32_t)split.size();
+  o.nslots = slots;
+  cudaStream_t s = 0;
+  auto up = [&](auto **dst, const auto &v) -> bsp_status {
+    using E = typename std::remove_reference<decltype(v)>::type::value_type;
+    E *p = nullptr;
+    BSP_TRY(dalloc(&p, std::max<size_t>(1, v.size()), s));
+    if (!v.empty()) BSP_CUDA(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(E), cudaMemcpyHostToDevice, s));
+    *dst = reinterpret_cast<typename std::remove_pointer<decltype(dst)>::type>(p);
+    return BSP_OK;
+  };
+  bsp_status st = up(&o.piece_ptr, pptr);
+  if (st == BSP_OK) st = up(&o.piece_group, pgroup);
+  if (st == BSP_OK) st = up(&o.piece_slot, pslot);
+  if (st == BSP_OK) st = up(&o.group_piece, gpiece);
+  if (st == BSP_OK) st = up(&o.split_groups, split);
+  if (st == BSP_OK) st = up(&o.chunk_cols, hcols);
+  T *tiles = nullptr;
+  if (st == BSP_OK) st = up(&tiles, htiles);
+  o.chunk_tiles = tiles;
+  if (st == BSP_OK) st = dalloc(&o.err, 1, s);
+  if (st == BSP_OK && cudaMemsetAsync(o.err, 0, sizeof(int32_t), s) != cudaSuccess) st = BSP_ERR_CUDA;
+  if (st == BSP_OK && cudaStreamSynchronize(s) != cudaSuccess) st = BSP_ERR_CUDA;   // host vectors go away
+  *g = o;
+  return st;
+}
+}  // namespace bsp
+
+extern "C" bsp_status bsp_gtile_free(bsp_gtile *g) {
+  clear_error();
+  if (!g) return BSP_OK;
+  cudaStream_t s = 0;
+  dfree(g->piece_ptr, s);
+  dfree(g->piece_group, s);
+  dfree(g->piece_slot, s);
+  dfree(g->group_piece, s);
+  dfree(g->split_groups, s);
+  dfree(g->chunk_cols, s);
+  if (g->chunk_tiles) cudaFreeAsync(g->chunk_tiles, s);
+  g->chunk_tiles = nullptr;
+  dfree(g->err, s);
+  BSP_CUDA(cudaStreamSynchronize(s));
+  return BSP_OK;
+}
+
+extern "C" bsp_status bsp_gtile_create_host(int32_t rows, int32_t cols, int32_t nnz, const int32_t *rowPtr,
+                                            const int32_t *colIdx, const double *values, bsp_dtype dtype,
+                                            bsp_gtile *out) {
+  clear_error();
+  BSP_CHECK_ARG(out && rowPtr && rows >= 0 && cols >= 0 && nnz >= 0, "bad argument");
+  BSP_CHECK_ARG(nnz == 0 || (colIdx && values), "null pointer");
+  BSP_CHECK_ARG(dtype == BSP_F16 || dtype == BSP_BF16, "gathered tiles are F16 or BF16");
+  BSP_CHECK_ARG(rowPtr[0] == 0 && rowPtr[rows] == nnz, "rowPtr[0] must be 0 and rowPtr[rows] == nnz");
+  *out = bsp_gtile{};
+  bsp_status st = dtype == BSP_F16 ? gtile_build<__half>(rows, cols, nnz, rowPtr, colIdx, values, out)
+                                   : gtile_build<__nv_bfloat16>(rows, cols, nnz, rowPtr, colIdx, values, out);
+  if (st != BSP_OK) bsp_gtile_free(out);
+  return st;
+}
+
+extern "C" size_t bsp_gtile_workspace(const bsp_gtile *g, int32_t N) {
+  return g ? (size_t)g->nslots * kTS * (size_t)(N > 0 ? N : 0) * sizeof(float) : 0;
+}
+
+extern "C" bsp_status bsp_gtile_spmm(const bsp_gtile *g, const void *B, int32_t N, int64_t ldb, float *C,
+                                     int64_t ldc, float alpha, float beta, void *workspace, size_t workspace_bytes,
+                                     bsp_stream_t stream) {
+  clear_error();
+  BSP_CHECK_ARG(g && B && C, "null pointer");
+  BSP_CHECK_ARG(N > 0 && N % 8 == 0, "N must be a positive multiple of 8");
+  BSP_CHECK_ARG(ldb >= N && ldc >= N, "leading dimension smaller than N");
+  BSP_CHECK_ARG((uintptr_t)B % 16 == 0 && (ldb * 2) % 16 == 0, "B must be 16-byte aligned with ldb % 8 == 0");
+  const size_t need = bsp_gtile_workspace(g, N);
+  BSP_CHECK_ARG(workspace_bytes >= need && (need == 0 || workspace), "workspace too small");
+  if (g->ngroups == 0) return BSP_OK;
+  cudaStream_t s = as_stream(stream);
+  const int32_t W = N >= 128 ? 128 : 64;
+  const int64_t total = (int64_t)g->npieces * ceil_div(N, W);
+  const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(total, (int64_t)sm_count() * 8));
+  float *part = static_cast<float *>(workspace);
+  if (g->dtype == BSP_F16)
+    spmm_gtc_kernel<__half><<<grid, kTcpThreads, kTcpSmem, s>>>(
+        g->rows, N, W, g->npieces, g->piece_ptr, g->piece_group, g->piece_slot, g->chunk_cols,
+        (const __half *)g->chunk_tiles, (const __half *)B, ldb, C, ldc, part, alpha, beta, g->err);
+  else
+    spmm_gtc_kernel<__nv_bfloat16><<<grid, kTcpThreads, kTcpSmem, s>>>(
+        g->rows, N, W, g->npieces, g->piece_ptr, g->piece_group, g->piece_slot, g->chunk_cols,
+        (const __nv_bfloat16 *)g->chunk_tiles, (const __nv_bfloat16 *)B, ldb, C, ldc, part, alpha, beta, g->err);
+  BSP_LAUNCH_CHECK();
+  if (g->nsplit > 0) {
+    const int64_t work = (int64_t)g->nsplit * kTS * N;
+    const unsigned rg = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div(work, 256), (int64_t)sm_count() * 16));
+    gtile_reduce_kernel<<<rg, 256, 0, s>>>(g->nsplit, g->split_groups, g->group_piece, g->piece_slot, g->rows, N,
+                                           part, C, ldc, alpha, beta);
+    BSP_LAUNCH_CHECK();
+  }
+  return BSP_OK;
+}
+
+extern "C" bsp_status bsp_gtile_check(const bsp_gtile *g, bsp_stream_t stream) {
+  clear_error();
+  BSP_CHECK_ARG(g, "null pointer");
+  int32_t h = 0;
+  cudaStream_t s = as_stream(stream);
+  BSP_CUDA(cudaMemcpyAsync(&h, g->err, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  BSP_CUDA(cudaStreamSynchronize(s));
+  if (h) BSP_FAIL(BSP_ERR_TIMEOUT, "a bounded wait of the gathered-tile kernel gave up");
+  return BSP_OK;
+}

@@ -519,6 +519,41 @@ bsp_status bsp_smat_spmm_path(const bsp_smat *m, const void *B, int32_t N,
  * bounded copy wait gave up. */
 bsp_status bsp_smat_check(const bsp_smat *m, bsp_stream_t stream);
 
+/* Gathered-tile form of the SMaT SpMM for matrices whose nonzeros scatter
+ * over all columns (graph adjacency), where 16x16 tiles of the matrix as
+ * given hold a handful of entries (the 2^20-row power-law graph: 14.9M
+ * tiles, 0.8% full, 7.6 GB in FP16, more than int32 tile indexing holds).
+ * Each group of 16 rows keeps its distinct columns in chunks of 16 and the
+ * 16x16 tile of its values in those columns; the product gathers a chunk's
+ * 16 B rows into shared memory and runs the same tcgen05.mma as the block
+ * path (persistent CTAs, two TMEM accumulators).  No reference counterpart
+ * (the reference's SMaT, src/smat.cu:22-91, only has the plain tiles).
+ * Built on the host from host CSR arrays; FP16 or BF16; N % 8 == 0; groups
+ * with more than 64 chunks are split and summed in a fixed order through a
+ * workspace of bsp_gtile_workspace(g, N) bytes. */
+typedef struct {
+  int32_t rows, cols, nnz, dtype;
+  int64_t nchunks;
+  int32_t ngroups, npieces, nsplit, nslots;
+  int32_t *piece_ptr;    /* [npieces+1] chunk ranges */
+  int32_t *piece_group;  /* [npieces] */
+  int32_t *piece_slot;   /* [npieces] partial-row slot, -1 when the piece is its group's only one */
+  int32_t *group_piece;  /* [ngroups+1] piece ranges of each group */
+  int32_t *split_groups; /* [nsplit] groups with more than one piece */
+  int32_t *chunk_cols;   /* [nchunks*16] gathered B rows (0 in padding slots) */
+  void *chunk_tiles;     /* [nchunks*256] FP16/BF16 tiles, tcgen05 K-major core layout */
+  int32_t *err;          /* device flag: a bounded wait gave up */
+} bsp_gtile;
+bsp_status bsp_gtile_create_host(int32_t rows, int32_t cols, int32_t nnz, const int32_t *rowPtr,
+                                 const int32_t *colIdx, const double *values, bsp_dtype dtype,
+                                 bsp_gtile *out);
+size_t bsp_gtile_workspace(const bsp_gtile *g, int32_t N);
+bsp_status bsp_gtile_spmm(const bsp_gtile *g, const void *B, int32_t N, int64_t ldb, float *C,
+                          int64_t ldc, float alpha, float beta, void *workspace,
+                          size_t workspace_bytes, bsp_stream_t stream);
+bsp_status bsp_gtile_check(const bsp_gtile *g, bsp_stream_t stream);
+bsp_status bsp_gtile_free(bsp_gtile *g);
+
 /* ---------------------------------------------------------------------- */
 /* Conjugate gradients (absent in the reference): plain FP64 CG, or
  * mixed-precision CG with reliable updates -- iterations run on the matrix

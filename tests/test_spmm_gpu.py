@@ -315,3 +315,40 @@ def test_smat_tcgen05_persistent_many_block_rows(cuda, N):
     tol = 2.0 * (L * u / (1 - L * u)) * 1.5 * absC + 4 * u * (1.5 * absC + 0.5 * np.abs(Cin.cpu().numpy())) + 1e-30
     assert np.all(np.abs(C1.cpu().numpy().astype(np.float64) - want) <= tol)
     M.free()
+
+
+@pytest.mark.parametrize("name", ["f16", "bf16"])
+@pytest.mark.parametrize("N", [32, 64, 128, 256])
+def test_gtile_spmm_matches_fp64(cuda, name, N):
+    """Gathered-tile tensor-core SpMM on a power-law graph (rows up to
+    thousands of nonzeros, so some 16-row groups span several 64-chunk
+    pieces summed through the workspace): each group's chunk columns are its
+    distinct columns in ascending order, the product is within the FP32
+    bound of the FP64 oracle (L = 16 x the group's chunks + pieces + 2 terms
+    per output) and repeat calls give the same bits; alpha and beta."""
+    import torch
+    A = bsp.gen_graph(12000, 1.8, 24, 5)
+    vals_t, vals64, B_t, B64 = _case(A, N, name, N + 3)
+    Aq = bsp.HostCSR(A.rows, A.cols, A.rowptr, A.colidx, vals64)
+    G = bsp.GatherTileMatrix(Aq, dtype=name)
+    assert G.nsplit > 0 and G.ngroups == (A.rows + 15) // 16
+    cpg = G.chunks_per_group()
+    cols = bsp.api._d2h(G.chunk_cols, G.nchunks * 16, np.int32).reshape(-1, 16)
+    starts = np.concatenate([[0], np.cumsum(cpg)])
+    for g in (0, 7, G.ngroups - 1, int(np.argmax(cpg))):
+        u = np.unique(A.colidx[A.rowptr[16 * g]:A.rowptr[min(A.rows, 16 * g + 16)]])
+        got = cols[starts[g]:starts[g + 1]].reshape(-1)
+        assert np.array_equal(got[:u.size], u) and not got[u.size:].any()
+    Bd = B_t.to(cuda)
+    Cin = torch.from_numpy(np.random.default_rng(N).uniform(-1, 1, (A.rows, N)).astype(np.float32)).to(cuda)
+    C1 = G.spmm(Bd, Cin.clone(), alpha=0.75, beta=-2.0)
+    C2 = G.spmm(Bd, Cin.clone(), alpha=0.75, beta=-2.0)
+    G.check()
+    assert torch.equal(C1, C2)
+    Cref, absC = pyoracle.spmm_f64(A.rowptr, A.colidx, vals64, B64)
+    want = 0.75 * Cref - 2.0 * Cin.cpu().numpy().astype(np.float64)
+    L = (16.0 * np.repeat(cpg, 16)[:A.rows] + 2.0 + 64)[:, None]
+    u = 2.0 ** -24
+    tol = 2.0 * (L * u / (1 - L * u)) * 0.75 * absC + 4 * u * (0.75 * absC + 2.0 * np.abs(Cin.cpu().numpy())) + 1e-30
+    assert np.all(np.abs(C1.cpu().numpy().astype(np.float64) - want) <= tol)
+    G.free()
