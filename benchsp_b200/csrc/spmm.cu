@@ -294,6 +294,13 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
       : "memory");
   return ok != 0;
 }
+// alpha * acc + beta * c with a fixed rounding (one product, one fused
+// multiply-add) so that every tensor-core kernel stores the same bits for the
+// same accumulator, whatever contraction the compiler would choose.
+__device__ __forceinline__ float scale_out(float alpha, float acc, float beta, const float *cp) {
+  const float o = __fmul_rn(alpha, acc);
+  return beta != 0.f ? __fmaf_rn(beta, *cp, o) : o;
+}
 // Bounded wait; returns false on timeout.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity) {
   for (long long i = 0; i < kSpinLimit; ++i)
@@ -642,9 +649,7 @@ __global__ void __launch_bounds__(kTcThreads) spmm_tc_kernel(const __grid_consta
       const int64_t row = (int64_t)br * kTS + j;
       if (mine && row < M) {
         float *cp = C + row * ldc + col;
-        float o = alpha * v[j];
-        if (beta != 0.f) o += beta * *cp;
-        *cp = o;
+        *cp = scale_out(alpha, v[j], beta, cp);
       }
     }
   } else if (threadIdx.x == 0) {
@@ -660,7 +665,7 @@ __global__ void __launch_bounds__(kTcThreads) spmm_tc_kernel(const __grid_consta
 // ---------------------------------------------------------------------------
 // Persistent, warp-specialised form of the tcgen05 block SpMM.  The CTAs of
 // one launch stay resident and walk the work items w = blockIdx.x +
-// j * gridDim.x (item = (16-row block br, slab of W C columns), slab-major),
+// j * gridDim.x (item = (16-row block br, slab of WT C columns), slab-major),
 // so the set-up (barriers, TMEM allocation) is paid once per CTA instead of
 // once per block row, and the tile stream runs on across block rows:
 //   warp 0 (one lane): producer -- per tile, waits for its stage to be free,
@@ -675,8 +680,24 @@ __global__ void __launch_bounds__(kTcThreads) spmm_tc_kernel(const __grid_consta
 // Every wait is bounded; a timeout sets the shared abort flag, which the
 // other roles see at their next wait, and the error flag; the producer then
 // waits (bounded) for the copies it issued before leaving.
+//
+// WT = 64 or 128 C columns per item, S stages of WT x 16 B values + one
+// 512-byte tile.  With WT = 64 the MMA still has M = 128: its A rows 64..127
+// read the 2 KB that follow the stage (the next stage, or for the last stage
+// the tile area, S * 512 >= 2048 bytes), and the matching D lanes are never
+// read back.  HINT: L2 cache policies -- the B boxes are loaded evict-last (a
+// slab pass re-reads each B block row once per tile that uses it), the tiles
+// evict-first and C stored streaming, so that the one-use data does not push
+// B out of L2.
 constexpr int kTcpThreads = 192;
-constexpr int kTcpSmem = 1024 + kTcStages * (kTcBBytes + kTcABytes) + 256;
+
+template <int WT, int S>
+struct TcpCfg {
+  static constexpr int kBBytes = WT * kTS * 2;
+  static constexpr int kSmem = 1024 + S * (kBBytes + kTcABytes) + 256;
+  static_assert(WT == 64 || WT == 128, "slab width");
+  static_assert(WT == 128 || S * kTcABytes >= 2048, "the last stage's upper A rows must stay in the CTA's memory");
+};
 
 __device__ __forceinline__ bool tcp_wait(uint64_t *bar, unsigned parity, volatile int *abort_flag) {
   for (long long i = 0; i < kSpinLimit; ++i) {
@@ -691,34 +712,61 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
-template <typename T>
+__device__ __forceinline__ uint64_t l2_evict_last_policy() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t l2_evict_first_policy() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ void tma_load_2d_hint(void *dst, const CUtensorMap *map, int32_t c0, int32_t c1,
+                                                 uint64_t *bar, uint64_t policy) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1, {%2, "
+      "%3}], [%4], %5;" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(smem_u32(bar)), "l"(policy)
+      : "memory");
+}
+__device__ __forceinline__ void bulk_g2s_hint(void *dst, const void *src, unsigned bytes, uint64_t *bar,
+                                              uint64_t policy) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], "
+      "%4;" ::"r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(policy)
+      : "memory");
+}
+
+template <typename T, int WT, int S, bool HINT>
 __global__ void __launch_bounds__(kTcpThreads) spmm_tcp_kernel(const __grid_constant__ CUtensorMap tmB, int32_t M,
-                                                               int32_t N, int32_t W, int32_t nbr,
+                                                               int32_t N, int32_t nbr,
                                                                const int32_t *__restrict__ bptr,
                                                                const int32_t *__restrict__ bcol,
                                                                const T *__restrict__ tiles, float *__restrict__ C,
                                                                int64_t ldc, float alpha, float beta,
                                                                int32_t *__restrict__ err) {
+  using Cfg = TcpCfg<WT, S>;
   extern __shared__ unsigned char smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
   unsigned char *sm = smem_raw + ((1024u - (raw & 1023u)) & 1023u);
   unsigned char *bslab = sm;
-  unsigned char *atile = sm + kTcStages * kTcBBytes;
-  uint64_t *full = reinterpret_cast<uint64_t *>(atile + kTcStages * kTcABytes);
-  uint64_t *empty = full + kTcStages;
-  uint64_t *done = empty + kTcStages;   // [2]
+  unsigned char *atile = sm + S * Cfg::kBBytes;
+  uint64_t *full = reinterpret_cast<uint64_t *>(atile + S * kTcABytes);
+  uint64_t *empty = full + S;
+  uint64_t *done = empty + S;           // [2]
   uint64_t *accfree = done + 2;         // [2]
   uint64_t *drain = accfree + 2;        // the MMA issuer's last commit
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
   volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int nslab = (N + W - 1) / W;
+  const int nslab = (N + WT - 1) / WT;
   const int64_t total = (int64_t)nbr * nslab;
-  const bool two_boxes = W > 64;
 
   if (threadIdx.x == 0) {
-    for (int i = 0; i < kTcStages; ++i) {
+    for (int i = 0; i < S; ++i) {
       mbar_init(&full[i], 1);
       mbar_init(&empty[i], 1);
     }
@@ -743,34 +791,44 @@ __global__ void __launch_bounds__(kTcpThreads) spmm_tcp_kernel(const __grid_cons
 
   if (warp == 0 && lane == 0) {
     // ---- producer
+    const uint64_t keep = HINT ? l2_evict_last_policy() : 0, stream = HINT ? l2_evict_first_policy() : 0;
     int64_t it = 0;
     bool ok = true;
     for (int64_t w = blockIdx.x; w < total && ok; w += gridDim.x) {
       const int32_t br = (int32_t)(w % nbr);
-      const int32_t n0 = (int32_t)(w / nbr) * W;
+      const int32_t n0 = (int32_t)(w / nbr) * WT;
       const int32_t k0 = bptr[br], nk = bptr[br + 1] - k0;
       for (int32_t i = 0; i < nk; ++i, ++it) {
-        const int st = (int)(it % kTcStages);
-        if (it >= kTcStages && !tcp_wait(&empty[st], (unsigned)((it / kTcStages - 1) & 1), abort_flag)) {
+        const int st = (int)(it % S);
+        if (it >= S && !tcp_wait(&empty[st], (unsigned)((it / S - 1) & 1), abort_flag)) {
           ok = false;
           break;
         }
         const int32_t bc = bcol[k0 + i];
-        mbar_expect_tx(&full[st], (two_boxes ? kTcBBytes : kTcBBytes / 2) + kTcABytes);
-        tma_load_2d(bslab + st * kTcBBytes, &tmB, n0, bc * kTS, &full[st]);
-        if (two_boxes) tma_load_2d(bslab + st * kTcBBytes + kTcBBytes / 2, &tmB, n0 + 64, bc * kTS, &full[st]);
-        bulk_g2s(atile + st * kTcABytes, tiles + (int64_t)(k0 + i) * kTS * kTS, kTcABytes, &full[st]);
+        unsigned char *bs = bslab + st * Cfg::kBBytes;
+        const T *tp = tiles + (int64_t)(k0 + i) * kTS * kTS;
+        mbar_expect_tx(&full[st], Cfg::kBBytes + kTcABytes);
+        if (HINT) {
+          tma_load_2d_hint(bs, &tmB, n0, bc * kTS, &full[st], keep);
+          if (WT > 64) tma_load_2d_hint(bs + 2048, &tmB, n0 + 64, bc * kTS, &full[st], keep);
+          bulk_g2s_hint(atile + st * kTcABytes, tp, kTcABytes, &full[st], stream);
+        } else {
+          tma_load_2d(bs, &tmB, n0, bc * kTS, &full[st]);
+          if (WT > 64) tma_load_2d(bs + 2048, &tmB, n0 + 64, bc * kTS, &full[st]);
+          bulk_g2s(atile + st * kTcABytes, tp, kTcABytes, &full[st]);
+        }
       }
     }
     if (!ok) {
-      // the copies issued into the last kTcStages stages land before the CTA goes away
-      for (int64_t j = it > kTcStages ? it - kTcStages : 0; j < it; ++j)
-        (void)mbar_wait(&full[j % kTcStages], (unsigned)((j / kTcStages) & 1));
+      // the copies issued into the last S stages land before the CTA goes away
+      for (int64_t j = it > S ? it - S : 0; j < it; ++j) (void)mbar_wait(&full[j % S], (unsigned)((j / S) & 1));
       atomicExch(err, 1);
     }
   } else if (warp == 1 && lane == 0) {
     // ---- MMA issuer
     constexpr uint32_t fmt = std::is_same<T, __nv_bfloat16>::value ? 1u : 0u;
+    // kind::f16 instruction descriptor: D FP32, A and B in `fmt`, A MN-major,
+    // B K-major, N = 16, M = 128
     constexpr uint32_t idesc = (1u << 4) | (fmt << 7) | (fmt << 10) | (1u << 15) | ((16u >> 3) << 17) |
                                ((uint32_t)(kTcSlab >> 4) << 24);
     int64_t it = 0, j = 0;
@@ -785,12 +843,15 @@ __global__ void __launch_bounds__(kTcpThreads) spmm_tcp_kernel(const __grid_cons
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       for (int32_t i = 0; i < nk; ++i, ++it) {
-        const int st = (int)(it % kTcStages);
-        if (!tcp_wait(&full[st], (unsigned)((it / kTcStages) & 1), abort_flag)) {
+        const int st = (int)(it % S);
+        if (!tcp_wait(&full[st], (unsigned)((it / S) & 1), abort_flag)) {
           ok = false;
           break;
         }
-        const uint64_t adesc = umma_smem_desc(smem_u32(bslab + st * kTcBBytes), 2048u, 1024u, 2u);
+        // A: the B slab, 128-byte swizzle, 64-column halves 2 KB apart (LBO),
+        // 8-row K groups 1 KB apart (SBO).  B: the tile, no swizzle, K halves
+        // 128 B apart (LBO), 8-row groups 256 B apart (SBO).
+        const uint64_t adesc = umma_smem_desc(smem_u32(bslab + st * Cfg::kBBytes), 2048u, 1024u, 2u);
         const uint64_t bdesc = umma_smem_desc(smem_u32(atile + st * kTcABytes), 128u, 256u, 0u);
         umma_f16(tmem + 16u * (uint32_t)buf, adesc, bdesc, idesc, i > 0 ? 1u : 0u);
         umma_commit(&empty[st]);
@@ -807,7 +868,7 @@ __global__ void __launch_bounds__(kTcpThreads) spmm_tcp_kernel(const __grid_cons
     int64_t j = 0;
     for (int64_t w = blockIdx.x; w < total; w += gridDim.x, ++j) {
       const int32_t br = (int32_t)(w % nbr);
-      const int32_t n0 = (int32_t)(w / nbr) * W;
+      const int32_t n0 = (int32_t)(w / nbr) * WT;
       const int32_t nk = bptr[br + 1] - bptr[br];
       const int buf = (int)(j & 1);
       if (!tcp_wait(&done[buf], (unsigned)((j / 2) & 1), abort_flag)) {
@@ -834,15 +895,17 @@ __global__ void __launch_bounds__(kTcpThreads) spmm_tcp_kernel(const __grid_cons
       __syncwarp();
       if (lane == 0) mbar_arrive(&accfree[buf]);
       const int64_t col = (int64_t)n0 + q * 32 + lane;
-      if (q * 32 < W && col < N) {
+      if (q * 32 < WT && col < N) {
 #pragma unroll
         for (int r = 0; r < 16; ++r) {
           const int64_t row = (int64_t)br * kTS + r;
           if (row < M) {
             float *cp = C + row * ldc + col;
-            float o = alpha * v[r];
-            if (beta != 0.f) o += beta * *cp;
-            *cp = o;
+            const float o = scale_out(alpha, v[r], beta, cp);
+            if (HINT)
+              __stcs(cp, o);
+            else
+              *cp = o;
           }
         }
       }
@@ -870,6 +933,7 @@ __global__ void __launch_bounds__(kTcpThreads) spmm_tcp_kernel(const __grid_cons
 // kGtPieceChunks chunks of one group; groups with several pieces write
 // partial rows, summed in piece order by gtile_reduce_kernel.
 constexpr int kGtPieceChunks = 64;
+constexpr int kGtcSmem = TcpCfg<128, kTcStages>::kSmem;
 
 __device__ __forceinline__ void cp_async16(void *dst, const void *src, bool valid) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src),
@@ -1050,9 +1114,7 @@ __global__ void __launch_bounds__(kTcpThreads) spmm_gtc_kernel(
             part[((int64_t)slot * kTS + r) * N + col] = v[r];
           } else {
             float *cp = C + row * ldc + col;
-            float o = alpha * v[r];
-            if (beta != 0.f) o += beta * *cp;
-            *cp = o;
+            *cp = scale_out(alpha, v[r], beta, cp);
           }
         }
       }
@@ -1082,9 +1144,7 @@ __global__ void gtile_reduce_kernel(int32_t nsplit, const int32_t *__restrict__ 
     for (int32_t p = group_piece[g]; p < group_piece[g + 1]; ++p)
       acc += part[((int64_t)piece_slot[p] * kTS + r) * N + col];
     float *cp = C + row * ldc + col;
-    float o = alpha * acc;
-    if (beta != 0.f) o += beta * *cp;
-    *cp = o;
+    *cp = scale_out(alpha, acc, beta, cp);
   }
 }
 
@@ -1322,13 +1382,31 @@ static int tc_slab_width(int32_t N, int32_t cols) {
   return N >= 128 ? 128 : 64;
 }
 
-// Resident CTAs per SM for the persistent kernel: 8 (the register and
-// shared-memory limits at 40 registers x 192 threads and 20.7 KB; TMEM 8 x
-// 32 of 512 columns).  The occupancy API's answer here left one CTA per SM
-// (148 CTAs, 9.4% of warps active).
-template <typename T>
-static int tcp_blocks_per_sm() {
-  return 8;
+// Resident CTAs per SM for the persistent kernel: at most 8 (40 registers x
+// 192 threads; TMEM 8 x 32 of 512 columns), fewer when the stages' shared
+// memory (plus 1 KB the system keeps per CTA) does not fit 228 KB.  The
+// occupancy API's answer here left one CTA per SM (148 CTAs, 9.4% of warps
+// active).
+static int tcp_blocks_per_sm(int smem) {
+  const int by_smem = (228 * 1024) / (smem + 1024);
+  return std::max(1, std::min(8, by_smem));
+}
+
+// Stages per slab width and whether the L2 policies are used.
+constexpr int kTcpStages64 = 8;
+constexpr int kTcpStages128 = 4;
+constexpr bool kTcpHint = true;
+
+template <typename T, int WT, int S>
+static void tcp_launch(const CUtensorMap &map, const bsp_smat *m, int32_t N, float *C, int64_t ldc, float alpha,
+                       float beta, cudaStream_t s) {
+  using Cfg = TcpCfg<WT, S>;
+  const int64_t total = (int64_t)m->tiles.rowRegions * ceil_div(N, WT);
+  const int per_sm = tcp_blocks_per_sm(Cfg::kSmem);
+  const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(total, (int64_t)sm_count() * per_sm));
+  spmm_tcp_kernel<T, WT, S, kTcpHint><<<grid, kTcpThreads, Cfg::kSmem, s>>>(
+      map, m->rows, N, m->tiles.rowRegions, m->tiles.bcsrRowPtr, m->tiles.bcsrcolIdx, (const T *)m->tile_val, C,
+      ldc, alpha, beta, m->err);
 }
 
 // Persistent form: one wave of resident CTAs walking all (block row, slab)
@@ -1337,19 +1415,18 @@ static bsp_status smat_spmm_tcp(const bsp_smat *m, const void *B, int32_t N, int
                                 float alpha, float beta, int32_t W, cudaStream_t s) {
   CUtensorMap map;
   BSP_TRY(make_b_map(&map, B, m->cols, N, ldb, m->dtype == BSP_BF16));
-  const int64_t total = (int64_t)m->tiles.rowRegions * ceil_div(N, W);
   const bool bf = m->dtype == BSP_BF16;
-  const int per_sm = bf ? tcp_blocks_per_sm<__nv_bfloat16>() : tcp_blocks_per_sm<__half>();
-  const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(total, (int64_t)sm_count() * per_sm));
-  if (!bf)
-    spmm_tcp_kernel<__half><<<grid, kTcpThreads, kTcpSmem, s>>>(map, m->rows, N, W, m->tiles.rowRegions,
-                                                                m->tiles.bcsrRowPtr, m->tiles.bcsrcolIdx,
-                                                                (const __half *)m->tile_val, C, ldc, alpha, beta,
-                                                                m->err);
-  else
-    spmm_tcp_kernel<__nv_bfloat16><<<grid, kTcpThreads, kTcpSmem, s>>>(
-        map, m->rows, N, W, m->tiles.rowRegions, m->tiles.bcsrRowPtr, m->tiles.bcsrcolIdx,
-        (const __nv_bfloat16 *)m->tile_val, C, ldc, alpha, beta, m->err);
+  if (W == 128) {
+    if (bf)
+      tcp_launch<__nv_bfloat16, 128, kTcpStages128>(map, m, N, C, ldc, alpha, beta, s);
+    else
+      tcp_launch<__half, 128, kTcpStages128>(map, m, N, C, ldc, alpha, beta, s);
+  } else {
+    if (bf)
+      tcp_launch<__nv_bfloat16, 64, kTcpStages64>(map, m, N, C, ldc, alpha, beta, s);
+    else
+      tcp_launch<__half, 64, kTcpStages64>(map, m, N, C, ldc, alpha, beta, s);
+  }
   BSP_LAUNCH_CHECK();
   return BSP_OK;
 }
@@ -2189,11 +2266,11 @@ extern "C" bsp_status bsp_gtile_spmm(const bsp_gtile *g, const void *B, int32_t 
   const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(total, (int64_t)sm_count() * 8));
   float *part = static_cast<float *>(workspace);
   if (g->dtype == BSP_F16)
-    spmm_gtc_kernel<__half><<<grid, kTcpThreads, kTcpSmem, s>>>(
+    spmm_gtc_kernel<__half><<<grid, kTcpThreads, kGtcSmem, s>>>(
         g->rows, N, W, g->npieces, g->piece_ptr, g->piece_group, g->piece_slot, g->chunk_cols,
         (const __half *)g->chunk_tiles, (const __half *)B, ldb, C, ldc, part, alpha, beta, g->err);
   else
-    spmm_gtc_kernel<__nv_bfloat16><<<grid, kTcpThreads, kTcpSmem, s>>>(
+    spmm_gtc_kernel<__nv_bfloat16><<<grid, kTcpThreads, kGtcSmem, s>>>(
         g->rows, N, W, g->npieces, g->piece_ptr, g->piece_group, g->piece_slot, g->chunk_cols,
         (const __nv_bfloat16 *)g->chunk_tiles, (const __nv_bfloat16 *)B, ldb, C, ldc, part, alpha, beta, g->err);
   BSP_LAUNCH_CHECK();
