@@ -715,6 +715,7 @@ def run_suite(args) -> None:
     _emit("spmm_graph_1M_zipf1.8_deg32", n=A.rows, nnz=A.nnz, max_row=int(np.diff(A.rowptr).max()), variants=res)
     run_smat_graph(bsp, dev, up, A)
     del rp, ci, v64, A64
+    run_gtile(bsp, dev, up, A, gpk)
 
     # --- block SpMM on dense 16x16 tiles: tcgen05 vs mma.sync vs CSR
     A = bsp.gen_random_bsr(32768, 16, 8, 1.0, 1.0, SEED + 5)
@@ -812,6 +813,72 @@ def run_smat_graph(bsp, dev, up, A) -> None:
           tiles=Sm.tiles, tile_fill=round(Sm.fill, 4), variants=res)
     Sm.free()
     P.free()
+
+
+def _permute_columns(A, seed: int):
+    """A with its columns renumbered by a seeded random permutation (each
+    row's entries re-sorted by the new column)."""
+    perm = np.random.default_rng(seed).permutation(A.cols).astype(np.int32)
+    rows = np.repeat(np.arange(A.rows, dtype=np.int32), np.diff(A.rowptr))
+    nc = perm[A.colidx]
+    o = np.lexsort((nc, rows))
+    return type(A)(A.rows, A.cols, A.rowptr, np.ascontiguousarray(nc[o]), np.ascontiguousarray(A.values[o]))
+
+
+def run_gtile(bsp, dev, up, graph, gpk) -> None:
+    """Gathered-tile tcgen05 SpMM (bsp_gtile: every 16-row group's distinct
+    columns in chunks of 16 with their 16x16 value tiles, the chunk's B rows
+    gathered into shared memory) beside the slab CSR engine, FP16, N = 32 /
+    128 / 256: a 27-point stencil 48^3 x 4 dof with its columns permuted at
+    random (a group's rows share columns scattered over the whole range, so
+    the matrix's own 16x16 tiles are nearly empty while its chunks are half
+    full) and the power-law graph (chunks about 1/16 full).  The engine
+    choice's pick and estimates; the product against torch.sparse FP64 on
+    the same FP16 values."""
+    import time
+
+    import torch
+    for label, A in (("stencil27_48cubed_4dof_columns_permuted", _permute_columns(make_matrix(48)[0], SEED + 7)),
+                     ("graph_1M_zipf1.8_deg32", graph)):
+        rp, ci, v64 = up(A.rowptr, A.colidx, A.values)
+        vh = v64.half()
+        Ah = bsp.HostCSR(A.rows, A.cols, A.rowptr, A.colidx, vh.double().cpu().numpy())
+        t0 = time.perf_counter()
+        G = bsp.GatherTileMatrix(Ah, "f16")
+        build_s = time.perf_counter() - t0
+        chunks = int(G.nchunks)
+        A64 = torch.sparse_csr_tensor(rp.long(), ci.long(), vh.double(), size=(A.rows, A.cols))
+        P = bsp.SpmmPlan(rp, ci, vh, cols=A.cols, chunk=256)
+        res = {}
+        for N in (32, 128, 256):
+            g = torch.Generator(device="cpu").manual_seed(N)
+            B = (torch.rand(A.cols, N, generator=g, dtype=torch.float64) * 2 - 1).half().to(dev)
+            Cg = G.spmm(B)
+            Cs = P.spmm(B)
+            Cref = A64 @ B.double()
+            err = float(torch.linalg.norm(Cg.double() - Cref) / torch.linalg.norm(Cref))
+            tg = _timed(lambda: G.spmm(B, Cg), 10)
+            ts = _timed(lambda: P.spmm(B, Cs), 10)
+            choice, _ = bsp.choose_spmm_host(A, N, reorder=False)
+            gathered = chunks * 16 * N * 2
+            w = min(256, 2 * N)
+            res[f"N{N}"] = {"gtile_ms": round(tg * 1e3, 3), "slab_csr_ms": round(ts * 1e3, 3),
+                            "speedup_vs_slab": round(ts / tg, 2), "tflops": round(2 * A.nnz * N / tg / 1e12, 2),
+                            "rel_err_vs_fp64": err, "chooser": choice["engine"],
+                            "est_ms": {"gtile": round(choice["est_seconds_gtile_given"] * 1e3, 3),
+                                       "csr": round(choice["est_seconds_csr"] * 1e3, 3)},
+                            "gather_roofline": {"bound": "random gathers", "achieved": round(gathered / tg / 1e9, 1),
+                                                "peak": gpk[f"w{w}_dram"]["gbs"], "unit": "GB/s",
+                                                "frac": round(gathered / tg / 1e9 / gpk[f"w{w}_dram"]["gbs"], 3),
+                                                "peak_src": f"bsp_gather_probe width {w} B, "
+                                                            f"{gpk[f'w{w}_dram']['buffer_mb']} MB buffer"}}
+        G.check()
+        _emit(f"gtile_spmm_{label}", rows=A.rows, nnz=A.nnz, build_host_s=round(build_s, 2), chunks=chunks,
+              chunk_fill=round(A.nnz / (256.0 * chunks), 4), tiles_16x16=choice["tiles_given"],
+              tile_fill=round(A.nnz / (256.0 * choice["tiles_given"]), 4), variants=res)
+        G.free()
+        P.free()
+        del rp, ci, v64, vh, A64
 
 
 def run_scaled_bsr(bsp, dev, pk, up) -> None:

@@ -183,10 +183,11 @@ class BspSpmmChoice(C.Structure):
     _fields_ = [("engine", C.c_int32), ("smat_path", C.c_int32), ("reorder", C.c_int32), ("reserved", C.c_int32),
                 ("tiles_given", C.c_int64), ("tiles_reordered", C.c_int64),
                 ("est_seconds_smat_given", C.c_double), ("est_seconds_smat_reordered", C.c_double),
-                ("est_seconds_csr", C.c_double)]
+                ("est_seconds_csr", C.c_double), ("chunks_given", C.c_int64), ("chunks_reordered", C.c_int64),
+                ("est_seconds_gtile_given", C.c_double), ("est_seconds_gtile_reordered", C.c_double)]
 
 
-BSP_SPMM_ENGINE_CSR, BSP_SPMM_ENGINE_SMAT = 0, 1
+BSP_SPMM_ENGINE_CSR, BSP_SPMM_ENGINE_SMAT, BSP_SPMM_ENGINE_GTILE = 0, 1, 2
 
 
 class BspCgResult(C.Structure):

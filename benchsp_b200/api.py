@@ -1074,10 +1074,11 @@ def permute_rows_csr_host(A: "HostCSR", perm: np.ndarray) -> "HostCSR":
 
 
 def choose_spmm_host(A: "HostCSR", N: int, reorder: bool = True) -> tuple:
-    """SpMM engine for C = A B with N columns of B: ({engine: "smat" or
-    "csr", smat_path, reorder, tiles and time estimates}, perm or None).
-    With reorder, perm is the row-similarity order (apply it with
-    permute_rows_csr_host when the choice says reorder)."""
+    """SpMM engine for C = A B with N columns of B: ({engine: "smat",
+    "gtile" or "csr", smat_path, reorder, tile and chunk counts, time
+    estimates}, perm or None).  With reorder, perm is the row-similarity
+    order (apply it with permute_rows_csr_host when the choice says
+    reorder)."""
     rp = np.ascontiguousarray(A.rowptr, np.int32)
     ci = np.ascontiguousarray(A.colidx, np.int32)
     perm = np.empty(A.rows, np.int32) if reorder else None
@@ -1085,7 +1086,7 @@ def choose_spmm_host(A: "HostCSR", N: int, reorder: bool = True) -> tuple:
     check(lib().bsp_spmm_choose_host(A.rows, A.cols, ci.size, _np_ptr(rp), _np_ptr(ci), N,
                                      _np_ptr(perm) if perm is not None else None, C.byref(c)))
     d = {k: getattr(c, k) for k, _ in _lib.BspSpmmChoice._fields_ if k != "reserved"}
-    d["engine"] = "smat" if c.engine == _lib.BSP_SPMM_ENGINE_SMAT else "csr"
+    d["engine"] = {_lib.BSP_SPMM_ENGINE_SMAT: "smat", _lib.BSP_SPMM_ENGINE_GTILE: "gtile"}.get(c.engine, "csr")
     d["smat_path"] = {v: k for k, v in SmatMatrix._PATHS.items()}[c.smat_path]
     d["reorder"] = bool(c.reorder)
     return d, perm

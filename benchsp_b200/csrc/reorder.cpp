@@ -350,6 +350,34 @@ int64_t count_tiles(int32_t n, const int32_t *rp, const int32_t *ci, const int32
 // 1.93 ms for 67.1M nonzeros (2.3e-13 s per nonzero-column).
 constexpr double kTileColSecTc = 4.9e-12;
 constexpr double kNnzColSecCsr = 2.3e-13;
+// Gathered-tile tcgen05 kernel (bsp_gtile): 366,808 chunks of a
+// column-permuted 27-point stencil (48^3 x 4 dof) in 0.668 ms at N = 128 and
+// 1.33 ms at N = 256, 2.01M chunks of a power-law graph in 4.30 ms at N = 128:
+// 1.45e-11 s per chunk-column; below N = 128 the slab is 64 columns and a
+// chunk took 1.2-1.5 ns at N = 32 (counted as 96 columns).
+constexpr double kChunkColSecGt = 1.45e-11;
+
+// Chunks of the gathered-tile form with A's rows in the order `perm` (null:
+// as given): every 16-row group's distinct columns, in chunks of 16, summed.
+int64_t count_chunks(int32_t n, const int32_t *rp, const int32_t *ci, const int32_t *perm) {
+  const int32_t ng = (int32_t)(((int64_t)n + 15) / 16);
+  int64_t total = 0;
+#pragma omp parallel reduction(+ : total)
+  {
+    std::vector<int32_t> t;
+#pragma omp for schedule(dynamic, 256)
+    for (int32_t g = 0; g < ng; ++g) {
+      t.clear();
+      for (int32_t i = g * 16; i < std::min<int32_t>(n, g * 16 + 16); ++i) {
+        const int32_t r = perm ? perm[i] : i;
+        t.insert(t.end(), ci + rp[r], ci + rp[r + 1]);
+      }
+      std::sort(t.begin(), t.end());
+      total += ((int64_t)(std::unique(t.begin(), t.end()) - t.begin()) + 15) / 16;
+    }
+  }
+  return total;
+}
 
 bool valid_csr(int32_t n, int32_t nnz, const int32_t *rp) {
   if (rp[0] != 0 || rp[n] != nnz) return false;
@@ -525,16 +553,26 @@ extern "C" bsp_status bsp_spmm_choose_host(int32_t rows, int32_t cols, int32_t n
   c.est_seconds_csr = kNnzColSecCsr * N * (double)nnz;
   c.est_seconds_smat_given = smat_ok ? per_tile * (double)c.tiles_given : -1.0;
   c.est_seconds_smat_reordered = smat_ok && c.tiles_reordered >= 0 ? per_tile * (double)c.tiles_reordered : -1.0;
+  // the gathered-tile kernel: N % 8 == 0, slabs of 64 or 128 C columns
+  const bool gt_ok = N % 8 == 0;
+  const double per_chunk = kChunkColSecGt * (double)std::max<int64_t>(96, ((int64_t)N + 63) / 64 * 64);
+  c.chunks_given = count_chunks(rows, rowPtr, colIdx, nullptr);
+  c.chunks_reordered = c.tiles_reordered >= 0 ? count_chunks(rows, rowPtr, colIdx, perm) : -1;
+  c.est_seconds_gtile_given = gt_ok ? per_chunk * (double)c.chunks_given : -1.0;
+  c.est_seconds_gtile_reordered = gt_ok && c.chunks_reordered >= 0 ? per_chunk * (double)c.chunks_reordered : -1.0;
   c.engine = BSP_SPMM_ENGINE_CSR;
   double best = c.est_seconds_csr;
-  if (smat_ok && c.est_seconds_smat_given < best) {
-    best = c.est_seconds_smat_given;
-    c.engine = BSP_SPMM_ENGINE_SMAT;
-  }
-  if (c.est_seconds_smat_reordered >= 0 && c.est_seconds_smat_reordered < best) {
-    c.engine = BSP_SPMM_ENGINE_SMAT;
-    c.reorder = 1;
-  }
+  auto take = [&](double est, int32_t engine, int32_t reorder) {
+    if (est >= 0 && est < best) {
+      best = est;
+      c.engine = engine;
+      c.reorder = reorder;
+    }
+  };
+  take(c.est_seconds_smat_given, BSP_SPMM_ENGINE_SMAT, 0);
+  take(c.est_seconds_smat_reordered, BSP_SPMM_ENGINE_SMAT, 1);
+  take(c.est_seconds_gtile_given, BSP_SPMM_ENGINE_GTILE, 0);
+  take(c.est_seconds_gtile_reordered, BSP_SPMM_ENGINE_GTILE, 1);
   *out = c;
   return BSP_OK;
 }

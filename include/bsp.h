@@ -703,23 +703,28 @@ bsp_status bsp_reorder_similarity_host(int32_t rows, int32_t cols, int32_t nnz,
                                        int32_t group_rows, int32_t block_cols,
                                        int32_t *perm);
 /* SpMM engine choice for C = A B with N columns of B, sharing the
- * reordering with the SMaT path: counts the 16x16 tiles of A as given and,
- * when `perm` (rows entries) is not NULL, after bsp_reorder_similarity
+ * reordering with the SMaT path: counts the 16x16 tiles of A and the chunks
+ * of its gathered-tile form (16 distinct columns of a 16-row group) as given
+ * and, when `perm` (rows entries) is not NULL, after bsp_reorder_similarity
  * (written to perm), and estimates each engine from B200 measurements
- * (SMaT time per tile, grouped CSR time per nonzero, both per column of B).
- * engine = BSP_SPMM_ENGINE_SMAT (build the SMaT matrix from the rows in
- * perm order when reorder = 1, and read row i of C as original row perm[i];
- * smat_path says which tile path) or BSP_SPMM_ENGINE_CSR (bsp_spmm_csr on A
- * as given).  SMaT needs N % 32 == 0; the estimates are -1 where an engine
- * does not apply.  Host code, a one-time decision per matrix. */
-enum { BSP_SPMM_ENGINE_CSR = 0, BSP_SPMM_ENGINE_SMAT = 1 };
+ * (SMaT time per tile, gathered-tile time per chunk, grouped CSR time per
+ * nonzero, all per column of B).  engine = BSP_SPMM_ENGINE_SMAT or
+ * BSP_SPMM_ENGINE_GTILE (build that matrix from the rows in perm order when
+ * reorder = 1, and read row i of C as original row perm[i]; smat_path says
+ * which tile path) or BSP_SPMM_ENGINE_CSR (bsp_spmm_csr on A as given).
+ * SMaT needs N % 32 == 0, the gathered tiles N % 8 == 0; the estimates are
+ * -1 where an engine does not apply.  Host code, a one-time decision per
+ * matrix. */
+enum { BSP_SPMM_ENGINE_CSR = 0, BSP_SPMM_ENGINE_SMAT = 1, BSP_SPMM_ENGINE_GTILE = 2 };
 typedef struct bsp_spmm_choice {
   int32_t engine;
   int32_t smat_path;   /* BSP_SMAT_TCGEN05 */
-  int32_t reorder;     /* 1: the SMaT matrix is built from the rows in perm order */
+  int32_t reorder;     /* 1: the chosen matrix is built from the rows in perm order */
   int32_t reserved;
   int64_t tiles_given, tiles_reordered;   /* tiles_reordered = -1 without perm */
   double est_seconds_smat_given, est_seconds_smat_reordered, est_seconds_csr;
+  int64_t chunks_given, chunks_reordered; /* chunks_reordered = -1 without perm */
+  double est_seconds_gtile_given, est_seconds_gtile_reordered;
 } bsp_spmm_choice;
 bsp_status bsp_spmm_choose_host(int32_t rows, int32_t cols, int32_t nnz,
                                 const int32_t *rowPtr, const int32_t *colIdx,

@@ -181,11 +181,29 @@ def test_similarity_group_size_empty_rows_and_bad_input():
 
 def _argmin_engine(d):
     est = {"csr": d["est_seconds_csr"]}
-    if d["est_seconds_smat_given"] >= 0:
-        est["smat_given"] = d["est_seconds_smat_given"]
-    if d["est_seconds_smat_reordered"] >= 0:
-        est["smat_reordered"] = d["est_seconds_smat_reordered"]
+    for e in ("smat", "gtile"):
+        for o in ("given", "reordered"):
+            if d[f"est_seconds_{e}_{o}"] >= 0:
+                est[f"{e}_{o}"] = d[f"est_seconds_{e}_{o}"]
     return min(est, key=lambda k: (est[k], k))
+
+
+def _chunks(A, perm=None):
+    """Gathered-tile chunks: ceil(distinct columns / 16) per 16-row group."""
+    order = np.arange(A.rows) if perm is None else perm
+    total = 0
+    for g in range(0, A.rows, 16):
+        cols = [A.colidx[A.rowptr[r]:A.rowptr[r + 1]] for r in order[g:g + 16]]
+        total += (np.unique(np.concatenate(cols)).size + 15) // 16
+    return total
+
+
+def _permute_columns(A, seed):
+    perm = np.random.default_rng(seed).permutation(A.cols).astype(np.int32)
+    rows = np.repeat(np.arange(A.rows, dtype=np.int32), np.diff(A.rowptr))
+    nc = perm[A.colidx]
+    o = np.lexsort((nc, rows))
+    return bsp.HostCSR(A.rows, A.cols, A.rowptr, np.ascontiguousarray(nc[o]), np.ascontiguousarray(A.values[o]))
 
 
 def test_spmm_choice_uses_the_similarity_order():
@@ -211,6 +229,21 @@ def test_spmm_choice_scattered_rows_and_n():
     assert d["engine"] == "csr" and d["est_seconds_smat_given"] == -1.0
     with pytest.raises(bsp.BspError):
         bsp.choose_spmm_host(S, 0)
+
+
+def test_spmm_choice_picks_gathered_tiles_for_shared_scattered_columns():
+    """A stencil with its columns permuted: 16x16 tiles are almost empty but
+    the rows of a 16-row group share their columns, so the gathered-tile
+    chunks are half full and that engine is estimated fastest."""
+    P = _permute_columns(bsp.gen_stencil27(8, 4, 3), 5)
+    d, perm = bsp.choose_spmm_host(P, 128)
+    assert d["chunks_given"] == _chunks(P) and d["chunks_reordered"] == _chunks(P, perm)
+    assert d["engine"] == "gtile" and d["engine"] == _argmin_engine(d).split("_")[0]
+    assert P.nnz / (16 * 16 * d["chunks_given"]) > 0.4 and P.nnz / (256 * d["tiles_given"]) < 0.1
+    d, _ = bsp.choose_spmm_host(P, 100, reorder=False)          # the gathered tiles need N % 8 == 0
+    assert d["est_seconds_gtile_given"] == -1.0 and d["chunks_reordered"] == -1 and d["engine"] == "csr"
+    d, _ = bsp.choose_spmm_host(P, 104, reorder=False)
+    assert d["engine"] == "gtile" and d["reorder"] is False
 
 
 @pytest.mark.gpu

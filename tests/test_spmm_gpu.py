@@ -352,3 +352,28 @@ def test_gtile_spmm_matches_fp64(cuda, name, N):
     tol = 2.0 * (L * u / (1 - L * u)) * 0.75 * absC + 4 * u * (0.75 * absC + 2.0 * np.abs(Cin.cpu().numpy())) + 1e-30
     assert np.all(np.abs(C1.cpu().numpy().astype(np.float64) - want) <= tol)
     G.free()
+
+
+@pytest.mark.parametrize("N", [24, 64, 136])
+def test_gtile_column_permuted_stencil(cuda, N):
+    """Gathered tiles on a 27-point stencil (4 dof) with its columns
+    permuted at random: half-full 16x16 chunk tiles although the matrix's
+    own 16x16 tiles are nearly empty; N not a multiple of 32 (slab edges),
+    no long groups (no pieces).  Within the FP32 bound of the FP64 oracle."""
+    A0 = bsp.gen_stencil27(8, 4, 13)
+    perm = np.random.default_rng(3).permutation(A0.cols).astype(np.int32)
+    rows = np.repeat(np.arange(A0.rows, dtype=np.int32), np.diff(A0.rowptr))
+    nc = perm[A0.colidx]
+    o = np.lexsort((nc, rows))
+    A = bsp.HostCSR(A0.rows, A0.cols, A0.rowptr, np.ascontiguousarray(nc[o]), np.ascontiguousarray(A0.values[o]))
+    vals_t, vals64, B_t, B64 = _case(A, N, "f16", 41)
+    G = bsp.GatherTileMatrix(bsp.HostCSR(A.rows, A.cols, A.rowptr, A.colidx, vals64), dtype="f16")
+    cpg = G.chunks_per_group()
+    assert G.nsplit == 0 and A.nnz / (256.0 * cpg.sum()) > 0.4
+    C = G.spmm(B_t.to(cuda)).cpu().numpy().astype(np.float64)
+    G.check()
+    Cref, absC = pyoracle.spmm_f64(A.rowptr, A.colidx, vals64, B64)
+    L = (16.0 * np.repeat(cpg, 16)[:A.rows] + 2.0)[:, None]
+    u = 2.0 ** -24
+    assert np.all(np.abs(C - Cref) <= 2.0 * (L * u / (1 - L * u)) * absC + 1e-30)
+    G.free()
