@@ -681,11 +681,12 @@ __global__ void __launch_bounds__(kTcThreads) spmm_tc_kernel(const __grid_consta
 // other roles see at their next wait, and the error flag; the producer then
 // waits (bounded) for the copies it issued before leaving.
 //
-// WT = 64 or 128 C columns per item, S stages of WT x 16 B values + one
-// 512-byte tile.  With WT = 64 the MMA still has M = 128: its A rows 64..127
-// read the 2 KB that follow the stage (the next stage, or for the last stage
-// the tile area, S * 512 >= 2048 bytes), and the matching D lanes are never
-// read back.  HINT: L2 cache policies -- the B boxes are loaded evict-last (a
+// WT = 64 or 128 C columns per item, S stages of 128 x 16 B values (one or
+// two 64-column TMA boxes) + one 512-byte tile.  With WT = 64 the MMA still
+// has M = 128: its A rows 64..127 read the stage's upper 2 KB, which no copy
+// writes (a stride of 2 KB, with those rows reading the next stage while TMA
+// filled it, measured 1.4-2.5x slower at N = 128 / 256), and the matching D
+// lanes are never read back.  HINT: L2 cache policies -- the B boxes are loaded evict-last (a
 // slab pass re-reads each B block row once per tile that uses it), the tiles
 // evict-first and C stored streaming, so that the one-use data does not push
 // B out of L2.
@@ -693,10 +694,10 @@ constexpr int kTcpThreads = 192;
 
 template <int WT, int S>
 struct TcpCfg {
-  static constexpr int kBBytes = WT * kTS * 2;
+  static constexpr int kBBytes = kTcSlab * kTS * 2;   // stage stride: the MMA's 128 A rows
+  static constexpr int kLoadBytes = WT * kTS * 2;     // what the boxes bring
   static constexpr int kSmem = 1024 + S * (kBBytes + kTcABytes) + 256;
   static_assert(WT == 64 || WT == 128, "slab width");
-  static_assert(WT == 128 || S * kTcABytes >= 2048, "the last stage's upper A rows must stay in the CTA's memory");
 };
 
 __device__ __forceinline__ bool tcp_wait(uint64_t *bar, unsigned parity, volatile int *abort_flag) {
@@ -739,10 +740,30 @@ __device__ __forceinline__ void bulk_g2s_hint(void *dst, const void *src, unsign
       : "memory");
 }
 
+// The items w = blockIdx.x + j * gridDim.x of an n x nslab item grid as
+// (r, s) = (w % n, w / n), stepped without a division per item.
+struct ItemWalk {
+  int32_t r, s, dr, ds, n;
+  __device__ __forceinline__ explicit ItemWalk(int32_t n_) : n(n_) {
+    r = (int32_t)(blockIdx.x % (unsigned)n_);
+    s = (int32_t)(blockIdx.x / (unsigned)n_);
+    dr = (int32_t)(gridDim.x % (unsigned)n_);
+    ds = (int32_t)(gridDim.x / (unsigned)n_);
+  }
+  __device__ __forceinline__ void next() {
+    r += dr;
+    s += ds;
+    if (r >= n) {
+      r -= n;
+      ++s;
+    }
+  }
+};
+
 template <typename T, int WT, int S, bool HINT>
 __global__ void __launch_bounds__(kTcpThreads) spmm_tcp_kernel(const __grid_constant__ CUtensorMap tmB, int32_t M,
-                                                               int32_t N, int32_t nbr,
-                                                               const int32_t *__restrict__ bptr,
+                                                               int32_t N, int32_t col0, int32_t nslab,
+                                                               int32_t nbr, const int32_t *__restrict__ bptr,
                                                                const int32_t *__restrict__ bcol,
                                                                const T *__restrict__ tiles, float *__restrict__ C,
                                                                int64_t ldc, float alpha, float beta,
@@ -762,8 +783,6 @@ __global__ void __launch_bounds__(kTcpThreads) spmm_tcp_kernel(const __grid_cons
   volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int nslab = (N + WT - 1) / WT;
-  const int64_t total = (int64_t)nbr * nslab;
 
   if (threadIdx.x == 0) {
     for (int i = 0; i < S; ++i) {
@@ -794,9 +813,9 @@ __global__ void __launch_bounds__(kTcpThreads) spmm_tcp_kernel(const __grid_cons
     const uint64_t keep = HINT ? l2_evict_last_policy() : 0, stream = HINT ? l2_evict_first_policy() : 0;
     int64_t it = 0;
     bool ok = true;
-    for (int64_t w = blockIdx.x; w < total && ok; w += gridDim.x) {
-      const int32_t br = (int32_t)(w % nbr);
-      const int32_t n0 = (int32_t)(w / nbr) * WT;
+    for (ItemWalk iw(nbr); iw.s < nslab && ok; iw.next()) {
+      const int32_t br = iw.r;
+      const int32_t n0 = col0 + iw.s * WT;
       const int32_t k0 = bptr[br], nk = bptr[br + 1] - k0;
       for (int32_t i = 0; i < nk; ++i, ++it) {
         const int st = (int)(it % S);
@@ -807,7 +826,7 @@ __global__ void __launch_bounds__(kTcpThreads) spmm_tcp_kernel(const __grid_cons
         const int32_t bc = bcol[k0 + i];
         unsigned char *bs = bslab + st * Cfg::kBBytes;
         const T *tp = tiles + (int64_t)(k0 + i) * kTS * kTS;
-        mbar_expect_tx(&full[st], Cfg::kBBytes + kTcABytes);
+        mbar_expect_tx(&full[st], Cfg::kLoadBytes + kTcABytes);
         if (HINT) {
           tma_load_2d_hint(bs, &tmB, n0, bc * kTS, &full[st], keep);
           if (WT > 64) tma_load_2d_hint(bs + 2048, &tmB, n0 + 64, bc * kTS, &full[st], keep);
@@ -833,8 +852,8 @@ __global__ void __launch_bounds__(kTcpThreads) spmm_tcp_kernel(const __grid_cons
                                ((uint32_t)(kTcSlab >> 4) << 24);
     int64_t it = 0, j = 0;
     bool ok = true;
-    for (int64_t w = blockIdx.x; w < total && ok; w += gridDim.x, ++j) {
-      const int32_t br = (int32_t)(w % nbr);
+    for (ItemWalk iw(nbr); iw.s < nslab && ok; iw.next(), ++j) {
+      const int32_t br = iw.r;
       const int32_t nk = bptr[br + 1] - bptr[br];
       const int buf = (int)(j & 1);
       if (j >= 2 && !tcp_wait(&accfree[buf], (unsigned)((j / 2 - 1) & 1), abort_flag)) {
@@ -866,9 +885,9 @@ __global__ void __launch_bounds__(kTcpThreads) spmm_tcp_kernel(const __grid_cons
     // ---- epilogue: warp w reads TMEM lanes 32 * (w % 4) .. + 31
     const int q = warp & 3;
     int64_t j = 0;
-    for (int64_t w = blockIdx.x; w < total; w += gridDim.x, ++j) {
-      const int32_t br = (int32_t)(w % nbr);
-      const int32_t n0 = (int32_t)(w / nbr) * WT;
+    for (ItemWalk iw(nbr); iw.s < nslab; iw.next(), ++j) {
+      const int32_t br = iw.r;
+      const int32_t n0 = col0 + iw.s * WT;
       const int32_t nk = bptr[br + 1] - bptr[br];
       const int buf = (int)(j & 1);
       if (!tcp_wait(&done[buf], (unsigned)((j / 2) & 1), abort_flag)) {
@@ -934,6 +953,7 @@ __global__ void __launch_bounds__(kTcpThreads) spmm_tcp_kernel(const __grid_cons
 // partial rows, summed in piece order by gtile_reduce_kernel.
 constexpr int kGtPieceChunks = 64;
 constexpr int kGtcSmem = TcpCfg<128, kTcStages>::kSmem;
+constexpr bool kGtcPerSlab = true;
 
 __device__ __forceinline__ void cp_async16(void *dst, const void *src, bool valid) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src),
@@ -946,7 +966,8 @@ __device__ __forceinline__ void cp_async_arrive_noinc(uint64_t *bar) {
 
 template <typename T>
 __global__ void __launch_bounds__(kTcpThreads) spmm_gtc_kernel(
-    int32_t M, int32_t N, int32_t W, int32_t npieces, const int32_t *__restrict__ piece_ptr,
+    int32_t M, int32_t N, int32_t W, int32_t col0, int32_t nslab, int32_t npieces,
+    const int32_t *__restrict__ piece_ptr,
     const int32_t *__restrict__ piece_group, const int32_t *__restrict__ piece_slot,
     const int32_t *__restrict__ chunk_cols, const T *__restrict__ tiles, const T *__restrict__ B, int64_t ldb,
     float *__restrict__ C, int64_t ldc, float *__restrict__ part, float alpha, float beta,
@@ -965,8 +986,6 @@ __global__ void __launch_bounds__(kTcpThreads) spmm_gtc_kernel(
   volatile int *abort_flag = reinterpret_cast<volatile int *>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int nslab = (N + W - 1) / W;
-  const int64_t total = (int64_t)npieces * nslab;
 
   if (threadIdx.x == 0) {
     for (int i = 0; i < kTcStages; ++i) {
@@ -997,9 +1016,9 @@ __global__ void __launch_bounds__(kTcpThreads) spmm_gtc_kernel(
     const int cpr = W / 8;   // 16-byte pieces per gathered row
     int64_t it = 0;
     bool ok = true;
-    for (int64_t w = blockIdx.x; w < total && ok; w += gridDim.x) {
-      const int32_t p = (int32_t)(w % npieces);
-      const int32_t n0 = (int32_t)(w / npieces) * W;
+    for (ItemWalk iw(npieces); iw.s < nslab && ok; iw.next()) {
+      const int32_t p = iw.r;
+      const int32_t n0 = col0 + iw.s * W;
       const int32_t c0 = piece_ptr[p], c1 = piece_ptr[p + 1];
       for (int32_t c = c0; c < c1; ++c, ++it) {
         const int st = (int)(it % kTcStages);
@@ -1044,8 +1063,8 @@ __global__ void __launch_bounds__(kTcpThreads) spmm_gtc_kernel(
                                ((uint32_t)(kTcSlab >> 4) << 24);
     int64_t it = 0, j = 0;
     bool ok = true;
-    for (int64_t w = blockIdx.x; w < total && ok; w += gridDim.x, ++j) {
-      const int32_t p = (int32_t)(w % npieces);
+    for (ItemWalk iw(npieces); iw.s < nslab && ok; iw.next(), ++j) {
+      const int32_t p = iw.r;
       const int32_t nk = piece_ptr[p + 1] - piece_ptr[p];
       const int buf = (int)(j & 1);
       if (j >= 2 && !tcp_wait(&accfree[buf], (unsigned)((j / 2 - 1) & 1), abort_flag)) {
@@ -1075,9 +1094,9 @@ __global__ void __launch_bounds__(kTcpThreads) spmm_gtc_kernel(
     // ---- epilogue
     const int q = warp & 3;
     int64_t j = 0;
-    for (int64_t w = blockIdx.x; w < total; w += gridDim.x, ++j) {
-      const int32_t p = (int32_t)(w % npieces);
-      const int32_t n0 = (int32_t)(w / npieces) * W;
+    for (ItemWalk iw(npieces); iw.s < nslab; iw.next(), ++j) {
+      const int32_t p = iw.r;
+      const int32_t n0 = col0 + iw.s * W;
       const int32_t nk = piece_ptr[p + 1] - piece_ptr[p];
       const int32_t g = piece_group[p], slot = piece_slot[p];
       const int buf = (int)(j & 1);
@@ -1393,7 +1412,7 @@ static int tcp_blocks_per_sm(int smem) {
 }
 
 // Stages per slab width and whether the L2 policies are used.
-constexpr int kTcpStages64 = 8;
+constexpr int kTcpStages64 = 4;
 constexpr int kTcpStages128 = 4;
 constexpr bool kTcpHint = true;
 
@@ -1401,16 +1420,21 @@ template <typename T, int WT, int S>
 static void tcp_launch(const CUtensorMap &map, const bsp_smat *m, int32_t N, float *C, int64_t ldc, float alpha,
                        float beta, cudaStream_t s) {
   using Cfg = TcpCfg<WT, S>;
-  const int64_t total = (int64_t)m->tiles.rowRegions * ceil_div(N, WT);
+  const int64_t total = (int64_t)m->tiles.rowRegions;
   const int per_sm = tcp_blocks_per_sm(Cfg::kSmem);
   const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(total, (int64_t)sm_count() * per_sm));
-  spmm_tcp_kernel<T, WT, S, kTcpHint><<<grid, kTcpThreads, Cfg::kSmem, s>>>(
-      map, m->rows, N, m->tiles.rowRegions, m->tiles.bcsrRowPtr, m->tiles.bcsrcolIdx, (const T *)m->tile_val, C,
-      ldc, alpha, beta, m->err);
+  for (int32_t c0 = 0; c0 < N; c0 += WT)
+    spmm_tcp_kernel<T, WT, S, kTcpHint><<<grid, kTcpThreads, Cfg::kSmem, s>>>(
+        map, m->rows, N, c0, 1, m->tiles.rowRegions, m->tiles.bcsrRowPtr, m->tiles.bcsrcolIdx,
+        (const T *)m->tile_val, C, ldc, alpha, beta, m->err);
 }
 
-// Persistent form: one wave of resident CTAs walking all (block row, slab)
-// items, slab-major.
+// Persistent form: one wave of resident CTAs walking all block rows, one
+// launch per slab of WT C columns.  A single launch over all slabs (items
+// slab-major) let CTAs drift into the next slab while others finished the
+// last, so two slabs of B competed for L2 (dense tiles, N = 256: 310 us with
+// the item walk dividing per item, 329 us without; 64-column slabs 500 ->
+// 1140 us); launches per slab keep one slab's B in flight at a time.
 static bsp_status smat_spmm_tcp(const bsp_smat *m, const void *B, int32_t N, int64_t ldb, float *C, int64_t ldc,
                                 float alpha, float beta, int32_t W, cudaStream_t s) {
   CUtensorMap map;
@@ -2262,17 +2286,23 @@ extern "C" bsp_status bsp_gtile_spmm(const bsp_gtile *g, const void *B, int32_t 
   if (g->ngroups == 0) return BSP_OK;
   cudaStream_t s = as_stream(stream);
   const int32_t W = N >= 128 ? 128 : 64;
-  const int64_t total = (int64_t)g->npieces * ceil_div(N, W);
+  // one launch per slab of W columns, as the block kernel's (smat_spmm_tcp),
+  // or all slabs in one launch
+  const int32_t per = kGtcPerSlab ? 1 : (int32_t)ceil_div(N, W);
+  const int64_t total = (int64_t)g->npieces * per;
   const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(total, (int64_t)sm_count() * 8));
   float *part = static_cast<float *>(workspace);
-  if (g->dtype == BSP_F16)
-    spmm_gtc_kernel<__half><<<grid, kTcpThreads, kGtcSmem, s>>>(
-        g->rows, N, W, g->npieces, g->piece_ptr, g->piece_group, g->piece_slot, g->chunk_cols,
-        (const __half *)g->chunk_tiles, (const __half *)B, ldb, C, ldc, part, alpha, beta, g->err);
-  else
-    spmm_gtc_kernel<__nv_bfloat16><<<grid, kTcpThreads, kGtcSmem, s>>>(
-        g->rows, N, W, g->npieces, g->piece_ptr, g->piece_group, g->piece_slot, g->chunk_cols,
-        (const __nv_bfloat16 *)g->chunk_tiles, (const __nv_bfloat16 *)B, ldb, C, ldc, part, alpha, beta, g->err);
+  for (int32_t c0 = 0; c0 < N; c0 += W * per) {
+    if (g->dtype == BSP_F16)
+      spmm_gtc_kernel<__half><<<grid, kTcpThreads, kGtcSmem, s>>>(
+          g->rows, N, W, c0, per, g->npieces, g->piece_ptr, g->piece_group, g->piece_slot, g->chunk_cols,
+          (const __half *)g->chunk_tiles, (const __half *)B, ldb, C, ldc, part, alpha, beta, g->err);
+    else
+      spmm_gtc_kernel<__nv_bfloat16><<<grid, kTcpThreads, kGtcSmem, s>>>(
+          g->rows, N, W, c0, per, g->npieces, g->piece_ptr, g->piece_group, g->piece_slot, g->chunk_cols,
+          (const __nv_bfloat16 *)g->chunk_tiles, (const __nv_bfloat16 *)B, ldb, C, ldc, part, alpha, beta,
+          g->err);
+  }
   BSP_LAUNCH_CHECK();
   if (g->nsplit > 0) {
     const int64_t work = (int64_t)g->nsplit * kTS * N;
