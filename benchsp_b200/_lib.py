@@ -22,7 +22,7 @@ STATUS_NAMES = {0: "BSP_OK", 1: "BSP_ERR_INVALID", 2: "BSP_ERR_CUDA", 3: "BSP_ER
 
 F64, F32, F16, BF16 = 0, 1, 2, 3
 
-CSR_AUTO, CSR_VECTOR, CSR_MERGE, CSR_SCALAR = 0, 1, 2, 3
+CSR_AUTO, CSR_VECTOR, CSR_MERGE, CSR_SCALAR, CSR_STREAM = 0, 1, 2, 3, 4
 BSR_AUTO, BSR_FFMA, BSR_DMMA, BSR_ADAPTIVE = 0, 1, 2, 3
 
 
@@ -280,7 +280,8 @@ class BspSpmmPlan(C.Structure):
     _fields_ = [("rows", C.c_int32), ("chunk", C.c_int32), ("nchunks", C.c_int64), ("nparts", C.c_int64),
                 ("nsplit", C.c_int32), ("chunk_ptr", C.c_void_p), ("part_ptr", C.c_void_p),
                 ("chunk_row", C.c_void_p), ("split_rows", C.c_void_p), ("nshort", C.c_int32),
-                ("short_rows", C.c_void_p), ("long_chunk", C.c_void_p)]
+                ("short_rows", C.c_void_p), ("long_chunk", C.c_void_p), ("long_se", C.c_void_p),
+                ("short_se", C.c_void_p), ("slab_l2_hints", C.c_int32)]
 
 
 _PROTOS.update({

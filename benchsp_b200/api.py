@@ -18,7 +18,7 @@ from . import _lib
 from ._lib import BspBsr, check, lib
 
 _ALGO_CSR = {"auto": _lib.CSR_AUTO, "vector": _lib.CSR_VECTOR, "merge": _lib.CSR_MERGE,
-             "scalar": _lib.CSR_SCALAR}
+             "scalar": _lib.CSR_SCALAR, "stream": _lib.CSR_STREAM}
 _ALGO_BSR = {"auto": _lib.BSR_AUTO, "ffma": _lib.BSR_FFMA, "dmma": _lib.BSR_DMMA,
              "adaptive": _lib.BSR_ADAPTIVE}
 
@@ -687,6 +687,16 @@ class SpmmPlan:
 
     def workspace_bytes(self, N: int) -> int:
         return lib().bsp_spmm_plan_workspace(C.byref(self._d), N)
+
+    @property
+    def slab_l2_hints(self) -> int:
+        return self._d.slab_l2_hints
+
+    @slab_l2_hints.setter
+    def slab_l2_hints(self, v: int) -> None:
+        if v not in (0, 1, 2):
+            raise ValueError("slab_l2_hints is 0, 1 or 2")
+        self._d.slab_l2_hints = v
 
     _ENGINES = {"auto": 0, "grouped": 1, "slab": 2}
 

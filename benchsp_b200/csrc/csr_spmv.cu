@@ -108,6 +108,70 @@ __global__ void __launch_bounds__(256) csr_vector_kernel(int32_t rows, const int
   }
 }
 
+// Warp per 32 consecutive rows ("stream").  The warp's nonzero range
+// [rowPtr[r0], rowPtr[r0+32]) is read in pieces of kStreamPiece entries:
+// every lane loads kStreamPiece/32 values and column indices (one coalesced
+// 256-byte access per array and step), issues their x gathers together and
+// stores the products to shared memory; then each lane adds its own row's
+// products of the piece left to right.  Every row costs the same dependent
+// chain (rowPtr -> entries -> x) as in the thread-per-row kernel, but the
+// entry loads are coalesced and all of a piece's gathers are in flight at
+// once.  Multiply and add are rounded separately in column order, so the
+// result equals csr_scalar_kernel's (and ref_spmv_fp64's) bit for bit.
+constexpr int kStreamPiece = 256;
+constexpr int kStreamThreads = 256;
+
+// 48 registers (5 CTAs per SM).  Capped at 40 / 32 registers it measured
+// 16.7 / 17.3 us against 16.5 us on the 7-point Poisson 64^3 (L2 flushed).
+template <typename V>
+__global__ void __launch_bounds__(kStreamThreads) csr_stream_kernel(int32_t rows, const int32_t *__restrict__ rowPtr,
+                                                                    const int32_t *__restrict__ colIdx,
+                                                                    const V *__restrict__ val,
+                                                                    const V *__restrict__ x, V *__restrict__ y,
+                                                                    typename AccOf<V>::T alpha,
+                                                                    typename AccOf<V>::T beta) {
+  using A = typename AccOf<V>::T;
+  constexpr int K = kStreamPiece / 32;
+  __shared__ A prod[kStreamThreads / 32][kStreamPiece];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  A *pw = prod[wib];
+  const int64_t nblk = ((int64_t)rows + 31) / 32;
+  const int64_t nwarps = (int64_t)gridDim.x * (kStreamThreads / 32);
+  for (int64_t wb = (int64_t)blockIdx.x * (kStreamThreads / 32) + wib; wb < nblk; wb += nwarps) {
+    const int64_t r = wb * 32 + lane;
+    const bool active = r < rows;
+    const int32_t rs = active ? rowPtr[r] : 0, re = active ? rowPtr[r + 1] : 0;
+    const int32_t base = __shfl_sync(0xffffffffu, rs, 0);
+    const int64_t last = min((int64_t)rows, wb * 32 + 32) - 1 - wb * 32;   // last active lane
+    const int32_t end = __shfl_sync(0xffffffffu, re, (int)last);
+    A sum = A(0);
+    for (int32_t pb = base; pb < end; pb += kStreamPiece) {   // warp-uniform
+      int32_t c[K];
+      V a[K];
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        const int32_t j = pb + k * 32 + lane;
+        c[k] = j < end ? colIdx[j] : -1;
+        a[k] = j < end ? val[j] : V(0);
+      }
+#pragma unroll
+      for (int k = 0; k < K; ++k)
+        if (c[k] >= 0) pw[k * 32 + lane] = mul_rn(to_acc<V>(a[k]), to_acc<V>(__ldg(&x[c[k]])));
+      __syncwarp();
+      const int32_t lo = rs > pb ? rs : pb;
+      const int32_t hi = re < pb + kStreamPiece ? re : pb + kStreamPiece;
+      for (int32_t j = lo; j < hi; ++j) sum = add_rn(sum, pw[j - pb]);
+      __syncwarp();
+    }
+    if (active) {
+      if (alpha == A(1) && beta == A(0))
+        y[r] = from_acc<V>(sum);
+      else
+        store_y<V, A>(y, r, sum, alpha, beta);
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Merge-path SpMV (FP64).  Merge items are the rows' end offsets
 // (rowPtr[1..rows]) interleaved with the nnz indices 0..nnz-1; every thread
@@ -281,6 +345,19 @@ static bsp_status launch_scalar(int32_t rows, const int32_t *rp, const int32_t *
   return BSP_OK;
 }
 
+template <typename V>
+static bsp_status launch_stream(int32_t rows, const int32_t *rp, const int32_t *ci, const V *v, const V *x, V *y,
+                                typename AccOf<V>::T a, typename AccOf<V>::T b, cudaStream_t s) {
+  const int64_t warps = ceil_div(rows, 32);
+  int64_t blocks = ceil_div(warps, kStreamThreads / 32);
+  const int64_t cap = (int64_t)sm_count() * 32;
+  if (blocks > cap) blocks = cap;
+  if (blocks < 1) blocks = 1;
+  csr_stream_kernel<V><<<(unsigned)blocks, kStreamThreads, 0, s>>>(rows, rp, ci, v, x, y, a, b);
+  BSP_LAUNCH_CHECK();
+  return BSP_OK;
+}
+
 // Lanes per row from the mean row length: one lane per row up to 8 entries
 // (those are loaded together), then the smallest power of two >= mean/4,
 // up to 32.
@@ -298,6 +375,7 @@ static bsp_status csr_dispatch(int32_t rows, int32_t nnz, const int32_t *rp, con
                                cudaStream_t s) {
   using A = typename AccOf<V>::T;
   if (algo == BSP_CSR_SCALAR) return launch_scalar<V>(rows, rp, ci, v, x, y, (A)alpha, (A)beta, s);
+  if (algo == BSP_CSR_STREAM) return launch_stream<V>(rows, rp, ci, v, x, y, (A)alpha, (A)beta, s);
   if (lpr <= 0) lpr = auto_lanes(rows, nnz);
   return launch_vector<V>(lpr, rows, rp, ci, v, x, y, (A)alpha, (A)beta, s);
 }
@@ -358,7 +436,7 @@ extern "C" bsp_status bsp_csr_spmv(int32_t rows, int32_t cols, int32_t nnz, cons
     // with lanes from the mean.  Plans pick MERGE from measured features.
     algo = BSP_CSR_VECTOR;
   }
-  BSP_CHECK_ARG(algo == BSP_CSR_VECTOR || algo == BSP_CSR_SCALAR, "unknown algo");
+  BSP_CHECK_ARG(algo == BSP_CSR_VECTOR || algo == BSP_CSR_SCALAR || algo == BSP_CSR_STREAM, "unknown algo");
   switch (dtype) {
     case BSP_F64:
       return csr_dispatch<double>(rows, nnz, rowPtr, colIdx, (const double *)values, (const double *)x,

@@ -1686,6 +1686,28 @@ __global__ void spmm_short_key_kernel(int32_t rows, const int32_t *__restrict__ 
   }
 }
 
+// Nonzero ranges for the slab engine: (start, end) of each partial-row
+// slot's chunk and of each listed short row.
+__global__ void spmm_range_kernel(int64_t nparts, const int32_t *__restrict__ long_chunk,
+                                  const int32_t *__restrict__ chunk_row, const int32_t *__restrict__ chunk_ptr,
+                                  int32_t chunk, int32_t nshort, const int32_t *__restrict__ short_rows,
+                                  const int32_t *__restrict__ rowPtr, int2 *__restrict__ long_se,
+                                  int2 *__restrict__ short_se) {
+  const int64_t n = nparts > nshort ? nparts : nshort;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    if (i < nparts) {
+      const int32_t w = long_chunk[i];
+      const int32_t r = chunk_row[w];
+      const int32_t st = rowPtr[r] + (w - chunk_ptr[r]) * chunk;
+      long_se[i] = make_int2(st, min(st + chunk, rowPtr[r + 1]));
+    }
+    if (i < nshort) {
+      const int32_t r = short_rows[i];
+      short_se[i] = make_int2(rowPtr[r], rowPtr[r + 1]);
+    }
+  }
+}
+
 __global__ void spmm_split_flag_kernel(int32_t rows, const int32_t *__restrict__ chunk_ptr,
                                        int32_t *__restrict__ flag) {
   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r <= rows; r += (int64_t)gridDim.x * blockDim.x)
@@ -1755,6 +1777,17 @@ extern "C" bsp_status bsp_spmm_plan_create(int32_t rows, int32_t nnz, const int3
     dfree(keys, s);
     BSP_TRY(st);
   }
+  BSP_TRY(dalloc(&p.long_se, (size_t)2 * (p.nparts > 0 ? p.nparts : 1), s));
+  BSP_TRY(dalloc(&p.short_se, (size_t)2 * (p.nshort > 0 ? p.nshort : 1), s));
+  if (p.nparts > 0 || p.nshort > 0) {
+    const int64_t n = std::max<int64_t>(p.nparts, p.nshort);
+    const unsigned gr = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div(n, 256), (int64_t)sm_count() * 32));
+    spmm_range_kernel<<<gr, 256, 0, s>>>(p.nparts, p.long_chunk, p.chunk_row, p.chunk_ptr, chunk, p.nshort,
+                                         p.short_rows, rowPtr, reinterpret_cast<int2 *>(p.long_se),
+                                         reinterpret_cast<int2 *>(p.short_se));
+    BSP_LAUNCH_CHECK();
+  }
+  p.slab_l2_hints = 1;
   BSP_CUDA(cudaStreamSynchronize(s));
   *out = p;
   return BSP_OK;
@@ -1770,6 +1803,8 @@ extern "C" bsp_status bsp_spmm_plan_free(bsp_spmm_plan *p) {
   dfree(p->split_rows, s);
   dfree(p->short_rows, s);
   dfree(p->long_chunk, s);
+  dfree(p->long_se, s);
+  dfree(p->short_se, s);
   BSP_CUDA(cudaStreamSynchronize(s));
   return BSP_OK;
 }
@@ -1879,26 +1914,71 @@ static bsp_status chunked_typed(const bsp_spmm_plan *p, int32_t N, const int32_t
 // B's slab (B rows x NS) is small enough to stay in L2 for the whole pass, so
 // every gathered B row after the first touch is an L2 hit, at the price of
 // reading A once per slab.  Warp tasks [0, nlong) are the long rows' chunks,
-// a warp each (the grouped segment: G groups of LPR lanes split the chunk's
-// nonzeros, then a fixed shuffle tree), written to their partial-row slot;
-// the remaining tasks take G consecutive rows of the length-sorted short-row
-// list, one row per group of LPR lanes, so a warp has G rows' load chains in
-// flight at once instead of one.  A group issues the column index and value
-// loads of its next U nonzeros before the U gathers of the current ones are
-// consumed.
+// a warp each (G groups of LPR lanes split the chunk's nonzeros, then a
+// fixed shuffle tree), written to their partial-row slot; the remaining tasks
+// take G consecutive rows of the length-sorted short-row list, one row per
+// group of LPR lanes, so a warp has G rows' load chains in flight at once
+// instead of one.  Every task reads its nonzero range from the plan in one
+// load (no slot -> chunk -> row -> rowPtr walk).  A chunk's next 32 column
+// indices and values are loaded before the current 32 gathers are consumed;
+// a short row's group loads its next U entries the same way.  With `hints`
+// (bsp_spmm_plan.slab_l2_hints) 1 or 2, A's entries are loaded and C is
+// stored evict-first, so the streamed A and C do not push the slab out of L2
+// during the pass; with 1 the B rows are also gathered evict-last.
+__device__ __forceinline__ uint64_t l2_policy(bool on, bool keep) {
+  uint64_t p;
+  if (!on)
+    asm volatile("createpolicy.fractional.L2::evict_normal.b64 %0, 1.0;" : "=l"(p));
+  else if (keep)
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  else
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ int32_t ld_hint_s32(const int32_t *p, uint64_t pol) {
+  int32_t r;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.s32 %0, [%1], %2;" : "=r"(r) : "l"(p), "l"(pol));
+  return r;
+}
+template <typename T> __device__ __forceinline__ float ld_hint_val(const T *p, uint64_t pol);
+template <> __device__ __forceinline__ float ld_hint_val<float>(const float *p, uint64_t pol) {
+  float r;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(r) : "l"(p), "l"(pol));
+  return r;
+}
+template <> __device__ __forceinline__ float ld_hint_val<__half>(const __half *p, uint64_t pol) {
+  unsigned short r;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.u16 %0, [%1], %2;" : "=h"(r) : "l"(p), "l"(pol));
+  return __half2float(__ushort_as_half(r));
+}
+template <> __device__ __forceinline__ float ld_hint_val<__nv_bfloat16>(const __nv_bfloat16 *p, uint64_t pol) {
+  unsigned short r;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.u16 %0, [%1], %2;" : "=h"(r) : "l"(p), "l"(pol));
+  return __bfloat162float(__ushort_as_bfloat16(r));
+}
+__device__ __forceinline__ uint4 ld_hint_b16(const void *p, uint64_t pol) {
+  uint4 r;
+  asm("ld.global.nc.L2::cache_hint.v4.u32 {%0,%1,%2,%3}, [%4], %5;"
+      : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
+      : "l"(p), "l"(pol));
+  return r;
+}
+
 template <typename T, int LPR, int U>
-__global__ void __launch_bounds__(256) spmm_slab_kernel(
-    int64_t nlong, const int32_t *__restrict__ long_chunk, const int32_t *__restrict__ chunk_row,
-    const int32_t *__restrict__ chunk_ptr, int32_t chunk, int32_t nshort, const int32_t *__restrict__ short_rows,
-    const int32_t *__restrict__ rowPtr, const int32_t *__restrict__ colIdx, const T *__restrict__ val,
+__global__ void __launch_bounds__(256, LPR >= 8 && LPR <= 16 ? (std::is_same<T, __nv_bfloat16>::value ? 4 : 5) : 0)
+    spmm_slab_kernel(
+    int64_t nlong, const int2 *__restrict__ long_se, int32_t nshort, const int32_t *__restrict__ short_rows,
+    const int2 *__restrict__ short_se, const int32_t *__restrict__ colIdx, const T *__restrict__ val,
     const T *__restrict__ B, int64_t ldb, int32_t col0, float *__restrict__ C, int64_t ldc,
-    float *__restrict__ part, float alpha, float beta) {
+    float *__restrict__ part, float alpha, float beta, int32_t hints) {
   constexpr int VEC = SpmmVec<T>::VEC;
   constexpr int NS = LPR * VEC;
   constexpr int G = 32 / LPR;
   const int lane = threadIdx.x & 31;
   const int li = lane % LPR;
+  const int g = lane / LPR;
   const int32_t cl = col0 + li * VEC;
+  const uint64_t pa = l2_policy(hints != 0, false), pb = l2_policy(hints == 1, true);
   const int64_t ntasks = nlong + (nshort + G - 1) / G;
   const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
   for (int64_t task = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; task < ntasks; task += nwarps) {
@@ -1906,11 +1986,63 @@ __global__ void __launch_bounds__(256) spmm_slab_kernel(
 #pragma unroll
     for (int k = 0; k < VEC; ++k) acc[k] = 0.f;
     if (task < nlong) {   // warp-uniform
-      const int32_t w = long_chunk[task];
-      const int32_t r = chunk_row[w];
-      const int32_t s = rowPtr[r] + (w - chunk_ptr[r]) * chunk;
-      const int32_t e = min(s + chunk, rowPtr[r + 1]);
-      spmm_segment<T, LPR>(s, e, colIdx, val, B, ldb, cl, lane, acc);
+      // Batches of BQ = 32*Q nonzeros: Q = 1 while a warp step's G*U gathers
+      // fit in 32 (LPR >= 4), else one step takes the whole batch, so narrow
+      // B rows still keep G*U gathers in flight per warp.
+      constexpr int GU = G * kSpmmU;
+      constexpr int Q = GU > 32 ? GU / 32 : 1;
+      constexpr int BQ = 32 * Q;
+      const int2 se = long_se[task];
+      const int32_t e = se.y;
+      int32_t cj[Q];
+      float vj[Q];
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        const int32_t j = se.x + q * 32 + lane;
+        cj[q] = j < e ? ld_hint_s32(colIdx + j, pa) : 0;
+        vj[q] = j < e ? ld_hint_val<T>(val + j, pa) : 0.f;
+      }
+      for (int32_t j0 = se.x; j0 < e; j0 += BQ) {   // warp-uniform bounds
+        int32_t cn[Q];
+        float vn[Q];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+          const int32_t jn = j0 + BQ + q * 32 + lane;
+          cn[q] = jn < e ? ld_hint_s32(colIdx + jn, pa) : 0;
+          vn[q] = jn < e ? ld_hint_val<T>(val + jn, pa) : 0.f;
+        }
+        const int cnt = e - j0 < BQ ? e - j0 : BQ;
+        for (int t = 0; t < cnt; t += GU) {   // one trip when Q > 1
+          uint4 raw[kSpmmU];
+          float v[kSpmmU];
+#pragma unroll
+          for (int u = 0; u < kSpmmU; ++u) {
+            const int src = t + u * G + g;
+            const int q = Q > 1 ? (u * G) >> 5 : 0;   // t == 0 when Q > 1
+            const int32_t c = __shfl_sync(0xffffffffu, cj[q], src & 31);
+            const float vv = __shfl_sync(0xffffffffu, vj[q], src & 31);
+            const bool ok = src < cnt;
+            v[u] = ok ? vv : 0.f;
+            raw[u] = ok ? ld_hint_b16(B + (int64_t)c * ldb + cl, pb) : make_uint4(0, 0, 0, 0);
+          }
+#pragma unroll
+          for (int u = 0; u < kSpmmU; ++u) {
+            float b[VEC];
+            unpack16<T>(raw[u], b);
+#pragma unroll
+            for (int k = 0; k < VEC; ++k) acc[k] = fmaf(v[u], b[k], acc[k]);
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+          cj[q] = cn[q];
+          vj[q] = vn[q];
+        }
+      }
+#pragma unroll
+      for (int o = LPR; o < 32; o <<= 1)
+#pragma unroll
+        for (int k = 0; k < VEC; ++k) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
       if (lane < LPR) {
         float *pp = part + task * NS + li * VEC;
 #pragma unroll
@@ -1918,17 +2050,18 @@ __global__ void __launch_bounds__(256) spmm_slab_kernel(
       }
       continue;
     }
-    const int64_t i = (task - nlong) * G + lane / LPR;
+    const int64_t i = (task - nlong) * G + g;
     if (i >= nshort) continue;
     const int32_t r = short_rows[i];
-    const int32_t s = rowPtr[r], e = rowPtr[r + 1];
+    const int2 se = short_se[i];
+    const int32_t s = se.x, e = se.y;
     int32_t cn[U];
     float vn[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const bool ok = s + u < e;
-      cn[u] = ok ? __ldg(colIdx + s + u) : 0;
-      vn[u] = ok ? sp_to_float<T>(__ldg(val + s + u)) : 0.f;
+      cn[u] = ok ? ld_hint_s32(colIdx + s + u, pa) : 0;
+      vn[u] = ok ? ld_hint_val<T>(val + s + u, pa) : 0.f;
     }
     for (int32_t j = s; j < e; j += U) {
       uint4 raw[U];
@@ -1936,15 +2069,14 @@ __global__ void __launch_bounds__(256) spmm_slab_kernel(
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         v[u] = vn[u];
-        raw[u] = j + u < e ? __ldg(reinterpret_cast<const uint4 *>(B + (int64_t)cn[u] * ldb + cl))
-                           : make_uint4(0, 0, 0, 0);
+        raw[u] = j + u < e ? ld_hint_b16(B + (int64_t)cn[u] * ldb + cl, pb) : make_uint4(0, 0, 0, 0);
       }
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         const int32_t jj = j + U + u;
         const bool ok = jj < e;
-        cn[u] = ok ? __ldg(colIdx + jj) : 0;
-        vn[u] = ok ? sp_to_float<T>(__ldg(val + jj)) : 0.f;
+        cn[u] = ok ? ld_hint_s32(colIdx + jj, pa) : 0;
+        vn[u] = ok ? ld_hint_val<T>(val + jj, pa) : 0.f;
       }
 #pragma unroll
       for (int u = 0; u < U; ++u) {
@@ -1955,19 +2087,27 @@ __global__ void __launch_bounds__(256) spmm_slab_kernel(
       }
     }
     float *cp = C + (int64_t)r * ldc + cl;
+    if (beta != 0.f) {
 #pragma unroll
-    for (int k = 0; k < VEC; ++k) {
-      float o = alpha * acc[k];
-      if (beta != 0.f) o += beta * cp[k];
-      cp[k] = o;
+      for (int k = 0; k < VEC; ++k) {
+        float o = alpha * acc[k];
+        o += beta * cp[k];
+        cp[k] = o;
+      }
+    } else if (hints) {
+#pragma unroll
+      for (int k = 0; k < VEC; ++k) __stcs(cp + k, alpha * acc[k]);
+    } else {
+#pragma unroll
+      for (int k = 0; k < VEC; ++k) cp[k] = alpha * acc[k];
     }
   }
 }
 
 template <typename T, int LPR>
-static bsp_status launch_slab(const bsp_spmm_plan *p, const int32_t *rp, const int32_t *ci, const void *val,
-                              const void *B, int64_t ldb, int32_t col0, float *C, int64_t ldc, float *part, float a,
-                              float b, cudaStream_t s) {
+static bsp_status launch_slab(const bsp_spmm_plan *p, const int32_t *ci, const void *val, const void *B,
+                              int64_t ldb, int32_t col0, float *C, int64_t ldc, float *part, float a, float b,
+                              int32_t hints, cudaStream_t s) {
   constexpr int G = 32 / LPR;
   const int64_t ntasks = p->nparts + (p->nshort + G - 1) / G;
   int64_t blocks = ceil_div(ntasks, 8);
@@ -1975,8 +2115,9 @@ static bsp_status launch_slab(const bsp_spmm_plan *p, const int32_t *rp, const i
   if (blocks > cap) blocks = cap;
   if (blocks < 1) blocks = 1;
   spmm_slab_kernel<T, LPR, 4><<<(unsigned)blocks, 256, 0, s>>>(
-      p->nparts, p->long_chunk, p->chunk_row, p->chunk_ptr, p->chunk, p->nshort, p->short_rows, rp, ci,
-      (const T *)val, (const T *)B, ldb, col0, C, ldc, part, a, b);
+      p->nparts, reinterpret_cast<const int2 *>(p->long_se), p->nshort, p->short_rows,
+      reinterpret_cast<const int2 *>(p->short_se), ci, (const T *)val, (const T *)B, ldb, col0, C, ldc, part, a, b,
+      hints);
   BSP_LAUNCH_CHECK();
   return BSP_OK;
 }
@@ -2005,20 +2146,27 @@ static int slab_width(int32_t N, int32_t cols, const void *B, int64_t ldb, int32
   return l * VEC;
 }
 
+// The plan's L2 hints apply to slabs of B of at most kHintSlabBytes
+// (cols x slab width), the size that stays in L2 during a pass; wider slabs
+// gather with default caching (graph 2^20, FP16: hints at N = 32 (64 MB)
+// 0.489 -> 0.473 ms, at N = 128 (one 268 MB slab) 1.822 -> 1.853 ms).
+constexpr double kHintSlabBytes = 64.0 * 1024 * 1024;
+
 template <typename T>
-static bsp_status slab_typed(const bsp_spmm_plan *p, int32_t N, int32_t ns, const int32_t *rp, const int32_t *ci,
+static bsp_status slab_typed(const bsp_spmm_plan *p, int32_t N, int32_t cols, int32_t ns, const int32_t *ci,
                              const void *val, const void *B, int64_t ldb, float *C, int64_t ldc, float *part,
                              float a, float b, cudaStream_t s) {
   constexpr int VEC = SpmmVec<T>::VEC;
+  const int32_t hints = (double)cols * ns * sizeof(T) <= kHintSlabBytes ? p->slab_l2_hints : 0;
   for (int32_t col0 = 0; col0 < N; col0 += ns) {
     bsp_status st;
     switch (ns / VEC) {
-      case 32: st = launch_slab<T, 32>(p, rp, ci, val, B, ldb, col0, C, ldc, part, a, b, s); break;
-      case 16: st = launch_slab<T, 16>(p, rp, ci, val, B, ldb, col0, C, ldc, part, a, b, s); break;
-      case 8: st = launch_slab<T, 8>(p, rp, ci, val, B, ldb, col0, C, ldc, part, a, b, s); break;
-      case 4: st = launch_slab<T, 4>(p, rp, ci, val, B, ldb, col0, C, ldc, part, a, b, s); break;
-      case 2: st = launch_slab<T, 2>(p, rp, ci, val, B, ldb, col0, C, ldc, part, a, b, s); break;
-      case 1: st = launch_slab<T, 1>(p, rp, ci, val, B, ldb, col0, C, ldc, part, a, b, s); break;
+      case 32: st = launch_slab<T, 32>(p, ci, val, B, ldb, col0, C, ldc, part, a, b, hints, s); break;
+      case 16: st = launch_slab<T, 16>(p, ci, val, B, ldb, col0, C, ldc, part, a, b, hints, s); break;
+      case 8: st = launch_slab<T, 8>(p, ci, val, B, ldb, col0, C, ldc, part, a, b, hints, s); break;
+      case 4: st = launch_slab<T, 4>(p, ci, val, B, ldb, col0, C, ldc, part, a, b, hints, s); break;
+      case 2: st = launch_slab<T, 2>(p, ci, val, B, ldb, col0, C, ldc, part, a, b, hints, s); break;
+      case 1: st = launch_slab<T, 1>(p, ci, val, B, ldb, col0, C, ldc, part, a, b, hints, s); break;
       default: BSP_FAIL(BSP_ERR_UNSUPPORTED, "slab width");
     }
     BSP_TRY(st);
@@ -2104,10 +2252,10 @@ static bsp_status spmm_planned_impl(const bsp_spmm_plan *p, int32_t cols, int32_
   if (ns > 0) {
     if (nnz > 0 && !(colIdx && values && B)) BSP_FAIL(BSP_ERR_INVALID, "null pointer");
     switch (dtype) {
-      case BSP_F16: return slab_typed<__half>(p, N, ns, rowPtr, colIdx, values, B, ldb, C, ldc, part, alpha, beta, s);
+      case BSP_F16: return slab_typed<__half>(p, N, cols, ns, colIdx, values, B, ldb, C, ldc, part, alpha, beta, s);
       case BSP_BF16:
-        return slab_typed<__nv_bfloat16>(p, N, ns, rowPtr, colIdx, values, B, ldb, C, ldc, part, alpha, beta, s);
-      default: return slab_typed<float>(p, N, ns, rowPtr, colIdx, values, B, ldb, C, ldc, part, alpha, beta, s);
+        return slab_typed<__nv_bfloat16>(p, N, cols, ns, colIdx, values, B, ldb, C, ldc, part, alpha, beta, s);
+      default: return slab_typed<float>(p, N, cols, ns, colIdx, values, B, ldb, C, ldc, part, alpha, beta, s);
     }
   }
   switch (dtype) {

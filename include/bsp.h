@@ -90,7 +90,12 @@ typedef enum {
   BSP_CSR_AUTO = 0,
   BSP_CSR_VECTOR = 1,
   BSP_CSR_MERGE = 2,
-  BSP_CSR_SCALAR = 3 /* one thread per row, summing left to right */
+  BSP_CSR_SCALAR = 3, /* one thread per row, summing left to right */
+  /* a warp per 32 consecutive rows: their nonzero range loaded coalesced in
+   * 256-entry pieces, all x gathers of a piece in flight at once, products
+   * through shared memory, each row summed left to right by its lane with
+   * separately rounded multiply and add (the same results as SCALAR) */
+  BSP_CSR_STREAM = 4
 } bsp_csr_algo;
 
 /* Values, x and y all have `dtype` storage; F64 accumulates in FP64, the
@@ -446,6 +451,14 @@ typedef struct {
   int32_t nshort;      /* rows of at most `chunk` nonzeros (empty rows included) */
   int32_t *short_rows; /* [nshort] those rows, longest first (stable) */
   int32_t *long_chunk; /* [nparts] chunk index of each partial-row slot */
+  int32_t *long_se;    /* [2*nparts] (start, end) nonzero range of each slot's chunk */
+  int32_t *short_se;   /* [2*nshort] (start, end) nonzero range of each listed short row */
+  int32_t slab_l2_hints; /* slab engine cache policy for slabs of B of at most 64 MiB
+                            (cols x slab width; wider slabs use default caching), set to
+                            1 by bsp_spmm_plan_create: 1 = A's entries loaded and C
+                            stored as evict-first, the gathered B slab rows as
+                            evict-last, so the slab stays in L2 for the pass; 2 = A and
+                            C evict-first, B default; 0 = default caching */
 } bsp_spmm_plan;
 
 bsp_status bsp_spmm_plan_create(int32_t rows, int32_t nnz, const int32_t *rowPtr,

@@ -33,6 +33,55 @@ def test_scalar_fp64_is_bit_exact_with_reference(cuda, golden, name):
 
 
 @pytest.mark.parametrize("name", SPMV)
+def test_stream_is_bit_exact_with_reference(cuda, golden, name):
+    """The warp-per-32-rows stream kernel sums each row left to right with
+    separately rounded multiply and add: the reference's own results, bit for
+    bit, in FP64, FP32 and FP16."""
+    import torch
+    g = golden(name)
+    rp, ci, va, x = _dev(cuda, g["rowptr"], g["colidx"], g["values"], g["x"])
+    y = bsp.csr_spmv(rp, ci, va, x, algo="stream").cpu().numpy()
+    assert np.array_equal(y.view(np.uint64), g["y_fp64"].view(np.uint64))
+    v32 = torch.from_numpy(g["values"].astype(np.float32)).to(cuda)
+    x32 = torch.from_numpy(g["x"].astype(np.float32)).to(cuda)
+    y32 = bsp.csr_spmv(rp, ci, v32, x32, algo="stream").cpu().numpy()
+    assert np.array_equal(y32.view(np.uint32), g["y_fp32"].view(np.uint32))
+    y16 = bsp.csr_spmv(rp, ci, v32.half(), x32.half(), algo="stream").float().cpu().numpy()
+    assert np.array_equal(y16.view(np.uint32), g["y_fp16"].view(np.uint32))
+
+
+def test_stream_long_rows_bit_exact(cuda):
+    """Rows far longer than a 256-entry piece (and warps whose 32 rows span
+    many pieces) give the scalar kernel's results exactly."""
+    A = bsp.gen_powerlaw(200000, 1.6, 100000, 12)
+    assert np.diff(A.rowptr).max() > 10000
+    x = bsp.gen_uniform(A.cols, 13)
+    ref = pyoracle.spmv_f64(A.rowptr, A.colidx, A.values, x)
+    rp, ci, va, xx = _dev(cuda, A.rowptr, A.colidx, A.values, x)
+    y = bsp.csr_spmv(rp, ci, va, xx, algo="stream").cpu().numpy()
+    assert np.array_equal(y, ref)
+    ys = bsp.csr_spmv(rp, ci, va, xx, algo="scalar").cpu().numpy()
+    assert np.array_equal(y, ys)
+
+
+@pytest.mark.parametrize("rows", [1, 31, 33, 1000])
+def test_stream_ragged_tail_warp(cuda, rows):
+    """Row counts that leave the last warp partly empty."""
+    rng = np.random.default_rng(rows)
+    lens = rng.integers(0, 40, rows)
+    rp = np.zeros(rows + 1, np.int32)
+    rp[1:] = np.cumsum(lens)
+    cols = 500
+    ci = np.concatenate([np.sort(rng.choice(cols, l, replace=False)) for l in lens]).astype(np.int32)
+    va = rng.standard_normal(ci.size)
+    x = rng.uniform(-1, 1, cols)
+    ref = pyoracle.spmv_f64(rp, ci, va, x)
+    d = _dev(cuda, rp, ci, va, x)
+    y = bsp.csr_spmv(*d, algo="stream").cpu().numpy()
+    assert np.array_equal(y, ref)
+
+
+@pytest.mark.parametrize("name", SPMV)
 @pytest.mark.parametrize("algo,lanes", [("vector", 0), ("vector", 1), ("vector", 4), ("vector", 32),
                                         ("merge", 0)])
 def test_fp64_kernels_within_rounding_bound(cuda, golden, name, algo, lanes):
@@ -75,14 +124,14 @@ def test_reduced_precision_vector_kernels(cuda, dt):
     _within(y, ref, tol * 1.01)
 
 
-@pytest.mark.parametrize("algo", ["vector", "merge", "scalar"])
+@pytest.mark.parametrize("algo", ["vector", "merge", "scalar", "stream"])
 def test_laplace_512_config(cuda, algo):
     A = bsp.gen_laplace2d(512, 512)
     x = bsp.gen_uniform(A.cols, 20261203)
     ref = pyoracle.spmv_f64(A.rowptr, A.colidx, A.values, x)
     rp, ci, va, xx = _dev(cuda, A.rowptr, A.colidx, A.values, x)
     y = bsp.csr_spmv(rp, ci, va, xx, algo=algo).cpu().numpy()
-    if algo == "scalar":
+    if algo in ("scalar", "stream"):
         assert np.array_equal(y, ref)
     else:
         _within(y, ref, pyoracle.spmv_tolerance(A.rowptr, A.colidx, A.values, x))
@@ -99,7 +148,7 @@ def test_merge_path_power_law_long_rows(cuda):
     _within(bsp.csr_spmv(rp, ci, va, xx, algo="vector", lanes=32).cpu().numpy(), ref, tol)
 
 
-@pytest.mark.parametrize("algo", ["vector", "merge", "scalar"])
+@pytest.mark.parametrize("algo", ["vector", "merge", "scalar", "stream"])
 def test_alpha_beta_and_empty_rows(cuda, algo):
     import torch
     rng = np.random.default_rng(0)
@@ -127,7 +176,7 @@ def test_empty_matrix(cuda):
     ci = torch.zeros(0, dtype=torch.int32, device=cuda)
     va = torch.zeros(0, dtype=torch.float64, device=cuda)
     x = torch.ones(100, dtype=torch.float64, device=cuda)
-    for algo in ("vector", "merge", "scalar"):
+    for algo in ("vector", "merge", "scalar", "stream"):
         y = torch.full((100,), 7.0, dtype=torch.float64, device=cuda)
         bsp.csr_spmv(rp, ci, va, x, y=y, algo=algo)
         assert torch.all(y == 0)

@@ -268,6 +268,39 @@ def test_spmm_slab_engine_matches_fp64(cuda, name, N, slab):
     P.spmm(Bd, Cd, alpha=0.5, beta=-1.5, engine="slab", slab_cols=slab)
     want = 0.5 * Cref - 1.5 * Cin.astype(np.float64)
     assert np.all(np.abs(Cd.cpu().numpy().astype(np.float64) - want) <= _tol(A, absC, 0.5, Cin, -1.5))
+    # the L2 cache policies change where lines stay, not the sums
+    for hints in (0, 2, 1):
+        P.slab_l2_hints = hints
+        assert torch.equal(C1, P.spmm(Bd, engine="slab", slab_cols=slab))
+    P.free()
+
+
+def test_spmm_plan_ranges_match_row_pointers(cuda):
+    """The plan's per-slot and per-short-row nonzero ranges agree with the
+    row pointers: long-row chunks tile each split row in order, and the
+    short-row list is sorted longest first with each row's own range."""
+    rng = np.random.default_rng(3)
+    n = 3000
+    lens = rng.integers(0, 30, n)
+    lens[[5, 700, 2999]] = [1000, 257, 2900]
+    rp = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    ci = np.concatenate([np.sort(rng.choice(n, l, replace=False)) for l in lens]).astype(np.int32)
+    import torch
+    rpd, cid = _dev(cuda, rp, ci)
+    v = torch.ones(int(rp[-1]), dtype=torch.float16, device=cuda)
+    P = bsp.SpmmPlan(rpd, cid, v, cols=n, chunk=256)
+    d = P._d
+    from benchsp_b200.api import _d2h
+    long_se = _d2h(d.long_se, 2 * d.nparts, np.int32).reshape(-1, 2)
+    short_se = _d2h(d.short_se, 2 * d.nshort, np.int32).reshape(-1, 2)
+    short_rows = _d2h(d.short_rows, d.nshort, np.int32)
+    split = np.flatnonzero(lens > 256)
+    want_long = [(rp[r] + k * 256, min(rp[r] + (k + 1) * 256, rp[r + 1]))
+                 for r in split for k in range((lens[r] + 255) // 256)]
+    assert sorted(map(tuple, long_se.tolist())) == sorted(want_long)
+    assert np.array_equal(short_se[:, 0], rp[short_rows]) and np.array_equal(short_se[:, 1], rp[short_rows + 1])
+    ln = lens[short_rows]
+    assert np.all(ln[:-1] >= ln[1:]) and set(short_rows.tolist()) == set(np.flatnonzero(lens <= 256).tolist())
     P.free()
 
 
