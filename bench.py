@@ -1211,13 +1211,17 @@ def run_profile(args) -> None:
         C_out = torch.empty(A.rows, 128, dtype=torch.float32, device=dev)
         for _ in range(reps):
             bsp.spmm_csr(rp, ci, v, B, C_out)
-    elif w == "batch":   # the 512-matrix batch, FP64, one RHS
+    elif w in ("batch", "batch8"):   # the 512-matrix batch, FP64, one RHS (batch8: 8 right-hand sides)
         mats = bsp.gen_batch(512, SEED + 6)
+        nrhs = 8 if w == "batch8" else 1
         d = []
         for m in mats:
-            rp, ci, va, x = up(m.rowptr, m.colidx, m.values, bsp.gen_uniform(m.cols, 1))
-            d.append((rp, ci, va, x, torch.empty(m.rows, dtype=torch.float64, device=dev)))
-        P = bsp.BatchPlan(d, use_graph=False)
+            rp, ci, va = up(m.rowptr, m.colidx, m.values)
+            shp = (m.cols, nrhs) if nrhs > 1 else (m.cols,)
+            x = (torch.rand(shp, generator=torch.Generator().manual_seed(1), dtype=torch.float64) * 2 - 1).to(dev)
+            d.append((rp, ci, va, x, torch.empty((m.rows, nrhs) if nrhs > 1 else (m.rows,), dtype=torch.float64,
+                                                 device=dev)))
+        P = bsp.BatchPlan(d, nrhs=nrhs, use_graph=False)
         for _ in range(reps):
             P.run()
     else:
@@ -1239,7 +1243,7 @@ def main():
                     "smaller values only for profiling captures)")
     ap.add_argument("--profile", choices=["dasp", "cg_fp64", "cg_f16", "spmm", "batch", "smat_tc", "smat_mma", "csr",
                                           "pcg_bj", "spmm_grouped", "cg_multi", "smat_tc_w64", "smat_tc_w128",
-                                          "bsr_scaled", "smat_tcp", "smat_tcp_w64"],
+                                          "bsr_scaled", "smat_tcp", "smat_tcp_w64", "batch8"],
                     help="a few calls of one workload's kernels (for ncu captures)")
     ap.add_argument("--pn", type=int, default=0, help="columns of B for the SpMM profile workloads "
                     "(default 128 for spmm, 256 for the smat ones)")

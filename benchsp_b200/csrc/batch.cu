@@ -20,6 +20,10 @@
 // Run: warps take items from a global counter; the long segments come first in
 // the list so the critical path starts at time zero.  Counter reset + kernel
 // are captured once in a CUDA graph.
+//
+// With 8 right-hand sides (x, y row-major n x 8) the lanes of a row split its
+// columns into 16-byte pieces and its nonzeros as above; FP64 SELL slices
+// stage their window of x rows in shared memory (see sell_item_piece).
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -48,7 +52,14 @@ struct BatchMatDev {
   const int32_t *sell_perm;
   const int32_t *sell_col;
   int32_t sell_rows;
+  // narrow form with several right-hand sides: per slice the lowest column
+  // its entries (padding included) touch when all of them lie in a window of
+  // kWinRows x rows from there, else -1; null when not built
+  const int32_t *sell_lo;
 };
+
+// x rows a warp stages per SELL slice (several right-hand sides).
+constexpr int kWinRows = 64;
 
 // info == kSellItem / kSellWideItem: SELL slices [a, b) (narrow / wide form).
 // info >= 0 otherwise: row item, rows [a, b), info = lanes per row.
@@ -276,6 +287,247 @@ __device__ __forceinline__ void sell_item(const BatchMatDev &M, int32_t s0, int3
   }
 }
 
+// ---------------------------------------------------------------------------
+// Several right-hand sides (x and y row-major, NRHS values per row): the
+// CPL = NRHS * sizeof(V) / 16 lanes of a row split its columns, one 16-byte
+// piece each, so a gathered x row is one contiguous access of the row's
+// lanes and a lane keeps VW = 16 / sizeof(V) sums instead of NRHS (FP64, 8
+// vectors: 4 lanes of 2 columns).  L lanes per row split the nonzeros as in
+// the one-vector items; each column is summed in the same order as there
+// (lane sub takes entries s+sub, s+sub+L, ... in order, then a fixed shuffle
+// tree over the L lanes).
+template <typename V> struct Piece { static constexpr int VW = 16 / (int)sizeof(V); };
+
+template <typename V>
+__device__ __forceinline__ void load_piece(const V *__restrict__ p, V (&o)[Piece<V>::VW]) {
+  if constexpr (sizeof(V) == 8) {
+    const double2 t = __ldg(reinterpret_cast<const double2 *>(p));
+    o[0] = t.x;
+    o[1] = t.y;
+  } else {
+    const float4 t = __ldg(reinterpret_cast<const float4 *>(p));
+    o[0] = t.x;
+    o[1] = t.y;
+    o[2] = t.z;
+    o[3] = t.w;
+  }
+}
+
+template <typename V>
+__device__ __forceinline__ void store_piece(V *p, const V (&v)[Piece<V>::VW]) {
+  if constexpr (sizeof(V) == 8)
+    *reinterpret_cast<double2 *>(p) = make_double2(v[0], v[1]);
+  else
+    *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+
+// acc (columns [cp*VW, cp*VW + VW)) += sum over entries j, j + stride, ... < e
+// in order, in predicated groups of U: a group's entry loads go out together,
+// then its U gathers together, so a short row costs one entries -> x round
+// trip instead of one per entry.
+template <typename V, int NRHS>
+__device__ __forceinline__ void strided_piece_dot(const int32_t *__restrict__ ci, const V *__restrict__ val,
+                                                  const V *__restrict__ x, int cp, int32_t j, int32_t e,
+                                                  int32_t stride, V (&acc)[Piece<V>::VW]) {
+  constexpr int VW = Piece<V>::VW;
+  constexpr int U = 4;
+  for (; j < e; j += U * stride) {
+    int32_t c[U];
+    V a[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const bool ok = j + u * stride < e;
+      c[u] = ok ? __ldg(ci + j + u * stride) : -1;
+      a[u] = ok ? __ldg(val + j + u * stride) : V(0);
+    }
+    V xr[U][VW];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (c[u] >= 0) {
+        load_piece<V>(x + (int64_t)c[u] * NRHS + cp * VW, xr[u]);
+      } else {
+#pragma unroll
+        for (int k = 0; k < VW; ++k) xr[u][k] = V(0);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      if (c[u] >= 0) {
+#pragma unroll
+        for (int k = 0; k < VW; ++k) acc[k] = fma(a[u], xr[u][k], acc[k]);
+      }
+  }
+}
+
+// The whole warp on one row: 32 / CPL nonzero lanes; every lane returns the
+// sums of its column piece.
+template <typename V, int NRHS>
+__device__ __forceinline__ void warp_row_piece(const int32_t *ci, const V *val, const V *x, int32_t s, int32_t e,
+                                               int lane, V (&acc)[Piece<V>::VW]) {
+  constexpr int VW = Piece<V>::VW;
+  constexpr int CPL = NRHS / VW;
+#pragma unroll
+  for (int k = 0; k < VW; ++k) acc[k] = V(0);
+  strided_piece_dot<V, NRHS>(ci, val, x, lane % CPL, s + lane / CPL, e, 32 / CPL, acc);
+#pragma unroll
+  for (int o = 16; o >= CPL; o >>= 1)
+#pragma unroll
+    for (int k = 0; k < VW; ++k) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
+}
+
+template <typename V, int NRHS, int L>
+__device__ __forceinline__ void rows_item_piece(const BatchMatDev &M, int32_t r0, int32_t r1, int32_t long_thr,
+                                                int lane) {
+  constexpr int VW = Piece<V>::VW;
+  constexpr int CPL = NRHS / VW;
+  constexpr int LT = CPL * L;   // lanes per row
+  static_assert(LT <= 32, "lanes per row");
+  constexpr int RPP = 32 / LT;
+  const int cp = lane % CPL, sub = (lane / CPL) % L, rl = lane / LT;
+  const V *val = static_cast<const V *>(M.val);
+  const V *x = static_cast<const V *>(M.x);
+  V *y = static_cast<V *>(M.y);
+  // the next pass's row pointers are loaded while this pass's rows are summed
+  int32_t ns = 0, ne = 0;
+  if (r0 + rl < r1) {
+    ns = __ldg(M.rp + r0 + rl);
+    ne = __ldg(M.rp + r0 + rl + 1);
+  }
+  for (int32_t base = r0; base < r1; base += RPP) {
+    const int32_t row = base + rl;
+    const bool active = row < r1;
+    int32_t s = ns, e = ne;
+    ns = ne = 0;
+    if (row + RPP < r1) {
+      ns = __ldg(M.rp + row + RPP);
+      ne = __ldg(M.rp + row + RPP + 1);
+    }
+    const int32_t len = e - s;
+    const bool mine = len <= kMedFactor * L && len <= long_thr;
+    const bool medium = active && len > kMedFactor * L && len <= long_thr;
+    if (!mine) e = s;
+    V acc[VW];
+#pragma unroll
+    for (int k = 0; k < VW; ++k) acc[k] = V(0);
+    strided_piece_dot<V, NRHS>(M.ci, val, x, cp, s + sub, e, L, acc);
+#pragma unroll
+    for (int o = L / 2; o > 0; o >>= 1)
+#pragma unroll
+      for (int k = 0; k < VW; ++k) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o * CPL);
+    if (active && sub == 0 && mine) store_piece<V>(y + (int64_t)row * NRHS + cp * VW, acc);
+    unsigned med = __ballot_sync(0xffffffffu, medium && sub == 0 && cp == 0);
+    while (med) {
+      const int b = __ffs(med) - 1;
+      med &= med - 1;
+      const int32_t mrow = base + b / LT;
+      const int32_t ms = __ldg(M.rp + mrow), me = __ldg(M.rp + mrow + 1);
+      V w[VW];
+      warp_row_piece<V, NRHS>(M.ci, val, x, ms, me, lane, w);
+      if (lane < CPL) store_piece<V>(y + (int64_t)mrow * NRHS + lane * VW, w);
+    }
+  }
+}
+
+// SELL-32 slices with several right-hand sides: a pass takes 32 / CPL of the
+// slice's rows, CPL lanes each; every row's entries in stored order.
+//
+// A narrow-form slice whose entries all lie in kWinRows x rows from
+// sell_lo[slice] (banded matrices) first copies that window of x into the
+// warp's shared-memory buffer `xw` (kWinRows * NRHS values, coalesced
+// 16-byte loads) and gathers from there: the 32 rows' overlapping x rows are
+// read once per slice instead of once per entry, and each entry's gather no
+// longer waits on L1/L2.  The arithmetic and its order are unchanged.
+template <typename V, int NRHS>
+__device__ __forceinline__ void fetch_piece(const V *__restrict__ x, const V *xw, int32_t lo, int32_t c, int cp,
+                                            V (&o)[Piece<V>::VW]) {
+  constexpr int VW = Piece<V>::VW;
+  if (lo >= 0) {
+    const V *p = xw + (c - lo) * NRHS + cp * VW;
+    if constexpr (VW == 2) {
+      const double2 t = *reinterpret_cast<const double2 *>(p);
+      o[0] = t.x;
+      o[1] = t.y;
+    } else {
+      const float4 t = *reinterpret_cast<const float4 *>(p);
+      o[0] = t.x;
+      o[1] = t.y;
+      o[2] = t.z;
+      o[3] = t.w;
+    }
+  } else {
+    load_piece<V>(x + (int64_t)c * NRHS + cp * VW, o);
+  }
+}
+
+template <typename V, int NRHS, bool WIDE>
+__device__ __forceinline__ void sell_item_piece(const BatchMatDev &M, int32_t s0, int32_t s1, int lane, V *xw) {
+  constexpr int VW = Piece<V>::VW;
+  constexpr int CPL = NRHS / VW;
+  constexpr int RPP = 32 / CPL;
+  constexpr int U = 4;
+  const int cp = lane % CPL;
+  const V *sv = static_cast<const V *>(M.sell_val);
+  const V *x = static_cast<const V *>(M.x);
+  V *y = static_cast<V *>(M.y);
+  for (int32_t sl = s0; sl < s1; ++sl) {
+    const int32_t p0 = __ldg(M.sell_ptr + sl);
+    const int32_t w = (__ldg(M.sell_ptr + sl + 1) - p0) >> 5;
+    const int32_t lo = (!WIDE && M.sell_lo) ? __ldg(M.sell_lo + sl) : -1;   // warp-uniform
+    if (lo >= 0) {
+      __syncwarp();   // the previous slice's reads of xw are done
+      for (int t = lane; t < kWinRows * CPL; t += 32) {
+        const int32_t r = lo + t / CPL;
+        if (r < M.cols) {
+          V v[VW];
+          load_piece<V>(x + (int64_t)r * NRHS + (t % CPL) * VW, v);
+          store_piece<V>(xw + t * VW, v);
+        }
+      }
+      __syncwarp();
+    }
+    for (int q = 0; q < CPL; ++q) {
+      const int l = q * RPP + lane / CPL;   // slice row
+      const int32_t pos = sl * 32 + l;
+      const bool live = pos < (WIDE ? M.sell_rows : M.rows);
+      const int32_t row = WIDE ? (live ? __ldg(M.sell_perm + pos) : 0) : pos;
+      const int32_t wl = live ? w : 0;
+      const V *vp = sv + p0 + l;
+      const int16_t *op = M.sell_off + p0 + l;
+      const int32_t *cpp = M.sell_col + p0 + l;
+      V acc[VW];
+#pragma unroll
+      for (int k = 0; k < VW; ++k) acc[k] = V(0);
+      for (int32_t k = 0; k < wl; k += U) {   // predicated groups of U, entries in stored order
+        V a[U];
+        int32_t c[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const bool ok = k + u < wl;
+          a[u] = ok ? __ldg(vp + 32 * (k + u)) : V(0);
+          c[u] = !ok ? -1 : WIDE ? __ldg(cpp + 32 * (k + u)) : row + (int32_t)__ldg(op + 32 * (k + u));
+        }
+        V xr[U][VW];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          if (c[u] >= 0) {
+            fetch_piece<V, NRHS>(x, xw, lo, c[u], cp, xr[u]);
+          } else {
+#pragma unroll
+            for (int t = 0; t < VW; ++t) xr[u][t] = V(0);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+          if (c[u] >= 0) {
+#pragma unroll
+            for (int t = 0; t < VW; ++t) acc[t] = fma(a[u], xr[u][t], acc[t]);
+          }
+      }
+      if (live) store_piece<V>(y + (int64_t)row * NRHS + cp * VW, acc);
+    }
+  }
+}
+
 // Fills the SELL-32 copy of one matrix: thread per row; padding entries get
 // value 0 and the column min(row, cols - 1).  *bad is set when a column
 // lies 32768 or more from its row.
@@ -319,6 +571,29 @@ __global__ void batch_sell_fill_wide_kernel(int32_t nrows, const int32_t *__rest
   }
 }
 
+// Per narrow SELL slice: the lowest column its 32 rows' stored entries read
+// (a padding entry of row r reads column min(r, cols - 1)), or -1 when they
+// span kWinRows or more columns.  Thread per row, a warp per slice (the loop
+// bound is rounded up to whole warps so every lane reaches the reductions).
+__global__ void batch_sell_window_kernel(int32_t rows, int32_t cols, const int32_t *__restrict__ rp,
+                                         const int32_t *__restrict__ ci, int32_t *__restrict__ lo_out) {
+  const int64_t n = ((int64_t)rows + 31) / 32 * 32;
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+    int32_t mn = INT32_MAX, mx = INT32_MIN;
+    if (r < rows) {
+      mn = mx = (int32_t)(r < (int64_t)cols - 1 ? r : (int64_t)cols - 1);
+      for (int32_t j = rp[r]; j < rp[r + 1]; ++j) {
+        const int32_t c = ci[j];
+        mn = min(mn, c);
+        mx = max(mx, c);
+      }
+    }
+    mn = __reduce_min_sync(0xffffffffu, mn);
+    mx = __reduce_max_sync(0xffffffffu, mx);
+    if ((r & 31) == 0) lo_out[r >> 5] = (int64_t)mx - mn < kWinRows ? mn : -1;
+  }
+}
+
 template <typename V, int NRHS>
 __device__ __forceinline__ void segment_item(const BatchMatDev &M, int32_t row, int32_t seg, int32_t lid,
                                              int32_t seg_nnz, const LongRow *__restrict__ longs,
@@ -329,15 +604,21 @@ __device__ __forceinline__ void segment_item(const BatchMatDev &M, int32_t row, 
   const int32_t s0 = __ldg(M.rp + row), e0 = __ldg(M.rp + row + 1);
   const int32_t s = s0 + seg * seg_nnz;
   const int32_t e = min(s + seg_nnz, e0);
-  V w[NRHS];
-  warp_row<V, NRHS>(M.ci, val, x, s, e, lane, w);
-  if (lane < NRHS) {
-    V o = w[0];
-#pragma unroll
-    for (int k = 1; k < NRHS; ++k)
-      if (lane == k) o = w[k];
-    part[(int64_t)(lr.part_base + seg) * NRHS + lane] = o;
-    __threadfence();
+  if constexpr (NRHS > 1) {
+    constexpr int VW = Piece<V>::VW;
+    V w[VW];
+    warp_row_piece<V, NRHS>(M.ci, val, x, s, e, lane, w);
+    if (lane < NRHS / VW) {
+      store_piece<V>(part + (int64_t)(lr.part_base + seg) * NRHS + lane * VW, w);
+      __threadfence();
+    }
+  } else {
+    V w[1];
+    warp_row<V, 1>(M.ci, val, x, s, e, lane, w);
+    if (lane == 0) {
+      part[lr.part_base + seg] = w[0];
+      __threadfence();
+    }
   }
   __syncwarp();
   int last = 0;
@@ -366,6 +647,9 @@ __global__ void __launch_bounds__(kBatchThreads, (NRHS == 1 && sizeof(V) == 4) ?
                                                               V *__restrict__ part, int32_t *__restrict__ arrive,
                                                               int32_t seg_nnz, int32_t long_thr) {
   const int lane = threadIdx.x & 31;
+  constexpr bool kWin = NRHS > 1 && sizeof(V) == 8;
+  __shared__ __align__(16) V xwin[kWin ? (kBatchThreads / 32) * kWinRows * NRHS : 1];
+  V *xw = xwin + (kWin ? (threadIdx.x >> 5) * kWinRows * NRHS : 0);
   for (;;) {
     int32_t it = 0;
     if (lane == 0) it = atomicAdd(next, 1);
@@ -373,25 +657,48 @@ __global__ void __launch_bounds__(kBatchThreads, (NRHS == 1 && sizeof(V) == 4) ?
     if (it >= nitems) return;
     const BatchItem I = items[it];
     const BatchMatDev M = mats[I.mat];
+    // SELL slices with several FP64 right-hand sides: column pieces and the
+    // shared-memory x window (512-matrix batch, banded half, 8 vectors: 517 ->
+    // 371 us); FP32 keeps a lane per row over all columns there (197 us
+    // against 224 us in pieces)
     if (I.info == kSellItem) {
-      sell_item<V, NRHS, false>(M, I.a, I.b, lane);
+      if constexpr (NRHS > 1 && sizeof(V) == 8)
+        sell_item_piece<V, NRHS, false>(M, I.a, I.b, lane, xw);
+      else
+        sell_item<V, NRHS, false>(M, I.a, I.b, lane);
       continue;
     }
     if (I.info == kSellWideItem) {
-      sell_item<V, NRHS, true>(M, I.a, I.b, lane);
+      if constexpr (NRHS > 1 && sizeof(V) == 8)
+        sell_item_piece<V, NRHS, true>(M, I.a, I.b, lane, xw);
+      else
+        sell_item<V, NRHS, true>(M, I.a, I.b, lane);
       continue;
     }
     if (I.info < 0) {
       segment_item<V, NRHS>(M, I.a, I.b, -(I.info + 1), seg_nnz, longs, part, arrive, lane);
       continue;
     }
-    switch (I.info) {
-      case 1: rows_item<V, NRHS, 1>(M, I.a, I.b, long_thr, lane); break;
-      case 2: rows_item<V, NRHS, 2>(M, I.a, I.b, long_thr, lane); break;
-      case 4: rows_item<V, NRHS, 4>(M, I.a, I.b, long_thr, lane); break;
-      case 8: rows_item<V, NRHS, 8>(M, I.a, I.b, long_thr, lane); break;
-      case 16: rows_item<V, NRHS, 16>(M, I.a, I.b, long_thr, lane); break;
-      default: rows_item<V, NRHS, 32>(M, I.a, I.b, long_thr, lane); break;
+    if constexpr (NRHS > 1) {
+      // lanes per row split the nonzeros; at most 32 / CPL of them
+      constexpr int LMAX = 32 / (NRHS / Piece<V>::VW);
+      const int32_t L = I.info < LMAX ? I.info : LMAX;
+      switch (L) {
+        case 1: rows_item_piece<V, NRHS, 1>(M, I.a, I.b, long_thr, lane); break;
+        case 2: rows_item_piece<V, NRHS, 2>(M, I.a, I.b, long_thr, lane); break;
+        case 4: rows_item_piece<V, NRHS, 4>(M, I.a, I.b, long_thr, lane); break;
+        case 8: rows_item_piece<V, NRHS, (LMAX >= 8 ? 8 : LMAX)>(M, I.a, I.b, long_thr, lane); break;
+        default: rows_item_piece<V, NRHS, LMAX>(M, I.a, I.b, long_thr, lane); break;
+      }
+    } else {
+      switch (I.info) {
+        case 1: rows_item<V, NRHS, 1>(M, I.a, I.b, long_thr, lane); break;
+        case 2: rows_item<V, NRHS, 2>(M, I.a, I.b, long_thr, lane); break;
+        case 4: rows_item<V, NRHS, 4>(M, I.a, I.b, long_thr, lane); break;
+        case 8: rows_item<V, NRHS, 8>(M, I.a, I.b, long_thr, lane); break;
+        case 16: rows_item<V, NRHS, 16>(M, I.a, I.b, long_thr, lane); break;
+        default: rows_item<V, NRHS, 32>(M, I.a, I.b, long_thr, lane); break;
+      }
     }
   }
 }
@@ -417,6 +724,7 @@ struct bsp_batch_plan_s {
   int32_t *d_sell_ptr = nullptr;
   int32_t *d_sell_col = nullptr;
   int32_t *d_sell_perm = nullptr;
+  int32_t *d_sell_lo = nullptr;
   BatchMatDev *d_mats = nullptr;
   // batched list (long segments first) and per-matrix lists
   BatchItem *d_items = nullptr, *d_items_sep = nullptr;
@@ -724,6 +1032,7 @@ extern "C" bsp_status bsp_batch_destroy(bsp_batch_plan P) {
   if (P->d_sell_val) cudaFreeAsync(P->d_sell_val, s);
   dfree(P->d_sell_off, s);
   dfree(P->d_sell_ptr, s);
+  dfree(P->d_sell_lo, s);
   dfree(P->d_sell_col, s);
   dfree(P->d_sell_perm, s);
   cudaStreamSynchronize(s);
@@ -780,6 +1089,7 @@ bsp_status build_sell(bsp_batch_plan P, cudaStream_t s) {
   BSP_TRY(dalloc(&P->d_sell_col, (size_t)std::max<int64_t>(tot_wide, 1), s));
   BSP_TRY(dalloc(&P->d_sell_perm, (size_t)std::max<int64_t>(tot_perm, 1), s));
   BSP_TRY(dalloc(&P->d_sell_ptr, (size_t)tot_ptr, s));
+  if (P->nrhs > 1 && P->dtype == BSP_F64) BSP_TRY(dalloc(&P->d_sell_lo, (size_t)tot_ptr, s));
   int32_t *bad = nullptr;
   BSP_TRY(dalloc(&bad, (size_t)count, s));
   BSP_CUDA(cudaMemsetAsync(bad, 0, sizeof(int32_t) * count, s));
@@ -806,6 +1116,12 @@ bsp_status build_sell(bsp_batch_plan P, cudaStream_t s) {
                                                            static_cast<float *>(v), off, bad + m);
       P->dm[m].sell_off = off;
       P->dm[m].sell_rows = A.rows;
+      if (P->d_sell_lo) {
+        int32_t *lo = P->d_sell_lo + ptr_off[m];
+        batch_sell_window_kernel<<<grid, 256, 0, s>>>(A.rows, A.cols, A.rowPtr, A.colIdx, lo);
+        BSP_LAUNCH_CHECK();
+        P->dm[m].sell_lo = lo;
+      }
     } else {
       const int32_t nr = (int32_t)perms[m].size();
       int32_t *perm = P->d_sell_perm + perm_off[m];
@@ -839,6 +1155,7 @@ bsp_status build_sell(bsp_batch_plan P, cudaStream_t s) {
       P->dm[m].sell_ptr = nullptr;
       P->dm[m].sell_val = nullptr;
       P->dm[m].sell_off = nullptr;
+      P->dm[m].sell_lo = nullptr;
     }
   return BSP_OK;
 }
