@@ -66,6 +66,8 @@ __global__ void __launch_bounds__(256) csr_scalar_kernel(int32_t rows, const int
   }
 }
 
+constexpr int kWarpRowFactor = 64;
+
 // LPR lanes per row (LPR in {1,2,4,8,16,32}); grid-stride over rows.
 template <typename V, int LPR>
 __global__ void __launch_bounds__(256) csr_vector_kernel(int32_t rows, const int32_t *__restrict__ rowPtr,
@@ -82,7 +84,12 @@ __global__ void __launch_bounds__(256) csr_vector_kernel(int32_t rows, const int
   for (int64_t base = warp_first; base < rows; base += groups) {
     const int64_t r = base + (threadIdx.x & 31) / LPR;
     const bool active = r < rows;
-    const int32_t s = active ? rowPtr[r] : 0, e = active ? rowPtr[r + 1] : 0;
+    const int32_t s = active ? rowPtr[r] : 0, e0 = active ? rowPtr[r + 1] : 0;
+    // rows longer than kWarpRowFactor entries per lane are summed by the
+    // whole warp after the pass, so one long row does not hold its warp's
+    // other rows (power-law rows at one lane per row)
+    const bool big = LPR < 32 && e0 - s > kWarpRowFactor * LPR;
+    const int32_t e = big ? s : e0;
     // The first kFirst entries of each lane are loaded together, then their x
     // gathers together: the rowPtr -> column -> x chain is paid once per
     // kFirst entries instead of once per entry.
@@ -104,7 +111,34 @@ __global__ void __launch_bounds__(256) csr_vector_kernel(int32_t rows, const int
       sum = fma(to_acc<V>(val[j]), to_acc<V>(__ldg(&x[colIdx[j]])), sum);
 #pragma unroll
     for (int o = LPR / 2; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o, LPR);
-    if (active && sub == 0) store_y<V, A>(y, r, sum, alpha, beta);
+    if (active && sub == 0 && !big) store_y<V, A>(y, r, sum, alpha, beta);
+    if constexpr (LPR < 32) {
+      unsigned todo = __ballot_sync(0xffffffffu, big && sub == 0);
+      const int lane = threadIdx.x & 31;
+      while (todo) {   // warp-uniform
+        const int b = __ffs(todo) - 1;
+        todo &= todo - 1;
+        const int64_t br = base + b / LPR;
+        const int32_t bs = rowPtr[br], be = rowPtr[br + 1];
+        A ws = A(0);
+        int32_t j = bs + lane;
+        for (; j + 96 < be; j += 128) {
+          int32_t c[4];
+          V a[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            c[u] = colIdx[j + 32 * u];
+            a[u] = val[j + 32 * u];
+          }
+#pragma unroll
+          for (int u = 0; u < 4; ++u) ws = fma(to_acc<V>(a[u]), to_acc<V>(__ldg(&x[c[u]])), ws);
+        }
+        for (; j < be; j += 32) ws = fma(to_acc<V>(val[j]), to_acc<V>(__ldg(&x[colIdx[j]])), ws);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) ws += __shfl_xor_sync(0xffffffffu, ws, o);
+        if (lane == 0) store_y<V, A>(y, br, ws, alpha, beta);
+      }
+    }
   }
 }
 

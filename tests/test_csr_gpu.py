@@ -145,7 +145,33 @@ def test_merge_path_power_law_long_rows(cuda):
     rp, ci, va, xx = _dev(cuda, A.rowptr, A.colidx, A.values, x)
     tol = pyoracle.spmv_tolerance(A.rowptr, A.colidx, A.values, x)
     _within(bsp.csr_spmv_merge(rp, ci, va, xx).cpu().numpy(), ref, tol)
-    _within(bsp.csr_spmv(rp, ci, va, xx, algo="vector", lanes=32).cpu().numpy(), ref, tol)
+    # lanes 1 / 4 / auto: rows above 64 entries per lane go to the whole warp
+    for lanes in (32, 4, 1, 0):
+        _within(bsp.csr_spmv(rp, ci, va, xx, algo="vector", lanes=lanes).cpu().numpy(), ref, tol)
+
+
+@pytest.mark.parametrize("lanes", [1, 2, 8])
+def test_vector_warp_rows_alpha_beta(cuda, lanes):
+    """Rows just above and below the whole-warp threshold (64 entries per
+    lane), with alpha and beta, in every position of a warp's row group."""
+    import torch
+    rng = np.random.default_rng(lanes)
+    n, cols = 700, 5000
+    lens = rng.integers(0, 8, n)
+    thr = 64 * lanes
+    lens[rng.choice(n, 60, replace=False)] = rng.choice([thr - 1, thr, thr + 1, 3 * thr + 7], 60)
+    rp = np.zeros(n + 1, np.int32)
+    rp[1:] = np.cumsum(lens)
+    ci = np.concatenate([np.sort(rng.choice(cols, l, replace=False)) for l in lens]).astype(np.int32)
+    va = rng.standard_normal(ci.size)
+    x = rng.uniform(-1, 1, cols)
+    y0 = rng.uniform(-1, 1, n)
+    ref = 1.5 * pyoracle.spmv_f64(rp, ci, va, x) + 0.25 * y0
+    d = _dev(cuda, rp, ci, va, x)
+    y = torch.from_numpy(y0.copy()).to(cuda)
+    bsp.csr_spmv(*d, y=y, alpha=1.5, beta=0.25, algo="vector", lanes=lanes)
+    tol = 1.5 * pyoracle.spmv_tolerance(rp, ci, va, x) + 4 * 2.0 ** -53 * (np.abs(ref) + 1)
+    _within(y.cpu().numpy(), ref, tol)
 
 
 @pytest.mark.parametrize("algo", ["vector", "merge", "scalar", "stream"])
