@@ -1964,7 +1964,16 @@ __device__ __forceinline__ uint4 ld_hint_b16(const void *p, uint64_t pol) {
   return r;
 }
 
-template <typename T, int LPR, int U>
+// Gathers in flight per lane group: U for a short row, UL per warp step of a
+// long chunk.  8 at 4 lanes per B row (graph 2^20, FP16, N = 32) took 78
+// registers and 0.551 ms (UL alone 0.605 ms, UL capped at 64 registers
+// 0.507 ms) against 0.470 ms with 4.
+template <int LPR> struct SlabU {
+  static constexpr int U = 4;
+  static constexpr int UL = 4;
+};
+
+template <typename T, int LPR, int U, int UL>
 __global__ void __launch_bounds__(256, LPR >= 8 && LPR <= 16 ? (std::is_same<T, __nv_bfloat16>::value ? 4 : 5) : 0)
     spmm_slab_kernel(
     int64_t nlong, const int2 *__restrict__ long_se, int32_t nshort, const int32_t *__restrict__ short_rows,
@@ -1989,7 +1998,7 @@ __global__ void __launch_bounds__(256, LPR >= 8 && LPR <= 16 ? (std::is_same<T, 
       // Batches of BQ = 32*Q nonzeros: Q = 1 while a warp step's G*U gathers
       // fit in 32 (LPR >= 4), else one step takes the whole batch, so narrow
       // B rows still keep G*U gathers in flight per warp.
-      constexpr int GU = G * kSpmmU;
+      constexpr int GU = G * UL;
       constexpr int Q = GU > 32 ? GU / 32 : 1;
       constexpr int BQ = 32 * Q;
       const int2 se = long_se[task];
@@ -2013,10 +2022,10 @@ __global__ void __launch_bounds__(256, LPR >= 8 && LPR <= 16 ? (std::is_same<T, 
         }
         const int cnt = e - j0 < BQ ? e - j0 : BQ;
         for (int t = 0; t < cnt; t += GU) {   // one trip when Q > 1
-          uint4 raw[kSpmmU];
-          float v[kSpmmU];
+          uint4 raw[UL];
+          float v[UL];
 #pragma unroll
-          for (int u = 0; u < kSpmmU; ++u) {
+          for (int u = 0; u < UL; ++u) {
             const int src = t + u * G + g;
             const int q = Q > 1 ? (u * G) >> 5 : 0;   // t == 0 when Q > 1
             const int32_t c = __shfl_sync(0xffffffffu, cj[q], src & 31);
@@ -2026,7 +2035,7 @@ __global__ void __launch_bounds__(256, LPR >= 8 && LPR <= 16 ? (std::is_same<T, 
             raw[u] = ok ? ld_hint_b16(B + (int64_t)c * ldb + cl, pb) : make_uint4(0, 0, 0, 0);
           }
 #pragma unroll
-          for (int u = 0; u < kSpmmU; ++u) {
+          for (int u = 0; u < UL; ++u) {
             float b[VEC];
             unpack16<T>(raw[u], b);
 #pragma unroll
@@ -2114,7 +2123,7 @@ static bsp_status launch_slab(const bsp_spmm_plan *p, const int32_t *ci, const v
   const int64_t cap = (int64_t)sm_count() * 32;
   if (blocks > cap) blocks = cap;
   if (blocks < 1) blocks = 1;
-  spmm_slab_kernel<T, LPR, 4><<<(unsigned)blocks, 256, 0, s>>>(
+  spmm_slab_kernel<T, LPR, SlabU<LPR>::U, SlabU<LPR>::UL><<<(unsigned)blocks, 256, 0, s>>>(
       p->nparts, reinterpret_cast<const int2 *>(p->long_se), p->nshort, p->short_rows,
       reinterpret_cast<const int2 *>(p->short_se), ci, (const T *)val, (const T *)B, ldb, col0, C, ldc, part, a, b,
       hints);
