@@ -127,6 +127,7 @@ _PROTOS = {
     "bsp_bsr_spmv_host_pipelined": (C.c_int, [C.c_void_p, _P, _P, _D, _D, _P]),
     "bsp_bsr_host_plan_destroy": (C.c_int, [C.c_void_p]),
     "bsp_bsr_host_plan_set_graph": (C.c_int, [C.c_void_p, _I32]),
+    "bsp_bsr_host_plan_set_ctas": (C.c_int, [C.c_void_p, _I32]),
     "bsp_csr2bcsr": (C.c_int, [_I32, _I32, _I32, _P, _P, _P, _I32, _I32, _I32, C.POINTER(BspBcsr), _P]),
     "bsp_bcsr_free": (C.c_int, [C.POINTER(BspBcsr)]),
     "bsp_bcsr_spmv": (C.c_int, [C.POINTER(BspBcsr), _P, _P, _D, _D, _P]),
@@ -281,7 +282,8 @@ class BspSpmmPlan(C.Structure):
                 ("nsplit", C.c_int32), ("chunk_ptr", C.c_void_p), ("part_ptr", C.c_void_p),
                 ("chunk_row", C.c_void_p), ("split_rows", C.c_void_p), ("nshort", C.c_int32),
                 ("short_rows", C.c_void_p), ("long_chunk", C.c_void_p), ("long_se", C.c_void_p),
-                ("short_se", C.c_void_p), ("slab_l2_hints", C.c_int32)]
+                ("short_se", C.c_void_p), ("slab_l2_hints", C.c_int32), ("ngroups", C.c_int32),
+                ("group_ptr", C.c_void_p), ("group_split", C.c_void_p)]
 
 
 _PROTOS.update({

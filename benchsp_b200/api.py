@@ -207,6 +207,11 @@ class BsrHostPlan:
         if not use_graph:
             check(lib().bsp_bsr_host_plan_set_graph(self._h, 0))
 
+    def set_ctas(self, max_ctas: int) -> None:
+        """Caps each range's SpMV grid (0 = the kernel's own; the plan
+        starts at one wave, 8 CTAs per SM)."""
+        check(lib().bsp_bsr_host_plan_set_ctas(self._h, int(max_ctas)))
+
     def spmv(self, x_host: np.ndarray, y_host: np.ndarray, *, alpha: float = 1.0, beta: float = 0.0,
              stream=None) -> np.ndarray:
         _host_vec(x_host, self._m._d.col, "x_host")

@@ -445,10 +445,11 @@ __global__ void __launch_bounds__(256) bsr4_dmma_kernel(int32_t blc_row, int32_t
 }
 
 template <int BS, int LG, int U, bool PF>
-static bsp_status launch_ffma(const bsp_bsr *m, const double *x, double *y, double a, double b, cudaStream_t s) {
+static bsp_status launch_ffma(const bsp_bsr *m, const double *x, double *y, double a, double b, int64_t max_blocks,
+                              cudaStream_t s) {
   const int threads = 256;
   int64_t blocks = ceil_div(m->blc_row, threads / LG);
-  const int64_t cap = (int64_t)sm_count() * 64;
+  const int64_t cap = max_blocks > 0 ? max_blocks : (int64_t)sm_count() * 64;
   if (blocks > cap) blocks = cap;
   if (blocks < 1) blocks = 1;
   if (((uintptr_t)x & 31) == 0)
@@ -461,7 +462,8 @@ static bsp_status launch_ffma(const bsp_bsr *m, const double *x, double *y, doub
   return BSP_OK;
 }
 
-using FfmaLauncher = bsp_status (*)(const bsp_bsr *, const double *, double *, double, double, cudaStream_t);
+using FfmaLauncher = bsp_status (*)(const bsp_bsr *, const double *, double *, double, double, int64_t,
+                                    cudaStream_t);
 
 // Variant table: (bs, lanes per block-row, unroll, L2 256-byte hint).
 struct FfmaVariant {
@@ -515,20 +517,22 @@ bsp_status bsr_spmv_impl(const bsp_bsr *m, const double *x, double *y, double al
   }
   if (algo != BSP_BSR_FFMA) BSP_FAIL(BSP_ERR_INVALID, "unknown BSR algo");
   if (m->bs != 4 && m->bs != 8) BSP_FAIL(BSP_ERR_UNSUPPORTED, "block size must be 4 or 8");
-  return default_ffma(m)->fn(m, x, y, alpha, beta, s);
+  return default_ffma(m)->fn(m, x, y, alpha, beta, 0, s);
 }
 
 // FFMA SpMV of block rows [lo, hi) only (y given for the whole matrix), with
 // the kernel shape chosen for the whole matrix.
+// Block rows [lo, hi) (the host-buffer plan's ranges); max_blocks > 0 caps
+// the grid (the kernel strides over its block rows).
 bsp_status bsr_spmv_rows(const bsp_bsr *m, int32_t lo, int32_t hi, const double *x, double *y, double alpha,
-                         double beta, cudaStream_t s) {
+                         double beta, int64_t max_blocks, cudaStream_t s) {
   if (hi <= lo) return BSP_OK;
   if (((uintptr_t)m->blcVal & 31) != 0) BSP_FAIL(BSP_ERR_INVALID, "blcVal must be 32-byte aligned");
   bsp_bsr sub = *m;
   sub.blcPtr = m->blcPtr + lo;  // block offsets stay absolute
   sub.blc_row = hi - lo;
   sub.row = std::min<int64_t>((int64_t)m->row - (int64_t)lo * m->bs, (int64_t)(hi - lo) * m->bs);
-  return default_ffma(m)->fn(&sub, x, y + (int64_t)lo * m->bs, alpha, beta, s);
+  return default_ffma(m)->fn(&sub, x, y + (int64_t)lo * m->bs, alpha, beta, max_blocks, s);
 }
 
 bsp_status bsr_spmv_variant(const bsp_bsr *m, const double *x, double *y, double alpha, double beta, int lanes,
@@ -537,7 +541,7 @@ bsp_status bsr_spmv_variant(const bsp_bsr *m, const double *x, double *y, double
   if (((uintptr_t)m->blcVal & 31) != 0) BSP_FAIL(BSP_ERR_INVALID, "blcVal must be 32-byte aligned");
   const FfmaVariant *v = find_ffma(m->bs, lanes, unroll, pf);
   if (!v) BSP_FAIL(BSP_ERR_UNSUPPORTED, "no FFMA variant with these lanes/unroll/prefetch");
-  return v->fn(m, x, y, alpha, beta, s);
+  return v->fn(m, x, y, alpha, beta, 0, s);
 }
 
 }  // namespace bsp

@@ -19,7 +19,7 @@
 namespace bsp {
 
 bsp_status bsr_spmv_rows(const bsp_bsr *m, int32_t lo, int32_t hi, const double *x, double *y, double alpha,
-                         double beta, cudaStream_t s);
+                         double beta, int64_t max_blocks, cudaStream_t s);
 
 // Largest block column of each block-row range (atomicMax per range).
 __global__ void chunk_maxcol_kernel(int32_t nchunks, const int32_t *__restrict__ lo,
@@ -58,6 +58,12 @@ struct bsp_bsr_host_plan_s {
   double *g_y = nullptr;
   double g_alpha = 0.0, g_beta = 0.0;
   int32_t use_graph = 1;
+  // grid cap of each range's SpMV (0 = the kernel's own grid).  Default: one
+  // wave, 8 CTAs of 256 per SM, the rows walked by grid stride (27-point
+  // stencil 64^3 x 4 dof, 8 ranges, pinned 8 MB up and down per call: 311-316
+  // us per call against 316-327 us with the kernel's 1.7-wave grid, four
+  // interleaved repetitions; 6 CTAs per SM 334-338 us)
+  int32_t max_ctas = 0;
 };
 
 static void plan_release(bsp_bsr_host_plan_s *P) {
@@ -84,6 +90,7 @@ extern "C" bsp_status bsp_bsr_host_plan_create(const bsp_bsr *m, int32_t chunks,
   cudaStream_t s = as_stream(stream);
   auto *P = new bsp_bsr_host_plan_s();
   P->m = m;
+  P->max_ctas = sm_count() * 8;
   P->chunks = std::max<int32_t>(1, std::min<int32_t>(chunks, std::max<int32_t>(1, m->blc_row)));
   const int32_t C = P->chunks;
   P->lo.resize(C + 1);
@@ -157,7 +164,7 @@ static bsp_status enqueue(bsp_bsr_host_plan P, const double *x_host, double *y_h
     if (beta != 0.0 && r1 > r0)
       BSP_CUDA(cudaMemcpyAsync(P->dy + r0, y_host + r0, sizeof(double) * (r1 - r0), cudaMemcpyHostToDevice,
                                P->run));
-    BSP_TRY(bsr_spmv_rows(m, P->lo[c], P->lo[c + 1], P->dx, P->dy, alpha, beta, P->run));
+    BSP_TRY(bsr_spmv_rows(m, P->lo[c], P->lo[c + 1], P->dx, P->dy, alpha, beta, P->max_ctas, P->run));
     BSP_CUDA(cudaEventRecord(P->yev[c], P->run));
     BSP_CUDA(cudaStreamWaitEvent(P->down, P->yev[c], 0));
     if (r1 > r0)
@@ -214,6 +221,18 @@ extern "C" bsp_status bsp_bsr_host_plan_set_graph(bsp_bsr_host_plan P, int32_t u
   clear_error();
   BSP_CHECK_ARG(P, "null plan");
   P->use_graph = use_graph ? 1 : 0;
+  return BSP_OK;
+}
+
+extern "C" bsp_status bsp_bsr_host_plan_set_ctas(bsp_bsr_host_plan P, int32_t max_ctas) {
+  clear_error();
+  BSP_CHECK_ARG(P, "null plan");
+  BSP_CHECK_ARG(max_ctas >= 0, "max_ctas must be >= 0");
+  if (P->max_ctas != max_ctas && P->graph) {   // the recorded graph holds the old grids
+    cudaGraphExecDestroy(P->graph);
+    P->graph = nullptr;
+  }
+  P->max_ctas = max_ctas;
   return BSP_OK;
 }
 

@@ -1636,27 +1636,112 @@ __global__ void __launch_bounds__(256) spmm_chunk_kernel(int64_t nchunks, int32_
   }
 }
 
-// One warp per split row: C row = alpha * sum of its chunk partials (in order).
-__global__ void spmm_split_reduce_kernel(int32_t nsplit, const int32_t *__restrict__ split_rows,
-                                         const int32_t *__restrict__ chunk_ptr,
-                                         const int32_t *__restrict__ part_ptr, int32_t N,
-                                         const float *__restrict__ part, float *__restrict__ C, int64_t ldc,
-                                         float alpha, float beta) {
+// Split-row sums in two stages, so a row of many chunks (a 337,738-entry
+// row is 1,320 chunks of 256) is not one warp's serial sum.  Stage one: a
+// warp per group of up to 32 consecutive chunks of a row, lanes over the
+// columns, 4 sums in flight per lane (chunk k into sum k % 4, added in a fixed
+// order at the end); a row of one group is finished here.  Stage two: a warp
+// per row of several groups adds its group sums the same way.
+__device__ __forceinline__ float sum4_strided(const float *__restrict__ p, int64_t stride, int32_t n) {
+  float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+  int32_t k = 0;
+  for (; k + 3 < n; k += 4) {
+    a0 += p[(int64_t)k * stride];
+    a1 += p[(int64_t)(k + 1) * stride];
+    a2 += p[(int64_t)(k + 2) * stride];
+    a3 += p[(int64_t)(k + 3) * stride];
+  }
+  if (k < n) a0 += p[(int64_t)k * stride];
+  if (k + 1 < n) a1 += p[(int64_t)(k + 1) * stride];
+  if (k + 2 < n) a2 += p[(int64_t)(k + 2) * stride];
+  return (a0 + a1) + (a2 + a3);
+}
+
+__device__ __forceinline__ void store_c(float *cp, float acc, float alpha, float beta) {
+  float o = alpha * acc;
+  if (beta != 0.f) o += beta * *cp;
+  *cp = o;
+}
+
+__global__ void spmm_split_group_kernel(int32_t ngroups, const int32_t *__restrict__ group_split,
+                                        const int32_t *__restrict__ group_ptr,
+                                        const int32_t *__restrict__ split_rows,
+                                        const int32_t *__restrict__ chunk_ptr,
+                                        const int32_t *__restrict__ part_ptr, int32_t N,
+                                        const float *__restrict__ part, float *__restrict__ gpart,
+                                        float *__restrict__ C, int64_t ldc, float alpha, float beta) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t g = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < ngroups; g += nwarps) {
+    const int32_t i = group_split[g];
+    const int32_t r = split_rows[i];
+    const int32_t nc = chunk_ptr[r + 1] - chunk_ptr[r];
+    const int32_t gi = (int32_t)g - group_ptr[i];
+    const int32_t k0 = gi * 32, n = min(32, nc - k0);
+    const bool single = group_ptr[i + 1] - group_ptr[i] == 1;
+    const float *pp = part + ((int64_t)part_ptr[r] + k0) * N;
+    for (int32_t c = lane; c < N; c += 32) {
+      const float acc = sum4_strided(pp + c, N, n);
+      if (single)
+        store_c(C + (int64_t)r * ldc + c, acc, alpha, beta);
+      else
+        gpart[g * N + c] = acc;
+    }
+  }
+}
+
+__global__ void spmm_split_rows_kernel(int32_t nsplit, const int32_t *__restrict__ split_rows,
+                                       const int32_t *__restrict__ group_ptr, int32_t N,
+                                       const float *__restrict__ gpart, float *__restrict__ C, int64_t ldc,
+                                       float alpha, float beta) {
   const int lane = threadIdx.x & 31;
   const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
   for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < nsplit; i += nwarps) {
+    const int32_t g0 = group_ptr[i], ng = group_ptr[i + 1] - g0;
+    if (ng <= 1) continue;   // finished by the group kernel
     const int32_t r = split_rows[i];
-    const int32_t nc = chunk_ptr[r + 1] - chunk_ptr[r];
-    const float *pp = part + (int64_t)part_ptr[r] * N;
-    for (int32_t c = lane; c < N; c += 32) {
-      float acc = 0.f;
-      for (int32_t k = 0; k < nc; ++k) acc += pp[(int64_t)k * N + c];
-      float *cp = C + (int64_t)r * ldc + c;
-      float o = alpha * acc;
-      if (beta != 0.f) o += beta * *cp;
-      *cp = o;
+    const float *gp = gpart + (int64_t)g0 * N;
+    for (int32_t c = lane; c < N; c += 32) store_c(C + (int64_t)r * ldc + c, sum4_strided(gp + c, N, ng), alpha, beta);
+  }
+}
+
+// Groups of the split rows: ng[i] = ceil(chunks / 32) (scanned into
+// group_ptr), then group_split lists the split row of every group.
+__global__ void spmm_group_count_kernel(int32_t nsplit, const int32_t *__restrict__ split_rows,
+                                        const int32_t *__restrict__ chunk_ptr, int32_t *__restrict__ ng) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= nsplit; i += (int64_t)gridDim.x * blockDim.x) {
+    if (i == nsplit) {
+      ng[i] = 0;
+    } else {
+      const int32_t r = split_rows[i];
+      ng[i] = (chunk_ptr[r + 1] - chunk_ptr[r] + 31) / 32;
     }
   }
+}
+
+__global__ void spmm_group_fill_kernel(int32_t nsplit, const int32_t *__restrict__ group_ptr,
+                                       int32_t *__restrict__ group_split) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nsplit; i += (int64_t)gridDim.x * blockDim.x)
+    for (int32_t g = group_ptr[i]; g < group_ptr[i + 1]; ++g) group_split[g] = (int32_t)i;
+}
+
+// Sums the split rows' partials (`ncol` columns of `part`) into C; gpart
+// holds the group sums of rows of more than 32 chunks.
+static bsp_status split_reduce(const bsp_spmm_plan *p, int32_t ncol, const float *part, float *gpart, float *C,
+                               int64_t ldc, float a, float b, cudaStream_t s) {
+  if (p->nsplit <= 0) return BSP_OK;
+  const int64_t cap = (int64_t)sm_count() * 32;
+  const int64_t bg = std::min<int64_t>(std::max<int64_t>(1, ceil_div(p->ngroups, 8)), cap);
+  spmm_split_group_kernel<<<(unsigned)bg, 256, 0, s>>>(p->ngroups, p->group_split, p->group_ptr, p->split_rows,
+                                                      p->chunk_ptr, p->part_ptr, ncol, part, gpart, C, ldc, a, b);
+  BSP_LAUNCH_CHECK();
+  if (p->ngroups > p->nsplit) {   // some row has more than one group
+    const int64_t br = std::min<int64_t>(std::max<int64_t>(1, ceil_div(p->nsplit, 8)), cap);
+    spmm_split_rows_kernel<<<(unsigned)br, 256, 0, s>>>(p->nsplit, p->split_rows, p->group_ptr, ncol, gpart, C, ldc, a,
+                                                       b);
+    BSP_LAUNCH_CHECK();
+  }
+  return BSP_OK;
 }
 
 __global__ void spmm_split_list_kernel(int32_t rows, const int32_t *__restrict__ chunk_ptr,
@@ -1760,6 +1845,25 @@ extern "C" bsp_status bsp_spmm_plan_create(int32_t rows, int32_t nnz, const int3
     spmm_split_list_kernel<<<g, 256, 0, s>>>(rows, p.chunk_ptr, flag, p.split_rows);
     BSP_LAUNCH_CHECK();
   }
+  // reduce groups of the split rows
+  BSP_TRY(dalloc(&p.group_ptr, (size_t)p.nsplit + 1, s));
+  if (p.nsplit > 0) {
+    const unsigned gs = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div((int64_t)p.nsplit + 1, 256),
+                                                                         (int64_t)sm_count() * 32));
+    spmm_group_count_kernel<<<gs, 256, 0, s>>>(p.nsplit, p.split_rows, p.chunk_ptr, p.group_ptr);
+    BSP_LAUNCH_CHECK();
+  } else {
+    BSP_CUDA(cudaMemsetAsync(p.group_ptr, 0, sizeof(int32_t), s));
+  }
+  BSP_TRY(exclusive_scan_i32(p.group_ptr, p.group_ptr, (int64_t)p.nsplit + 1, tot, s));
+  BSP_TRY(read_i64(tot, &h, s));
+  p.ngroups = (int32_t)h;
+  BSP_TRY(dalloc(&p.group_split, (size_t)(p.ngroups > 0 ? p.ngroups : 1), s));
+  if (p.nsplit > 0) {
+    const unsigned gs = (unsigned)std::max<int64_t>(1, std::min<int64_t>(ceil_div(p.nsplit, 256), (int64_t)sm_count() * 32));
+    spmm_group_fill_kernel<<<gs, 256, 0, s>>>(p.nsplit, p.group_ptr, p.group_split);
+    BSP_LAUNCH_CHECK();
+  }
   dfree(flag, s);
   dfree(tot, s);
   // slab engine: the long chunks in partial-slot order, the short rows by length
@@ -1805,6 +1909,8 @@ extern "C" bsp_status bsp_spmm_plan_free(bsp_spmm_plan *p) {
   dfree(p->long_chunk, s);
   dfree(p->long_se, s);
   dfree(p->short_se, s);
+  dfree(p->group_ptr, s);
+  dfree(p->group_split, s);
   BSP_CUDA(cudaStreamSynchronize(s));
   return BSP_OK;
 }
@@ -2179,20 +2285,14 @@ static bsp_status slab_typed(const bsp_spmm_plan *p, int32_t N, int32_t cols, in
       default: BSP_FAIL(BSP_ERR_UNSUPPORTED, "slab width");
     }
     BSP_TRY(st);
-    if (p->nsplit > 0) {
-      int64_t blocks = ceil_div(p->nsplit, 8);
-      if (blocks > (int64_t)sm_count() * 32) blocks = (int64_t)sm_count() * 32;
-      spmm_split_reduce_kernel<<<(unsigned)blocks, 256, 0, s>>>(p->nsplit, p->split_rows, p->chunk_ptr, p->part_ptr,
-                                                                ns, part, C + col0, ldc, a, b);
-      BSP_LAUNCH_CHECK();
-    }
+    BSP_TRY(split_reduce(p, ns, part, part + (int64_t)p->nparts * N, C + col0, ldc, a, b, s));
   }
   return BSP_OK;
 }
 }  // namespace bsp
 
 extern "C" size_t bsp_spmm_plan_workspace(const bsp_spmm_plan *p, int32_t N) {
-  return p ? (size_t)p->nparts * (size_t)(N > 0 ? N : 0) * sizeof(float) : 0;
+  return p ? ((size_t)p->nparts + (size_t)p->ngroups) * (size_t)(N > 0 ? N : 0) * sizeof(float) : 0;
 }
 
 namespace bsp {
@@ -2281,13 +2381,7 @@ static bsp_status spmm_planned_impl(const bsp_spmm_plan *p, int32_t cols, int32_
       BSP_FAIL(BSP_ERR_UNSUPPORTED, "SpMM takes F16, BF16 or F32 values");
   }
   if (st != BSP_OK) return st;
-  if (p->nsplit > 0) {
-    int64_t blocks = ceil_div(p->nsplit, 8);
-    if (blocks > (int64_t)sm_count() * 32) blocks = (int64_t)sm_count() * 32;
-    spmm_split_reduce_kernel<<<(unsigned)blocks, 256, 0, s>>>(p->nsplit, p->split_rows, p->chunk_ptr, p->part_ptr,
-                                                              N, part, C, ldc, alpha, beta);
-    BSP_LAUNCH_CHECK();
-  }
+  BSP_TRY(split_reduce(p, N, part, part + (int64_t)p->nparts * N, C, ldc, alpha, beta, s));
   return BSP_OK;
 }
 }  // namespace bsp

@@ -148,5 +148,13 @@ def test_bsr_host_pipelined_matches_host_call(cuda, kind, chunks):
     P.spmv(x, got)
     ref = pyoracle.spmv_f64(A.rowptr, A.colidx, A.values, x)
     assert np.all(np.abs(got - ref) <= pyoracle.spmv_tolerance(A.rowptr, A.colidx, A.values, x))
+    # the grid cap of the ranges changes the schedule, not the sums
+    for ctas in (0, 1, 37):
+        P.set_ctas(ctas)
+        got2 = np.empty(A.rows)
+        P.spmv(x, got2)
+        assert np.array_equal(got2, got), ctas
+    with pytest.raises(bsp.BspError):
+        P.set_ctas(-1)
     P.close()
     M.free()
