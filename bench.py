@@ -700,8 +700,10 @@ def run_suite(args) -> None:
             nb = A.nnz * 6 + (A.rows + 1) * 4 + A.cols * N * 2 + A.rows * N * 4
             gb = A.nnz * N * 2    # B-row bytes gathered (one B row per nonzero)
             w = min(256, 2 * N)
-            # B (cols x N FP16) fits in L2 at N = 32 (64 MB): the L2 probe; else the one past L2
-            where = "l2" if A.cols * N * 2 <= 0.6 * 126e6 else "dram"
+            # the probe of this gather width whose buffer is closest in size to B (cols x N FP16)
+            bmb = A.cols * N * 2 / 2 ** 20
+            cands = [k for k in gpk if k.startswith(f"w{w}_")]
+            where = min(cands, key=lambda k: abs(np.log(gpk[k]["buffer_mb"] / bmb))).split("_", 1)[1]
             res[f"{name}_N{N}"] = {"ms": round(t * 1e3, 3), "engine": "slab", "grouped_engine_ms": round(tg * 1e3, 3),
                                    "gflops": round(2 * A.nnz * N / t / 1e9, 1),
                                    "rel_err_vs_fp64": err, "cusparse_f32_ms": round(tcs * 1e3, 3),
@@ -758,11 +760,16 @@ def run_suite(args) -> None:
 def run_gather_peaks(bsp, dev) -> dict:
     """bsp_gather_probe: random gathers of 8 B (a CSR/DASP x gather), 64 B
     and 256 B (B-row slices of the SpMM) from a buffer that fits L2 (16 or 64
-    MB) and from one that does not (2 GB); 10 timed launches after 3."""
+    MB) and from one that does not (2 GB), and 256 B from 256 and 512 MB (the
+    sizes of the SpMM's B at N = 128 and 256, partly in L2); 10 timed
+    launches after 3."""
     import torch
     out = {}
     for width, count in ((8, 50_000_000), (64, 33_554_432), (256, 33_554_432)):
-        for where, mb in (("l2", 16 if width == 8 else 64), ("dram", 2048)):
+        sizes = [("l2", 16 if width == 8 else 64), ("dram", 2048)]
+        if width == 256:
+            sizes += [("m256", 256), ("m512", 512)]
+        for where, mb in sizes:
             buf = torch.zeros((mb << 20) // 4, dtype=torch.int32, device=dev)
             t = _timed(lambda: bsp.gather_probe(buf, width, count), 10)
             out[f"w{width}_{where}"] = {"buffer_mb": mb, "ggathers_s": round(count / t / 1e9, 2),
