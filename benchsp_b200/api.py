@@ -875,7 +875,7 @@ class BatchPlan:
     SELL-32); for the others tune=0 picks lanes per row from row statistics,
     tune=1 times the lane counts per matrix."""
 
-    def __init__(self, mats, *, nrhs: int = 1, tune: int = 0, seg_nnz: int = 1024, long_row_nnz: int = 2048,
+    def __init__(self, mats, *, nrhs: int = 1, tune: int = 0, seg_nnz: int = 512, long_row_nnz: int = 1024,
                  item_nnz: int = 0, use_graph: bool = True, sell: bool = True, sell_wide: bool = False,
                  stream=None):
         torch = _torch()

@@ -849,8 +849,8 @@ typedef struct {
 
 typedef struct {
   int32_t tune;         /* 0: row-statistics model, 1: time candidates */
-  int32_t seg_nnz;      /* nonzeros per long-row segment (default 1024) */
-  int32_t long_row_nnz; /* rows above this are split (default 2048) */
+  int32_t seg_nnz;      /* nonzeros per long-row segment (default 512) */
+  int32_t long_row_nnz; /* rows above this are split (default 1024) */
   int32_t item_nnz;     /* target nonzeros per row item, 0 = automatic */
   int32_t use_graph;    /* capture the launch in a CUDA graph (default 1) */
   int32_t sell;         /* 1: store qualifying matrices as SELL-32 (default 1) */
