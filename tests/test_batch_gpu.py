@@ -226,3 +226,48 @@ def test_batch_wide_sell_form(cuda, nrhs):
     for a, d in zip(first, dev):
         assert torch.equal(a, d[4])
     P.close()
+
+
+def _even_rows(rows, cols, per_row, span, seed):
+    """Every row `per_row` distinct columns within `span` of min(row, cols - 1):
+    even rows, so the batch stores the matrix as SELL-32."""
+    rng = np.random.default_rng(seed)
+    ci = []
+    for r in range(rows):
+        c0 = min(r, cols - 1)
+        lo, hi = max(0, c0 - span), min(cols, c0 + span + 1)
+        ci.append(np.sort(rng.choice(np.arange(lo, hi), per_row, replace=False)))
+    rp = np.arange(rows + 1, dtype=np.int32) * per_row
+    return bsp.HostCSR(rows, cols, rp, np.concatenate(ci).astype(np.int32), rng.standard_normal(rows * per_row))
+
+
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+def test_batch_sell_slices_with_and_without_x_window(cuda, dtype):
+    """8 right-hand sides on SELL-32 matrices: slices whose columns lie within
+    64 rows gather x from a shared-memory window (FP64), the others from
+    global memory; a rectangular matrix clips the window at its last column,
+    and a partial last slice has fewer than 32 rows.  Results against the
+    oracle, and the batched launch against the per-matrix launches."""
+    import torch
+    mats = [bsp.gen_banded(1000, 9, 1),                    # every slice windowed, last slice partial
+            _even_rows(777, 777, 8, 3000, 2),             # no slice windowed
+            _even_rows(1000, 700, 6, 12, 3),              # rectangular: window clipped at 700 columns
+            _even_rows(640, 640, 4, 40, 4)]               # spans just above and below the window
+    half = _even_rows(512, 512, 5, 6, 5)                  # banded rows, then scattered rows in one matrix
+    wide = _even_rows(512, 512, 5, 400, 6)
+    rp = np.concatenate([half.rowptr[:257], wide.rowptr[257:] - wide.rowptr[256] + half.rowptr[256]]).astype(np.int32)
+    ci = np.concatenate([half.colidx[:half.rowptr[256]], wide.colidx[wide.rowptr[256]:]]).astype(np.int32)
+    mats.append(bsp.HostCSR(512, 512, rp, ci, np.random.default_rng(7).standard_normal(ci.size)))
+    dev, host = _upload(cuda, mats, dtype, 8, 12)
+    P = bsp.BatchPlan(dev, nrhs=8)
+    assert np.all(P.formats() == 1), P.formats()
+    P.run()
+    torch.cuda.synchronize()
+    _check(mats, dev, host, dtype, 8)
+    first = [d[4].clone() for d in dev]
+    for d in dev:
+        d[4].fill_(float("nan"))
+    P.run_separate()
+    for a, d in zip(first, dev):
+        assert torch.equal(a, d[4])
+    P.close()
