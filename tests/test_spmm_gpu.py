@@ -410,3 +410,35 @@ def test_gtile_column_permuted_stencil(cuda, N):
     u = 2.0 ** -24
     assert np.all(np.abs(C - Cref) <= 2.0 * (L * u / (1 - L * u)) * absC + 1e-30)
     G.free()
+
+
+@pytest.mark.parametrize("engine,slab", [("slab", 0), ("slab", 16), ("grouped", 0)])
+def test_spmm_split_rows_of_many_chunk_groups(cuda, engine, slab):
+    """Split-row partials are summed in groups of up to 32 chunks and then per
+    row: rows at the group boundaries (32, 33, 64, 65 chunks of 32 nonzeros)
+    and one of 101 chunks, with alpha and beta, against the FP64 oracle;
+    repeated calls give the same bits."""
+    import torch
+    rng = np.random.default_rng(77)
+    rows, cols, N = 300, 4000, 32
+    lens = rng.integers(0, 20, rows)
+    for r, l in {3: 32 * 32, 50: 32 * 32 + 1, 120: 33 * 32, 200: 64 * 32, 201: 65 * 32 - 7, 299: 100 * 32 + 13}.items():
+        lens[r] = l
+    rp = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    ci = np.concatenate([np.sort(rng.choice(cols, l, replace=False)) for l in lens]).astype(np.int32)
+    A = bsp.HostCSR(rows, cols, rp, ci, rng.uniform(-1, 1, rp[-1]))
+    vals_t, vals64, B_t, B64 = _case(A, N, "f16", 5)
+    rpd, cid = _dev(cuda, A.rowptr, A.colidx)
+    P = bsp.SpmmPlan(rpd, cid, vals_t.to(cuda), cols=cols, chunk=32)
+    assert P._d.ngroups > P.nsplit   # some rows have several groups
+    Bd = B_t.to(cuda)
+    C1 = P.spmm(Bd, engine=engine, slab_cols=slab)
+    assert torch.equal(C1, P.spmm(Bd, engine=engine, slab_cols=slab))
+    Cref, absC = pyoracle.spmm_f64(A.rowptr, A.colidx, vals64, B64)
+    assert np.all(np.abs(C1.cpu().numpy().astype(np.float64) - Cref) <= _tol(A, absC))
+    Cin = rng.uniform(-1, 1, (rows, N)).astype(np.float32)
+    Cd = torch.from_numpy(Cin.copy()).to(cuda)
+    P.spmm(Bd, Cd, alpha=-2.0, beta=0.75, engine=engine, slab_cols=slab)
+    want = -2.0 * Cref + 0.75 * Cin.astype(np.float64)
+    assert np.all(np.abs(Cd.cpu().numpy().astype(np.float64) - want) <= _tol(A, absC, -2.0, Cin, 0.75))
+    P.free()
