@@ -700,10 +700,7 @@ def run_suite(args) -> None:
             nb = A.nnz * 6 + (A.rows + 1) * 4 + A.cols * N * 2 + A.rows * N * 4
             gb = A.nnz * N * 2    # B-row bytes gathered (one B row per nonzero)
             w = min(256, 2 * N)
-            # the probe of this gather width whose buffer is closest in size to B (cols x N FP16)
-            bmb = A.cols * N * 2 / 2 ** 20
-            cands = [k for k in gpk if k.startswith(f"w{w}_")]
-            where = min(cands, key=lambda k: abs(np.log(gpk[k]["buffer_mb"] / bmb))).split("_", 1)[1]
+            where = probe_for(gpk, w, A.cols * N * 2)
             res[f"{name}_N{N}"] = {"ms": round(t * 1e3, 3), "engine": "slab", "grouped_engine_ms": round(tg * 1e3, 3),
                                    "gflops": round(2 * A.nnz * N / t / 1e9, 1),
                                    "rel_err_vs_fp64": err, "cusparse_f32_ms": round(tcs * 1e3, 3),
@@ -777,6 +774,17 @@ def run_gather_peaks(bsp, dev) -> dict:
             del buf
     _emit("gather_probe", variants=out)
     return out
+
+
+def probe_for(gpk: dict, width: int, nbytes: float) -> str:
+    """The gather-probe entry of this width whose buffer is closest in size
+    (by ratio) to a gathered array of `nbytes` bytes: its key suffix."""
+    cands = [k for k in gpk if k.startswith(f"w{width}_")]
+    if not cands:
+        raise KeyError(f"no gather probe of width {width}")
+    mb = max(nbytes / 2 ** 20, 1e-9)
+    best = min(cands, key=lambda k: abs(np.log(gpk[k]["buffer_mb"] / mb)))
+    return best.split("_", 1)[1]
 
 
 def run_smat_graph(bsp, dev, up, A) -> None:

@@ -104,3 +104,21 @@ def test_reference_arm_never_loads_the_library():
     import bench
     assert line["config"] == bench.headline_config(8, 1)
     assert line["config"]["n"] == 8 ** 3 * 4 and line["config"]["nnz"] == 22 ** 3 * 16
+
+
+def test_gather_probe_choice_matches_the_array_size():
+    """The SpMM gather roofline uses the probe of the same gather width whose
+    buffer is closest in size (by ratio) to the gathered array."""
+    sys.path.insert(0, str(ROOT))
+    import bench
+    gpk = {"w64_l2": {"buffer_mb": 64}, "w64_dram": {"buffer_mb": 2048},
+           "w256_l2": {"buffer_mb": 64}, "w256_dram": {"buffer_mb": 2048},
+           "w256_m256": {"buffer_mb": 256}, "w256_m512": {"buffer_mb": 512}}
+    n = 1 << 20
+    assert bench.probe_for(gpk, 64, n * 32 * 2) == "l2"          # B of 64 MB at N = 32
+    assert bench.probe_for(gpk, 256, n * 128 * 2) == "m256"      # 256 MB at N = 128
+    assert bench.probe_for(gpk, 256, n * 256 * 2) == "m512"      # 512 MB at N = 256
+    assert bench.probe_for(gpk, 256, 3 << 30) == "dram"
+    assert bench.probe_for(gpk, 256, 1 << 20) == "l2"
+    with pytest.raises(KeyError):
+        bench.probe_for(gpk, 8, 1 << 20)
