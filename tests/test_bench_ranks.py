@@ -122,3 +122,22 @@ def test_gather_probe_choice_matches_the_array_size():
     assert bench.probe_for(gpk, 256, 1 << 20) == "l2"
     with pytest.raises(KeyError):
         bench.probe_for(gpk, 8, 1 << 20)
+
+
+def test_profile_summaries_run_committed_files_only():
+    """Every command quoted in profiles/*.md runs bench.py (or the oracle's
+    own programs) with a --profile mode bench.py accepts, and names no
+    scratch file."""
+    import re
+    sys.path.insert(0, str(ROOT))
+    src = (ROOT / "bench.py").read_text()
+    choices = re.search(r'"--profile", choices=\[([^\]]*)\]', src, re.S).group(1)
+    modes = set(re.findall(r'"([a-z0-9_]+)"', choices))
+    texts = {p.name: p.read_text() for p in (ROOT / "profiles").glob("*.md")}
+    assert texts
+    for name, t in texts.items():
+        assert "_work/" not in t, name
+        for m in re.findall(r"python bench\.py --profile ([a-z0-9_]+)", t):
+            assert m in modes, (name, m)
+        for script in re.findall(r"python ([A-Za-z0-9_/.]+\.py)", t):
+            assert (ROOT / script).exists(), (name, script)
